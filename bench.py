@@ -1,0 +1,368 @@
+"""Benchmark of the polygenic-score hot path on B200.
+
+Workload (the reference's bandwidth configuration): 50,000 samples x
+1,000,000 variants of SNP-major 2-bit PLINK rows (12.5 GB packed, resident in
+HBM), HWE genotypes with p ~ U(0.01, 0.5) and 0.5% missing calls, one FP32
+score over all variants with weights ~ N(0, 0.005^2) and 10% of variants
+effect-allele-flipped.  Data are synthetic (seeded counter-based generator).
+
+A step is one full scoring pass: reset + accumulate over all rows + finalize
+(baseline added, output rows gathered).  ``value`` is genotype*score pairs/s
+of the device-timed steps; ``e2e`` is the same metric through the public C ABI
+(``gnm_score_run_ex``) from pinned host buffers, host->device copy of the rows
+and device->host copy of the results inside the timed region.
+
+``--impl reference`` times the reference's CPU scoring engine (the C
+restatement under oracle/, all host threads) on a bounded sample of the same
+workload.  Multi-GPU (torchrun): person sharding — every rank scores its own
+50,000-person shard of an N x 50,000 cohort with no collective (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "bandwidth_50k_x_1m"
+METRIC = "genotype*score pairs/s"
+PROFILE = ROOT / "profiles" / "plain_accumulate_bandwidth_50k_x_1m.md"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    """dram bytes per launch recorded from the ncu capture (profiles/), else None."""
+    if not PROFILE.exists():
+        return None
+    for line in PROFILE.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (every 200 ms)."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class CpuReferenceSample:
+    """The restated reference CPU engine on a bounded sample of the workload:
+    all people, a prefix of the variants sized so one pass takes ~target_s."""
+
+    def __init__(self, w, target_s: float, threads: int):
+        self.w, self.threads = w, threads
+        nv = 512
+        while True:  # grow the prefix until one pass is long enough to extrapolate
+            self._make(nv)
+            t = min(self.time_once() for _ in range(2))
+            if t >= min(0.25, target_s) or nv >= w.variants:
+                break
+            nv = min(w.variants, nv * 4)
+        nv = int(min(w.variants, max(nv, nv * target_s / max(t, 1e-4))))
+        if nv != self.nv:
+            self._make(nv)
+
+    def _make(self, nv):
+        from oracle import oracle
+        from gnomon_b200 import synth
+        from gnomon_b200.prepare import PreparationResult
+        w = self.w
+        thr = synth.variant_thresholds(w.seed, 0, nv, w.p_lo, w.p_hi, w.missing_rate)
+        self.rows = oracle.synth_rows(w.seed, 0, nv, w.people, thr, w.bytes_per_variant)
+        rng = np.random.default_rng(w.seed)
+        wt = (rng.standard_normal(nv) * w.sigma).astype(np.float32)
+        fl = rng.random(nv) < w.flip_frac
+        self.prep = PreparationResult(
+            np.where(fl, -wt, wt).astype(np.float32),
+            np.where(fl, np.float32(2) * wt, np.float32(0)).astype(np.float32),
+            np.zeros(nv, np.uint32), np.arange(nv + 1, dtype=np.uint64), ["S000"], w.people)
+        self.nv = nv
+
+    def time_once(self):
+        from oracle import oracle
+        t0 = time.perf_counter()
+        oracle.score_reference(self.rows, self.prep, threads=self.threads)
+        return time.perf_counter() - t0
+
+    @property
+    def pairs(self):
+        return self.w.people * self.nv * self.w.scores
+
+    def describe(self, seconds):
+        return (f"{self.w.people} people x {self.nv} variants (prefix of {self.w.variants}), "
+                f"K=1, restated reference CPU engine (decide.rs routing, person-major f32 "
+                f"mini-batches, variant-major f64) on {self.threads} threads, {seconds:.2f} s/pass")
+
+
+def reference_arm(args, rank, world):
+    from gnomon_b200 import synth
+    if rank != 0:
+        return
+    w = synth.WORKLOADS[WORKLOAD]
+    threads = os.cpu_count() or 1
+    sample = CpuReferenceSample(w, args.ref_step_s, threads)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t = sample.time_once()
+        if i >= args.warmup:
+            times.append(t)
+    t_used = statistics.median(times)
+    value = sample.pairs / t_used
+    sample = sample.describe(t_used)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_used * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "samples": w.people, "variants": w.variants,
+                       "scores": w.scores, "engine": "cpu reference restatement"},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from gnomon_b200 import _lib, synth
+    from gnomon_b200.device import DevicePlan, row_pitch, synth_fill
+    from gnomon_b200.pipeline import BedSource, PipelineContext, try_run_cuda
+    from gnomon_b200.prepare import from_workload
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = synth.WORKLOADS[WORKLOAD]
+    if world > 1:  # person sharding: each rank owns a distinct 50,000-person shard
+        w = synth.Workload(w.name, w.people, w.variants, w.scores, w.p_lo, w.p_hi,
+                           w.missing_rate, w.sigma, w.flip_frac, w.size_lo, w.size_hi,
+                           w.config_id + 100 * rank)
+    P, V, K = w.people, w.variants, w.scores
+    bpv = w.bytes_per_variant
+    pitch = row_pitch(bpv)
+    prep = from_workload(w)
+    stream = torch.cuda.Stream(dev)
+
+    # synthetic rows generated on the device, in blocks of 100k variants
+    rows = torch.empty((V, pitch), dtype=torch.uint8, device=dev)
+    with torch.cuda.stream(stream):
+        for v0 in range(0, V, 100_000):
+            n = min(100_000, V - v0)
+            thr = synth.variant_thresholds(w.seed, v0, n, w.p_lo, w.p_hi, w.missing_rate)
+            synth_fill(rows[v0:v0 + n], pitch, v0, n, P, thr, w.seed, stream=stream)
+    stream.synchronize()
+
+    plan = DevicePlan(prep, engine=_lib.ENGINE_PLAIN, device=local_rank)
+    sums, counts = plan.outputs()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    k_stop = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+
+    def step(i=None):
+        plan.reset(stream)
+        if i is not None:
+            k_start[i].record(stream)
+        plan.accumulate(rows, pitch, 0, V, stream)
+        if i is not None:
+            k_stop[i].record(stream)
+        plan.finalize(sums, counts, stream)
+
+    for _ in range(args.warmup):
+        step()
+    plan.sync(stream)
+    launches0 = plan.launches
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        start.record(stream)
+        for i in range(args.steps):
+            step(i)
+        stop.record(stream)
+        stop.synchronize()
+    plan.sync(stream)
+    ms = start.elapsed_time(stop) / args.steps
+    kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(k_start, k_stop))
+    launches_per_step = 2 * K  # plain accumulate + finalize per score column
+    if world > 1:
+        t = torch.tensor([ms, kernel_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, kernel_ms = t.tolist()
+        dist.barrier()
+
+    pairs = P * V * K
+    value = world * pairs / (ms / 1e3)
+
+    # roofline of the dominant kernel (gnm_plain_accumulate): algorithmic bytes
+    # = packed rows + per-variant weight record read once per launch.
+    alg_bytes = V * bpv + V * K * 4.125
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = traffic_from_profile()
+
+    # checksum sanity: the result is consumed (and must be finite)
+    s_host = sums.cpu().numpy()
+    assert np.isfinite(s_host).all()
+
+    # end-to-end through the public C ABI from pinned host memory
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        host = torch.empty((V, bpv), dtype=torch.uint8, pin_memory=True)
+        host.copy_(rows[:, :bpv])
+        src = BedSource(host.numpy().reshape(-1))
+        ctx = PipelineContext(prep)
+        for _ in range(min(args.warmup, 1)):
+            try_run_cuda(ctx, src, engine=_lib.ENGINE_PLAIN, device=local_rank)
+        times = []
+        for _ in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = try_run_cuda(ctx, src, engine=_lib.ENGINE_PLAIN, device=local_rank)
+            times.append(time.perf_counter() - t0)
+        e_s, e_c = out
+        assert np.array_equal(e_c.astype(np.int64), counts.cpu().numpy().astype(np.int64))
+        rel = np.abs(e_s - s_host).max() / max(1.0, np.abs(s_host).max())
+        assert rel < 1e-9, rel
+        h2d = V * bpv + K * (V + 64) * 16 + K * 8 * 2 + 4
+        d2h = P * K * 12 + 4
+        e2e = {"value": pairs / statistics.median(times), "unit": "pairs/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "seconds_per_step": statistics.median(times),
+               "timing": "wall clock around gnm_score_run_ex (synchronous), pinned host rows"}
+        del host
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            threads = os.cpu_count() or 1
+            smp = CpuReferenceSample(w, args.cpu_s / 3, threads)
+            t = statistics.median(smp.time_once() for _ in range(3))
+            cpu = {"value": smp.pairs / t, "unit": "pairs/s", "cores": threads, "kind": "port",
+                   "sample": smp.describe(t) + ", median of 3"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "samples": P, "variants": V, "scores": K,
+                       "packed_bytes": V * bpv, "engine": "plain (FP32 CUDA-core LUT, FP64 reduce)",
+                       "parallelism": f"person-shard x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs (12.5 GB) larger than L2 (126 MB); no flush"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "gnm_plain_accumulate", "kernel_ms": kernel_ms,
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gnomon_b200", choices=["gnomon_b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-s", type=float, default=12.0, help="CPU baseline sample seconds")
+    ap.add_argument("--ref-step-s", type=float, default=4.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=None)
+    try:
+        gpu_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

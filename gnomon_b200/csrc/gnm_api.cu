@@ -1,0 +1,669 @@
+// gnm_api.cu — C ABI (include/gnomon_gpu.h) over the sm_100a kernels.
+//
+// The host side of try_run_cuda (score/cuda_backend.rs:604-1535) rebuilt for
+// B200: weights are compiled once per plan into per-variant device records,
+// packed rows are streamed from the caller's .bed bytes into HBM (pinned
+// double buffer, copy stream overlapped with the compute stream), kernels
+// accumulate FP64 partials on the device, and one finalize pass adds the
+// baseline and gathers output rows.  No cuBLAS, no NVRTC, no host-side
+// per-tile accumulation.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "gnm_plan.h"
+#include "gnm_tensor.h"
+
+namespace gnm {
+
+void fail(gnm_status s, const std::string& msg) { throw Failure{s, msg}; }
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear sticky-free errors so the context stays usable
+    fail(GNM_ERR_COMPUTE, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+DeviceGuard::DeviceGuard(int dev) {
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  if (dev >= 0 && dev != prev) check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+}
+DeviceGuard::~DeviceGuard() {
+  int cur = -1;
+  if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled is not available from the driver");
+  return fn;
+}
+
+CUtensorMap make_row_map(const uint8_t* d_rows, uint64_t bytes_per_row, uint64_t num_rows,
+                         uint64_t pitch, uint32_t box_x, uint32_t box_y) {
+  if (reinterpret_cast<uintptr_t>(d_rows) % 16 != 0)
+    fail(GNM_ERR_INVALID, "packed rows must start on a 16-byte boundary");
+  if (pitch % 16 != 0) fail(GNM_ERR_INVALID, "row pitch must be a multiple of 16 bytes");
+  if (bytes_per_row > pitch) fail(GNM_ERR_INVALID, "row pitch is smaller than bytes per row");
+  CUtensorMap map;
+  cuuint64_t dims[2] = {bytes_per_row, num_rows};
+  cuuint64_t strides[1] = {pitch};
+  cuuint32_t box[2] = {box_x, box_y};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(d_rows),
+                           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled failed for the row map");
+  return map;
+}
+
+template <class T>
+static T* dalloc(gnm_plan* p, uint64_t n, const char* what) {
+  void* ptr = nullptr;
+  const uint64_t bytes = std::max<uint64_t>(1, n * sizeof(T));
+  check_cuda(cudaMalloc(&ptr, bytes), what);
+  p->device_bytes += bytes;
+  return static_cast<T*>(ptr);
+}
+
+static void set_error(gnm_error* err, const std::string& m) {
+  if (!err) return;
+  std::snprintf(err->message, sizeof(err->message), "%s", m.c_str());
+}
+
+template <class F>
+static gnm_status guarded(gnm_error* err, F&& f) {
+  try {
+    f();
+    if (err) err->message[0] = '\0';
+    return GNM_OK;
+  } catch (const Failure& e) {
+    set_error(err, e.message);
+    return e.status;
+  } catch (const std::exception& e) {
+    set_error(err, std::string("internal error: ") + e.what());
+    return GNM_ERR_COMPUTE;
+  } catch (...) {
+    set_error(err, "internal error");
+    return GNM_ERR_COMPUTE;
+  }
+}
+
+// ---- validation (prepare.rs:760-790 invariants) ----------------------------
+static void validate_prep(const gnm_prep_view* p) {
+  if (!p) fail(GNM_ERR_INVALID, "prep is NULL");
+  if (p->num_scores == 0) fail(GNM_ERR_INVALID, "num_scores must be > 0");
+  if (p->bytes_per_variant != (p->total_people_in_fam + 3) / 4)
+    fail(GNM_ERR_INVALID, "bytes_per_variant != ceil(total_people_in_fam / 4)");
+  if (p->total_people_in_fam > (uint64_t(1) << 31))
+    fail(GNM_ERR_INVALID, "more than 2^31 people per row is not supported");
+  if (p->num_variants > 0 && (!p->sparse_row_offsets))
+    fail(GNM_ERR_INVALID, "sparse_row_offsets is NULL");
+  if (p->num_people > 0 && !p->output_idx_to_fam_idx && p->num_people > p->total_people_in_fam)
+    fail(GNM_ERR_INVALID, "num_people exceeds total_people_in_fam with identity mapping");
+  const uint64_t* offs = p->sparse_row_offsets;
+  if (p->num_variants > 0) {
+    if (offs[0] != 0) fail(GNM_ERR_INVALID, "sparse_row_offsets[0] must be 0");
+    for (uint64_t v = 0; v < p->num_variants; ++v)
+      if (offs[v + 1] < offs[v]) fail(GNM_ERR_INVALID, "sparse_row_offsets not monotone");
+    const uint64_t nnz = offs[p->num_variants];
+    if (nnz && (!p->sparse_weights || !p->sparse_missing_corrections || !p->sparse_score_columns))
+      fail(GNM_ERR_INVALID, "CSR arrays are NULL");
+    for (uint64_t v = 0; v < p->num_variants; ++v)
+      for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
+        if (p->sparse_score_columns[e] >= p->num_scores)
+          fail(GNM_ERR_INVALID, "CSR score column out of range");
+        if (e > offs[v] && p->sparse_score_columns[e] <= p->sparse_score_columns[e - 1])
+          fail(GNM_ERR_INVALID, "CSR columns must be strictly ascending within a row");
+      }
+  }
+  if (p->output_idx_to_fam_idx)
+    for (uint64_t o = 0; o < p->num_people; ++o)
+      if (p->output_idx_to_fam_idx[o] >= p->total_people_in_fam)
+        fail(GNM_ERR_INVALID, "output_idx_to_fam_idx entry out of range");
+}
+
+static bool device_available(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return false;
+  }
+  return device < n;
+}
+
+// ---- plan --------------------------------------------------------------------
+static void plain_geometry(gnm_plan* p) {
+  p->tiles = uint32_t(std::max<uint64_t>(1, (p->bpv + kPlainTileBytes - 1) / kPlainTileBytes));
+  p->part_stride = uint64_t(p->tiles) * kPlainTileBytes * 4;
+  int per_sm = 0;
+  cudaDeviceProp prop;
+  check_cuda(cudaGetDeviceProperties(&prop, p->device), "cudaGetDeviceProperties");
+  p->num_sms = prop.multiProcessorCount;
+  per_sm = 2;  // __launch_bounds__(256, 2) with ~108 KB of shared memory
+  const uint64_t slots = uint64_t(per_sm) * uint64_t(p->num_sms);
+  const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
+  uint64_t splits = std::max<uint64_t>(1, slots / p->tiles);
+  splits = std::min<uint64_t>(splits, stages);
+  // keep partials of all scores within ~1 GiB
+  const uint64_t per_split_bytes = p->K * p->part_stride * 12;
+  while (splits > 1 && splits * per_split_bytes > (uint64_t(1) << 30)) splits = (splits + 1) / 2;
+  p->splits = uint32_t(splits);
+}
+
+static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep) {
+  p->rec_stride = p->V + kRecordPad;
+  std::vector<float4> rec(p->K * p->rec_stride, make_float4(0.f, 0.f, 0.f, 0.f));
+  const uint32_t member_bits = 0x55555555u;
+  float member_f;
+  std::memcpy(&member_f, &member_bits, 4);
+  for (uint64_t v = 0; v < p->V; ++v)
+    for (uint64_t e = prep->sparse_row_offsets[v]; e < prep->sparse_row_offsets[v + 1]; ++e) {
+      const uint32_t k = prep->sparse_score_columns[e];
+      const float w = prep->sparse_weights[e];
+      const float c = prep->sparse_missing_corrections[e];
+      rec[k * p->rec_stride + v] = make_float4(-c, w, 2.0f * w, member_f);
+    }
+  p->d_records = dalloc<float4>(p, rec.size(), "cudaMalloc(records)");
+  check_cuda(cudaMemcpy(p->d_records, rec.data(), rec.size() * sizeof(float4),
+                        cudaMemcpyHostToDevice),
+             "upload records");
+  const uint64_t part = p->K * uint64_t(p->splits) * p->part_stride;
+  p->d_part_sum = dalloc<double>(p, part, "cudaMalloc(partial sums)");
+  p->d_part_cnt = dalloc<uint32_t>(p, part, "cudaMalloc(partial counts)");
+}
+
+static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, int device) {
+  validate_prep(prep);
+  if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
+  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  DeviceGuard g(device);
+  auto* p = new gnm_plan();
+  try {
+    p->device = device;
+    p->P = prep->num_people;
+    p->fam = prep->total_people_in_fam;
+    p->bpv = prep->bytes_per_variant;
+    p->K = prep->num_scores;
+    p->V = prep->num_variants;
+    if (engine == GNM_ENGINE_AUTO) engine = p->K > kTensorMinScores ? GNM_ENGINE_TENSOR : GNM_ENGINE_PLAIN;
+    p->engine = engine;
+
+    // baseline (prepare.rs:644-646), f64 in CSR order
+    p->h_baseline.assign(p->K, 0.0);
+    const uint64_t nnz = p->V ? prep->sparse_row_offsets[p->V] : 0;
+    if (prep->baseline) {
+      std::copy(prep->baseline, prep->baseline + p->K, p->h_baseline.begin());
+    } else {
+      for (uint64_t e = 0; e < nnz; ++e)
+        p->h_baseline[prep->sparse_score_columns[e]] += double(prep->sparse_missing_corrections[e]);
+    }
+    p->d_baseline = dalloc<double>(p, p->K, "cudaMalloc(baseline)");
+    check_cuda(cudaMemcpy(p->d_baseline, p->h_baseline.data(), p->K * sizeof(double),
+                          cudaMemcpyHostToDevice),
+               "upload baseline");
+    p->d_zero_base = dalloc<double>(p, p->K, "cudaMalloc(zero baseline)");
+    check_cuda(cudaMemset(p->d_zero_base, 0, p->K * sizeof(double)), "memset");
+    if (prep->output_idx_to_fam_idx) {
+      p->d_out_to_fam = dalloc<uint32_t>(p, p->P, "cudaMalloc(output map)");
+      check_cuda(cudaMemcpy(p->d_out_to_fam, prep->output_idx_to_fam_idx, p->P * 4,
+                            cudaMemcpyHostToDevice),
+                 "upload output map");
+    }
+    p->d_err = dalloc<uint32_t>(p, 1, "cudaMalloc(error word)");
+    check_cuda(cudaMemset(p->d_err, 0, 4), "memset");
+
+    p->h_offs.assign(prep->sparse_row_offsets, prep->sparse_row_offsets + p->V + 1);
+    if (nnz) {
+      p->h_w.assign(prep->sparse_weights, prep->sparse_weights + nnz);
+      p->h_corr.assign(prep->sparse_missing_corrections, prep->sparse_missing_corrections + nnz);
+      p->h_cols.assign(prep->sparse_score_columns, prep->sparse_score_columns + nnz);
+    }
+    if (p->engine == GNM_ENGINE_PLAIN) {
+      plain_geometry(p);
+      build_plain_records(p, prep);
+    } else {
+      tensor_plan_create(p);
+    }
+    check_cuda(cudaDeviceSynchronize(), "plan upload");
+  } catch (...) {
+    gnm_plan_destroy(p);
+    throw;
+  }
+  return p;
+}
+
+static void plan_reset_impl(gnm_plan* p, cudaStream_t s) {
+  DeviceGuard g(p->device);
+  if (p->engine == GNM_ENGINE_PLAIN) {
+    const uint64_t part = p->K * uint64_t(p->splits) * p->part_stride;
+    check_cuda(cudaMemsetAsync(p->d_part_sum, 0, part * sizeof(double), s), "reset partials");
+    check_cuda(cudaMemsetAsync(p->d_part_cnt, 0, part * sizeof(uint32_t), s), "reset partials");
+  } else {
+    tensor_reset(p, s);
+  }
+  check_cuda(cudaMemsetAsync(p->d_err, 0, 4, s), "reset error word");
+  p->launches = 0;
+}
+
+static void accumulate_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,
+                            uint64_t nv, cudaStream_t s) {
+  if (v0 + nv > p->V) fail(GNM_ERR_INVALID, "variant range exceeds num_variants");
+  if (nv == 0) return;
+  DeviceGuard g(p->device);
+  if (p->engine == GNM_ENGINE_TENSOR) {
+    tensor_accumulate(p, d_rows, pitch, v0, nv, s);
+    return;
+  }
+  const CUtensorMap map = make_row_map(d_rows, p->bpv, nv, pitch, kPlainBoxBytes, kPlainRows);
+  const uint64_t stages = (nv + kPlainRows - 1) / kPlainRows;
+  const uint32_t sps = uint32_t((stages + p->splits - 1) / p->splits);
+  const uint32_t splits = uint32_t((stages + sps - 1) / sps);
+  for (uint64_t k = 0; k < p->K; ++k) {
+    PlainArgs a;
+    a.records = p->d_records + k * p->rec_stride;
+    a.record_row0 = v0;
+    a.num_rows = nv;
+    a.stages_per_split = sps;
+    a.part_sum = p->d_part_sum + k * uint64_t(p->splits) * p->part_stride;
+    a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits) * p->part_stride;
+    a.part_stride = p->part_stride;
+    a.err = p->d_err;
+    check_cuda(launch_plain_accumulate(map, a, p->tiles, splits, s), "plain accumulate launch");
+    ++p->launches;
+  }
+}
+
+static void finalize_impl(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_baseline,
+                          cudaStream_t s) {
+  DeviceGuard g(p->device);
+  if (p->engine == GNM_ENGINE_TENSOR) {
+    tensor_finalize(p, d_sums, d_counts, add_baseline, s);
+    return;
+  }
+  for (uint64_t k = 0; k < p->K; ++k) {
+    FinalizeArgs a;
+    a.part_sum = p->d_part_sum + k * uint64_t(p->splits) * p->part_stride;
+    a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits) * p->part_stride;
+    a.part_stride = p->part_stride;
+    a.num_splits = p->splits;
+    a.baseline = add_baseline ? p->d_baseline : p->d_zero_base;
+    a.out_to_fam = p->d_out_to_fam;
+    a.num_people = p->P;
+    a.K = p->K;
+    a.k = k;
+    a.sums = d_sums;
+    a.counts = d_counts;
+    check_cuda(launch_finalize(a, s), "finalize launch");
+    ++p->launches;
+  }
+}
+
+static void sync_impl(gnm_plan* p, cudaStream_t s) {
+  DeviceGuard g(p->device);
+  check_cuda(cudaStreamSynchronize(s), "stream synchronize");
+  uint32_t e = 0;
+  check_cuda(cudaMemcpy(&e, p->d_err, 4, cudaMemcpyDeviceToHost), "read error word");
+  if (e & kErrTmaTimeout) fail(GNM_ERR_TIMEOUT, "device watchdog: a TMA wait expired");
+  if (e & kErrMmaTimeout) fail(GNM_ERR_TIMEOUT, "device watchdog: a tensor-core wait expired");
+  if (e) fail(GNM_ERR_COMPUTE, "device reported an error");
+}
+
+// ---- host streaming run ------------------------------------------------------
+struct HostRun {
+  gnm_plan* p;
+  const gnm_prep_view* prep;
+  const gnm_bed_view* bed;
+  uint64_t pitch;
+};
+
+static bool is_pinned(const void* ptr) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeManaged;
+}
+
+// Copy rows [v0, v0+n) into dst (pitch layout); zero the padding.
+static void gather_rows(const HostRun& r, uint64_t v0, uint64_t n, uint8_t* dst) {
+  const uint64_t bpv = r.p->bpv;
+  const uint64_t* map = r.prep->required_bim_indices;
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const unsigned nt = unsigned(std::min<uint64_t>(hw, std::max<uint64_t>(1, n / 256)));
+  std::atomic<int> bad{0};
+  auto work = [&](unsigned t) {
+    for (uint64_t i = t; i < n; i += nt) {
+      const uint64_t row = map ? map[v0 + i] : v0 + i;
+      uint8_t* d = dst + i * r.pitch;
+      if (r.bed->data) {
+        if ((row + 1) * bpv > r.bed->data_len) {
+          bad = 1;
+          return;
+        }
+        std::memcpy(d, r.bed->data + row * bpv, bpv);
+      } else if (r.bed->read_at(r.bed->user_ctx, row * bpv, d, bpv) != 0) {
+        bad = 2;
+        return;
+      }
+      std::memset(d + bpv, 0, r.pitch - bpv);
+    }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+  }
+  if (bad == 1) fail(GNM_ERR_IO, "truncated .bed: a required row lies past the end of the data");
+  if (bad == 2) fail(GNM_ERR_PRODUCER, "read_at callback failed");
+}
+
+static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
+                          const gnm_resume* resume, const gnm_run_options* opts,
+                          double* sums_out, uint32_t* missing_out) {
+  if (!bed || (!bed->data && !bed->read_at)) fail(GNM_ERR_INVALID, "bed view has no data source");
+  if (!sums_out || !missing_out) fail(GNM_ERR_INVALID, "output buffers are NULL");
+  gnm_run_options o{};
+  o.engine = GNM_ENGINE_AUTO;
+  o.device = -1;
+  if (opts) o = *opts;
+  gnm_plan* p = plan_create_impl(prep, o.engine, o.device);
+  struct PlanOwner {
+    gnm_plan* p;
+    ~PlanOwner() { gnm_plan_destroy(p); }
+  } owner{p};
+  DeviceGuard g(p->device);
+
+  const uint64_t P = p->P, K = p->K, V = p->V;
+  const uint64_t v_start = resume ? resume->completed_variants : 0;
+  if (v_start > V) fail(GNM_ERR_INVALID, "resume.completed_variants exceeds num_variants");
+  if (resume && (!resume->sums || !resume->counts))
+    fail(GNM_ERR_INVALID, "resume state has NULL buffers");
+  const uint64_t pitch = (p->bpv + 127) / 128 * 128;
+  HostRun r{p, prep, bed, pitch};
+
+  cudaStream_t cs = nullptr, xs = nullptr;
+  check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+  check_cuda(cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking), "stream");
+  struct Streams {
+    cudaStream_t a, b;
+    ~Streams() {
+      cudaStreamDestroy(a);
+      cudaStreamDestroy(b);
+    }
+  } st_owner{cs, xs};
+
+  // Block size: everything if it fits in ~60% of free memory, else two
+  // alternating blocks of block_variants rows.
+  size_t free_b = 0, total_b = 0;
+  check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  const uint64_t remaining = V - v_start;
+  uint64_t block = o.block_variants ? o.block_variants : remaining;
+  const uint64_t cap_rows = std::max<uint64_t>(kPlainRows, uint64_t(0.6 * double(free_b)) / pitch);
+  if (!o.block_variants && block > cap_rows) block = std::max<uint64_t>(kPlainRows, cap_rows / 2);
+  block = std::max<uint64_t>(1, std::min<uint64_t>(block, std::max<uint64_t>(1, remaining)));
+  const int nbuf = remaining > block ? 2 : 1;
+
+  std::vector<uint8_t*> dbuf(nbuf, nullptr);
+  struct DevBufs {
+    std::vector<uint8_t*>& v;
+    ~DevBufs() {
+      for (auto* b : v) cudaFree(b);
+    }
+  } db_owner{dbuf};
+  for (int i = 0; i < nbuf; ++i)
+    check_cuda(cudaMalloc(&dbuf[i], block * pitch), "cudaMalloc(row block)");
+  double* d_sums = nullptr;
+  uint32_t* d_cnt = nullptr;
+  check_cuda(cudaMalloc(&d_sums, std::max<uint64_t>(1, P * K) * sizeof(double)), "cudaMalloc(sums)");
+  check_cuda(cudaMalloc(&d_cnt, std::max<uint64_t>(1, P * K) * sizeof(uint32_t)), "cudaMalloc(counts)");
+  struct OutBufs {
+    double* a;
+    uint32_t* b;
+    ~OutBufs() {
+      cudaFree(a);
+      cudaFree(b);
+    }
+  } ob_owner{d_sums, d_cnt};
+
+  // Direct path: identity rows from pinned memory -> one 2D copy per block.
+  const bool identity = prep->required_bim_indices == nullptr;
+  const bool direct = identity && bed->data && is_pinned(bed->data);
+  const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(block, (uint64_t(128) << 20) / pitch));
+  uint8_t* pinned[2] = {nullptr, nullptr};
+  struct Pinned {
+    uint8_t** p;
+    ~Pinned() {
+      cudaFreeHost(p[0]);
+      cudaFreeHost(p[1]);
+    }
+  } pin_owner{pinned};
+  if (!direct)
+    for (int i = 0; i < 2; ++i)
+      check_cuda(cudaHostAlloc(&pinned[i], chunk * pitch, cudaHostAllocDefault), "cudaHostAlloc");
+  cudaEvent_t copied[2], consumed[2], staged[2];
+  for (int i = 0; i < 2; ++i) {
+    check_cuda(cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming), "event");
+    check_cuda(cudaEventCreateWithFlags(&consumed[i], cudaEventDisableTiming), "event");
+    check_cuda(cudaEventCreateWithFlags(&staged[i], cudaEventDisableTiming), "event");
+    check_cuda(cudaEventRecord(consumed[i], cs), "event");
+    check_cuda(cudaEventRecord(staged[i], xs), "event");
+  }
+  struct Events {
+    cudaEvent_t* a;
+    cudaEvent_t* b;
+    cudaEvent_t* c;
+    ~Events() {
+      for (int i = 0; i < 2; ++i) {
+        cudaEventDestroy(a[i]);
+        cudaEventDestroy(b[i]);
+        cudaEventDestroy(c[i]);
+      }
+    }
+  } ev_owner{copied, consumed, staged};
+
+  plan_reset_impl(p, cs);
+  uint64_t stage_idx = 0;
+  std::vector<double> cb_sums;
+  std::vector<uint32_t> cb_cnt;
+  for (uint64_t b0 = v_start, bi = 0; b0 < V; b0 += block, ++bi) {
+    const uint64_t nb = std::min(block, V - b0);
+    const int slot = int(bi % nbuf);
+    // the compute of the block that last used this device buffer must be done
+    check_cuda(cudaStreamWaitEvent(xs, consumed[slot], 0), "wait");
+    if (direct) {
+      check_cuda(cudaMemcpy2DAsync(dbuf[slot], pitch, bed->data + b0 * p->bpv, p->bpv, p->bpv, nb,
+                                   cudaMemcpyHostToDevice, xs),
+                 "H2D rows");
+    } else {
+      for (uint64_t c0 = 0; c0 < nb; c0 += chunk, ++stage_idx) {
+        const uint64_t nc = std::min(chunk, nb - c0);
+        const int ps = int(stage_idx & 1);
+        check_cuda(cudaEventSynchronize(staged[ps]), "wait pinned buffer");
+        gather_rows(r, b0 + c0, nc, pinned[ps]);
+        check_cuda(cudaMemcpyAsync(dbuf[slot] + c0 * pitch, pinned[ps], nc * pitch,
+                                   cudaMemcpyHostToDevice, xs),
+                   "H2D rows");
+        check_cuda(cudaEventRecord(staged[ps], xs), "event");
+      }
+    }
+    check_cuda(cudaEventRecord(copied[slot], xs), "event");
+    check_cuda(cudaStreamWaitEvent(cs, copied[slot], 0), "wait");
+    accumulate_impl(p, dbuf[slot], pitch, b0, nb, cs);
+    check_cuda(cudaEventRecord(consumed[slot], cs), "event");
+    if (o.on_block) {
+      finalize_impl(p, d_sums, d_cnt, resume == nullptr, cs);
+      sync_impl(p, cs);
+      cb_sums.resize(P * K);
+      cb_cnt.resize(P * K);
+      check_cuda(cudaMemcpy(cb_sums.data(), d_sums, P * K * 8, cudaMemcpyDeviceToHost), "D2H");
+      check_cuda(cudaMemcpy(cb_cnt.data(), d_cnt, P * K * 4, cudaMemcpyDeviceToHost), "D2H");
+      if (resume)
+        for (uint64_t x = 0; x < P * K; ++x) {
+          cb_sums[x] += resume->sums[x];
+          cb_cnt[x] += resume->counts[x];
+        }
+      if (o.on_block(o.on_block_ctx, b0 + nb, cb_sums.data(), cb_cnt.data()) != 0)
+        fail(GNM_ERR_PRODUCER, "block callback requested abort");
+    }
+  }
+  finalize_impl(p, d_sums, d_cnt, resume == nullptr, cs);
+  check_cuda(cudaMemcpyAsync(sums_out, d_sums, P * K * sizeof(double), cudaMemcpyDeviceToHost, cs),
+             "D2H sums");
+  check_cuda(
+      cudaMemcpyAsync(missing_out, d_cnt, P * K * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs),
+      "D2H counts");
+  sync_impl(p, cs);
+  if (resume)
+    for (uint64_t x = 0; x < P * K; ++x) {
+      sums_out[x] += resume->sums[x];
+      missing_out[x] += resume->counts[x];
+    }
+}
+
+}  // namespace gnm
+
+using namespace gnm;
+
+extern "C" {
+
+int gnm_abi_version(void) { return GNM_ABI_VERSION; }
+
+gnm_status gnm_score_run(const gnm_prep_view* prep, const gnm_bed_view* bed,
+                         const gnm_resume* resume, double* sums_out, uint32_t* missing_out,
+                         gnm_error* err) {
+  return gnm_score_run_ex(prep, bed, resume, nullptr, sums_out, missing_out, err);
+}
+
+gnm_status gnm_score_run_ex(const gnm_prep_view* prep, const gnm_bed_view* bed,
+                            const gnm_resume* resume, const gnm_run_options* opts,
+                            double* sums_out, uint32_t* missing_out, gnm_error* err) {
+  return guarded(err, [&] { host_run_impl(prep, bed, resume, opts, sums_out, missing_out); });
+}
+
+gnm_status gnm_plan_create(const gnm_prep_view* prep, gnm_engine engine, int device,
+                           gnm_plan** plan_out, gnm_error* err) {
+  if (!plan_out) return GNM_ERR_INVALID;
+  *plan_out = nullptr;
+  return guarded(err, [&] { *plan_out = plan_create_impl(prep, engine, device); });
+}
+
+void gnm_plan_destroy(gnm_plan* p) {
+  if (!p) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(p->device);
+  if (p->tensor) tensor_plan_destroy(p);
+  cudaFree(p->d_records);
+  cudaFree(p->d_part_sum);
+  cudaFree(p->d_part_cnt);
+  cudaFree(p->d_baseline);
+  cudaFree(p->d_zero_base);
+  cudaFree(p->d_out_to_fam);
+  cudaFree(p->d_err);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete p;
+}
+
+gnm_engine gnm_plan_engine(const gnm_plan* p) { return p ? p->engine : GNM_ENGINE_AUTO; }
+uint64_t gnm_plan_device_bytes(const gnm_plan* p) { return p ? p->device_bytes : 0; }
+uint64_t gnm_plan_launch_count(const gnm_plan* p) { return p ? p->launches : 0; }
+double gnm_plan_last_spotcheck(const gnm_plan* p) { return p ? p->last_spotcheck : 0.0; }
+
+gnm_status gnm_plan_reset(gnm_plan* p, void* stream, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] { plan_reset_impl(p, static_cast<cudaStream_t>(stream)); });
+}
+
+gnm_status gnm_plan_accumulate_device(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch,
+                                      uint64_t v0, uint64_t nv, void* stream, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] {
+    accumulate_impl(p, d_rows, pitch, v0, nv, static_cast<cudaStream_t>(stream));
+  });
+}
+
+gnm_status gnm_plan_finalize_device(gnm_plan* p, double* d_sums, uint32_t* d_counts, void* stream,
+                                    gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] {
+    if (!d_sums || !d_counts) fail(GNM_ERR_INVALID, "output buffers are NULL");
+    finalize_impl(p, d_sums, d_counts, true, static_cast<cudaStream_t>(stream));
+  });
+}
+
+gnm_status gnm_plan_sync(gnm_plan* p, void* stream, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] { sync_impl(p, static_cast<cudaStream_t>(stream)); });
+}
+
+gnm_status gnm_score_device(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, double* d_sums,
+                            uint32_t* d_counts, void* stream, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] {
+    if (!d_sums || !d_counts) fail(GNM_ERR_INVALID, "output buffers are NULL");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    plan_reset_impl(p, s);
+    accumulate_impl(p, d_rows, pitch, 0, p->V, s);
+    finalize_impl(p, d_sums, d_counts, true, s);
+  });
+}
+
+gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv, uint64_t np,
+                             int8_t* d_out, uint64_t out_pitch, void* stream, gnm_error* err) {
+  return guarded(err, [&] {
+    if (np > pitch * 4) fail(GNM_ERR_INVALID, "num_people exceeds 4*pitch");
+    if (out_pitch < np) fail(GNM_ERR_INVALID, "out_pitch < num_people");
+    check_cuda(launch_decode(d_rows, pitch, nv, np, d_out, out_pitch,
+                             static_cast<cudaStream_t>(stream)),
+               "decode launch");
+  });
+}
+
+gnm_status gnm_synth_fill_device(uint8_t* d_rows, uint64_t pitch, uint64_t v0, uint64_t nv,
+                                 uint64_t np, const uint32_t* d_thr, uint64_t seed, void* stream,
+                                 gnm_error* err) {
+  return guarded(err, [&] {
+    if (pitch % 16 != 0) fail(GNM_ERR_INVALID, "pitch must be a multiple of 16");
+    if ((np + 3) / 4 > pitch) fail(GNM_ERR_INVALID, "pitch smaller than ceil(num_people/4)");
+    check_cuda(launch_synth_fill(d_rows, pitch, v0, nv, np, d_thr, seed,
+                                 static_cast<cudaStream_t>(stream)),
+               "synth launch");
+  });
+}
+
+gnm_status gnm_backward_dw_device(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch,
+                                  const float* d_grad_s, float* d_grad_w, float* d_grad_corr,
+                                  void* stream, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] {
+    DeviceGuard g(p->device);
+    backward_dw(p, d_rows, pitch, d_grad_s, d_grad_w, d_grad_corr,
+                static_cast<cudaStream_t>(stream));
+  });
+}
+
+}  // extern "C"

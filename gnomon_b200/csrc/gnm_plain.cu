@@ -1,0 +1,323 @@
+// gnm_plain.cu — plain (FP32 CUDA-core) scoring path for sm_100a.
+//
+// Replaces the reference GPU engine's unpack_plink -> zero -> scatter ->
+// 3x SGEMM -> combine chain (score/cuda_backend.rs:62-218, 2067-2333) for small
+// score counts with ONE fused kernel per score column:
+//
+//   * packed .bed rows are TMA-staged (cp.async.bulk.tensor, no multicast)
+//     into shared memory in [48 rows x 1024 bytes] stages, double-buffered;
+//   * each thread owns one 32-bit word column = 16 people; every 3 variant
+//     rows it transposes the 2-bit codes into per-person 6-bit indices (one
+//     byte each, pre-scaled by 4) with a handful of shift/mask ops;
+//   * a 64-entry FP32 table per 3-variant group, built in shared memory from
+//     {-missing_correction, dosage_weight, 2*dosage_weight} (prepare.rs:197-208
+//     folding, code 00 contributes 0), turns 3 genotypes into ONE lookup:
+//     decode, effect-allele flip and the missing-call rule are all folded in;
+//   * missing calls (code 01) are counted with SWAR bit tricks on the raw row
+//     words (x & ~(x>>1) & member_mask, three rows summed with one add);
+//   * FP32 partial sums cover one 48-variant stage and are flushed to FP64
+//     registers; variant splits write FP64 partials that gnm_finalize reduces
+//     in a fixed order (deterministic) and gathers through
+//     output_idx_to_fam_idx, adding the FP64 baseline (pipeline.rs:1739-1775).
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "gnm_device.cuh"
+#include "gnm_internal.h"
+
+namespace gnm {
+
+// Shared-memory layout of one plain CTA (dynamic smem, offsets in bytes).
+struct PlainSmem {
+  static constexpr uint32_t kStageBytes = kPlainRows * kPlainTileBytes;      // 49152
+  static constexpr uint32_t kBoxBytes = kPlainRows * kPlainBoxBytes;         // 12288
+  static constexpr uint32_t kRecBytes = kPlainRows * 16;                     // 768
+  static constexpr uint32_t kLutBytes = (kPlainRows / 3) * 64 * 4;           // 4096
+  static constexpr uint32_t kStages = 2;
+  static constexpr uint32_t kTileOff = 0;
+  static constexpr uint32_t kRecOff = kTileOff + kStages * kStageBytes;
+  static constexpr uint32_t kLutOff = kRecOff + kStages * kRecBytes;
+  static constexpr uint32_t kBarOff = kLutOff + kStages * kLutBytes;
+  static constexpr uint32_t kTotal = kBarOff + 64;
+};
+
+__device__ __forceinline__ void plain_issue_stage(const CUtensorMap* map, const float4* recs,
+                                                  uint32_t smem_base, uint32_t buf,
+                                                  int32_t tile_x, int32_t row0,
+                                                  uint64_t rec_row0) {
+  const uint32_t bar = smem_base + PlainSmem::kBarOff + 8 * buf;
+  mbar_arrive_expect_tx(bar, PlainSmem::kStageBytes + PlainSmem::kRecBytes);
+  const uint32_t tile = smem_base + PlainSmem::kTileOff + buf * PlainSmem::kStageBytes;
+#pragma unroll
+  for (uint32_t b = 0; b < kPlainTileBytes / kPlainBoxBytes; ++b)
+    tma_load_2d(tile + b * PlainSmem::kBoxBytes, map, tile_x + int32_t(b * kPlainBoxBytes), row0,
+                bar);
+  bulk_load(smem_base + PlainSmem::kRecOff + buf * PlainSmem::kRecBytes, recs + rec_row0,
+            PlainSmem::kRecBytes, bar);
+}
+
+// grid = (people tiles, variant splits); block = kPlainThreads.
+__global__ void __launch_bounds__(kPlainThreads, 2)
+    gnm_plain_accumulate(const __grid_constant__ CUtensorMap map, PlainArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t tid = threadIdx.x;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t split = blockIdx.y;
+
+  const uint64_t rows_per_split = uint64_t(a.stages_per_split) * kPlainRows;
+  const uint64_t r_begin = uint64_t(split) * rows_per_split;
+  if (r_begin >= a.num_rows) return;
+  const uint64_t r_end = min(a.num_rows, r_begin + rows_per_split);
+  const uint32_t nstages = uint32_t((r_end - r_begin + kPlainRows - 1) / kPlainRows);
+  const int32_t tile_x = int32_t(tile * kPlainTileBytes);
+
+  if (tid == 0) {
+    prefetch_tmap(&map);
+    mbar_init(sbase + PlainSmem::kBarOff, 1);
+    mbar_init(sbase + PlainSmem::kBarOff + 8, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (uint32_t s = 0; s < 2 && s < nstages; ++s)
+      plain_issue_stage(&map, a.records, sbase, s, tile_x, int32_t(r_begin + s * kPlainRows),
+                        a.record_row0 + r_begin + s * kPlainRows);
+  }
+
+  float acc[16];
+  double acc64[16];
+  uint32_t cnt[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    acc[i] = 0.f;
+    acc64[i] = 0.0;
+    cnt[i] = 0u;
+  }
+
+  // Each thread reads word column `tid` of the 1024-byte stage row; the stage
+  // is stored as 4 TMA boxes of [48 rows][256 bytes].
+  const uint32_t word_off = (tid / (kPlainBoxBytes / 4)) * PlainSmem::kBoxBytes +
+                            (tid % (kPlainBoxBytes / 4)) * 4;
+
+  for (uint32_t st = 0; st < nstages; ++st) {
+    const uint32_t buf = st & 1u;
+    const uint32_t parity = (st >> 1) & 1u;
+    const bool ok = mbar_wait_bounded(sbase + PlainSmem::kBarOff + 8 * buf, parity);
+
+    // Build the 16 group tables of this stage: 1024 entries, 4 per thread.
+    {
+      const uint64_t row0 = r_begin + uint64_t(st) * kPlainRows;
+      const float* rec = reinterpret_cast<const float*>(smem + PlainSmem::kRecOff +
+                                                        buf * PlainSmem::kRecBytes);
+      float* lut = reinterpret_cast<float*>(smem + PlainSmem::kLutOff + buf * PlainSmem::kLutBytes);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t e = tid * 4 + q;          // 0..1023
+        const uint32_t g = e >> 6, idx = e & 63;  // group, index
+        float v = 0.f;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const uint32_t row = 3 * g + r;
+          const uint32_t code = (idx >> (2 * r)) & 3u;
+          float t = 0.f;
+          if (code != 0 && row0 + row < r_end) t = rec[row * 4 + (code - 1)];
+          v = (r == 0) ? t : v + t;
+        }
+        lut[e] = v;
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicOr(a.err, kErrTmaTimeout);
+      // Drain the other in-flight stage (bounded) before leaving.
+      if (st + 1 < nstages) mbar_wait_bounded(sbase + PlainSmem::kBarOff + 8 * (buf ^ 1u),
+                                              ((st + 1) >> 1) & 1u);
+      return;
+    }
+
+    const uint8_t* tbase = smem + PlainSmem::kTileOff + buf * PlainSmem::kStageBytes + word_off;
+    const uint32_t* rbase =
+        reinterpret_cast<const uint32_t*>(smem + PlainSmem::kRecOff + buf * PlainSmem::kRecBytes);
+    const uint8_t* lbase = smem + PlainSmem::kLutOff + buf * PlainSmem::kLutBytes;
+    const uint64_t row0 = r_begin + uint64_t(st) * kPlainRows;
+
+    uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
+    uint32_t by[4] = {0u, 0u, 0u, 0u};   // byte counters: byte j = person 4j+q
+#pragma unroll
+    for (uint32_t g = 0; g < kPlainRows / 3; ++g) {
+      const uint32_t xa = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 0) * kPlainBoxBytes);
+      const uint32_t xb = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 1) * kPlainBoxBytes);
+      const uint32_t xc = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 2) * kPlainBoxBytes);
+      // member masks (0x55555555 or 0) from the staged records (.w); rows past
+      // the split end are not members.
+      uint32_t ma = rbase[(3 * g + 0) * 4 + 3];
+      uint32_t mb = rbase[(3 * g + 1) * 4 + 3];
+      uint32_t mc = rbase[(3 * g + 2) * 4 + 3];
+      if (row0 + 3 * g + 0 >= r_end) ma = 0u;
+      if (row0 + 3 * g + 1 >= r_end) mb = 0u;
+      if (row0 + 3 * g + 2 >= r_end) mc = 0u;
+
+      // ---- per-person 6-bit indices (x4) ------------------------------
+      const uint32_t E = (xa & 0x33333333u) | ((xb << 2) & 0xCCCCCCCCu);
+      const uint32_t O = ((xa >> 2) & 0x33333333u) | (xb & 0xCCCCCCCCu);
+      uint32_t ix[4];
+      ix[0] = ((E << 2) & 0x3C3C3C3Cu) | ((xc << 6) & 0xC0C0C0C0u);
+      ix[1] = ((O << 2) & 0x3C3C3C3Cu) | ((xc << 4) & 0xC0C0C0C0u);
+      ix[2] = ((E >> 2) & 0x3C3C3C3Cu) | ((xc << 2) & 0xC0C0C0C0u);
+      ix[3] = ((O >> 2) & 0x3C3C3C3Cu) | (xc & 0xC0C0C0C0u);
+      const uint8_t* lg = lbase + g * 256;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint32_t off = __byte_perm(ix[q], 0u, 0x4440u + j);
+          acc[4 * j + q] += *reinterpret_cast<const float*>(lg + off);
+        }
+      }
+
+      // ---- missing counts ---------------------------------------------
+      const uint32_t c3 = (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
+      ev += c3 & 0x33333333u;
+      od += (c3 >> 2) & 0x33333333u;
+      if ((g % 5) == 4 || g == kPlainRows / 3 - 1) {
+        by[0] += ev & 0x0F0F0F0Fu;
+        by[2] += (ev >> 4) & 0x0F0F0F0Fu;
+        by[1] += od & 0x0F0F0F0Fu;
+        by[3] += (od >> 4) & 0x0F0F0F0Fu;
+        ev = 0u;
+        od = 0u;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) cnt[4 * j + q] += (by[q] >> (8 * j)) & 0xFFu;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      acc64[i] += double(acc[i]);
+      acc[i] = 0.f;
+    }
+
+    __syncthreads();  // every thread is done with stage buffer `buf`
+    if (tid == 0 && st + 2 < nstages) {
+      fence_proxy_async_smem();
+      plain_issue_stage(&map, a.records, sbase, buf, tile_x,
+                        int32_t(r_begin + (st + 2) * kPlainRows),
+                        a.record_row0 + r_begin + (st + 2) * kPlainRows);
+    }
+  }
+
+  // FP64 partials for this (split, person) accumulate across calls.
+  const uint64_t person0 = uint64_t(tile) * (kPlainTileBytes * 4) + uint64_t(tid) * 16;
+  double* ps = a.part_sum + uint64_t(split) * a.part_stride + person0;
+  uint32_t* pc = a.part_cnt + uint64_t(split) * a.part_stride + person0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    ps[i] += acc64[i];
+    pc[i] += cnt[i];
+  }
+}
+
+// out[o*K + k] = init + sum_s part[s][fam(o)] in split order.  One launch per
+// score column k (partials of column k).  init = baseline[k] (fresh run).
+__global__ void gnm_finalize(FinalizeArgs a) {
+  const uint64_t o = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (o >= a.num_people) return;
+  const uint64_t f = a.out_to_fam ? a.out_to_fam[o] : o;
+  double s = a.baseline[a.k];
+  uint32_t c = 0;
+  for (uint32_t sp = 0; sp < a.num_splits; ++sp) {
+    s += a.part_sum[uint64_t(sp) * a.part_stride + f];
+    c += a.part_cnt[uint64_t(sp) * a.part_stride + f];
+  }
+  a.sums[o * a.K + a.k] = s;
+  a.counts[o * a.K + a.k] = c;
+}
+
+__global__ void gnm_decode(const uint8_t* rows, uint64_t pitch, uint64_t nv, uint64_t np,
+                           int8_t* out, uint64_t out_pitch) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t v = blockIdx.y + uint64_t(blockIdx.z) * gridDim.y;
+  if (i >= np || v >= nv) return;
+  const uint32_t code = (rows[v * pitch + (i >> 2)] >> (2 * (i & 3))) & 3u;
+  // batch.rs:489-503: d = hi*(lo+1), code 01 -> missing
+  const int8_t d = code == 1u ? int8_t(-1) : int8_t((code >> 1) * ((code & 1u) + 1u));
+  out[v * out_pitch + i] = d;
+}
+
+// One thread per 32-bit word of a row (16 people).  Same generator as the
+// CPU oracle: key = mix64(seed) ^ v*C1 ^ i*C2, x = mix64(key).
+__global__ void gnm_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint64_t nv,
+                               uint64_t np, const uint32_t* thr, uint64_t seed) {
+  const uint64_t words = pitch / 4;
+  const uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t j = blockIdx.y + uint64_t(blockIdx.z) * gridDim.y;
+  if (w >= words || j >= nv) return;
+  const uint32_t tm = thr[3 * j], t0 = thr[3 * j + 1], t1 = thr[3 * j + 2];
+  const uint64_t v = v0 + j;
+  const uint64_t sk = mix64(seed) ^ (v * 0xD1B54A32D192ED03ull);
+  uint32_t word = 0;
+#pragma unroll 4
+  for (uint32_t q = 0; q < 16; ++q) {
+    const uint64_t i = w * 16 + q;
+    if (i < np) {
+      const uint64_t x = mix64(sk ^ (i * 0x8CB92BA72F3D8DD7ull));
+      const uint32_t um = uint32_t(x), ug = uint32_t(x >> 32);
+      const uint32_t code = um < tm ? 1u : (ug < t0 ? 0u : (ug < t1 ? 2u : 3u));
+      word |= code << (2 * q);
+    }
+  }
+  reinterpret_cast<uint32_t*>(rows + j * pitch)[w] = word;
+}
+
+// ---- host launchers --------------------------------------------------------
+
+cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tiles,
+                                    uint32_t splits, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(gnm_plain_accumulate,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(PlainSmem::kTotal));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  gnm_plain_accumulate<<<dim3(tiles, splits), kPlainThreads, PlainSmem::kTotal, s>>>(map, a);
+  return cudaGetLastError();
+}
+
+uint32_t plain_smem_bytes() { return PlainSmem::kTotal; }
+
+cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s) {
+  const uint32_t blocks = uint32_t((a.num_people + 255) / 256);
+  gnm_finalize<<<blocks ? blocks : 1, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+static dim3 rows_grid(uint64_t x_blocks, uint64_t nv) {
+  uint64_t y = nv, z = 1;
+  while (y > 65535) {
+    z *= 2;
+    y = (nv + z - 1) / z;
+  }
+  return dim3(uint32_t(x_blocks), uint32_t(y), uint32_t(z));
+}
+
+cudaError_t launch_decode(const uint8_t* rows, uint64_t pitch, uint64_t nv, uint64_t np,
+                          int8_t* out, uint64_t out_pitch, cudaStream_t s) {
+  if (nv == 0 || np == 0) return cudaSuccess;
+  gnm_decode<<<rows_grid((np + 255) / 256, nv), 256, 0, s>>>(rows, pitch, nv, np, out, out_pitch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint64_t nv,
+                              uint64_t np, const uint32_t* thr, uint64_t seed, cudaStream_t s) {
+  if (nv == 0) return cudaSuccess;
+  const uint64_t words = pitch / 4;
+  gnm_synth_fill<<<rows_grid((words + 255) / 256, nv), 256, 0, s>>>(rows, pitch, v0, nv, np, thr,
+                                                                    seed);
+  return cudaGetLastError();
+}
+
+}  // namespace gnm

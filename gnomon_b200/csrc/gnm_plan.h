@@ -1,0 +1,66 @@
+// gnm_plan.h — the plan object behind the C ABI (host side).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/gnomon_gpu.h"
+#include "gnm_internal.h"
+
+namespace gnm {
+
+struct TensorPlan;  // split-BF16 engine state (gnm_tensor.cu)
+
+// Thrown inside the library only; converted to a gnm_status at the ABI edge.
+struct Failure {
+  gnm_status status;
+  std::string message;
+};
+
+[[noreturn]] void fail(gnm_status s, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+
+// Scoped current-device switch.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+};
+
+CUtensorMap make_row_map(const uint8_t* d_rows, uint64_t bytes_per_row, uint64_t num_rows,
+                         uint64_t pitch, uint32_t box_x, uint32_t box_y);
+
+}  // namespace gnm
+
+struct gnm_plan {
+  int device = 0;
+  gnm_engine engine = GNM_ENGINE_PLAIN;
+  uint64_t P = 0, fam = 0, bpv = 0, K = 0, V = 0;
+  int num_sms = 0;
+
+  // plain engine
+  uint32_t tiles = 0;          // people tiles of kPlainTileBytes
+  uint32_t splits = 0;         // variant splits (partial slots)
+  uint64_t part_stride = 0;    // people per partial slot (tiles * 4096)
+  uint64_t rec_stride = 0;     // records per score (V + pad)
+  float4* d_records = nullptr; // [K][rec_stride]
+  double* d_part_sum = nullptr;
+  uint32_t* d_part_cnt = nullptr;
+
+  // shared
+  double* d_baseline = nullptr;    // [K]
+  double* d_zero_base = nullptr;   // [K] zeros (resume runs)
+  uint32_t* d_out_to_fam = nullptr;
+  uint32_t* d_err = nullptr;
+  std::vector<double> h_baseline;
+  uint64_t device_bytes = 0;
+  uint64_t launches = 0;
+  double last_spotcheck = 0.0;
+
+  // CSR kept on host for the tensor engine / backward
+  std::vector<float> h_w, h_corr;
+  std::vector<uint32_t> h_cols;
+  std::vector<uint64_t> h_offs;
+
+  gnm::TensorPlan* tensor = nullptr;
+};

@@ -1,0 +1,23 @@
+// gnm_tensor.h — split-BF16 tcgen05 engine and the backward kernel (host entry points).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+struct gnm_plan;
+
+namespace gnm {
+
+// AUTO picks the tensor engine above this many score columns.
+constexpr uint64_t kTensorMinScores = uint64_t(1) << 62;
+
+void tensor_plan_create(gnm_plan* p);
+void tensor_plan_destroy(gnm_plan* p);
+void tensor_reset(gnm_plan* p, cudaStream_t s);
+void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,
+                       uint64_t nv, cudaStream_t s);
+void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_baseline,
+                     cudaStream_t s);
+void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float* d_grad_s,
+                 float* d_grad_w, float* d_grad_corr, cudaStream_t s);
+
+}  // namespace gnm

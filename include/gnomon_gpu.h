@@ -1,0 +1,226 @@
+/*
+ * gnomon_gpu.h — C ABI of the B200 (sm_100a) polygenic-score engine.
+ *
+ * This library stands in for gnomon's GPU scoring backend.  Its entry points
+ * take exactly what gnomon's `score::pipeline` hands its engines: the prepared
+ * CSR of (variant, score) cells, the packed PLINK .bed rows, and an optional
+ * resume state.  They return gnomon's per-person result: row-major [P][K]
+ * final sums (baseline included, not averaged) and [P][K] missing counts.
+ *
+ * Reference interfaces each declaration replaces are cited by file:line in
+ * the SauersML/gnomon tree (crate `gnomon` v0.1.4).
+ *
+ * Conventions
+ *   - Plain C types only; no exceptions or aborts cross this boundary.  Every
+ *     CUDA error, invalid argument and device watchdog expiry becomes a
+ *     gnm_status plus a message in the caller-owned gnm_error.
+ *   - Outputs are caller-allocated.  Host entry points take host pointers;
+ *     `*_device` entry points take device pointers and a cudaStream_t passed
+ *     as `void*` (NULL = the legacy default stream).
+ *   - PLINK code per person per variant (SNP-major, 4 people per byte, person
+ *     i at bits 2*(i%4)): 00 -> dosage 0, 01 -> missing, 10 -> 1, 11 -> 2
+ *     (allele-2 dosage).  Cited: score/batch.rs:489-503,
+ *     score/cuda_backend.rs:106-117.
+ *   - Per (variant v, score k) cell the prepared weights are
+ *       dosage_weight  = +w (effect allele == BIM allele2) or -w (flipped),
+ *       missing_correction = 2w if flipped else 0 (duplicates summed),
+ *     and sum[p,k] = baseline[k] + sum_v dosage_weight*d(p,v)
+ *                    - sum_{v missing for p} missing_correction.
+ *     Cited: score/prepare.rs:197-208, 557-558, 630-650.
+ */
+#ifndef GNOMON_GPU_H
+#define GNOMON_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GNM_ABI_VERSION 1
+
+/* Status codes.  GNM_DECLINED mirrors `Ok(None)` of try_run_cuda
+ * (score/cuda_backend.rs:604-657): the caller falls back to its CPU pipeline.
+ * The error codes mirror PipelineError::{Io, Compute, Producer}
+ * (shared/pipeline_error.rs:5-9). */
+typedef enum gnm_status {
+  GNM_OK = 0,
+  GNM_DECLINED = 1,
+  GNM_ERR_IO = 2,
+  GNM_ERR_COMPUTE = 3,
+  GNM_ERR_PRODUCER = 4,
+  GNM_ERR_TIMEOUT = 5,  /* a bounded device wait expired; context still usable */
+  GNM_ERR_INVALID = 6   /* argument / shape validation failed */
+} gnm_status;
+
+typedef struct gnm_error {
+  char message[512];
+} gnm_error;
+
+/* Engine selection for gnm_score_run_ex. */
+typedef enum gnm_engine {
+  GNM_ENGINE_AUTO = 0,     /* plain for small K, split-BF16 tensor cores for large K */
+  GNM_ENGINE_PLAIN = 1,    /* FP32 CUDA-core LUT kernel, FP64 cross-block reduce */
+  GNM_ENGINE_TENSOR = 2    /* split-BF16 (hi/mid/lo) tcgen05 GEMM, FP32 TMEM accum */
+} gnm_engine;
+
+/* Read-only view of gnomon's PreparationResult (score/types.rs:167-327) for
+ * one scoring run.  All pointers are HOST pointers owned by the caller.
+ *   sparse_row_offsets[v]..[v+1] delimit reconciled variant v's cells,
+ *   columns strictly ascending within a row (prepare.rs:630-650). */
+typedef struct gnm_prep_view {
+  uint64_t num_people;            /* P = num_people_to_score                      */
+  uint64_t total_people_in_fam;   /* people per .bed row (sets bytes_per_variant) */
+  uint64_t bytes_per_variant;     /* ceil(total_people_in_fam / 4) (prepare.rs:811) */
+  uint64_t num_scores;            /* K = score_names.len()                        */
+  uint64_t num_variants;          /* V = num_reconciled_variants                  */
+  const float* sparse_weights;              /* [nnz] dosage_weight                */
+  const float* sparse_missing_corrections;  /* [nnz] missing_correction           */
+  const uint32_t* sparse_score_columns;     /* [nnz] score column < K             */
+  const uint64_t* sparse_row_offsets;       /* [V+1]                              */
+  const uint64_t* required_bim_indices;     /* [V] .bed row of variant v; NULL = identity */
+  const uint32_t* output_idx_to_fam_idx;    /* [P] fam index of output row; NULL = identity */
+  const double* baseline;         /* [K] sum of missing_correction; NULL = computed here */
+} gnm_prep_view;
+
+/* Genotype byte source (shared/files.rs:187-292).  Either `data` points at
+ * the .bed bytes AFTER the 3-byte magic (mmap or RAM; row r at r*bpv), or
+ * `read_at` fills dst with `len` bytes starting at row-data offset `offset`
+ * and returns 0 on success. */
+typedef struct gnm_bed_view {
+  const uint8_t* data;
+  uint64_t data_len;
+  int (*read_at)(void* user_ctx, uint64_t offset, uint8_t* dst, uint64_t len);
+  void* user_ctx;
+} gnm_bed_view;
+
+/* Resume state of a checkpoint (score/checkpoint.rs:293-340,
+ * score/pipeline.rs:1777-1800): the first `completed_variants` reconciled
+ * variants are already folded into `sums`/`counts` ([P][K], baseline
+ * included).  NULL = fresh run. */
+typedef struct gnm_resume {
+  uint64_t completed_variants;
+  const double* sums;
+  const uint32_t* counts;
+} gnm_resume;
+
+/* Optional progress / checkpoint callback, called on the calling thread after
+ * each completed variant block with the running [P][K] state (host memory,
+ * valid only during the call).  Return nonzero to abort with GNM_ERR_PRODUCER. */
+typedef int (*gnm_block_callback)(void* user_ctx, uint64_t completed_variants,
+                                  const double* sums, const uint32_t* counts);
+
+typedef struct gnm_run_options {
+  gnm_engine engine;
+  int device;                     /* CUDA ordinal; -1 = current device            */
+  uint64_t block_variants;        /* streaming block; 0 = whole matrix if it fits */
+  gnm_block_callback on_block;    /* may be NULL                                  */
+  void* on_block_ctx;
+} gnm_run_options;
+
+/* Library / ABI identification.  Returns GNM_ABI_VERSION. */
+int gnm_abi_version(void);
+
+/* Drop-in for `try_run_cuda(context) -> Result<Option<(Vec<f64>, Vec<u32>)>>`
+ * (score/cuda_backend.rs:604), called from pipeline::run
+ * (score/pipeline.rs:480-482).  Host buffers in, host buffers out:
+ *   sums_out    [P*K] row-major final sums (baseline included),
+ *   missing_out [P*K] missing counts.
+ * Returns GNM_DECLINED (leaving outputs untouched) when no usable CUDA device
+ * exists, mirroring the reference's CPU fallback. */
+gnm_status gnm_score_run(const gnm_prep_view* prep, const gnm_bed_view* bed,
+                         const gnm_resume* resume, double* sums_out,
+                         uint32_t* missing_out, gnm_error* err);
+
+/* gnm_score_run with explicit engine / streaming options (NULL = defaults). */
+gnm_status gnm_score_run_ex(const gnm_prep_view* prep, const gnm_bed_view* bed,
+                            const gnm_resume* resume, const gnm_run_options* opts,
+                            double* sums_out, uint32_t* missing_out, gnm_error* err);
+
+/* ---- Device-resident API (genotypes already in HBM) ---------------------
+ * A plan uploads the prepared weights once (the work of CudaRuntime::new,
+ * score/cuda_backend.rs:994-1190, minus NVRTC/cuBLAS) and then scores packed
+ * rows that already live in device memory. */
+typedef struct gnm_plan gnm_plan;
+
+gnm_status gnm_plan_create(const gnm_prep_view* prep, gnm_engine engine, int device,
+                           gnm_plan** plan_out, gnm_error* err);
+void gnm_plan_destroy(gnm_plan* plan);
+
+/* Which engine the plan resolved to (GNM_ENGINE_PLAIN or GNM_ENGINE_TENSOR). */
+gnm_engine gnm_plan_engine(const gnm_plan* plan);
+
+/* Bytes of device scratch the plan holds (partials, tables). */
+uint64_t gnm_plan_device_bytes(const gnm_plan* plan);
+
+/* Zero the plan's accumulators (start of a run).  Asynchronous on `stream`. */
+gnm_status gnm_plan_reset(gnm_plan* plan, void* stream, gnm_error* err);
+
+/* Accumulate reconciled variants [variant_begin, variant_begin+variant_count)
+ * whose packed rows sit at d_rows (row i of the block at d_rows + i*pitch;
+ * pitch a multiple of 16; d_rows 16-byte aligned).  Asynchronous on `stream`. */
+gnm_status gnm_plan_accumulate_device(gnm_plan* plan, const uint8_t* d_rows,
+                                      uint64_t pitch, uint64_t variant_begin,
+                                      uint64_t variant_count, void* stream,
+                                      gnm_error* err);
+
+/* Write final [P][K] sums (baseline added, output rows gathered through
+ * output_idx_to_fam_idx) and counts to DEVICE buffers.  Asynchronous; the
+ * status of the device watchdog is checked by gnm_plan_sync. */
+gnm_status gnm_plan_finalize_device(gnm_plan* plan, double* d_sums_out,
+                                    uint32_t* d_missing_out, void* stream,
+                                    gnm_error* err);
+
+/* Synchronize `stream` and report any device-side watchdog / error flag. */
+gnm_status gnm_plan_sync(gnm_plan* plan, void* stream, gnm_error* err);
+
+/* One-shot device scoring: reset + accumulate(all V rows) + finalize. */
+gnm_status gnm_score_device(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
+                            double* d_sums_out, uint32_t* d_missing_out,
+                            void* stream, gnm_error* err);
+
+/* Number of kernel launches the last accumulate+finalize issued (for audit). */
+uint64_t gnm_plan_launch_count(const gnm_plan* plan);
+
+/* ---- Packed-row utilities ------------------------------------------------ */
+
+/* Decode packed rows to int8 dosage codes on the device: out[v*out_pitch + i]
+ * = {0,1,2} or -1 for missing, for i < num_people.  Used for decode parity. */
+gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch,
+                             uint64_t num_variants, uint64_t num_people,
+                             int8_t* d_out, uint64_t out_pitch, void* stream,
+                             gnm_error* err);
+
+/* Fill a device matrix with the deterministic synthetic HWE genotype
+ * generator (see DESIGN.md "Synthetic data"): per-variant uint32 thresholds
+ * {t_missing, T0, T1}, code = u_m < t_m ? 01 : u_g < T0 ? 00 : u_g < T1 ? 10 : 11
+ * with (u_m, u_g) the two halves of mix64(key(seed, v, i)).  Padding people
+ * (i >= num_people) are 00. */
+gnm_status gnm_synth_fill_device(uint8_t* d_rows, uint64_t pitch, uint64_t variant_begin,
+                                 uint64_t num_variants, uint64_t num_people,
+                                 const uint32_t* d_thresholds /* [num_variants][3] */,
+                                 uint64_t seed, void* stream, gnm_error* err);
+
+/* ---- Split-BF16 tensor-core batched scoring ------------------------------ */
+
+/* Max relative error report of the last tensor-engine run versus its own
+ * FP64 spot check (0 if none). */
+double gnm_plan_last_spotcheck(const gnm_plan* plan);
+
+/* ---- Backward: dW = G^T dS by re-unpacking genotypes -------------------- */
+
+/* d_grad_w[v*K + k] = sum_p dosage'(p,v) * d_grad_s[p*K + k] where dosage' is
+ * the allele-2 dosage with missing -> 0 (the derivative of the plain score
+ * w.r.t. dosage_weight), and d_grad_corr[v*K+k] = -sum_{p missing} dS[p,k]
+ * (derivative w.r.t. missing_correction; may be NULL).  dS is [P][K] FP32
+ * over output rows (gathered through output_idx_to_fam_idx). */
+gnm_status gnm_backward_dw_device(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
+                                  const float* d_grad_s, float* d_grad_w,
+                                  float* d_grad_corr, void* stream, gnm_error* err);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GNOMON_GPU_H */

@@ -1,0 +1,171 @@
+"""Plain (FP32 CUDA-core) engine on the GPU versus the CPU oracle, through the C ABI."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gnomon_b200 import _lib, synth
+from gnomon_b200.pipeline import PipelineContext, PipelineError, ScoreCheckpoint, run
+from gnomon_b200.prepare import PreparationResult
+from helpers import GOLDEN, case_prep, cohort_prep, expected_final, known_answer_cases, synth_case
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+PLAIN = _lib.ENGINE_PLAIN
+CASES = known_answer_cases()["engine_cases"]
+
+
+def host_run(prep, rows, **kw):
+    return run(PipelineContext(prep), np.ascontiguousarray(rows).reshape(-1), engine=PLAIN, **kw)
+
+
+def assert_parity(got, want_ref, want_ext=None):
+    s, c = got
+    rs, rc = want_ref
+    np.testing.assert_array_equal(c, rc)                       # counts: bit exact
+    ok = oracle.within_reference_tolerance(s, rs)              # gpu_tests.rs:135-147
+    assert ok.all(), f"{(~ok).sum()} cells outside 1e-6; worst {oracle.rel_err(s, rs).max():.3e}"
+    if want_ext is not None:
+        assert oracle.rel_err(s, want_ext[0]).max() < 1e-9
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_known_answers(cuda, case):
+    prep, rows = case_prep(case)
+    s, c = host_run(prep, rows)
+    ws, wc = expected_final(case, prep)
+    np.testing.assert_allclose(s, ws, rtol=0, atol=1e-9)
+    np.testing.assert_array_equal(c, wc)
+
+
+def test_reference_gpu_tests_cohort(cuda):
+    prep, rows = cohort_prep(16)
+    assert_parity(host_run(prep, rows), oracle.score_reference(rows, prep, threads=4),
+                  oracle.score_extended(rows, prep))
+
+
+def test_plain_config_full_size(cuda):
+    """2,000 samples x 50,000 variants, one score, 1% missing, 10% flipped."""
+    _, prep, rows, _ = synth_case(2_000, 50_000)
+    got = host_run(prep, rows)
+    assert_parity(got, oracle.score_reference(rows, prep, threads=8),
+                  oracle.score_extended(rows, prep))
+    assert got[1].sum() > 0
+
+
+@pytest.mark.parametrize("people,variants", [(1, 1), (3, 47), (4, 48), (5, 49), (4095, 97),
+                                             (4097, 145), (8197, 50), (1030, 1000)])
+def test_edge_shapes(cuda, people, variants):
+    _, prep, rows, _ = synth_case(people, variants, seed_offset=people + variants)
+    assert_parity(host_run(prep, rows), oracle.score_reference(rows, prep, threads=2),
+                  oracle.score_extended(rows, prep))
+
+
+def test_multi_score_uneven_membership(cuda):
+    _, prep, rows, _ = synth_case(3000, 2000, scores=5, config="batched_100k_x_500k_k512")
+    assert len(set(np.diff(prep.sparse_row_offsets.astype(np.int64)))) > 1
+    assert_parity(host_run(prep, rows), oracle.score_reference(rows, prep, threads=4),
+                  oracle.score_extended(rows, prep))
+
+
+def test_keep_subset_and_row_map(cuda):
+    rng = np.random.default_rng(7)
+    _, prep, rows, _ = synth_case(5000, 900, scores=2, config="diff_20k_x_200k_k16")
+    # shuffle the .bed row order; required_bim_indices maps reconciled -> bed row
+    perm = rng.permutation(900)
+    bed = np.empty_like(rows)
+    bed[perm] = rows
+    keep = rng.choice(5000, 1234, replace=False).astype(np.uint32)
+    p2 = PreparationResult(prep.sparse_weights, prep.sparse_missing_corrections,
+                           prep.sparse_score_columns, prep.sparse_row_offsets, prep.score_names,
+                           5000, required_bim_indices=perm.astype(np.uint64),
+                           output_idx_to_fam_idx=keep)
+    got = host_run(p2, bed)
+    assert_parity(got, oracle.score_reference(rows, p2, threads=4),
+                  oracle.score_extended(rows, p2))
+
+
+def test_streaming_blocks_and_resume(cuda):
+    _, prep, rows, _ = synth_case(2500, 1000)
+    full = host_run(prep, rows)
+    streamed = host_run(prep, rows, block_variants=100)
+    np.testing.assert_array_equal(streamed[1], full[1])
+    assert oracle.rel_err(streamed[0], full[0]).max() < 1e-12
+    seen = []
+    host_run(prep, rows, block_variants=300, on_block=lambda n, s, c: seen.append(n))
+    assert seen == [300, 600, 900, 1000]
+    # resume: first 400 variants from a checkpoint computed on the CPU oracle
+    head = PreparationResult(prep.sparse_weights[:400], prep.sparse_missing_corrections[:400],
+                             prep.sparse_score_columns[:400], prep.sparse_row_offsets[:401],
+                             prep.score_names, 2500, baseline=prep.baseline)
+    hs, hc = oracle.score_extended(rows[:400], head)
+    ctx = PipelineContext(prep, ScoreCheckpoint(400, hs, hc))
+    got = run(ctx, rows.reshape(-1), engine=PLAIN)
+    np.testing.assert_array_equal(got[1], full[1])
+    assert oracle.rel_err(got[0], full[0]).max() < 1e-9
+
+
+def test_rows_without_cells(cuda):
+    _, prep, rows, _ = synth_case(700, 200, scores=3, config="diff_20k_x_200k_k16")
+    offs = prep.sparse_row_offsets.astype(np.int64)
+    keep_rows = np.ones(200, bool)
+    keep_rows[::7] = False   # every 7th variant loses all its cells (e.g. a complex-only row)
+    sel = np.repeat(keep_rows, np.diff(offs))
+    counts = np.where(keep_rows, np.diff(offs), 0)
+    new_offs = np.zeros(201, np.uint64)
+    np.cumsum(counts, out=new_offs[1:])
+    p2 = PreparationResult(prep.sparse_weights[sel], prep.sparse_missing_corrections[sel],
+                           prep.sparse_score_columns[sel], new_offs, prep.score_names, 700)
+    assert_parity(host_run(p2, rows), oracle.score_reference(rows, p2, threads=2),
+                  oracle.score_extended(rows, p2))
+
+
+def test_truncated_bed_is_an_io_error(cuda):
+    _, prep, rows, _ = synth_case(400, 100)
+    with pytest.raises(PipelineError) as e:
+        run(PipelineContext(prep), rows.reshape(-1)[:-5], engine=PLAIN)
+    assert e.value.kind == "Io"
+
+
+def test_device_api_matches_host_api(cuda):
+    import torch
+    from gnomon_b200.device import DevicePlan, row_pitch
+    _, prep, rows, _ = synth_case(3333, 777, scores=2, config="diff_20k_x_200k_k16")
+    pitch = row_pitch(prep.bytes_per_variant)
+    dev = np.zeros((777, pitch), np.uint8)
+    dev[:, :rows.shape[1]] = rows
+    d_rows = torch.from_numpy(dev).cuda()
+    plan = DevicePlan(prep, engine=PLAIN)
+    s, c = plan.score(d_rows, pitch)
+    plan.sync()
+    host = host_run(prep, rows)
+    np.testing.assert_array_equal(c.cpu().numpy().astype(np.uint32), host[1])
+    np.testing.assert_array_equal(s.cpu().numpy(), host[0])
+    assert plan.launches == 2 * 2   # one accumulate + one finalize launch per score
+
+
+def test_decode_parity_ld_fixture_and_synthetic(cuda):
+    import torch
+    from gnomon_b200.device import decode
+    z = np.load(GOLDEN / "ld_fixture.npz")
+    rows, P = z["rows"], int(z["num_people"])
+    for r, p in [(rows, P)] + [(synth_case(pp, 33)[2], pp) for pp in (1, 6, 4099)]:
+        pitch = (r.shape[1] + 15) // 16 * 16
+        dev = np.zeros((r.shape[0], pitch), np.uint8)
+        dev[:, :r.shape[1]] = r
+        got = decode(torch.from_numpy(dev).cuda(), pitch, r.shape[0], p).cpu().numpy()
+        np.testing.assert_array_equal(got, oracle.decode(r, p))
+
+
+@pytest.mark.parametrize("people", [1, 13, 4096, 50_000])
+def test_gpu_generator_matches_numpy(cuda, people):
+    import torch
+    from gnomon_b200.device import row_pitch, synth_fill
+    w = synth.WORKLOADS["bandwidth_50k_x_1m"]
+    n, v0 = 37, 123_456
+    thr = synth.variant_thresholds(w.seed, v0, n, w.p_lo, w.p_hi, w.missing_rate)
+    pitch = row_pitch((people + 3) // 4)
+    d = torch.full((n, pitch), 0xAB, dtype=torch.uint8, device="cuda")
+    synth_fill(d, pitch, v0, n, people, thr, w.seed)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), synth.synth_rows(w.seed, v0, n, people, thr, pitch))
