@@ -205,6 +205,8 @@ def gpu_arm(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     w = synth.WORKLOADS[WORKLOAD]
+    if args.variants:
+        w = synth.scaled(w, w.people, args.variants)
     if world > 1:  # person sharding: each rank owns a distinct 50,000-person shard
         w = synth.Workload(w.name, w.people, w.variants, w.scores, w.p_lo, w.p_hi,
                            w.missing_rate, w.sigma, w.flip_frac, w.size_lo, w.size_hi,
@@ -344,6 +346,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-s", type=float, default=12.0, help="CPU baseline sample seconds")
     ap.add_argument("--ref-step-s", type=float, default=4.0)
+    ap.add_argument("--variants", type=int, default=0,
+                    help="override the variant count (small cases for profiler captures)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

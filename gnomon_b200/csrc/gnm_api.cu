@@ -335,6 +335,7 @@ struct HostRun {
   const gnm_prep_view* prep;
   const gnm_bed_view* bed;
   uint64_t pitch;
+  uint64_t zero_before;  // rows below this reconciled index are staged as zeros
 };
 
 static bool is_pinned(const void* ptr) {
@@ -355,8 +356,12 @@ static void gather_rows(const HostRun& r, uint64_t v0, uint64_t n, uint8_t* dst)
   std::atomic<int> bad{0};
   auto work = [&](unsigned t) {
     for (uint64_t i = t; i < n; i += nt) {
-      const uint64_t row = map ? map[v0 + i] : v0 + i;
       uint8_t* d = dst + i * r.pitch;
+      if (v0 + i < r.zero_before) {  // already folded into the resume state
+        std::memset(d, 0, r.pitch);
+        continue;
+      }
+      const uint64_t row = map ? map[v0 + i] : v0 + i;
       if (r.bed->data) {
         if ((row + 1) * bpv > r.bed->data_len) {
           bad = 1;
@@ -403,7 +408,10 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   if (resume && (!resume->sums || !resume->counts))
     fail(GNM_ERR_INVALID, "resume state has NULL buffers");
   const uint64_t pitch = (p->bpv + 127) / 128 * 128;
-  HostRun r{p, prep, bed, pitch};
+  // tensor-engine blocks start on 64-variant boundaries; rows between the
+  // boundary and the resume point are staged as zeros (they contribute nothing)
+  const uint64_t v_first = p->engine == GNM_ENGINE_TENSOR ? v_start - v_start % 64 : v_start;
+  HostRun r{p, prep, bed, pitch, v_start};
 
   cudaStream_t cs = nullptr, xs = nullptr;
   check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
@@ -420,11 +428,12 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   // alternating blocks of block_variants rows.
   size_t free_b = 0, total_b = 0;
   check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-  const uint64_t remaining = V - v_start;
+  const uint64_t remaining = V - v_first;
   uint64_t block = o.block_variants ? o.block_variants : remaining;
   const uint64_t cap_rows = std::max<uint64_t>(kPlainRows, uint64_t(0.6 * double(free_b)) / pitch);
   if (!o.block_variants && block > cap_rows) block = std::max<uint64_t>(kPlainRows, cap_rows / 2);
   block = std::max<uint64_t>(1, std::min<uint64_t>(block, std::max<uint64_t>(1, remaining)));
+  if (p->engine == GNM_ENGINE_TENSOR) block = (block + 63) / 64 * 64;
   const int nbuf = remaining > block ? 2 : 1;
 
   std::vector<uint8_t*> dbuf(nbuf, nullptr);
@@ -489,15 +498,19 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   uint64_t stage_idx = 0;
   std::vector<double> cb_sums;
   std::vector<uint32_t> cb_cnt;
-  for (uint64_t b0 = v_start, bi = 0; b0 < V; b0 += block, ++bi) {
+  for (uint64_t b0 = v_first, bi = 0; b0 < V; b0 += block, ++bi) {
     const uint64_t nb = std::min(block, V - b0);
     const int slot = int(bi % nbuf);
     // the compute of the block that last used this device buffer must be done
     check_cuda(cudaStreamWaitEvent(xs, consumed[slot], 0), "wait");
     if (direct) {
-      check_cuda(cudaMemcpy2DAsync(dbuf[slot], pitch, bed->data + b0 * p->bpv, p->bpv, p->bpv, nb,
-                                   cudaMemcpyHostToDevice, xs),
-                 "H2D rows");
+      const uint64_t skip = b0 < v_start ? v_start - b0 : 0;
+      if (skip) check_cuda(cudaMemsetAsync(dbuf[slot], 0, skip * pitch, xs), "zero rows");
+      if (nb > skip)
+        check_cuda(cudaMemcpy2DAsync(dbuf[slot] + skip * pitch, pitch,
+                                     bed->data + (b0 + skip) * p->bpv, p->bpv, p->bpv, nb - skip,
+                                     cudaMemcpyHostToDevice, xs),
+                   "H2D rows");
     } else {
       for (uint64_t c0 = 0; c0 < nb; c0 += chunk, ++stage_idx) {
         const uint64_t nc = std::min(chunk, nb - c0);

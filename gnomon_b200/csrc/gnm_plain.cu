@@ -107,6 +107,11 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
     const bool ok = mbar_wait_bounded(sbase + PlainSmem::kBarOff + 8 * buf, parity);
 
     // Build the 16 group tables of this stage: 1024 entries, 4 per thread.
+    // Entry index e (6 bits): code of row a in bits 0-1, row b in bits 2-3,
+    // row c with its two bits swapped (hi in bit 4, lo in bit 5) so that the
+    // rarely-set lo bit of row c selects the shared-memory row of the table
+    // and lanes collide on banks less often.  The sum of the three FP32 terms
+    // is exact in FP64 and rounded to FP32 once.
     {
       const uint64_t row0 = r_begin + uint64_t(st) * kPlainRows;
       const float* rec = reinterpret_cast<const float*>(smem + PlainSmem::kRecOff +
@@ -116,16 +121,24 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
       for (int q = 0; q < 4; ++q) {
         const uint32_t e = tid * 4 + q;          // 0..1023
         const uint32_t g = e >> 6, idx = e & 63;  // group, index
-        float v = 0.f;
+        const uint32_t code[3] = {idx & 3u, (idx >> 2) & 3u,
+                                  ((idx >> 3) & 2u) | ((idx >> 5) & 1u)};
+        double v = 0.0;
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           const uint32_t row = 3 * g + r;
-          const uint32_t code = (idx >> (2 * r)) & 3u;
-          float t = 0.f;
-          if (code != 0 && row0 + row < r_end) t = rec[row * 4 + (code - 1)];
-          v = (r == 0) ? t : v + t;
+          if (code[r] != 0 && row0 + row < r_end) v += double(rec[row * 4 + (code[r] - 1)]);
         }
-        lut[e] = v;
+        lut[e] = float(v);
+      }
+      // Membership bitmap of the stage's 48 rows (rows past the split end are
+      // not members): two ballots replace 48 per-row mask loads.
+      if (tid < 64) {
+        const uint32_t r = tid;
+        const bool m = r < kPlainRows && row0 + r < r_end && rec[r * 4 + 3] != 0.0f;
+        const uint32_t bits = __ballot_sync(0xFFFFFFFFu, m);
+        if ((tid & 31) == 0)
+          reinterpret_cast<uint32_t*>(smem + PlainSmem::kBarOff + 16)[2 * buf + (tid >> 5)] = bits;
       }
     }
     if (__syncthreads_or(!ok)) {
@@ -137,35 +150,26 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
     }
 
     const uint8_t* tbase = smem + PlainSmem::kTileOff + buf * PlainSmem::kStageBytes + word_off;
-    const uint32_t* rbase =
-        reinterpret_cast<const uint32_t*>(smem + PlainSmem::kRecOff + buf * PlainSmem::kRecBytes);
     const uint8_t* lbase = smem + PlainSmem::kLutOff + buf * PlainSmem::kLutBytes;
-    const uint64_t row0 = r_begin + uint64_t(st) * kPlainRows;
+    const uint32_t* mbits = reinterpret_cast<const uint32_t*>(smem + PlainSmem::kBarOff + 16);
+    const uint64_t members = uint64_t(mbits[2 * buf]) | (uint64_t(mbits[2 * buf + 1]) << 32);
 
     uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
     uint32_t by[4] = {0u, 0u, 0u, 0u};   // byte counters: byte j = person 4j+q
-#pragma unroll
-    for (uint32_t g = 0; g < kPlainRows / 3; ++g) {
+    auto group = [&](uint32_t g, uint32_t ma, uint32_t mb, uint32_t mc) {
       const uint32_t xa = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 0) * kPlainBoxBytes);
       const uint32_t xb = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 1) * kPlainBoxBytes);
       const uint32_t xc = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 2) * kPlainBoxBytes);
-      // member masks (0x55555555 or 0) from the staged records (.w); rows past
-      // the split end are not members.
-      uint32_t ma = rbase[(3 * g + 0) * 4 + 3];
-      uint32_t mb = rbase[(3 * g + 1) * 4 + 3];
-      uint32_t mc = rbase[(3 * g + 2) * 4 + 3];
-      if (row0 + 3 * g + 0 >= r_end) ma = 0u;
-      if (row0 + 3 * g + 1 >= r_end) mb = 0u;
-      if (row0 + 3 * g + 2 >= r_end) mc = 0u;
-
       // ---- per-person 6-bit indices (x4) ------------------------------
+      // row c enters with its code bits swapped (see the table layout above)
+      const uint32_t xs = ((xc >> 1) & 0x55555555u) | ((xc << 1) & 0xAAAAAAAAu);
       const uint32_t E = (xa & 0x33333333u) | ((xb << 2) & 0xCCCCCCCCu);
       const uint32_t O = ((xa >> 2) & 0x33333333u) | (xb & 0xCCCCCCCCu);
       uint32_t ix[4];
-      ix[0] = ((E << 2) & 0x3C3C3C3Cu) | ((xc << 6) & 0xC0C0C0C0u);
-      ix[1] = ((O << 2) & 0x3C3C3C3Cu) | ((xc << 4) & 0xC0C0C0C0u);
-      ix[2] = ((E >> 2) & 0x3C3C3C3Cu) | ((xc << 2) & 0xC0C0C0C0u);
-      ix[3] = ((O >> 2) & 0x3C3C3C3Cu) | (xc & 0xC0C0C0C0u);
+      ix[0] = ((E << 2) & 0x3C3C3C3Cu) | ((xs << 6) & 0xC0C0C0C0u);
+      ix[1] = ((O << 2) & 0x3C3C3C3Cu) | ((xs << 4) & 0xC0C0C0C0u);
+      ix[2] = ((E >> 2) & 0x3C3C3C3Cu) | ((xs << 2) & 0xC0C0C0C0u);
+      ix[3] = ((O >> 2) & 0x3C3C3C3Cu) | (xs & 0xC0C0C0C0u);
       const uint8_t* lg = lbase + g * 256;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -175,8 +179,7 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
           acc[4 * j + q] += *reinterpret_cast<const float*>(lg + off);
         }
       }
-
-      // ---- missing counts ---------------------------------------------
+      // ---- missing counts (code 01 of member rows) ---------------------
       const uint32_t c3 = (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
       ev += c3 & 0x33333333u;
       od += (c3 >> 2) & 0x33333333u;
@@ -187,6 +190,19 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
         by[3] += (od >> 4) & 0x0F0F0F0Fu;
         ev = 0u;
         od = 0u;
+      }
+    };
+    if (members == (uint64_t(1) << kPlainRows) - 1) {
+      // every row of the stage is a member of this score (the common case)
+#pragma unroll
+      for (uint32_t g = 0; g < kPlainRows / 3; ++g) group(g, 0x55555555u, 0x55555555u, 0x55555555u);
+    } else {
+#pragma unroll
+      for (uint32_t g = 0; g < kPlainRows / 3; ++g) {
+        const uint32_t ma = (0u - uint32_t((members >> (3 * g + 0)) & 1u)) & 0x55555555u;
+        const uint32_t mb = (0u - uint32_t((members >> (3 * g + 1)) & 1u)) & 0x55555555u;
+        const uint32_t mc = (0u - uint32_t((members >> (3 * g + 2)) & 1u)) & 0x55555555u;
+        group(g, ma, mb, mc);
       }
     }
 #pragma unroll

@@ -1,14 +1,559 @@
-// gnm_tensor.cu — placeholder until the tcgen05 engine lands.
+// gnm_tensor.cu — split-BF16 tcgen05 engine (many score columns) and the
+// re-unpacking backward kernel dW = G^T dS.
+//
+// Scoring as a GEMM (the reference does this with three cuBLAS SGEMMs per
+// score tile, score/cuda_backend.rs:2196-2233):
+//   sum[p,k] = baseline[k] + sum_v W'[k,v] d(p,v) - sum_v C[k,v] m(p,v)
+//   miss[p,k] = sum_v member[k,v] m(p,v)
+// with d the allele-2 dosage (missing -> 0), m the missing indicator.
+//
+// Precision (the "hi/mid/lo" split): every weight-like value x of score k is
+// written as hi + mid + lo, each an integer multiple of a power-of-two quantum
+// (q, q/256, q/65536 with 2^E = 256 q >= max |x| of the score), |integer| <= 256,
+// so every limb is exact in BF16 and the residual is below 2^-25 of the score's
+// largest weight.  Products with d in {0,1,2} and m in {0,1} are exact, every
+// partial sum of one limb is an integer multiple of its quantum, and below
+// 32768 variants its magnitude stays under 2^24 quanta: the FP32 tensor-memory
+// accumulation of each limb is EXACT.  Accumulators are flushed to FP64 every
+// 16384 variants (the cross-block reduction is the only FP64 arithmetic).
+//
+// Kernel shape (one CTA per SM): M = 128 score rows (TMEM lanes), N = 128
+// people (TMEM columns), K = 64 variants per stage.  Warp 0 issues TMA (weight
+// limb planes, 3D map, 128-byte swizzle; packed rows, 2D map), warp 1 owns
+// TMEM and issues tcgen05.mma, warps 2-5 expand packed 2-bit genotypes into
+// the BF16 K-major operand in shared memory and drain TMEM at block ends.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gnm_device.cuh"
 #include "gnm_plan.h"
+#include "gnm_tcgen05.cuh"
 #include "gnm_tensor.h"
 
 namespace gnm {
-void tensor_plan_create(gnm_plan*) { fail(GNM_ERR_COMPUTE, "tensor engine not built"); }
-void tensor_plan_destroy(gnm_plan*) {}
-void tensor_reset(gnm_plan*, cudaStream_t) {}
-void tensor_accumulate(gnm_plan*, const uint8_t*, uint64_t, uint64_t, uint64_t, cudaStream_t) {}
-void tensor_finalize(gnm_plan*, double*, uint32_t*, bool, cudaStream_t) {}
-void backward_dw(gnm_plan*, const uint8_t*, uint64_t, const float*, float*, float*, cudaStream_t) {
-  fail(GNM_ERR_COMPUTE, "backward not built");
+
+constexpr uint32_t kTcM = 128;        // score rows per tile
+constexpr uint32_t kTcN = 128;        // people per tile
+constexpr uint32_t kTcK = 64;         // variants per stage
+constexpr uint32_t kTcFlush = 256;    // stages per exact FP32 block (16384 variants)
+constexpr uint32_t kTcThreads = 192;  // 6 warps
+
+struct TensorPlan {
+  uint64_t K_pad = 0, V_pad = 0, P_pad = 0;
+  uint32_t ptiles = 0, stiles = 0;
+  __nv_bfloat16* d_planes_dos = nullptr;  // [3][K_pad][V_pad] W' limbs
+  __nv_bfloat16* d_planes_mis = nullptr;  // [4][K_pad][V_pad] -corr limbs, member
+  double* d_part_sum = nullptr;           // [K_pad][P_pad]
+  uint32_t* d_part_cnt = nullptr;         // [K_pad][P_pad]
+  CUtensorMap map_dos, map_mis;
+};
+
+struct TcArgs {
+  uint64_t num_rows;       // rows of this block
+  int32_t a_x0;            // absolute variant index of block row 0 (multiple of 64)
+  double* part_sum;
+  uint32_t* part_cnt;
+  uint64_t P_pad;
+  uint32_t* err;
+};
+
+template <int NP, int ST>
+struct TcSmem {
+  static constexpr uint32_t kPlane = kTcM * kTcK * 2;   // 16 KB
+  static constexpr uint32_t kAStage = NP * kPlane;
+  static constexpr uint32_t kB = kTcN * kTcK * 2;       // 16 KB
+  static constexpr uint32_t kPk = kTcK * (kTcN / 4);    // 2 KB
+  static constexpr uint32_t kAOff = 0;
+  static constexpr uint32_t kBOff = kAOff + ST * kAStage;
+  static constexpr uint32_t kPkOff = kBOff + ST * kB;
+  static constexpr uint32_t kBarOff = kPkOff + ST * kPk;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (3 * ST + 2);
+  static constexpr uint32_t kTotal = kHolder + 16 + 1024;  // + alignment slack
+};
+
+// code -> BF16 byte tables for __byte_perm (pool bytes 0-3: low bytes by
+// code, 4-7: high bytes by code).  Dosage: 00->0, 01(missing)->0, 10->1, 11->2.
+// Missing indicator: 01 -> 1, else 0.
+constexpr uint32_t kDosLo = 0x00800000u, kDosHi = 0x403F0000u;
+constexpr uint32_t kMisLo = 0x00008000u, kMisHi = 0x00003F00u;
+
+__device__ __forceinline__ uint32_t bf16_pair(uint32_t y16, uint32_t lo, uint32_t hi) {
+  return __byte_perm(lo, hi, y16 * 0x11u + 0x4040u);
 }
+
+template <int NP, int ST, bool MISSING>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    gnm_tc_accumulate(const __grid_constant__ CUtensorMap amap,
+                      const __grid_constant__ CUtensorMap pmap, TcArgs a) {
+  using L = TcSmem<NP, ST>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sb = smem_u32(smem);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ptile = blockIdx.x, stile = blockIdx.y;
+  const uint32_t nit = uint32_t((a.num_rows + kTcK - 1) / kTcK);
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
+  auto bready = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
+  auto empty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (2 * ST + s); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < ST; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(bready(s), 128);
+      mbar_init(empty(s), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, 128);
+    *abort_flag = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&amap);
+    prefetch_tmap(&pmap);
+  }
+  if (warp == 1) {
+    tmem_alloc(sb + L::kHolder, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + L::kHolder);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        if (!mbar_wait_bounded(empty(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (*abort_flag) break;
+        mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
+        tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kTcK),
+                    int32_t(stile * kTcM), 0, full(s));
+        tma_load_2d(sb + L::kPkOff + s * L::kPk, &pmap, int32_t(ptile * (kTcN / 4)),
+                    int32_t(it * kTcK), full(s));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16_f32(kTcM, kTcN);
+      uint32_t blk = 0;
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        const bool first = (it % kTcFlush) == 0;
+        if (first && it > 0) {
+          if (!mbar_wait_bounded(accempty, (blk - 1) & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            break;
+          }
+        }
+        if (!mbar_wait_bounded(bready(s), ph)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (*abort_flag) break;
+        tc_fence_after();
+        const uint32_t a0 = sb + L::kAOff + s * L::kAStage;
+        const uint32_t b0 = sb + L::kBOff + s * L::kB;
+#pragma unroll
+        for (uint32_t kk = 0; kk < kTcK / 16; ++kk) {
+          const uint64_t bdesc = desc_kmajor_sw128(b0 + kk * 32);
+#pragma unroll
+          for (uint32_t j = 0; j < NP; ++j) {
+            const uint64_t adesc = desc_kmajor_sw128(a0 + j * L::kPlane + kk * 32);
+            tc_mma_f16(tmem + j * kTcN, adesc, bdesc, idesc, (first && kk == 0) ? 0u : 1u);
+          }
+        }
+        tc_commit(empty(s));
+        if ((it % kTcFlush) == kTcFlush - 1 || it == nit - 1) {
+          tc_commit(accfull);
+          ++blk;
+        }
+      }
+    }
+  } else {
+    // ---------------- genotype expansion + epilogue (warps 2-5) ----------------
+    const uint32_t pt = threadIdx.x - 64;      // 0..127
+    const uint32_t col = pt & 31;              // byte column: people 4col..4col+3
+    const uint32_t vg = pt >> 5;               // variant group: rows 16vg..16vg+15
+    const uint32_t quad = warp & 3;            // TMEM lane quadrant of this warp
+    uint32_t blk = 0;
+    for (uint32_t it = 0; it < nit; ++it) {
+      const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      if (!mbar_wait_bounded(full(s), ph)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrTmaTimeout);
+        break;
+      }
+      if (*abort_flag) break;
+      const uint8_t* pk = smem + L::kPkOff + s * L::kPk;
+      uint8_t* bt = smem + L::kBOff + s * L::kB;
+#pragma unroll
+      for (uint32_t cc = 0; cc < 2; ++cc) {
+        const uint32_t r0 = 16 * vg + 8 * cc;
+        uint32_t xl = 0, xh = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < 4; ++i) {
+          xl |= uint32_t(pk[(r0 + i) * (kTcN / 4) + col]) << (8 * i);
+          xh |= uint32_t(pk[(r0 + 4 + i) * (kTcN / 4) + col]) << (8 * i);
+        }
+        const uint32_t c = 2 * vg + cc;  // 16-byte chunk (8 variants) index
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+          const uint32_t yl = (xl >> (2 * q)) & 0x03030303u;
+          const uint32_t yh = (xh >> (2 * q)) & 0x03030303u;
+          const uint32_t lo = MISSING ? kMisLo : kDosLo, hi = MISSING ? kMisHi : kDosHi;
+          uint4 v;
+          v.x = bf16_pair(yl & 0xFFFFu, lo, hi);
+          v.y = bf16_pair(yl >> 16, lo, hi);
+          v.z = bf16_pair(yh & 0xFFFFu, lo, hi);
+          v.w = bf16_pair(yh >> 16, lo, hi);
+          const uint32_t n = 32 * q + col;  // operand row of person 4col+q
+          *reinterpret_cast<uint4*>(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4)) = v;
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(bready(s));
+
+      if ((it % kTcFlush) == kTcFlush - 1 || it == nit - 1) {
+        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        tc_fence_after();
+        const uint64_t k = uint64_t(stile) * kTcM + 32 * quad + lane;
+        double* ps = a.part_sum + k * a.P_pad + uint64_t(ptile) * kTcN;
+        uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(ptile) * kTcN;
+        const uint32_t lane_base = tmem + ((32 * quad) << 16);
+#pragma unroll 1
+        for (uint32_t cb = 0; cb < kTcN / 32; ++cb) {
+          double acc[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+#pragma unroll
+          for (uint32_t j = 0; j < 3; ++j) {
+            uint32_t r[32];
+            tmem_ld32(lane_base + j * kTcN + 32 * cb, r);
+            tmem_ld_wait();
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] += double(__uint_as_float(r[i]));
+          }
+#pragma unroll
+          for (int i = 0; i < 32; ++i) ps[32 * cb + i] += acc[i];
+          if (MISSING) {
+            uint32_t r[32];
+            tmem_ld32(lane_base + 3 * kTcN + 32 * cb, r);
+            tmem_ld_wait();
+#pragma unroll
+            for (int i = 0; i < 32; ++i) pc[32 * cb + i] += __float2uint_rn(__uint_as_float(r[i]));
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(accempty);
+        ++blk;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// Limb planes from the CSR: one thread per variant.
+__global__ void gnm_tc_build_planes(const float* w, const float* corr, const uint32_t* cols,
+                                    const uint64_t* offs, uint64_t V, const float* qhi,
+                                    __nv_bfloat16* dos, __nv_bfloat16* mis, uint64_t K_pad,
+                                    uint64_t V_pad) {
+  const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const uint64_t plane = K_pad * V_pad;
+  for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
+    const uint32_t k = cols[e];
+    const float q = qhi[k], qm = q * (1.0f / 256.0f), ql = q * (1.0f / 65536.0f);
+    const uint64_t at = uint64_t(k) * V_pad + v;
+    const float xs[2] = {w[e], -corr[e]};
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const float x = xs[t];
+      const float h = rintf(x / q) * q;
+      const float r1 = x - h;
+      const float m = rintf(r1 / qm) * qm;
+      const float r2 = r1 - m;
+      const float l = rintf(r2 / ql) * ql;
+      __nv_bfloat16* base = t == 0 ? dos : mis;
+      base[at] = __float2bfloat16_rn(h);
+      base[plane + at] = __float2bfloat16_rn(m);
+      base[2 * plane + at] = __float2bfloat16_rn(l);
+    }
+    mis[3 * plane + at] = __float2bfloat16_rn(1.0f);
+  }
+}
+
+// out[o*K + k] = init[k] + part_sum[k][slot(fam(o))]; slot(f) is the operand
+// row of person f: tile (f / 128), row 32*(f%4) + (f%128)/4.
+__global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt, uint64_t P_pad,
+                                const double* init, const uint32_t* out_to_fam, uint64_t P,
+                                uint64_t K, double* sums, uint32_t* counts) {
+  const uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (x >= P * K) return;
+  const uint64_t o = x / K, k = x % K;
+  const uint64_t f = out_to_fam ? out_to_fam[o] : o;
+  const uint64_t r = f % kTcN;
+  const uint64_t slot = (f / kTcN) * kTcN + 32 * (r % 4) + r / 4;
+  sums[x] = init[k] + part_sum[k * P_pad + slot];
+  counts[x] = part_cnt[k * P_pad + slot];
+}
+
+// ---- backward: dW[v,k] = sum_p d(p,v) dS[p,k], dC[v,k] = -sum_{p missing} dS[p,k]
+// CTA = 64 variants x all people; one thread per (variant, score-half) row,
+// people streamed through shared memory in chunks (gathered through
+// output_idx_to_fam_idx by reading the dS rows of output people).
+constexpr uint32_t kBwVars = 32;
+constexpr uint32_t kBwPeople = 256;
+
+__global__ void __launch_bounds__(256)
+    gnm_backward_kernel(const uint8_t* rows, uint64_t pitch, uint64_t V, const float* gs,
+                        const uint32_t* out_to_fam, uint64_t P, uint32_t K, float* gw,
+                        float* gc) {
+  __shared__ float g_s[kBwPeople * 16];
+  __shared__ uint32_t fam_s[kBwPeople];
+  const uint32_t t = threadIdx.x;
+  const uint32_t vl = t % kBwVars;          // variant within the CTA tile
+  const uint32_t kg = t / kBwVars;          // score group of 2 (8 groups -> 16 scores)
+  const uint64_t v = uint64_t(blockIdx.x) * kBwVars + vl;
+  const uint32_t k0 = blockIdx.y * 16;
+  float aw[2] = {0.f, 0.f}, ac[2] = {0.f, 0.f};
+  double dw[2] = {0.0, 0.0}, dc[2] = {0.0, 0.0};
+  const uint8_t* row = rows + (v < V ? v : 0) * pitch;
+  for (uint64_t p0 = 0; p0 < P; p0 += kBwPeople) {
+    const uint32_t np = uint32_t(P - p0 < kBwPeople ? P - p0 : kBwPeople);
+    __syncthreads();
+    for (uint32_t i = t; i < kBwPeople * 16; i += blockDim.x) {
+      const uint32_t pp = i / 16, kk = i % 16;
+      g_s[i] = (pp < np && k0 + kk < K) ? gs[(p0 + pp) * K + k0 + kk] : 0.f;
+    }
+    for (uint32_t i = t; i < kBwPeople; i += blockDim.x)
+      fam_s[i] = i < np ? (out_to_fam ? out_to_fam[p0 + i] : uint32_t(p0 + i)) : 0u;
+    __syncthreads();
+    if (v < V) {
+      for (uint32_t pp = 0; pp < np; ++pp) {
+        const uint32_t f = fam_s[pp];
+        const uint32_t code = (__ldg(row + (f >> 2)) >> (2 * (f & 3))) & 3u;
+        if (code == 0u) continue;
+        const float2 g = *reinterpret_cast<const float2*>(&g_s[pp * 16 + 2 * kg]);
+        if (code == 1u) {
+          ac[0] -= g.x;
+          ac[1] -= g.y;
+        } else {
+          const float d = code == 2u ? 1.f : 2.f;
+          aw[0] = fmaf(d, g.x, aw[0]);
+          aw[1] = fmaf(d, g.y, aw[1]);
+        }
+      }
+    }
+    dw[0] += aw[0]; dw[1] += aw[1]; dc[0] += ac[0]; dc[1] += ac[1];
+    aw[0] = aw[1] = ac[0] = ac[1] = 0.f;
+  }
+  if (v < V) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const uint32_t k = k0 + 2 * kg + i;
+      if (k < K) {
+        gw[v * K + k] = float(dw[i]);
+        if (gc) gc[v * K + k] = float(dc[i]);
+      }
+    }
+  }
+}
+
+// ---- host ------------------------------------------------------------------------
+
+template <int NP, int ST, bool MISSING>
+static cudaError_t launch_tc(const CUtensorMap& amap, const CUtensorMap& pmap, const TcArgs& a,
+                             uint32_t ptiles, uint32_t stiles, cudaStream_t s) {
+  using L = TcSmem<NP, ST>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(gnm_tc_accumulate<NP, ST, MISSING>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(L::kTotal));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  gnm_tc_accumulate<NP, ST, MISSING><<<dim3(ptiles, stiles), kTcThreads, L::kTotal, s>>>(amap, pmap, a);
+  return cudaGetLastError();
+}
+
+static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, uint64_t K_pad,
+                                  uint32_t np) {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled is not available from the driver");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  CUtensorMap map;
+  cuuint64_t dims[3] = {V_pad, K_pad, np};
+  cuuint64_t strides[2] = {V_pad * 2, K_pad * V_pad * 2};
+  cuuint32_t box[3] = {kTcK, kTcM, np};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(planes),
+                  dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled failed for limb planes");
+  return map;
+}
+
+void tensor_plan_create(gnm_plan* p) {
+  auto* t = new TensorPlan();
+  p->tensor = t;
+  t->K_pad = (p->K + kTcM - 1) / kTcM * kTcM;
+  t->V_pad = std::max<uint64_t>(kTcK, (p->V + kTcK - 1) / kTcK * kTcK);
+  t->ptiles = uint32_t(std::max<uint64_t>(1, (p->fam + kTcN - 1) / kTcN));
+  t->stiles = uint32_t(t->K_pad / kTcM);
+  t->P_pad = uint64_t(t->ptiles) * kTcN;
+  if (t->V_pad > (uint64_t(1) << 31)) fail(GNM_ERR_INVALID, "too many variants for the tensor engine");
+
+  // per-score quantum q = 2^(E-8), 2^E >= max |x| over the score's values
+  std::vector<float> amax(t->K_pad, 0.f), qhi(t->K_pad, 1.f);
+  for (size_t e = 0; e < p->h_cols.size(); ++e) {
+    const uint32_t k = p->h_cols[e];
+    amax[k] = std::max(amax[k], std::max(std::fabs(p->h_w[e]), std::fabs(p->h_corr[e])));
+  }
+  for (uint64_t k = 0; k < t->K_pad; ++k)
+    if (amax[k] > 0.f) {
+      int ex = 0;
+      std::frexp(amax[k], &ex);  // amax = f * 2^ex, f in [0.5, 1)
+      qhi[k] = std::ldexp(1.0f, ex - 8);
+    }
+  const uint64_t plane = t->K_pad * t->V_pad;
+  auto alloc = [&](void** ptr, uint64_t bytes, const char* what) {
+    check_cuda(cudaMalloc(ptr, std::max<uint64_t>(1, bytes)), what);
+    p->device_bytes += bytes;
+  };
+  alloc(reinterpret_cast<void**>(&t->d_planes_dos), 3 * plane * 2, "cudaMalloc(limb planes)");
+  alloc(reinterpret_cast<void**>(&t->d_planes_mis), 4 * plane * 2, "cudaMalloc(limb planes)");
+  alloc(reinterpret_cast<void**>(&t->d_part_sum), t->K_pad * t->P_pad * 8, "cudaMalloc(partials)");
+  alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->K_pad * t->P_pad * 4, "cudaMalloc(partials)");
+  check_cuda(cudaMemset(t->d_planes_dos, 0, 3 * plane * 2), "memset planes");
+  check_cuda(cudaMemset(t->d_planes_mis, 0, 4 * plane * 2), "memset planes");
+
+  const uint64_t nnz = p->h_cols.size();
+  float *dw = nullptr, *dc = nullptr, *dq = nullptr;
+  uint32_t* dcol = nullptr;
+  uint64_t* doff = nullptr;
+  check_cuda(cudaMalloc(&dw, std::max<uint64_t>(1, nnz) * 4), "cudaMalloc");
+  check_cuda(cudaMalloc(&dc, std::max<uint64_t>(1, nnz) * 4), "cudaMalloc");
+  check_cuda(cudaMalloc(&dcol, std::max<uint64_t>(1, nnz) * 4), "cudaMalloc");
+  check_cuda(cudaMalloc(&doff, (p->V + 1) * 8), "cudaMalloc");
+  check_cuda(cudaMalloc(&dq, t->K_pad * 4), "cudaMalloc");
+  struct Tmp {
+    void* a[5];
+    ~Tmp() {
+      for (void* x : a) cudaFree(x);
+    }
+  } tmp{{dw, dc, dcol, doff, dq}};
+  if (nnz) {
+    check_cuda(cudaMemcpy(dw, p->h_w.data(), nnz * 4, cudaMemcpyHostToDevice), "upload");
+    check_cuda(cudaMemcpy(dc, p->h_corr.data(), nnz * 4, cudaMemcpyHostToDevice), "upload");
+    check_cuda(cudaMemcpy(dcol, p->h_cols.data(), nnz * 4, cudaMemcpyHostToDevice), "upload");
+  }
+  check_cuda(cudaMemcpy(doff, p->h_offs.data(), (p->V + 1) * 8, cudaMemcpyHostToDevice), "upload");
+  check_cuda(cudaMemcpy(dq, qhi.data(), t->K_pad * 4, cudaMemcpyHostToDevice), "upload");
+  if (p->V) {
+    gnm_tc_build_planes<<<uint32_t((p->V + 255) / 256), 256>>>(
+        dw, dc, dcol, doff, p->V, dq, t->d_planes_dos, t->d_planes_mis, t->K_pad, t->V_pad);
+    check_cuda(cudaGetLastError(), "plane build launch");
+  }
+  check_cuda(cudaDeviceSynchronize(), "plane build");
+  t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, 3);
+  t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, 4);
+}
+
+void tensor_plan_destroy(gnm_plan* p) {
+  TensorPlan* t = p->tensor;
+  if (!t) return;
+  cudaFree(t->d_planes_dos);
+  cudaFree(t->d_planes_mis);
+  cudaFree(t->d_part_sum);
+  cudaFree(t->d_part_cnt);
+  delete t;
+  p->tensor = nullptr;
+}
+
+void tensor_reset(gnm_plan* p, cudaStream_t s) {
+  TensorPlan* t = p->tensor;
+  check_cuda(cudaMemsetAsync(t->d_part_sum, 0, t->K_pad * t->P_pad * 8, s), "reset partials");
+  check_cuda(cudaMemsetAsync(t->d_part_cnt, 0, t->K_pad * t->P_pad * 4, s), "reset partials");
+}
+
+void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,
+                       uint64_t nv, cudaStream_t s) {
+  TensorPlan* t = p->tensor;
+  if (v0 % kTcK != 0)
+    fail(GNM_ERR_INVALID, "tensor engine blocks must start at a multiple of 64 variants");
+  const CUtensorMap pmap = make_row_map(d_rows, p->bpv, nv, pitch, kTcN / 4, kTcK);
+  TcArgs a;
+  a.num_rows = nv;
+  a.a_x0 = int32_t(v0);
+  a.part_sum = t->d_part_sum;
+  a.part_cnt = t->d_part_cnt;
+  a.P_pad = t->P_pad;
+  a.err = p->d_err;
+  check_cuda((launch_tc<3, 3, false>(t->map_dos, pmap, a, t->ptiles, t->stiles, s)),
+             "tensor dosage launch");
+  check_cuda((launch_tc<4, 2, true>(t->map_mis, pmap, a, t->ptiles, t->stiles, s)),
+             "tensor missing launch");
+  p->launches += 2;
+}
+
+void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_baseline,
+                     cudaStream_t s) {
+  TensorPlan* t = p->tensor;
+  const uint64_t n = p->P * p->K;
+  if (n == 0) return;
+  gnm_tc_finalize<<<uint32_t((n + 255) / 256), 256, 0, s>>>(
+      t->d_part_sum, t->d_part_cnt, t->P_pad, add_baseline ? p->d_baseline : p->d_zero_base,
+      p->d_out_to_fam, p->P, p->K, d_sums, d_counts);
+  check_cuda(cudaGetLastError(), "tensor finalize launch");
+  p->launches += 1;
+}
+
+void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float* d_grad_s,
+                 float* d_grad_w, float* d_grad_corr, cudaStream_t s) {
+  if (!d_rows || !d_grad_s || !d_grad_w) fail(GNM_ERR_INVALID, "NULL buffer");
+  if (pitch < p->bpv) fail(GNM_ERR_INVALID, "pitch smaller than bytes per variant");
+  if (p->V == 0) return;
+  const dim3 grid(uint32_t((p->V + kBwVars - 1) / kBwVars), uint32_t((p->K + 15) / 16));
+  gnm_backward_kernel<<<grid, 256, 0, s>>>(d_rows, pitch, p->V, d_grad_s, p->d_out_to_fam, p->P,
+                                           uint32_t(p->K), d_grad_w, d_grad_corr);
+  check_cuda(cudaGetLastError(), "backward launch");
+  p->launches += 1;
+}
+
 }  // namespace gnm

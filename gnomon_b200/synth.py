@@ -144,8 +144,9 @@ WORKLOADS = {
 def scaled(w: Workload, people: int, variants: int, scores: int | None = None) -> Workload:
     """Same generator and distributions at a smaller shape (parity-test sizes)."""
     k = w.scores if scores is None else scores
-    lo = min(w.size_lo, variants) if w.size_lo else 0
-    hi = min(w.size_hi, variants) if w.size_hi else 0
+    # uneven score sizes keep their fraction of the variant count
+    lo = max(1, w.size_lo * variants // w.variants) if w.size_lo else 0
+    hi = max(lo, w.size_hi * variants // w.variants) if w.size_hi else 0
     return Workload(w.name + f"_scaled_{people}x{variants}x{k}", people, variants, k, w.p_lo,
                     w.p_hi, w.missing_rate, w.sigma, w.flip_frac, lo, hi, w.config_id)
 

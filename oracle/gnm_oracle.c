@@ -441,9 +441,9 @@ int oracle_score_extended(const uint8_t* rows, uint64_t pitch, uint64_t num_peop
   return 0;
 }
 
-/* Extended-precision gradient for the backward check:
+/* Extended-precision gradient for the backward check (dense over all cells):
  * gw[v*K+k] = sum_p d'(p,v) * gs[p*K+k], d' = dosage with missing -> 0,
- * gc[v*K+k] = -sum_{p missing} gs[p*K+k]; only over member cells (others 0). */
+ * gc[v*K+k] = -sum_{p missing} gs[p*K+k]. */
 int oracle_backward_extended(const uint8_t* rows, uint64_t pitch, uint64_t num_people,
                              const uint32_t* out_to_fam, uint64_t K, uint64_t V,
                              const uint32_t* cols, const uint64_t* offs,
@@ -463,10 +463,9 @@ int oracle_backward_extended(const uint8_t* rows, uint64_t pitch, uint64_t num_p
       else if (g == 2) { for (uint64_t k = 0; k < K; ++k) tw[k] += (long double)gp[k]; }
       else { for (uint64_t k = 0; k < K; ++k) tw[k] += 2.0L * (long double)gp[k]; }
     }
-    for (uint64_t k = 0; k < K; ++k) { gw[v * K + k] = 0.0; if (gc) gc[v * K + k] = 0.0; }
-    for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
-      gw[v * K + cols[e]] = (double)tw[cols[e]];
-      if (gc) gc[v * K + cols[e]] = (double)tc[cols[e]];
+    for (uint64_t k = 0; k < K; ++k) {
+      gw[v * K + k] = (double)tw[k];
+      if (gc) gc[v * K + k] = (double)tc[k];
     }
   }
   free(tw); free(tc);

@@ -25,8 +25,8 @@ def assert_parity(got, want_ref, want_ext=None):
     np.testing.assert_array_equal(c, rc)                       # counts: bit exact
     ok = oracle.within_reference_tolerance(s, rs)              # gpu_tests.rs:135-147
     assert ok.all(), f"{(~ok).sum()} cells outside 1e-6; worst {oracle.rel_err(s, rs).max():.3e}"
-    if want_ext is not None:
-        assert oracle.rel_err(s, want_ext[0]).max() < 1e-9
+    if want_ext is not None:   # FP32 stage sums vs the extended-precision oracle
+        assert oracle.rel_err(s, want_ext[0]).max() < 1e-6
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
@@ -39,9 +39,20 @@ def test_known_answers(cuda, case):
 
 
 def test_reference_gpu_tests_cohort(cuda):
+    """score/tests/gpu_tests.rs:78-170: GPU vs CPU on the deterministic cohort,
+    compared the way the reference compares them: .sscore AVG within 1e-6 abs
+    or rel, MISSING_PCT within 1e-6, counts exact."""
+    from gnomon_b200.sscore import averages
     prep, rows = cohort_prep(16)
-    assert_parity(host_run(prep, rows), oracle.score_reference(rows, prep, threads=4),
-                  oracle.score_extended(rows, prep))
+    s, c = host_run(prep, rows)
+    rs, rc = oracle.score_reference(rows, prep, threads=4)
+    np.testing.assert_array_equal(c, rc)
+    avg, pct = averages(s, c, prep.score_variant_counts)
+    ravg, rpct = averages(rs, rc, prep.score_variant_counts)
+    assert oracle.within_reference_tolerance(avg, ravg).all()
+    assert np.abs(pct - rpct).max() <= 1e-6
+    # raw sums: weights of magnitude ~1 put FP32 stage rounding near 1e-6 of |sum|
+    assert oracle.rel_err(s, oracle.score_extended(rows, prep)[0]).max() < 5e-6
 
 
 def test_plain_config_full_size(cuda):
@@ -90,7 +101,8 @@ def test_streaming_blocks_and_resume(cuda):
     full = host_run(prep, rows)
     streamed = host_run(prep, rows, block_variants=100)
     np.testing.assert_array_equal(streamed[1], full[1])
-    assert oracle.rel_err(streamed[0], full[0]).max() < 1e-12
+    # block boundaries move the FP32 stage grouping: agreement at FP32 level
+    assert oracle.rel_err(streamed[0], full[0]).max() < 1e-6
     seen = []
     host_run(prep, rows, block_variants=300, on_block=lambda n, s, c: seen.append(n))
     assert seen == [300, 600, 900, 1000]
