@@ -8,14 +8,18 @@
 // with d the allele-2 dosage (missing -> 0), m the missing indicator.
 //
 // Precision (the "hi/mid/lo" split): every weight-like value x of score k is
-// written as hi + mid + lo, each an integer multiple of a power-of-two quantum
-// (q, q/256, q/65536 with 2^E = 256 q >= max |x| of the score), |integer| <= 256,
-// so every limb is exact in BF16 and the residual is below 2^-25 of the score's
-// largest weight.  Products with d in {0,1,2} and m in {0,1} are exact, every
-// partial sum of one limb is an integer multiple of its quantum, and below
-// 32768 variants its magnitude stays under 2^24 quanta: the FP32 tensor-memory
-// accumulation of each limb is EXACT.  Accumulators are flushed to FP64 every
-// 16384 variants (the cross-block reduction is the only FP64 arithmetic).
+// written as hi + mid + lo (+ lo2 for dosage weights), each an integer multiple
+// of a power-of-two quantum (q, q/2^8, q/2^16, q/2^24 with 2^E = 256 q >= max |x|
+// of the score), |integer| <= 256, so every limb is exact in BF16.  Products with
+// d in {0,1,2} and m in {0,1} are exact, every partial sum of one limb is an
+// integer multiple of its quantum, and below 32768 variants its magnitude stays
+// under 2^24 quanta: the FP32 tensor-memory accumulation of each limb is EXACT.
+// Accumulators are flushed to FP64 every 16384 variants (the cross-block
+// reduction is the only FP64 arithmetic).  The only error left is the limb
+// residual: below 2^-33 of the score's largest weight for dosage weights (four
+// limbs; with three it was 2^-25, and ~10^5 such residuals per sum reached
+// 1e-6 of the score) and 2^-25 for missing corrections (three limbs; they touch
+// only the ~1% missing calls).
 //
 // Kernel shape (one CTA per SM): M = 128 score rows (TMEM lanes), N = 128
 // people (TMEM columns), K = 64 variants per stage.  Warp 0 issues TMA (weight
@@ -48,7 +52,7 @@ constexpr uint32_t kTcThreads = 192;  // 6 warps
 struct TensorPlan {
   uint64_t K_pad = 0, V_pad = 0, P_pad = 0;
   uint32_t ptiles = 0, stiles = 0;
-  __nv_bfloat16* d_planes_dos = nullptr;  // [3][K_pad][V_pad] W' limbs
+  __nv_bfloat16* d_planes_dos = nullptr;  // [4][K_pad][V_pad] W' limbs
   __nv_bfloat16* d_planes_mis = nullptr;  // [4][K_pad][V_pad] -corr limbs, member
   double* d_part_sum = nullptr;           // [K_pad][P_pad]
   uint32_t* d_part_cnt = nullptr;         // [K_pad][P_pad]
@@ -247,8 +251,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           double acc[32];
 #pragma unroll
           for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+          // limb accumulators: all NP planes for dosage weights, the three
+          // correction limbs in the missing pass (its plane 3 is the count)
+          constexpr uint32_t kSum = MISSING ? 3u : uint32_t(NP);
 #pragma unroll
-          for (uint32_t j = 0; j < 3; ++j) {
+          for (uint32_t j = 0; j < kSum; ++j) {
             uint32_t r[32];
             tmem_ld32(lane_base + j * kTcN + 32 * cb, r);
             tmem_ld_wait();
@@ -289,7 +296,10 @@ __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uin
   const uint64_t plane = K_pad * V_pad;
   for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
     const uint32_t k = cols[e];
-    const float q = qhi[k], qm = q * (1.0f / 256.0f), ql = q * (1.0f / 65536.0f);
+    // quanta q, q/2^8, q/2^16, q/2^24 (powers of two: the divisions are exact and
+    // every residual below is exact in FP32)
+    const float q = qhi[k], qm = q * (1.0f / 256.0f), ql = q * (1.0f / 65536.0f),
+                ql2 = q * (1.0f / 16777216.0f);
     const uint64_t at = uint64_t(k) * V_pad + v;
     const float xs[2] = {w[e], -corr[e]};
 #pragma unroll
@@ -304,6 +314,7 @@ __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uin
       base[at] = __float2bfloat16_rn(h);
       base[plane + at] = __float2bfloat16_rn(m);
       base[2 * plane + at] = __float2bfloat16_rn(l);
+      if (t == 0) base[3 * plane + at] = __float2bfloat16_rn(rintf((r2 - l) / ql2) * ql2);
     }
     mis[3 * plane + at] = __float2bfloat16_rn(1.0f);
   }
@@ -456,11 +467,11 @@ void tensor_plan_create(gnm_plan* p) {
     check_cuda(cudaMalloc(ptr, std::max<uint64_t>(1, bytes)), what);
     p->device_bytes += bytes;
   };
-  alloc(reinterpret_cast<void**>(&t->d_planes_dos), 3 * plane * 2, "cudaMalloc(limb planes)");
+  alloc(reinterpret_cast<void**>(&t->d_planes_dos), 4 * plane * 2, "cudaMalloc(limb planes)");
   alloc(reinterpret_cast<void**>(&t->d_planes_mis), 4 * plane * 2, "cudaMalloc(limb planes)");
   alloc(reinterpret_cast<void**>(&t->d_part_sum), t->K_pad * t->P_pad * 8, "cudaMalloc(partials)");
   alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->K_pad * t->P_pad * 4, "cudaMalloc(partials)");
-  check_cuda(cudaMemset(t->d_planes_dos, 0, 3 * plane * 2), "memset planes");
+  check_cuda(cudaMemset(t->d_planes_dos, 0, 4 * plane * 2), "memset planes");
   check_cuda(cudaMemset(t->d_planes_mis, 0, 4 * plane * 2), "memset planes");
 
   const uint64_t nnz = p->h_cols.size();
@@ -491,7 +502,7 @@ void tensor_plan_create(gnm_plan* p) {
     check_cuda(cudaGetLastError(), "plane build launch");
   }
   check_cuda(cudaDeviceSynchronize(), "plane build");
-  t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, 3);
+  t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, 4);
   t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, 4);
 }
 
@@ -525,7 +536,7 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
   a.part_cnt = t->d_part_cnt;
   a.P_pad = t->P_pad;
   a.err = p->d_err;
-  check_cuda((launch_tc<3, 3, false>(t->map_dos, pmap, a, t->ptiles, t->stiles, s)),
+  check_cuda((launch_tc<4, 2, false>(t->map_dos, pmap, a, t->ptiles, t->stiles, s)),
              "tensor dosage launch");
   check_cuda((launch_tc<4, 2, true>(t->map_mis, pmap, a, t->ptiles, t->stiles, s)),
              "tensor missing launch");

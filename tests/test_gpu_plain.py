@@ -114,7 +114,7 @@ def test_streaming_blocks_and_resume(cuda):
     ctx = PipelineContext(prep, ScoreCheckpoint(400, hs, hc))
     got = run(ctx, rows.reshape(-1), engine=PLAIN)
     np.testing.assert_array_equal(got[1], full[1])
-    assert oracle.rel_err(got[0], full[0]).max() < 1e-9
+    assert oracle.rel_err(got[0], full[0]).max() < 1e-6
 
 
 def test_rows_without_cells(cuda):
