@@ -90,6 +90,9 @@ SIGNATURES = {
     "gnm_backward_dw_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.POINTER(gnm_error)]),
+    "gnm_score_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.POINTER(gnm_error)]),
 }
 
 _LIB = None

@@ -219,6 +219,46 @@ gnm_status gnm_backward_dw_device(gnm_plan* plan, const uint8_t* d_rows, uint64_
                                   const float* d_grad_s, float* d_grad_w,
                                   float* d_grad_corr, void* stream, gnm_error* err);
 
+/* ---- Allocation-free scoring ---------------------------------------------
+ * No counterpart in the reference: an extra entry point of this library.
+ *
+ * Some callers cannot allocate device memory while they score: an application
+ * that has already handed the whole device to its own caching allocator (a
+ * cudaMalloc would fail, or force that allocator to give back cached blocks),
+ * or a host that calls the scorer from a callback in which a device
+ * allocation would implicitly synchronise the device and stall its other
+ * streams.  gnm_score_noalloc scores one score column with the plain kernel
+ * and allocates nothing: its scratch (per-variant weight records, FP64
+ * partial sums and counts, the watchdog word) lives in one statically sized
+ * device array of GNM_NOALLOC_SCRATCH_BYTES that every GPU loading this
+ * library holds until process exit.  The caller passes inputs and outputs:
+ *   d_rows                 packed rows (row v at d_rows + v*pitch, pitch a
+ *                          multiple of 16, 16-byte aligned), every person of
+ *                          the row scored (identity output order);
+ *   d_dosage_weight,       [num_variants] FP32 dosage_weight and
+ *   d_missing_correction   missing_correction of the score's cell;
+ *   d_member               [num_variants] 1 = the variant is in the score,
+ *                          0 = it is not (contributes nothing, its missing
+ *                          calls are not counted); NULL = all members;
+ *   baseline               the score's baseline (sum of corrections);
+ *   d_sums_out, d_missing_out [num_people].
+ * Limits: num_variants <= GNM_NOALLOC_MAX_VARIANTS and num_people <=
+ * GNM_NOALLOC_MAX_PEOPLE; larger inputs are rejected with GNM_ERR_INVALID
+ * before any device work.  The first call on a device looks up the scratch
+ * array's device address (once per device, that device current), so make
+ * that first call before any stream capture.  Every call reuses the same
+ * array and clears what must start at zero; calls that overlap on the GPU
+ * (other streams, other host threads) race on it.  The call returns after
+ * the work on `stream` has finished. */
+#define GNM_NOALLOC_MAX_VARIANTS 262144u
+#define GNM_NOALLOC_MAX_PEOPLE 65536u
+#define GNM_NOALLOC_SCRATCH_BYTES 16778496u
+gnm_status gnm_score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t num_variants,
+                             uint64_t num_people, const float* d_dosage_weight,
+                             const float* d_missing_correction, const uint8_t* d_member,
+                             double baseline, double* d_sums_out, uint32_t* d_missing_out,
+                             void* stream, gnm_error* err);
+
 #ifdef __cplusplus
 }
 #endif
