@@ -121,8 +121,8 @@ class CpuReferenceSample:
     """The restated reference CPU engine on a bounded sample of the workload:
     all people, a prefix of the variants sized so one pass takes ~target_s."""
 
-    def __init__(self, w, target_s: float, threads: int):
-        self.w, self.threads = w, threads
+    def __init__(self, w, target_s: float, threads: int, prep=None):
+        self.w, self.threads, self.full_prep = w, threads, prep
         nv = 512
         while True:  # grow the prefix until one pass is long enough to extrapolate
             self._make(nv)
@@ -141,6 +141,16 @@ class CpuReferenceSample:
         w = self.w
         thr = synth.variant_thresholds(w.seed, 0, nv, w.p_lo, w.p_hi, w.missing_rate)
         self.rows = oracle.synth_rows(w.seed, 0, nv, w.people, thr, w.bytes_per_variant)
+        self.nv = nv
+        if self.full_prep is not None:   # prefix of the workload's own cells
+            fp = self.full_prep
+            e = int(fp.sparse_row_offsets[nv])
+            self.prep = PreparationResult(fp.sparse_weights[:e], fp.sparse_missing_corrections[:e],
+                                          fp.sparse_score_columns[:e],
+                                          fp.sparse_row_offsets[:nv + 1], fp.score_names,
+                                          w.people)
+            self.cells = e
+            return
         rng = np.random.default_rng(w.seed)
         wt = (rng.standard_normal(nv) * w.sigma).astype(np.float32)
         fl = rng.random(nv) < w.flip_frac
@@ -162,7 +172,7 @@ class CpuReferenceSample:
 
     def describe(self, seconds):
         return (f"{self.w.people} people x {self.nv} variants (prefix of {self.w.variants}), "
-                f"K=1, restated reference CPU engine (decide.rs routing, person-major f32 "
+                f"K={self.w.scores}, restated reference CPU engine (decide.rs routing, person-major f32 "
                 f"mini-batches, variant-major f64) on {self.threads} threads, {seconds:.2f} s/pass")
 
 
@@ -194,6 +204,15 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _engine(args, K):
+    from gnomon_b200 import _lib
+    if args.engine == "plain":
+        return _lib.ENGINE_PLAIN
+    if args.engine == "tensor":
+        return _lib.ENGINE_TENSOR
+    return _lib.ENGINE_PLAIN if K < 32 else _lib.ENGINE_TENSOR
+
+
 def gpu_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -204,10 +223,10 @@ def gpu_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    w = synth.WORKLOADS[WORKLOAD]
+    w = synth.WORKLOADS[args.workload]
     if args.variants:
         w = synth.scaled(w, w.people, args.variants)
-    if world > 1:  # person sharding: each rank owns a distinct 50,000-person shard
+    if world > 1:  # person sharding: each rank owns a distinct shard of people
         w = synth.Workload(w.name, w.people, w.variants, w.scores, w.p_lo, w.p_hi,
                            w.missing_rate, w.sigma, w.flip_frac, w.size_lo, w.size_hi,
                            w.config_id + 100 * rank)
@@ -215,6 +234,9 @@ def gpu_arm(args, rank, world, local_rank):
     bpv = w.bytes_per_variant
     pitch = row_pitch(bpv)
     prep = from_workload(w)
+    nnz = int(prep.sparse_row_offsets[-1])
+    engine = _engine(args, K)
+    tensor = engine == _lib.ENGINE_TENSOR
     stream = torch.cuda.Stream(dev)
 
     # synthetic rows generated on the device, in blocks of 100k variants
@@ -226,25 +248,36 @@ def gpu_arm(args, rank, world, local_rank):
             synth_fill(rows[v0:v0 + n], pitch, v0, n, P, thr, w.seed, stream=stream)
     stream.synchronize()
 
-    plan = DevicePlan(prep, engine=_lib.ENGINE_PLAIN, device=local_rank)
+    plan = DevicePlan(prep, engine=engine, device=local_rank)
     sums, counts = plan.outputs()
+    grad_s = None
+    if args.backward:
+        g = torch.Generator(device=dev).manual_seed(w.seed)
+        grad_s = torch.randn(P, K, generator=g, device=dev, dtype=torch.float32)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    k_stop = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    k_ev = [(ev(), ev()) for _ in range(args.steps)]
+    b_ev = [(ev(), ev()) for _ in range(args.steps)]
 
     def step(i=None):
         plan.reset(stream)
         if i is not None:
-            k_start[i].record(stream)
+            k_ev[i][0].record(stream)
         plan.accumulate(rows, pitch, 0, V, stream)
         if i is not None:
-            k_stop[i].record(stream)
+            k_ev[i][1].record(stream)
         plan.finalize(sums, counts, stream)
+        if grad_s is not None:
+            if i is not None:
+                b_ev[i][0].record(stream)
+            plan.backward(rows, pitch, grad_s, grad_corr=True, stream=stream)
+            if i is not None:
+                b_ev[i][1].record(stream)
 
     for _ in range(args.warmup):
         step()
     plan.sync(stream)
-    launches0 = plan.launches
+    l0 = plan.launches
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -255,9 +288,13 @@ def gpu_arm(args, rank, world, local_rank):
         stop.record(stream)
         stop.synchronize()
     plan.sync(stream)
+    launches_last_step = plan.launches   # the library's own count (reset each step)
     ms = start.elapsed_time(stop) / args.steps
-    kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(k_start, k_stop))
-    launches_per_step = 2 * K  # plain accumulate + finalize per score column
+    kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in k_ev)
+    bwd_ms = statistics.mean(a.elapsed_time(b) for a, b in b_ev) if grad_s is not None else None
+    # tensor: dosage pass + missing pass + finalize; plain: accumulate + finalize
+    # per score column; + the backward kernel when requested
+    launches_per_step = launches_last_step
     if world > 1:
         t = torch.tensor([ms, kernel_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -266,15 +303,30 @@ def gpu_arm(args, rank, world, local_rank):
 
     pairs = P * V * K
     value = world * pairs / (ms / 1e3)
+    peak_hbm, peak_kind = peaks()
+    if tensor:
+        # executed tensor-core work: 8 limb MMAs (4 dosage, 3 correction, 1 count)
+        ptiles, kpad, vpad = -(-P // 128), -(-K // 128) * 128, -(-V // 64) * 64
+        flops = 2.0 * ptiles * 128 * vpad * kpad * 8
+        achieved = flops / (kernel_ms / 1e3) / 1e12
+        pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"] \
+            if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
+        roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
+                "frac": achieved / pk, "traffic": None,
+                "peak_kind": peak_kind + " (bf16 sustained)",
+                "kernel": "gnm_tc_accumulate (dosage + missing passes)", "kernel_ms": kernel_ms,
+                "algorithmic_flops_per_launch": flops}
+    else:
+        # algorithmic bytes = packed rows + one weight record per cell
+        alg_bytes = V * bpv + V * K * 4.125
+        achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
+                "frac": achieved / peak_hbm,
+                "traffic": traffic_from_profile() if args.workload == WORKLOAD and not args.variants
+                else None,
+                "peak_kind": peak_kind, "kernel": "gnm_plain_accumulate", "kernel_ms": kernel_ms,
+                "algorithmic_bytes_per_launch": alg_bytes}
 
-    # roofline of the dominant kernel (gnm_plain_accumulate): algorithmic bytes
-    # = packed rows + per-variant weight record read once per launch.
-    alg_bytes = V * bpv + V * K * 4.125
-    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-    peak, peak_kind = peaks()
-    traffic = traffic_from_profile()
-
-    # checksum sanity: the result is consumed (and must be finite)
     s_host = sums.cpu().numpy()
     assert np.isfinite(s_host).all()
 
@@ -286,18 +338,18 @@ def gpu_arm(args, rank, world, local_rank):
         src = BedSource(host.numpy().reshape(-1))
         ctx = PipelineContext(prep)
         for _ in range(min(args.warmup, 1)):
-            try_run_cuda(ctx, src, engine=_lib.ENGINE_PLAIN, device=local_rank)
+            try_run_cuda(ctx, src, engine=engine, device=local_rank)
         times = []
         for _ in range(args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            out = try_run_cuda(ctx, src, engine=_lib.ENGINE_PLAIN, device=local_rank)
+            out = try_run_cuda(ctx, src, engine=engine, device=local_rank)
             times.append(time.perf_counter() - t0)
         e_s, e_c = out
         assert np.array_equal(e_c.astype(np.int64), counts.cpu().numpy().astype(np.int64))
         rel = np.abs(e_s - s_host).max() / max(1.0, np.abs(s_host).max())
         assert rel < 1e-9, rel
-        h2d = V * bpv + K * (V + 64) * 16 + K * 8 * 2 + 4
+        h2d = V * bpv + (K * (V + 64) * 16 if not tensor else nnz * 12 + (V + 1) * 8) + K * 16 + 4
         d2h = P * K * 12 + 4
         e2e = {"value": pairs / statistics.median(times), "unit": "pairs/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -309,7 +361,7 @@ def gpu_arm(args, rank, world, local_rank):
         cpu = None
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
-            smp = CpuReferenceSample(w, args.cpu_s / 3, threads)
+            smp = CpuReferenceSample(w, args.cpu_s / 3, threads, prep=prep)
             t = statistics.median(smp.time_once() for _ in range(3))
             cpu = {"value": smp.pairs / t, "unit": "pairs/s", "cores": threads, "kind": "port",
                    "sample": smp.describe(t) + ", median of 3"}
@@ -317,21 +369,116 @@ def gpu_arm(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "samples": P, "variants": V, "scores": K,
-                       "packed_bytes": V * bpv, "engine": "plain (FP32 CUDA-core LUT, FP64 reduce)",
+            "dtype": "f32" if not tensor else "bf16 limbs, f32 accumulate", "data": "synthetic",
+            "config": {"workload": w.name, "samples": P, "variants": V, "scores": K,
+                       "cells": nnz, "useful_pairs_per_step": P * nnz,
+                       "packed_bytes": V * bpv,
+                       "engine": ("split-BF16 tcgen05 (4+3 limbs), FP64 block reduce" if tensor
+                                  else "plain (FP32 CUDA-core LUT, FP64 reduce)"),
                        "parallelism": f"person-shard x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs (12.5 GB) larger than L2 (126 MB); no flush"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "gnm_plain_accumulate", "kernel_ms": kernel_ms,
-                         "algorithmic_bytes_per_launch": alg_bytes},
+                       "l2": f"inputs ({V * bpv / 1e9:.1f} GB) larger than L2 (126 MB); no flush"},
+            "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks.summary(),
         }
+        if bwd_ms is not None:
+            line["backward"] = {"ms": bwd_ms, "pairs_per_s": P * V * K / (bwd_ms / 1e3),
+                                "kernel": "gnm_backward_kernel"}
         print(json.dumps(line), flush=True)
+    plan.close()
+
+
+def stream_arm(args, rank, world, local_rank):
+    """Biobank-style streaming: rows live in pinned host memory and are copied
+    block by block (double-buffered, copy stream overlapped with the compute
+    stream) into HBM while the previous block is scored.  The full packed matrix
+    does not fit host RAM, so two pre-generated blocks are cycled; every block
+    is scored against the real weights of its variant range."""
+    import torch
+    from gnomon_b200 import _lib, synth
+    from gnomon_b200.device import DevicePlan, row_pitch, synth_fill
+    from gnomon_b200.prepare import from_workload
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = synth.WORKLOADS[args.workload]
+    if args.variants:
+        w = synth.scaled(w, w.people, args.variants)
+    P, V, K = w.people, w.variants, w.scores
+    bpv, B = w.bytes_per_variant, args.stream_block
+    pitch = row_pitch(bpv)
+    prep = from_workload(w)
+    engine = _engine(args, K)
+    plan = DevicePlan(prep, engine=engine, device=local_rank)
+    comp, copy = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    dbuf = [torch.empty((B, pitch), dtype=torch.uint8, device=dev) for _ in range(2)]
+    pool = []
+    for i in range(2):   # two distinct blocks of synthetic rows, kept in pinned memory
+        thr = synth.variant_thresholds(w.seed, i * B, B, w.p_lo, w.p_hi, w.missing_rate)
+        synth_fill(dbuf[i], pitch, i * B, B, P, thr, w.seed, stream=comp)
+        h = torch.empty((B, pitch), dtype=torch.uint8, pin_memory=True)
+        comp.synchronize()
+        h.copy_(dbuf[i])
+        pool.append(h)
+    sums, counts = plan.outputs()
+    nblk = -(-V // B)
+    copied = [torch.cuda.Event() for _ in range(2)]
+    consumed = [torch.cuda.Event() for _ in range(2)]
+
+    def one_pass():
+        plan.reset(comp)
+        for b in range(nblk):
+            s = b % 2
+            n = min(B, V - b * B)
+            copy.wait_event(consumed[s])   # the block that last used buffer s is scored
+            with torch.cuda.stream(copy):
+                dbuf[s][:n].copy_(pool[b % 2][:n], non_blocking=True)
+                copied[s].record(copy)
+            comp.wait_event(copied[s])
+            plan.accumulate(dbuf[s], pitch, b * B, n, comp)
+            consumed[s].record(comp)
+        plan.finalize(sums, counts, comp)
+
+    for _ in range(args.warmup):
+        one_pass()
+    plan.sync(comp)
+    # pinned host -> device copy rate on its own (the link this mode is bound by)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(copy):
+        t0.record(copy)
+        for r in range(3):
+            dbuf[r % 2].copy_(pool[r % 2], non_blocking=True)
+        t1.record(copy)
+    t1.synchronize()
+    h2d_peak = 3 * B * pitch / (t0.elapsed_time(t1) / 1e3) / 1e9
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        start.record(comp)
+        for _ in range(args.steps):
+            one_pass()
+        stop.record(comp)
+        stop.synchronize()
+    plan.sync(comp)
+    ms = start.elapsed_time(stop) / args.steps
+    h2d_bytes = V * pitch
+    line = {"metric": METRIC, "value": P * V * K / (ms / 1e3), "unit": "pairs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if engine == _lib.ENGINE_PLAIN else "bf16 limbs, f32 accumulate",
+            "data": "synthetic (two pinned host blocks cycled through all variant blocks)",
+            "config": {"workload": w.name, "samples": P, "variants": V, "scores": K,
+                       "cells": int(prep.sparse_row_offsets[-1]), "block_variants": B,
+                       "blocks": nblk, "packed_bytes": V * bpv,
+                       "engine": "tensor" if engine == _lib.ENGINE_TENSOR else "plain"},
+            "stream": {"h2d_bytes_per_pass": h2d_bytes,
+                       "h2d_gbs_achieved": h2d_bytes / (ms / 1e3) / 1e9,
+                       "h2d_gbs_copy_alone": h2d_peak},
+            "gpu_launches": plan.launches * args.steps,
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
     plan.close()
 
 
@@ -346,6 +493,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-s", type=float, default=12.0, help="CPU baseline sample seconds")
     ap.add_argument("--ref-step-s", type=float, default=4.0)
+    ap.add_argument("--workload", default=WORKLOAD, help="synthetic workload name")
+    ap.add_argument("--engine", default="auto", choices=["auto", "plain", "tensor"])
+    ap.add_argument("--backward", action="store_true", help="add dW = G^T dS to each step")
+    ap.add_argument("--stream-block", type=int, default=0,
+                    help="stream rows from pinned host memory in blocks of this many variants")
     ap.add_argument("--variants", type=int, default=0,
                     help="override the variant count (small cases for profiler captures)")
     args = ap.parse_args()
@@ -354,6 +506,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.stream_block:
+        stream_arm(args, rank, world, local_rank)
         return
     if world > 1:
         import datetime

@@ -81,6 +81,9 @@ SIGNATURES = {
     "gnm_score_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.POINTER(gnm_error)]),
     "gnm_plan_launch_count": (C.c_uint64, [C.c_void_p]),
+    "gnm_plan_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p,
+                                    C.POINTER(gnm_error)]),
+    "gnm_plan_tuned_shape": (C.c_uint32, [C.c_void_p]),
     "gnm_decode_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_uint64, C.c_void_p, C.POINTER(gnm_error)]),
     "gnm_synth_fill_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,

@@ -165,10 +165,14 @@ static void plain_geometry(gnm_plan* p) {
   const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
   uint64_t splits = std::max<uint64_t>(1, slots / p->tiles);
   splits = std::min<uint64_t>(splits, stages);
-  // keep partials of all scores within ~1 GiB
+  // keep partials of all scores within ~1 GiB; allocate up to 4x the default
+  // split count so that gnm_plan_autotune can try finer splits
   const uint64_t per_split_bytes = p->K * p->part_stride * 12;
   while (splits > 1 && splits * per_split_bytes > (uint64_t(1) << 30)) splits = (splits + 1) / 2;
+  uint64_t alloc = std::min<uint64_t>(4 * splits, stages);
+  while (alloc > splits && alloc * per_split_bytes > (uint64_t(1) << 30)) --alloc;
   p->splits = uint32_t(splits);
+  p->splits_alloc = uint32_t(alloc);
 }
 
 static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep) {
@@ -188,7 +192,7 @@ static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep) {
   check_cuda(cudaMemcpy(p->d_records, rec.data(), rec.size() * sizeof(float4),
                         cudaMemcpyHostToDevice),
              "upload records");
-  const uint64_t part = p->K * uint64_t(p->splits) * p->part_stride;
+  const uint64_t part = p->K * uint64_t(p->splits_alloc) * p->part_stride;
   p->d_part_sum = dalloc<double>(p, part, "cudaMalloc(partial sums)");
   p->d_part_cnt = dalloc<uint32_t>(p, part, "cudaMalloc(partial counts)");
 }
@@ -256,7 +260,7 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
 static void plan_reset_impl(gnm_plan* p, cudaStream_t s) {
   DeviceGuard g(p->device);
   if (p->engine == GNM_ENGINE_PLAIN) {
-    const uint64_t part = p->K * uint64_t(p->splits) * p->part_stride;
+    const uint64_t part = p->K * uint64_t(p->splits_alloc) * p->part_stride;
     check_cuda(cudaMemsetAsync(p->d_part_sum, 0, part * sizeof(double), s), "reset partials");
     check_cuda(cudaMemsetAsync(p->d_part_cnt, 0, part * sizeof(uint32_t), s), "reset partials");
   } else {
@@ -284,9 +288,10 @@ static void accumulate_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, 
     a.records = p->d_records + k * p->rec_stride;
     a.record_row0 = v0;
     a.num_rows = nv;
+    a.bytes_per_row = p->bpv;
     a.stages_per_split = sps;
-    a.part_sum = p->d_part_sum + k * uint64_t(p->splits) * p->part_stride;
-    a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits) * p->part_stride;
+    a.part_sum = p->d_part_sum + k * uint64_t(p->splits_alloc) * p->part_stride;
+    a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_stride = p->part_stride;
     a.err = p->d_err;
     check_cuda(launch_plain_accumulate(map, a, p->tiles, splits, s), "plain accumulate launch");
@@ -303,8 +308,8 @@ static void finalize_impl(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool 
   }
   for (uint64_t k = 0; k < p->K; ++k) {
     FinalizeArgs a;
-    a.part_sum = p->d_part_sum + k * uint64_t(p->splits) * p->part_stride;
-    a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits) * p->part_stride;
+    a.part_sum = p->d_part_sum + k * uint64_t(p->splits_alloc) * p->part_stride;
+    a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_stride = p->part_stride;
     a.num_splits = p->splits;
     a.baseline = add_baseline ? p->d_baseline : p->d_zero_base;
@@ -327,6 +332,63 @@ static void sync_impl(gnm_plan* p, cudaStream_t s) {
   if (e & kErrTmaTimeout) fail(GNM_ERR_TIMEOUT, "device watchdog: a TMA wait expired");
   if (e & kErrMmaTimeout) fail(GNM_ERR_TIMEOUT, "device watchdog: a tensor-core wait expired");
   if (e) fail(GNM_ERR_COMPUTE, "device reported an error");
+}
+
+// ---- autotuner -----------------------------------------------------------------
+// Times candidate launch shapes of the plan's accumulate on the caller's
+// resident rows and keeps the fastest: the plain engine's variant-split count
+// (1x, 2x, 4x the occupancy-derived default: more, shorter splits balance the
+// last wave at the cost of more FP64 partials), or the tensor engine's CTA
+// order (people tiles fastest: CTAs in flight share weight-limb tiles in L2;
+// score tiles fastest: they share genotype tiles).
+static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t nv,
+                          cudaStream_t s) {
+  DeviceGuard g(p->device);
+  if (nv == 0 || nv > p->V) fail(GNM_ERR_INVALID, "autotune: variant_count out of range");
+  cudaEvent_t e0, e1;
+  check_cuda(cudaEventCreate(&e0), "event");
+  check_cuda(cudaEventCreate(&e1), "event");
+  struct Ev {
+    cudaEvent_t a, b;
+    ~Ev() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } ev{e0, e1};
+  auto time_once = [&]() {
+    plan_reset_impl(p, s);
+    check_cuda(cudaEventRecord(e0, s), "event");
+    accumulate_impl(p, d_rows, pitch, 0, nv, s);
+    check_cuda(cudaEventRecord(e1, s), "event");
+    sync_impl(p, s);
+    float ms = 0.f;
+    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event time");
+    return ms;
+  };
+  const bool plain = p->engine == GNM_ENGINE_PLAIN;
+  std::vector<uint32_t> cand;
+  if (plain) {
+    for (uint32_t m : {1u, 2u, 4u})
+      if (p->splits * m <= p->splits_alloc && (cand.empty() || p->splits * m != cand.back()))
+        cand.push_back(p->splits * m);
+  } else {
+    cand = {0u, 1u};
+  }
+  const uint32_t base = plain ? p->splits : p->raster;
+  uint32_t best = base;
+  float best_ms = 1e30f;
+  for (uint32_t c : cand) {
+    (plain ? p->splits : p->raster) = c;
+    time_once();  // warm-up
+    const float ms = std::min(time_once(), time_once());
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  (plain ? p->splits : p->raster) = best;
+  plan_reset_impl(p, s);
+  sync_impl(p, s);
 }
 
 // ---- host streaming run ------------------------------------------------------
@@ -597,6 +659,7 @@ void gnm_plan_destroy(gnm_plan* p) {
   cudaFree(p->d_zero_base);
   cudaFree(p->d_out_to_fam);
   cudaFree(p->d_err);
+  cudaFree(p->d_grad_fam);
   if (prev >= 0) cudaSetDevice(prev);
   delete p;
 }
@@ -643,6 +706,19 @@ gnm_status gnm_score_device(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, 
     accumulate_impl(p, d_rows, pitch, 0, p->V, s);
     finalize_impl(p, d_sums, d_counts, true, s);
   });
+}
+
+gnm_status gnm_plan_autotune(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch,
+                             uint64_t variant_count, void* stream, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] {
+    autotune_impl(p, d_rows, pitch, variant_count, static_cast<cudaStream_t>(stream));
+  });
+}
+
+uint32_t gnm_plan_tuned_shape(const gnm_plan* p) {
+  if (!p) return 0;
+  return p->engine == GNM_ENGINE_PLAIN ? p->splits : p->raster;
 }
 
 gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv, uint64_t np,

@@ -26,6 +26,7 @@ struct PlainArgs {
   const float4* records;   // [V + pad] {-corr, w', 2w', member mask bits} of one score
   uint64_t record_row0;    // absolute variant index of block row 0
   uint64_t num_rows;       // rows in this block
+  uint64_t bytes_per_row;  // meaningful bytes of a row (ceil(people / 4))
   uint32_t stages_per_split;
   double* part_sum;        // [splits][part_stride] partials of this score
   uint32_t* part_cnt;

@@ -119,6 +119,7 @@ static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uin
   a.records = recs;
   a.record_row0 = 0;
   a.num_rows = V;
+  a.bytes_per_row = bpv;
   a.stages_per_split = sps;
   a.part_sum = part_sum;
   a.part_cnt = part_cnt;

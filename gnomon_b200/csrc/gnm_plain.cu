@@ -42,6 +42,19 @@ struct PlainSmem {
   static constexpr uint32_t kTotal = kBarOff + 64;
 };
 
+// Two FP32 additions in one instruction (sm_100 packed f32x2): acc += {lo, hi}.
+__device__ __forceinline__ uint64_t add_f32x2(uint64_t acc, float lo, float hi) {
+  uint64_t r;
+  asm("{\n\t.reg .b64 t;\n\tmov.b64 t, {%2, %3};\n\tadd.rn.f32x2 %0, %1, t;\n\t}"
+      : "=l"(r)
+      : "l"(acc), "f"(lo), "f"(hi));
+  return r;
+}
+
+__device__ __forceinline__ void unpack_f32x2(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
 __device__ __forceinline__ void plain_issue_stage(const CUtensorMap* map, const float4* recs,
                                                   uint32_t smem_base, uint32_t buf,
                                                   int32_t tile_x, int32_t row0,
@@ -86,20 +99,27 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
                         a.record_row0 + r_begin + s * kPlainRows);
   }
 
-  float acc[16];
+  // FP32 sums as packed pairs for add.rn.f32x2: accp[2q] holds people
+  // (q, 4+q), accp[2q+1] people (8+q, 12+q) of this thread's 16.
+  uint64_t accp[8];
   double acc64[16];
   uint32_t cnt[16];
+  uint32_t by[4] = {0u, 0u, 0u, 0u};   // byte counters: byte j = person 4j+q
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
-    acc[i] = 0.f;
     acc64[i] = 0.0;
     cnt[i] = 0u;
   }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) accp[i] = 0ull;
 
   // Each thread reads word column `tid` of the 1024-byte stage row; the stage
   // is stored as 4 TMA boxes of [48 rows][256 bytes].
   const uint32_t word_off = (tid / (kPlainBoxBytes / 4)) * PlainSmem::kBoxBytes +
                             (tid % (kPlainBoxBytes / 4)) * 4;
+  // warps whose 128 bytes all lie past the row's last byte only hold padding
+  const bool warp_active =
+      uint64_t(tile) * kPlainTileBytes + uint64_t(tid & ~31u) * 4 < a.bytes_per_row;
 
   for (uint32_t st = 0; st < nstages; ++st) {
     const uint32_t buf = st & 1u;
@@ -155,7 +175,6 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
     const uint64_t members = uint64_t(mbits[2 * buf]) | (uint64_t(mbits[2 * buf + 1]) << 32);
 
     uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
-    uint32_t by[4] = {0u, 0u, 0u, 0u};   // byte counters: byte j = person 4j+q
     auto group = [&](uint32_t g, uint32_t ma, uint32_t mb, uint32_t mc) {
       const uint32_t xa = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 0) * kPlainBoxBytes);
       const uint32_t xb = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 1) * kPlainBoxBytes);
@@ -173,11 +192,12 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
       const uint8_t* lg = lbase + g * 256;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        float v[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const uint32_t off = __byte_perm(ix[q], 0u, 0x4440u + j);
-          acc[4 * j + q] += *reinterpret_cast<const float*>(lg + off);
-        }
+        for (int j = 0; j < 4; ++j)
+          v[j] = *reinterpret_cast<const float*>(lg + __byte_perm(ix[q], 0u, 0x4440u + j));
+        accp[2 * q] = add_f32x2(accp[2 * q], v[0], v[1]);
+        accp[2 * q + 1] = add_f32x2(accp[2 * q + 1], v[2], v[3]);
       }
       // ---- missing counts (code 01 of member rows) ---------------------
       const uint32_t c3 = (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
@@ -192,7 +212,9 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
         od = 0u;
       }
     };
-    if (members == (uint64_t(1) << kPlainRows) - 1) {
+    if (!warp_active) {
+      // padding-only warp: nothing to score
+    } else if (members == (uint64_t(1) << kPlainRows) - 1) {
       // every row of the stage is a member of this score (the common case)
 #pragma unroll
       for (uint32_t g = 0; g < kPlainRows / 3; ++g) group(g, 0x55555555u, 0x55555555u, 0x55555555u);
@@ -205,14 +227,24 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
         group(g, ma, mb, mc);
       }
     }
+    // FP32 sums and byte counters span two stages (96 variants, <= 96 calls
+    // per byte counter) before they are flushed to FP64 / 32-bit counts.
+    if ((st & 1u) || st + 1 == nstages) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < 4; ++q) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) cnt[4 * j + q] += (by[q] >> (8 * j)) & 0xFFu;
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      acc64[i] += double(acc[i]);
-      acc[i] = 0.f;
+        for (int j = 0; j < 4; ++j) cnt[4 * j + q] += (by[q] >> (8 * j)) & 0xFFu;
+        by[q] = 0u;
+        float lo, hi;
+        unpack_f32x2(accp[2 * q], lo, hi);
+        acc64[q] += double(lo);
+        acc64[4 + q] += double(hi);
+        unpack_f32x2(accp[2 * q + 1], lo, hi);
+        acc64[8 + q] += double(lo);
+        acc64[12 + q] += double(hi);
+        accp[2 * q] = 0ull;
+        accp[2 * q + 1] = 0ull;
+      }
     }
 
     __syncthreads();  // every thread is done with stage buffer `buf`

@@ -40,7 +40,9 @@ struct gnm_plan {
 
   // plain engine
   uint32_t tiles = 0;          // people tiles of kPlainTileBytes
-  uint32_t splits = 0;         // variant splits (partial slots)
+  uint32_t splits = 0;         // variant splits in use (partial slots)
+  uint32_t splits_alloc = 0;   // partial slots allocated per score (autotune range)
+  uint32_t raster = 0;         // tensor engine CTA order: 0 people-tile fastest, 1 score-tile
   uint64_t part_stride = 0;    // people per partial slot (tiles * 4096)
   uint64_t rec_stride = 0;     // records per score (V + pad)
   float4* d_records = nullptr; // [K][rec_stride]
@@ -52,6 +54,7 @@ struct gnm_plan {
   double* d_zero_base = nullptr;   // [K] zeros (resume runs)
   uint32_t* d_out_to_fam = nullptr;
   uint32_t* d_err = nullptr;
+  float* d_grad_fam = nullptr;     // backward: dS in .bed person order (keep subsets)
   std::vector<double> h_baseline;
   uint64_t device_bytes = 0;
   uint64_t launches = 0;

@@ -66,6 +66,7 @@ struct TcArgs {
   uint32_t* part_cnt;
   uint64_t P_pad;
   uint32_t* err;
+  uint32_t raster;         // 0: blockIdx.x = people tile, 1: blockIdx.x = score tile
 };
 
 template <int NP, int ST>
@@ -102,7 +103,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t sb = smem_u32(smem);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t ptile = blockIdx.x, stile = blockIdx.y;
+  const uint32_t ptile = a.raster ? blockIdx.y : blockIdx.x;
+  const uint32_t stile = a.raster ? blockIdx.x : blockIdx.y;
   const uint32_t nit = uint32_t((a.num_rows + kTcK - 1) / kTcK);
   auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
   auto bready = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
@@ -336,62 +338,111 @@ __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt
 }
 
 // ---- backward: dW[v,k] = sum_p d(p,v) dS[p,k], dC[v,k] = -sum_{p missing} dS[p,k]
-// CTA = 64 variants x all people; one thread per (variant, score-half) row,
-// people streamed through shared memory in chunks (gathered through
-// output_idx_to_fam_idx by reading the dS rows of output people).
-constexpr uint32_t kBwVars = 32;
-constexpr uint32_t kBwPeople = 256;
+// One thread per variant row, 16 score columns per CTA column block.  dS comes
+// in .bed (fam) person order, [fam][K] (scattered from output order when a keep
+// subset is used); 512-person chunks of the block's 16 columns are staged in
+// shared memory and read as broadcasts, genotypes come straight from the
+// packed row as 16-byte vectors (64 people), and the 16 products per person
+// are two-wide FMAs (fma.rn.f32x2).  FP32 sums per chunk, FP64 across chunks.
+constexpr uint32_t kBwThreads = 128;
+constexpr uint32_t kBwChunk = 512;
 
-__global__ void __launch_bounds__(256)
-    gnm_backward_kernel(const uint8_t* rows, uint64_t pitch, uint64_t V, const float* gs,
-                        const uint32_t* out_to_fam, uint64_t P, uint32_t K, float* gw,
-                        float* gc) {
-  __shared__ float g_s[kBwPeople * 16];
-  __shared__ uint32_t fam_s[kBwPeople];
+__device__ __forceinline__ uint64_t fma_f32x2(float d, uint64_t g, uint64_t acc) {
+  uint64_t r;
+  asm("{\n\t.reg .b64 dd;\n\tmov.b64 dd, {%1, %1};\n\tfma.rn.f32x2 %0, dd, %2, %3;\n\t}"
+      : "=l"(r)
+      : "f"(d), "l"(g), "l"(acc));
+  return r;
+}
+__device__ __forceinline__ uint64_t sub_f32x2(uint64_t acc, uint64_t g) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(acc), "l"(g));
+  return r;
+}
+
+// dS in output order -> fam order (zero for people outside the keep set).
+__global__ void gnm_scatter_grad(const float* gs, const uint32_t* out_to_fam, uint64_t P,
+                                 uint64_t K, float* gsf) {
+  const uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (x >= P * K) return;
+  const uint64_t o = x / K, k = x % K;
+  gsf[uint64_t(out_to_fam[o]) * K + k] = gs[x];
+}
+
+__global__ void __launch_bounds__(kBwThreads)
+    gnm_backward_kernel(const uint8_t* rows, uint64_t pitch, uint64_t bpv, uint64_t V,
+                        const float* gsf, uint64_t fam, uint32_t K, float* gw, float* gc) {
+  __shared__ __align__(16) float g_s[kBwChunk * 16];
   const uint32_t t = threadIdx.x;
-  const uint32_t vl = t % kBwVars;          // variant within the CTA tile
-  const uint32_t kg = t / kBwVars;          // score group of 2 (8 groups -> 16 scores)
-  const uint64_t v = uint64_t(blockIdx.x) * kBwVars + vl;
+  const uint64_t v = uint64_t(blockIdx.x) * kBwThreads + t;
   const uint32_t k0 = blockIdx.y * 16;
-  float aw[2] = {0.f, 0.f}, ac[2] = {0.f, 0.f};
-  double dw[2] = {0.0, 0.0}, dc[2] = {0.0, 0.0};
   const uint8_t* row = rows + (v < V ? v : 0) * pitch;
-  for (uint64_t p0 = 0; p0 < P; p0 += kBwPeople) {
-    const uint32_t np = uint32_t(P - p0 < kBwPeople ? P - p0 : kBwPeople);
+  uint64_t aw[8], ac[8];
+  double dw[16];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) aw[j] = ac[j] = 0ull;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) dw[j] = 0.0;
+  for (uint64_t p0 = 0; p0 < fam; p0 += kBwChunk) {
+    const uint32_t np = uint32_t(fam - p0 < kBwChunk ? fam - p0 : kBwChunk);
     __syncthreads();
-    for (uint32_t i = t; i < kBwPeople * 16; i += blockDim.x) {
+    for (uint32_t i = t; i < kBwChunk * 16; i += kBwThreads) {
       const uint32_t pp = i / 16, kk = i % 16;
-      g_s[i] = (pp < np && k0 + kk < K) ? gs[(p0 + pp) * K + k0 + kk] : 0.f;
+      g_s[i] = (pp < np && k0 + kk < K) ? __ldg(gsf + (p0 + pp) * K + k0 + kk) : 0.f;
     }
-    for (uint32_t i = t; i < kBwPeople; i += blockDim.x)
-      fam_s[i] = i < np ? (out_to_fam ? out_to_fam[p0 + i] : uint32_t(p0 + i)) : 0u;
     __syncthreads();
     if (v < V) {
-      for (uint32_t pp = 0; pp < np; ++pp) {
-        const uint32_t f = fam_s[pp];
-        const uint32_t code = (__ldg(row + (f >> 2)) >> (2 * (f & 3))) & 3u;
-        if (code == 0u) continue;
-        const float2 g = *reinterpret_cast<const float2*>(&g_s[pp * 16 + 2 * kg]);
-        if (code == 1u) {
-          ac[0] -= g.x;
-          ac[1] -= g.y;
-        } else {
-          const float d = code == 2u ? 1.f : 2.f;
-          aw[0] = fmaf(d, g.x, aw[0]);
-          aw[1] = fmaf(d, g.y, aw[1]);
+      for (uint32_t seg = 0; seg < kBwChunk / 64; ++seg) {
+        const uint64_t b0 = p0 / 4 + seg * 16;  // 16 bytes = 64 people
+        if (b0 >= bpv) break;
+        const uint4 x4 = *reinterpret_cast<const uint4*>(row + b0);
+        const uint32_t xw[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+        for (int wi = 0; wi < 4; ++wi) {
+          const uint32_t x = xw[wi];
+          if (x == 0u) continue;   // 16 homozygous-reference calls
+#pragma unroll 4
+          for (int i = 0; i < 16; ++i) {
+            const uint32_t c = (x >> (2 * i)) & 3u;
+            const uint64_t* gp =
+                reinterpret_cast<const uint64_t*>(&g_s[(seg * 64 + wi * 16 + i) * 16]);
+            uint64_t g[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) g[j] = gp[j];
+            // dosage 0 for codes 00 and 01 (missing): one FMA path for everyone
+            const float d = c == 3u ? 2.f : (c == 2u ? 1.f : 0.f);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) aw[j] = fma_f32x2(d, g[j], aw[j]);
+            if (c == 1u) {
+#pragma unroll
+              for (int j = 0; j < 8; ++j) ac[j] = sub_f32x2(ac[j], g[j]);
+            }
+          }
         }
       }
     }
-    dw[0] += aw[0]; dw[1] += aw[1]; dc[0] += ac[0]; dc[1] += ac[1];
-    aw[0] = aw[1] = ac[0] = ac[1] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float lo, hi;
+      asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(aw[j]));
+      dw[2 * j] += double(lo);
+      dw[2 * j + 1] += double(hi);
+      aw[j] = 0ull;
+    }
   }
   if (v < V) {
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const uint32_t k = k0 + 2 * kg + i;
+    for (int j = 0; j < 8; ++j) {
+      float lo, hi;
+      asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(ac[j]));
+      const uint32_t k = k0 + 2 * j;
       if (k < K) {
-        gw[v * K + k] = float(dw[i]);
-        if (gc) gc[v * K + k] = float(dc[i]);
+        gw[v * K + k] = float(dw[2 * j]);
+        if (gc) gc[v * K + k] = lo;
+      }
+      if (k + 1 < K) {
+        gw[v * K + k + 1] = float(dw[2 * j + 1]);
+        if (gc) gc[v * K + k + 1] = hi;
       }
     }
   }
@@ -411,7 +462,8 @@ static cudaError_t launch_tc(const CUtensorMap& amap, const CUtensorMap& pmap, c
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  gnm_tc_accumulate<NP, ST, MISSING><<<dim3(ptiles, stiles), kTcThreads, L::kTotal, s>>>(amap, pmap, a);
+  const dim3 grid = a.raster ? dim3(stiles, ptiles) : dim3(ptiles, stiles);
+  gnm_tc_accumulate<NP, ST, MISSING><<<grid, kTcThreads, L::kTotal, s>>>(amap, pmap, a);
   return cudaGetLastError();
 }
 
@@ -536,6 +588,8 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
   a.part_cnt = t->d_part_cnt;
   a.P_pad = t->P_pad;
   a.err = p->d_err;
+  a.raster = p->raster;
+  if (a.raster && t->ptiles > 65535u) a.raster = 0;  // grid.y limit
   check_cuda((launch_tc<4, 2, false>(t->map_dos, pmap, a, t->ptiles, t->stiles, s)),
              "tensor dosage launch");
   check_cuda((launch_tc<4, 2, true>(t->map_mis, pmap, a, t->ptiles, t->stiles, s)),
@@ -559,10 +613,30 @@ void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float
                  float* d_grad_w, float* d_grad_corr, cudaStream_t s) {
   if (!d_rows || !d_grad_s || !d_grad_w) fail(GNM_ERR_INVALID, "NULL buffer");
   if (pitch < p->bpv) fail(GNM_ERR_INVALID, "pitch smaller than bytes per variant");
+  if (pitch % 16 != 0 || reinterpret_cast<uintptr_t>(d_rows) % 16 != 0)
+    fail(GNM_ERR_INVALID, "packed rows must be 16-byte aligned with a pitch multiple of 16");
   if (p->V == 0) return;
-  const dim3 grid(uint32_t((p->V + kBwVars - 1) / kBwVars), uint32_t((p->K + 15) / 16));
-  gnm_backward_kernel<<<grid, 256, 0, s>>>(d_rows, pitch, p->V, d_grad_s, p->d_out_to_fam, p->P,
-                                           uint32_t(p->K), d_grad_w, d_grad_corr);
+  const float* gsf = d_grad_s;
+  if (p->d_out_to_fam || p->P != p->fam) {
+    // dS rows in .bed person order: zero for people outside the keep set
+    if (!p->d_grad_fam) {
+      check_cuda(cudaMalloc(&p->d_grad_fam, std::max<uint64_t>(1, p->fam * p->K) * 4),
+                 "cudaMalloc(fam-order gradient)");
+      p->device_bytes += p->fam * p->K * 4;
+    }
+    check_cuda(cudaMemsetAsync(p->d_grad_fam, 0, p->fam * p->K * 4, s), "memset");
+    const uint64_t n = p->P * p->K;
+    if (n) {
+      gnm_scatter_grad<<<uint32_t((n + 255) / 256), 256, 0, s>>>(
+          d_grad_s, p->d_out_to_fam, p->P, p->K, p->d_grad_fam);
+      check_cuda(cudaGetLastError(), "gradient scatter launch");
+      p->launches += 1;
+    }
+    gsf = p->d_grad_fam;
+  }
+  const dim3 grid(uint32_t((p->V + kBwThreads - 1) / kBwThreads), uint32_t((p->K + 15) / 16));
+  gnm_backward_kernel<<<grid, kBwThreads, 0, s>>>(d_rows, pitch, p->bpv, p->V, gsf, p->fam,
+                                                  uint32_t(p->K), d_grad_w, d_grad_corr);
   check_cuda(cudaGetLastError(), "backward launch");
   p->launches += 1;
 }

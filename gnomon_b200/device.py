@@ -106,6 +106,31 @@ class DevicePlan:
                                              _stream_ptr(stream), C.byref(e)), e)
         return sums, counts
 
+    def autotune(self, rows: torch.Tensor, pitch: int, variant_count: Optional[int] = None,
+                 stream=None) -> int:
+        """Time candidate launch shapes on resident rows, keep the fastest; returns it."""
+        n = self.prep.num_reconciled_variants if variant_count is None else variant_count
+        e = self._err()
+        _lib.check(self.lib.gnm_plan_autotune(self.handle, rows.data_ptr(), pitch, n,
+                                              _stream_ptr(stream), C.byref(e)), e)
+        return int(self.lib.gnm_plan_tuned_shape(self.handle))
+
+    def capture(self, rows: torch.Tensor, pitch: int, sums=None, counts=None):
+        """Record one full scoring pass (reset + accumulate + finalize) into a CUDA
+        graph; ``graph.replay()`` reruns it with no per-launch host work.  Returns
+        (graph, sums, counts) — the output tensors the graph writes."""
+        if sums is None:
+            sums, counts = self.outputs()
+        side = torch.cuda.Stream(rows.device)
+        with torch.cuda.stream(side):     # warm-up outside capture (sets kernel attributes)
+            self.score(rows, pitch, sums, counts, stream=side)
+        side.synchronize()
+        self.sync(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=side):
+            self.score(rows, pitch, sums, counts, stream=torch.cuda.current_stream())
+        return graph, sums, counts
+
     def backward(self, rows: torch.Tensor, pitch: int, grad_s: torch.Tensor,
                  grad_corr: bool = False, stream=None):
         """dW = G^T dS by re-unpacking the packed rows; returns dense [V, K] float32."""

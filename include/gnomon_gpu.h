@@ -183,6 +183,18 @@ gnm_status gnm_score_device(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitc
 /* Number of kernel launches the last accumulate+finalize issued (for audit). */
 uint64_t gnm_plan_launch_count(const gnm_plan* plan);
 
+/* Autotuner (no reference counterpart; the reference sizes its tiles from free
+ * memory only, score/cuda_backend.rs:803-975): times the plan's accumulate on
+ * the first `variant_count` resident rows for each candidate launch shape —
+ * plain engine: variant-split count (1x/2x/4x of the default); tensor engine:
+ * CTA raster order — keeps the fastest, and leaves the plan reset.  Blocks
+ * until done. */
+gnm_status gnm_plan_autotune(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
+                             uint64_t variant_count, void* stream, gnm_error* err);
+
+/* The tuned shape: split count (plain) or raster order (tensor). */
+uint32_t gnm_plan_tuned_shape(const gnm_plan* plan);
+
 /* ---- Packed-row utilities ------------------------------------------------ */
 
 /* Decode packed rows to int8 dosage codes on the device: out[v*out_pitch + i]

@@ -181,3 +181,35 @@ def test_gpu_generator_matches_numpy(cuda, people):
     synth_fill(d, pitch, v0, n, people, thr, w.seed)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(d.cpu().numpy(), synth.synth_rows(w.seed, v0, n, people, thr, pitch))
+
+
+@pytest.mark.parametrize("engine", [PLAIN, _lib.ENGINE_TENSOR])
+def test_cuda_graph_replay_and_autotune(cuda, engine):
+    """A captured scoring pass replays to the same result; autotuning picks a
+    candidate shape and leaves results unchanged (up to FP32 regrouping)."""
+    import torch
+    from gnomon_b200.device import DevicePlan, row_pitch
+    _, prep, rows, _ = synth_case(6000, 1500, scores=3, config="diff_20k_x_200k_k16")
+    pitch = row_pitch(prep.bytes_per_variant)
+    dev = np.zeros((1500, pitch), np.uint8)
+    dev[:, :rows.shape[1]] = rows
+    d_rows = torch.from_numpy(dev).cuda()
+    plan = DevicePlan(prep, engine=engine)
+    s0, c0 = plan.score(d_rows, pitch)
+    plan.sync()
+    s0, c0 = s0.cpu().numpy(), c0.cpu().numpy()
+    graph, gs, gc = plan.capture(d_rows, pitch)
+    for _ in range(3):
+        gs.fill_(float("nan"))
+        graph.replay()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(gs.cpu().numpy(), s0)
+        np.testing.assert_array_equal(gc.cpu().numpy(), c0)
+    del graph
+    shape = plan.autotune(d_rows, pitch)
+    assert shape >= 0
+    s1, c1 = plan.score(d_rows, pitch)
+    plan.sync()
+    np.testing.assert_array_equal(c1.cpu().numpy(), c0)
+    assert oracle.rel_err(s1.cpu().numpy(), s0).max() < 1e-6
+    plan.close()
