@@ -165,12 +165,14 @@ static void plain_geometry(gnm_plan* p) {
   const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
   uint64_t splits = std::max<uint64_t>(1, slots / p->tiles);
   splits = std::min<uint64_t>(splits, stages);
-  // keep partials of all scores within ~1 GiB; allocate up to 4x the default
-  // split count so that gnm_plan_autotune can try finer splits
+  // keep partials of all scores within 8 GiB (many score columns still get a
+  // full-occupancy grid); allocate up to 4x the default split count so that
+  // gnm_plan_autotune can try finer splits
   const uint64_t per_split_bytes = p->K * p->part_stride * 12;
-  while (splits > 1 && splits * per_split_bytes > (uint64_t(1) << 30)) splits = (splits + 1) / 2;
+  const uint64_t cap = uint64_t(8) << 30;
+  while (splits > 1 && splits * per_split_bytes > cap) splits = (splits + 1) / 2;
   uint64_t alloc = std::min<uint64_t>(4 * splits, stages);
-  while (alloc > splits && alloc * per_split_bytes > (uint64_t(1) << 30)) --alloc;
+  while (alloc > splits && alloc * per_split_bytes > cap) --alloc;
   p->splits = uint32_t(splits);
   p->splits_alloc = uint32_t(alloc);
 }
