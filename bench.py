@@ -216,7 +216,7 @@ def _engine(args, K):
 def gpu_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
-    from gnomon_b200 import _lib, synth
+    from gnomon_b200 import _lib, sharding, synth
     from gnomon_b200.device import DevicePlan, row_pitch, synth_fill
     from gnomon_b200.pipeline import BedSource, PipelineContext, try_run_cuda
     from gnomon_b200.prepare import from_workload
@@ -226,14 +226,19 @@ def gpu_arm(args, rank, world, local_rank):
     w = synth.WORKLOADS[args.workload]
     if args.variants:
         w = synth.scaled(w, w.people, args.variants)
-    if world > 1:  # person sharding: each rank owns a distinct shard of people
-        w = synth.Workload(w.name, w.people, w.variants, w.scores, w.p_lo, w.p_hi,
-                           w.missing_rate, w.sigma, w.flip_frac, w.size_lo, w.size_hi,
-                           w.config_id + 100 * rank)
-    P, V, K = w.people, w.variants, w.scores
-    bpv = w.bytes_per_variant
+    # person sharding (weak scaling): the cohort has world x w.people people and
+    # rank r owns .fam range [r * w.people, (r + 1) * w.people), generated as
+    # that column slice of the cohort; weights are shared, no collective runs
+    # in the scoring pass.
+    cohort = synth.Workload(w.name, w.people * world, w.variants, w.scores, w.p_lo, w.p_hi,
+                            w.missing_rate, w.sigma, w.flip_frac, w.size_lo, w.size_hi,
+                            w.config_id)
+    shard = sharding.make_shard(from_workload(cohort), rank, world)
+    person_begin = shard.start
+    P, V, K = shard.num_people, w.variants, w.scores
+    bpv = shard.prep.bytes_per_variant
     pitch = row_pitch(bpv)
-    prep = from_workload(w)
+    prep = shard.prep
     nnz = int(prep.sparse_row_offsets[-1])
     engine = _engine(args, K)
     tensor = engine == _lib.ENGINE_TENSOR
@@ -245,7 +250,8 @@ def gpu_arm(args, rank, world, local_rank):
         for v0 in range(0, V, 100_000):
             n = min(100_000, V - v0)
             thr = synth.variant_thresholds(w.seed, v0, n, w.p_lo, w.p_hi, w.missing_rate)
-            synth_fill(rows[v0:v0 + n], pitch, v0, n, P, thr, w.seed, stream=stream)
+            synth_fill(rows[v0:v0 + n], pitch, v0, n, P, thr, w.seed, stream=stream,
+                       person_begin=person_begin)
     stream.synchronize()
 
     plan = DevicePlan(prep, engine=engine, device=local_rank)
@@ -330,9 +336,10 @@ def gpu_arm(args, rank, world, local_rank):
     s_host = sums.cpu().numpy()
     assert np.isfinite(s_host).all()
 
-    # end-to-end through the public C ABI from pinned host memory
+    # end-to-end through the public C ABI from pinned host memory; every rank
+    # runs its shard in lockstep and a step takes the slowest rank's time
     e2e = None
-    if rank == 0 and not args.no_e2e:
+    if not args.no_e2e:
         host = torch.empty((V, bpv), dtype=torch.uint8, pin_memory=True)
         host.copy_(rows[:, :bpv])
         src = BedSource(host.numpy().reshape(-1))
@@ -341,6 +348,8 @@ def gpu_arm(args, rank, world, local_rank):
             try_run_cuda(ctx, src, engine=engine, device=local_rank)
         times = []
         for _ in range(args.e2e_steps):
+            if world > 1:
+                dist.barrier()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             out = try_run_cuda(ctx, src, engine=engine, device=local_rank)
@@ -349,12 +358,17 @@ def gpu_arm(args, rank, world, local_rank):
         assert np.array_equal(e_c.astype(np.int64), counts.cpu().numpy().astype(np.int64))
         rel = np.abs(e_s - s_host).max() / max(1.0, np.abs(s_host).max())
         assert rel < 1e-9, rel
+        if world > 1:
+            t = torch.tensor(times, dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            times = t.tolist()
         h2d = V * bpv + (K * (V + 64) * 16 if not tensor else nnz * 12 + (V + 1) * 8) + K * 16 + 4
         d2h = P * K * 12 + 4
-        e2e = {"value": pairs / statistics.median(times), "unit": "pairs/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+        e2e = {"value": world * pairs / statistics.median(times), "unit": "pairs/s",
+               "h2d_bytes_per_step": world * h2d, "d2h_bytes_per_step": world * d2h,
                "seconds_per_step": statistics.median(times),
-               "timing": "wall clock around gnm_score_run_ex (synchronous), pinned host rows"}
+               "timing": "wall clock around gnm_score_run_ex (synchronous), pinned host rows"
+                         + (", max over ranks" if world > 1 else "")}
         del host
 
     if rank == 0:

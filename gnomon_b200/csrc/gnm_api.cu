@@ -197,6 +197,58 @@ static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep) {
   const uint64_t part = p->K * uint64_t(p->splits_alloc) * p->part_stride;
   p->d_part_sum = dalloc<double>(p, part, "cudaMalloc(partial sums)");
   p->d_part_cnt = dalloc<uint32_t>(p, part, "cudaMalloc(partial counts)");
+
+  // Stage tables (the 3-variant lookup tables) of every score, built once on
+  // the device while they fit the cache budget; blocks that start on a
+  // 24-variant boundary read them directly.  Otherwise each accumulate call
+  // builds the tables of its block into a one-score scratch.
+  const uint64_t stages = (p->V + kPlainRows - 1) / kPlainRows;
+  if (p->K * stages * kPlainTableBytes <= kTableCacheBytes) {
+    p->tab_stages = stages;
+    p->d_tables = dalloc<uint8_t>(p, p->K * stages * kPlainTableBytes, "cudaMalloc(stage tables)");
+    for (uint64_t k = 0; k < p->K; ++k) {
+      TableArgs t{};
+      t.records = p->d_records + k * p->rec_stride;
+      t.row0 = 0;
+      t.num_rows = p->V;
+      t.tables = p->d_tables + k * stages * kPlainTableBytes;
+      check_cuda(launch_plain_tables(t, 0), "stage table launch");
+    }
+  }
+}
+
+// Stage tables for score k over block rows [v0, v0 + nv): the cached tables
+// when the block starts on a stage boundary, else a fresh build into scratch.
+static const uint8_t* plain_tables_for(gnm_plan* p, uint64_t k, uint64_t v0, uint64_t nv,
+                                       cudaStream_t s) {
+  if (p->d_tables && v0 % kPlainRows == 0)
+    return p->d_tables + (k * p->tab_stages + v0 / kPlainRows) * kPlainTableBytes;
+  const uint64_t stages = (nv + kPlainRows - 1) / kPlainRows;
+  if (stages > p->tab_scratch_stages) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    check_cuda(cudaStreamIsCapturing(s, &cs), "cudaStreamIsCapturing");
+    if (cs != cudaStreamCaptureStatusNone)
+      fail(GNM_ERR_INVALID, "stage-table scratch must grow during stream capture: run one "
+                            "uncaptured pass over the same block first, or start blocks on "
+                            "a multiple of 24 variants");
+    check_cuda(cudaStreamSynchronize(s), "stream synchronize");
+    if (p->d_tab_scratch) {
+      cudaFree(p->d_tab_scratch);
+      p->device_bytes -= p->tab_scratch_stages * kPlainTableBytes;
+      p->d_tab_scratch = nullptr;
+      p->tab_scratch_stages = 0;
+    }
+    p->d_tab_scratch = dalloc<uint8_t>(p, stages * kPlainTableBytes, "cudaMalloc(table scratch)");
+    p->tab_scratch_stages = stages;
+  }
+  TableArgs t{};
+  t.records = p->d_records + k * p->rec_stride;
+  t.row0 = v0;
+  t.num_rows = nv;
+  t.tables = p->d_tab_scratch;
+  check_cuda(launch_plain_tables(t, s), "stage table launch");
+  ++p->launches;
+  return p->d_tab_scratch;
 }
 
 static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, int device) {
@@ -287,8 +339,7 @@ static void accumulate_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, 
   const uint32_t splits = uint32_t((stages + sps - 1) / sps);
   for (uint64_t k = 0; k < p->K; ++k) {
     PlainArgs a;
-    a.records = p->d_records + k * p->rec_stride;
-    a.record_row0 = v0;
+    a.tables = plain_tables_for(p, k, v0, nv, s);
     a.num_rows = nv;
     a.bytes_per_row = p->bpv;
     a.stages_per_split = sps;
@@ -655,6 +706,8 @@ void gnm_plan_destroy(gnm_plan* p) {
   cudaSetDevice(p->device);
   if (p->tensor) tensor_plan_destroy(p);
   cudaFree(p->d_records);
+  cudaFree(p->d_tables);
+  cudaFree(p->d_tab_scratch);
   cudaFree(p->d_part_sum);
   cudaFree(p->d_part_cnt);
   cudaFree(p->d_baseline);
@@ -735,12 +788,12 @@ gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv,
 }
 
 gnm_status gnm_synth_fill_device(uint8_t* d_rows, uint64_t pitch, uint64_t v0, uint64_t nv,
-                                 uint64_t np, const uint32_t* d_thr, uint64_t seed, void* stream,
-                                 gnm_error* err) {
+                                 uint64_t i0, uint64_t np, const uint32_t* d_thr, uint64_t seed,
+                                 void* stream, gnm_error* err) {
   return guarded(err, [&] {
     if (pitch % 16 != 0) fail(GNM_ERR_INVALID, "pitch must be a multiple of 16");
     if ((np + 3) / 4 > pitch) fail(GNM_ERR_INVALID, "pitch smaller than ceil(num_people/4)");
-    check_cuda(launch_synth_fill(d_rows, pitch, v0, nv, np, d_thr, seed,
+    check_cuda(launch_synth_fill(d_rows, pitch, v0, nv, i0, np, d_thr, seed,
                                  static_cast<cudaStream_t>(stream)),
                "synth launch");
   });

@@ -19,12 +19,28 @@ enum : uint32_t {
 constexpr uint32_t kPlainThreads = 256;      // one 32-bit word column (16 people) each
 constexpr uint32_t kPlainTileBytes = 1024;   // bytes of a row per CTA (4096 people)
 constexpr uint32_t kPlainBoxBytes = 256;     // TMA box inner extent (max 256 elements)
-constexpr uint32_t kPlainRows = 48;          // variant rows per pipeline stage (16 groups of 3)
+constexpr uint32_t kPlainRows = 24;          // variant rows per pipeline stage (8 groups of 3)
+constexpr uint32_t kPlainGroups = kPlainRows / 3;
+// One stage table: 8 group tables of 64 FP32 entries (256 B each) + the
+// stage's membership word, padded to a multiple of 16 bytes (bulk copies).
+constexpr uint32_t kPlainTableBytes = kPlainGroups * 256 + 16;   // 2064
 constexpr uint32_t kRecordPad = 64;          // zero records past the last variant
+constexpr uint64_t kTableCacheBytes = uint64_t(4) << 30;  // per-plan stage-table cache budget
+
+// Source of the per-row terms {-corr, w', 2w'} and membership for the stage
+// table builder: the plan's records, or raw per-row arrays (no-alloc path).
+struct TableArgs {
+  const float4* records;   // {-corr, w', 2w', member mask bits} per row, or null
+  const float* w;          // raw arrays (used when records is null)
+  const float* corr;
+  const uint8_t* member;   // null = every row is a member
+  uint64_t row0;           // index of table row 0 in the source arrays
+  uint64_t num_rows;       // rows covered; tables for ceil(num_rows / 24) stages
+  uint8_t* tables;         // out: [stages][kPlainTableBytes]
+};
 
 struct PlainArgs {
-  const float4* records;   // [V + pad] {-corr, w', 2w', member mask bits} of one score
-  uint64_t record_row0;    // absolute variant index of block row 0
+  const uint8_t* tables;   // [stages of this block][kPlainTableBytes], stage 0 = block row 0
   uint64_t num_rows;       // rows in this block
   uint64_t bytes_per_row;  // meaningful bytes of a row (ceil(people / 4))
   uint32_t stages_per_split;
@@ -47,6 +63,7 @@ struct FinalizeArgs {
   uint32_t* counts;
 };
 
+cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s);
 cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tiles,
                                     uint32_t splits, cudaStream_t s);
 uint32_t plain_smem_bytes();
@@ -54,6 +71,7 @@ cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
 cudaError_t launch_decode(const uint8_t* rows, uint64_t pitch, uint64_t nv, uint64_t np,
                           int8_t* out, uint64_t out_pitch, cudaStream_t s);
 cudaError_t launch_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint64_t nv,
-                              uint64_t np, const uint32_t* thr, uint64_t seed, cudaStream_t s);
+                              uint64_t i0, uint64_t np, const uint32_t* thr, uint64_t seed,
+                              cudaStream_t s);
 
 }  // namespace gnm

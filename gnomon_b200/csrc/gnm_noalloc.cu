@@ -13,14 +13,18 @@
 
 namespace gnm {
 
-// Scratch layout (bytes, 256-aligned): weight records for up to
-// GNM_NOALLOC_MAX_VARIANTS rows (+ kRecordPad zero rows), FP64 partial sums and
-// u32 partial counts for up to kNaSplits splits of GNM_NOALLOC_MAX_PEOPLE
-// people, then the baseline (FP64) and the watchdog word.
+// Scratch layout (bytes, 256-aligned): a stage-table region (the 3-variant
+// lookup tables of one chunk of kNaChunkRows rows; the variants are scored
+// chunk by chunk), FP64 partial sums and u32 partial counts for up to
+// kNaSplits splits of GNM_NOALLOC_MAX_PEOPLE people, then the baseline (FP64)
+// and the watchdog word.
 constexpr uint32_t kNaSplits = 16;
-constexpr uint64_t kNaRecOff = 0;
-constexpr uint64_t kNaRecBytes = (uint64_t(GNM_NOALLOC_MAX_VARIANTS) + kRecordPad) * 16;
-constexpr uint64_t kNaSumOff = kNaRecOff + kNaRecBytes;
+constexpr uint64_t kNaTabOff = 0;
+constexpr uint64_t kNaTabBytes = (uint64_t(GNM_NOALLOC_MAX_VARIANTS) + kRecordPad) * 16;
+// stage tables are built and consumed one chunk of rows at a time
+constexpr uint64_t kNaChunkStages = kNaTabBytes / kPlainTableBytes;
+constexpr uint64_t kNaChunkRows = kNaChunkStages * kPlainRows;
+constexpr uint64_t kNaSumOff = kNaTabOff + kNaTabBytes;
 constexpr uint64_t kNaSumBytes = uint64_t(kNaSplits) * GNM_NOALLOC_MAX_PEOPLE * 8;
 constexpr uint64_t kNaCntOff = kNaSumOff + kNaSumBytes;
 constexpr uint64_t kNaCntBytes = uint64_t(kNaSplits) * GNM_NOALLOC_MAX_PEOPLE * 4;
@@ -56,21 +60,9 @@ static unsigned char* scratch_on_current_device() {
 
 // Records {-corr, w', 2w', member mask} for rows [0, V + pad), baseline, and a
 // cleared watchdog word.
-__global__ void gnm_noalloc_records(const float* w, const float* corr, const uint8_t* member,
-                                    uint64_t V, float4* recs, double baseline, double* base_out,
-                                    uint32_t* err) {
-  const uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r == 0) {
-    *base_out = baseline;
-    *err = 0u;
-  }
-  if (r >= V + kRecordPad) return;
-  float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (r < V && (member == nullptr || member[r] != 0)) {
-    const float x = w[r];
-    rec = make_float4(-corr[r], x, 2.0f * x, __uint_as_float(0x55555555u));
-  }
-  recs[r] = rec;
+__global__ void gnm_noalloc_init(double baseline, double* base_out, uint32_t* err) {
+  *base_out = baseline;
+  *err = 0u;
 }
 
 static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uint64_t P,
@@ -87,7 +79,7 @@ static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uin
     fail(GNM_ERR_INVALID, "gnm_score_noalloc: NULL buffer");
   const uint64_t bpv = (P + 3) / 4;
   unsigned char* sc = scratch_on_current_device();
-  float4* recs = reinterpret_cast<float4*>(sc + kNaRecOff);
+  uint8_t* tables = reinterpret_cast<uint8_t*>(sc + kNaTabOff);
   double* part_sum = reinterpret_cast<double*>(sc + kNaSumOff);
   uint32_t* part_cnt = reinterpret_cast<uint32_t*>(sc + kNaCntOff);
   double* base = reinterpret_cast<double*>(sc + kNaMiscOff);
@@ -99,7 +91,9 @@ static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uin
   check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
   const uint32_t tiles = uint32_t((bpv + kPlainTileBytes - 1) / kPlainTileBytes);
   const uint64_t stride = uint64_t(tiles) * kPlainTileBytes * 4;
-  const uint64_t stages = (V + kPlainRows - 1) / kPlainRows;
+  // splits per chunk of rows; every chunk adds into the same partial slots
+  const uint64_t chunk_rows = V < kNaChunkRows ? V : kNaChunkRows;
+  const uint64_t stages = (chunk_rows + kPlainRows - 1) / kPlainRows;
   uint64_t splits = uint64_t(2 * sms) / tiles;
   splits = splits < 1 ? 1 : splits;
   splits = splits > kNaSplits ? kNaSplits : splits;
@@ -110,22 +104,34 @@ static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uin
   // the array keeps the previous call's contents: clear the partials
   check_cuda(cudaMemsetAsync(part_sum, 0, grid_splits * stride * 8, s), "clear scratch");
   check_cuda(cudaMemsetAsync(part_cnt, 0, grid_splits * stride * 4, s), "clear scratch");
-  gnm_noalloc_records<<<uint32_t((V + kRecordPad + 255) / 256), 256, 0, s>>>(
-      d_w, d_corr, d_member, V, recs, baseline, base, err);
-  check_cuda(cudaGetLastError(), "record launch");
+  gnm_noalloc_init<<<1, 1, 0, s>>>(baseline, base, err);
+  check_cuda(cudaGetLastError(), "init launch");
 
-  const CUtensorMap map = make_row_map(d_rows, bpv, V, pitch, kPlainBoxBytes, kPlainRows);
-  PlainArgs a;
-  a.records = recs;
-  a.record_row0 = 0;
-  a.num_rows = V;
-  a.bytes_per_row = bpv;
-  a.stages_per_split = sps;
-  a.part_sum = part_sum;
-  a.part_cnt = part_cnt;
-  a.part_stride = stride;
-  a.err = err;
-  check_cuda(launch_plain_accumulate(map, a, tiles, grid_splits, s), "plain accumulate launch");
+  for (uint64_t c0 = 0; c0 < V; c0 += kNaChunkRows) {
+    const uint64_t nv = V - c0 < kNaChunkRows ? V - c0 : kNaChunkRows;
+    TableArgs t{};
+    t.w = d_w;
+    t.corr = d_corr;
+    t.member = d_member;
+    t.row0 = c0;
+    t.num_rows = nv;
+    t.tables = tables;
+    check_cuda(launch_plain_tables(t, s), "stage table launch");
+    const CUtensorMap map = make_row_map(d_rows + c0 * pitch, bpv, nv, pitch, kPlainBoxBytes,
+                                         kPlainRows);
+    const uint64_t cst = (nv + kPlainRows - 1) / kPlainRows;
+    PlainArgs a;
+    a.tables = tables;
+    a.num_rows = nv;
+    a.bytes_per_row = bpv;
+    a.stages_per_split = sps;
+    a.part_sum = part_sum;
+    a.part_cnt = part_cnt;
+    a.part_stride = stride;
+    a.err = err;
+    check_cuda(launch_plain_accumulate(map, a, tiles, uint32_t((cst + sps - 1) / sps), s),
+               "plain accumulate launch");
+  }
   FinalizeArgs f;
   f.part_sum = part_sum;
   f.part_cnt = part_cnt;

@@ -2,23 +2,32 @@
 //
 // Replaces the reference GPU engine's unpack_plink -> zero -> scatter ->
 // 3x SGEMM -> combine chain (score/cuda_backend.rs:62-218, 2067-2333) for small
-// score counts with ONE fused kernel per score column:
+// score counts with one fused accumulate kernel per score column:
 //
-//   * packed .bed rows are TMA-staged (cp.async.bulk.tensor, no multicast)
-//     into shared memory in [48 rows x 1024 bytes] stages, double-buffered;
-//   * each thread owns one 32-bit word column = 16 people; every 3 variant
-//     rows it transposes the 2-bit codes into per-person 6-bit indices (one
-//     byte each, pre-scaled by 4) with a handful of shift/mask ops;
-//   * a 64-entry FP32 table per 3-variant group, built in shared memory from
-//     {-missing_correction, dosage_weight, 2*dosage_weight} (prepare.rs:197-208
-//     folding, code 00 contributes 0), turns 3 genotypes into ONE lookup:
-//     decode, effect-allele flip and the missing-call rule are all folded in;
+//   * the weights of every 3 consecutive variant rows are folded once per plan
+//     (gnm_plain_tables) into a 64-entry FP32 table: entry (ca, cb, cc) is the
+//     exactly rounded T_a[ca] + T_b[cb] + T_c[cc] with T = {0, -missing
+//     correction, dosage_weight, 2*dosage_weight} (prepare.rs:197-208 folding;
+//     code 00 contributes 0), so decode, effect-allele flip and the
+//     missing-call rule become ONE lookup per person per 3 variants; eight
+//     group tables and a membership word make one 2064-byte stage table;
+//   * packed .bed rows are TMA-staged (cp.async.bulk.tensor, no multicast) in
+//     [24 rows x 1024 bytes] stages together with their stage table (a 1D bulk
+//     copy on the same mbarrier), four buffers deep;
+//   * each thread owns one 32-bit word column = 16 people; per 3 rows it
+//     transposes the 2-bit codes into per-person 6-bit indices (one byte each,
+//     pre-scaled by 4) with shift/mask ops and turns each byte into a
+//     shared-memory address with one byte permute;
+//   * warps run the stages independently: a warp waits only for the stage's
+//     TMA, and releases the buffer through a shared counter whose last arriver
+//     issues the TMA of the stage four ahead — no CTA-wide barrier per stage;
 //   * missing calls (code 01) are counted with SWAR bit tricks on the raw row
 //     words (x & ~(x>>1) & member_mask, three rows summed with one add);
-//   * FP32 partial sums cover one 48-variant stage and are flushed to FP64
-//     registers; variant splits write FP64 partials that gnm_finalize reduces
-//     in a fixed order (deterministic) and gathers through
-//     output_idx_to_fam_idx, adding the FP64 baseline (pipeline.rs:1739-1775).
+//   * FP32 partial sums (packed pairs, add.rn.f32x2) cover 96 variants and are
+//     flushed to FP64 registers; variant splits write FP64 partials that
+//     gnm_finalize reduces in a fixed order (deterministic) and gathers
+//     through output_idx_to_fam_idx, adding the FP64 baseline
+//     (pipeline.rs:1739-1775).
 #include <cstdint>
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -30,16 +39,22 @@ namespace gnm {
 
 // Shared-memory layout of one plain CTA (dynamic smem, offsets in bytes).
 struct PlainSmem {
-  static constexpr uint32_t kStageBytes = kPlainRows * kPlainTileBytes;      // 49152
-  static constexpr uint32_t kBoxBytes = kPlainRows * kPlainBoxBytes;         // 12288
-  static constexpr uint32_t kRecBytes = kPlainRows * 16;                     // 768
-  static constexpr uint32_t kLutBytes = (kPlainRows / 3) * 64 * 4;           // 4096
-  static constexpr uint32_t kStages = 2;
-  static constexpr uint32_t kTileOff = 0;
-  static constexpr uint32_t kRecOff = kTileOff + kStages * kStageBytes;
-  static constexpr uint32_t kLutOff = kRecOff + kStages * kRecBytes;
-  static constexpr uint32_t kBarOff = kLutOff + kStages * kLutBytes;
-  static constexpr uint32_t kTotal = kBarOff + 64;
+  static constexpr uint32_t kStages = 4;
+  static constexpr uint32_t kWarps = kPlainThreads / 32;
+  static constexpr uint32_t kStageBytes = kPlainRows * kPlainTileBytes;      // 24576
+  static constexpr uint32_t kBoxBytes = kPlainRows * kPlainBoxBytes;         // 6144
+  static constexpr uint32_t kTabStride = 2304;   // one stage table, padded to 256 B
+  static constexpr uint32_t kTabOff = 0;
+  static constexpr uint32_t kTileOff = kTabOff + kStages * kTabStride;      // 9216
+  static constexpr uint32_t kBarOff = kTileOff + kStages * kStageBytes;     // 4 mbarriers
+  static constexpr uint32_t kRelOff = kBarOff + 8 * kStages;                // 4 release counters
+  static constexpr uint32_t kLastOff = kRelOff + 4 * kStages;               // 4 last-issued stages
+  static constexpr uint32_t kTotal = kLastOff + 4 * kStages;
+  static_assert(kPlainRows % 3 == 0 && kPlainRows <= 32, "groups of 3 rows, one ballot");
+  static_assert(kTabStride >= kPlainTableBytes && kTabStride % 256 == 0, "table stride");
+  static_assert(kTileOff % 1024 == 0, "tile alignment");
+  // Each 64-entry group table starts on a 256-byte boundary, so a lookup
+  // address is the table address with its low byte replaced by the index.
 };
 
 // Two FP32 additions in one instruction (sm_100 packed f32x2): acc += {lo, hi}.
@@ -55,19 +70,76 @@ __device__ __forceinline__ void unpack_f32x2(uint64_t v, float& lo, float& hi) {
   asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
 }
 
-__device__ __forceinline__ void plain_issue_stage(const CUtensorMap* map, const float4* recs,
+// Shared-memory atomic add with acquire-release ordering at CTA scope.
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t addr, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], %2;"
+               : "=r"(old) : "r"(addr), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void sts_u32(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+// ---- stage tables ------------------------------------------------------------
+// Entry index e (6 bits) = bank (bits 0-4) + table row (bit 5).  The row bit
+// is lc, the lo bit of row c's code; the bank bits are row a's and row b's
+// codes with lc XORed into their lo bits (bits 0-1, 2-3) and the hi bit of row
+// c (bit 4).  The two entries that share a bank therefore differ in the lo bit
+// of all three codes (code 01 missing / 11 hom-alt), so one of them needs two
+// such calls in one person and lanes rarely meet on a bank with different
+// addresses.  The sum of the three FP32 terms is exact in FP64 and rounded to
+// FP32 once.
+
+__device__ __forceinline__ float table_term(const TableArgs& a, uint64_t row, uint32_t j) {
+  if (a.records) return reinterpret_cast<const float*>(a.records + a.row0 + row)[j];
+  const uint64_t r = a.row0 + row;
+  if (a.member && a.member[r] == 0) return 0.0f;
+  const float w = a.w[r];
+  return j == 0 ? -a.corr[r] : (j == 1 ? w : 2.0f * w);
+}
+
+__device__ __forceinline__ bool table_member(const TableArgs& a, uint64_t row) {
+  if (a.records) return a.records[a.row0 + row].w != 0.0f;
+  return a.member == nullptr || a.member[a.row0 + row] != 0;
+}
+
+// grid.x = stages, block = 8 groups x 64 entries.
+__global__ void __launch_bounds__(kPlainGroups * 64) gnm_plain_tables(TableArgs a) {
+  const uint64_t stage = blockIdx.x;
+  const uint32_t e = threadIdx.x, g = e >> 6, idx = e & 63u;
+  const uint32_t lc = (idx >> 5) & 1u;
+  const uint32_t code[3] = {(idx & 3u) ^ lc, ((idx >> 2) & 3u) ^ lc, ((idx >> 3) & 2u) | lc};
+  const uint64_t row0 = stage * kPlainRows + 3 * g;
+  double v = 0.0;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    if (code[r] != 0 && row0 + r < a.num_rows) v += double(table_term(a, row0 + r, code[r] - 1));
+  uint8_t* tab = a.tables + stage * kPlainTableBytes;
+  reinterpret_cast<float*>(tab)[e] = float(v);
+  if (e < 32) {
+    const uint64_t row = stage * kPlainRows + e;
+    const bool m = e < kPlainRows && row < a.num_rows && table_member(a, row);
+    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, m);
+    if (e < 4) reinterpret_cast<uint32_t*>(tab + kPlainGroups * 256)[e] = e == 0 ? bits : 0u;
+  }
+}
+
+// ---- accumulate --------------------------------------------------------------
+
+__device__ __forceinline__ void plain_issue_stage(const CUtensorMap* map, const uint8_t* tables,
                                                   uint32_t smem_base, uint32_t buf,
-                                                  int32_t tile_x, int32_t row0,
-                                                  uint64_t rec_row0) {
+                                                  int32_t tile_x, int32_t row0, uint64_t stage) {
   const uint32_t bar = smem_base + PlainSmem::kBarOff + 8 * buf;
-  mbar_arrive_expect_tx(bar, PlainSmem::kStageBytes + PlainSmem::kRecBytes);
+  mbar_arrive_expect_tx(bar, PlainSmem::kStageBytes + kPlainTableBytes);
   const uint32_t tile = smem_base + PlainSmem::kTileOff + buf * PlainSmem::kStageBytes;
 #pragma unroll
   for (uint32_t b = 0; b < kPlainTileBytes / kPlainBoxBytes; ++b)
     tma_load_2d(tile + b * PlainSmem::kBoxBytes, map, tile_x + int32_t(b * kPlainBoxBytes), row0,
                 bar);
-  bulk_load(smem_base + PlainSmem::kRecOff + buf * PlainSmem::kRecBytes, recs + rec_row0,
-            PlainSmem::kRecBytes, bar);
+  bulk_load(smem_base + PlainSmem::kTabOff + buf * PlainSmem::kTabStride,
+            tables + stage * kPlainTableBytes, kPlainTableBytes, bar);
 }
 
 // grid = (people tiles, variant splits); block = kPlainThreads.
@@ -75,28 +147,42 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
     gnm_plain_accumulate(const __grid_constant__ CUtensorMap map, PlainArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t sbase = smem_u32(smem);
-  const uint32_t tid = threadIdx.x;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u;
   const uint32_t tile = blockIdx.x;
   const uint32_t split = blockIdx.y;
 
   const uint64_t rows_per_split = uint64_t(a.stages_per_split) * kPlainRows;
   const uint64_t r_begin = uint64_t(split) * rows_per_split;
   if (r_begin >= a.num_rows) return;
+  // table addresses are formed by byte replacement: the window must be aligned
+  if ((sbase & 255u) != 0u) {
+    if (tid == 0) atomicOr(a.err, kErrShape);
+    return;
+  }
   const uint64_t r_end = min(a.num_rows, r_begin + rows_per_split);
   const uint32_t nstages = uint32_t((r_end - r_begin + kPlainRows - 1) / kPlainRows);
+  const uint64_t stage0 = r_begin / kPlainRows;   // block stage of this split's stage 0
   const int32_t tile_x = int32_t(tile * kPlainTileBytes);
+  const uint32_t bar0 = sbase + PlainSmem::kBarOff;
+  const uint32_t rel0 = sbase + PlainSmem::kRelOff;
+  uint32_t* last_issued = reinterpret_cast<uint32_t*>(smem + PlainSmem::kLastOff);
 
   if (tid == 0) {
     prefetch_tmap(&map);
-    mbar_init(sbase + PlainSmem::kBarOff, 1);
-    mbar_init(sbase + PlainSmem::kBarOff + 8, 1);
+    for (uint32_t b = 0; b < PlainSmem::kStages; ++b) {
+      mbar_init(bar0 + 8 * b, 1);
+      sts_u32(rel0 + 4 * b, 0u);
+      last_issued[b] = 0xFFFFFFFFu;
+    }
     fence_mbar_init();
   }
   __syncthreads();
   if (tid == 0) {
-    for (uint32_t s = 0; s < 2 && s < nstages; ++s)
-      plain_issue_stage(&map, a.records, sbase, s, tile_x, int32_t(r_begin + s * kPlainRows),
-                        a.record_row0 + r_begin + s * kPlainRows);
+    for (uint32_t s = 0; s < PlainSmem::kStages && s < nstages; ++s) {
+      last_issued[s] = s;
+      plain_issue_stage(&map, a.tables, sbase, s, tile_x, int32_t(r_begin + s * kPlainRows),
+                        stage0 + s);
+    }
   }
 
   // FP32 sums as packed pairs for add.rn.f32x2: accp[2q] holds people
@@ -114,65 +200,27 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
   for (int i = 0; i < 8; ++i) accp[i] = 0ull;
 
   // Each thread reads word column `tid` of the 1024-byte stage row; the stage
-  // is stored as 4 TMA boxes of [48 rows][256 bytes].
+  // is stored as 4 TMA boxes of [kPlainRows rows][256 bytes].
   const uint32_t word_off = (tid / (kPlainBoxBytes / 4)) * PlainSmem::kBoxBytes +
                             (tid % (kPlainBoxBytes / 4)) * 4;
   // warps whose 128 bytes all lie past the row's last byte only hold padding
   const bool warp_active =
       uint64_t(tile) * kPlainTileBytes + uint64_t(tid & ~31u) * 4 < a.bytes_per_row;
 
+  bool failed = false;
   for (uint32_t st = 0; st < nstages; ++st) {
-    const uint32_t buf = st & 1u;
-    const uint32_t parity = (st >> 1) & 1u;
-    const bool ok = mbar_wait_bounded(sbase + PlainSmem::kBarOff + 8 * buf, parity);
-
-    // Build the 16 group tables of this stage: 1024 entries, 4 per thread.
-    // Entry index e (6 bits): code of row a in bits 0-1, row b in bits 2-3,
-    // row c with its two bits swapped (hi in bit 4, lo in bit 5) so that the
-    // rarely-set lo bit of row c selects the shared-memory row of the table
-    // and lanes collide on banks less often.  The sum of the three FP32 terms
-    // is exact in FP64 and rounded to FP32 once.
-    {
-      const uint64_t row0 = r_begin + uint64_t(st) * kPlainRows;
-      const float* rec = reinterpret_cast<const float*>(smem + PlainSmem::kRecOff +
-                                                        buf * PlainSmem::kRecBytes);
-      float* lut = reinterpret_cast<float*>(smem + PlainSmem::kLutOff + buf * PlainSmem::kLutBytes);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t e = tid * 4 + q;          // 0..1023
-        const uint32_t g = e >> 6, idx = e & 63;  // group, index
-        const uint32_t code[3] = {idx & 3u, (idx >> 2) & 3u,
-                                  ((idx >> 3) & 2u) | ((idx >> 5) & 1u)};
-        double v = 0.0;
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-          const uint32_t row = 3 * g + r;
-          if (code[r] != 0 && row0 + row < r_end) v += double(rec[row * 4 + (code[r] - 1)]);
-        }
-        lut[e] = float(v);
-      }
-      // Membership bitmap of the stage's 48 rows (rows past the split end are
-      // not members): two ballots replace 48 per-row mask loads.
-      if (tid < 64) {
-        const uint32_t r = tid;
-        const bool m = r < kPlainRows && row0 + r < r_end && rec[r * 4 + 3] != 0.0f;
-        const uint32_t bits = __ballot_sync(0xFFFFFFFFu, m);
-        if ((tid & 31) == 0)
-          reinterpret_cast<uint32_t*>(smem + PlainSmem::kBarOff + 16)[2 * buf + (tid >> 5)] = bits;
-      }
-    }
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicOr(a.err, kErrTmaTimeout);
-      // Drain the other in-flight stage (bounded) before leaving.
-      if (st + 1 < nstages) mbar_wait_bounded(sbase + PlainSmem::kBarOff + 8 * (buf ^ 1u),
-                                              ((st + 1) >> 1) & 1u);
-      return;
+    const uint32_t buf = st % PlainSmem::kStages;
+    const uint32_t parity = (st / PlainSmem::kStages) & 1u;
+    if (!mbar_wait_bounded(bar0 + 8 * buf, parity)) {
+      if (lane == 0) atomicOr(a.err, kErrTmaTimeout);
+      failed = true;
+      break;
     }
 
     const uint8_t* tbase = smem + PlainSmem::kTileOff + buf * PlainSmem::kStageBytes + word_off;
-    const uint8_t* lbase = smem + PlainSmem::kLutOff + buf * PlainSmem::kLutBytes;
-    const uint32_t* mbits = reinterpret_cast<const uint32_t*>(smem + PlainSmem::kBarOff + 16);
-    const uint64_t members = uint64_t(mbits[2 * buf]) | (uint64_t(mbits[2 * buf + 1]) << 32);
+    const uint32_t lbase = sbase + PlainSmem::kTabOff + buf * PlainSmem::kTabStride;
+    const uint64_t members = *reinterpret_cast<const uint32_t*>(
+        smem + PlainSmem::kTabOff + buf * PlainSmem::kTabStride + kPlainGroups * 256);
 
     uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
     auto group = [&](uint32_t g, uint32_t ma, uint32_t mb, uint32_t mc) {
@@ -180,22 +228,25 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
       const uint32_t xb = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 1) * kPlainBoxBytes);
       const uint32_t xc = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 2) * kPlainBoxBytes);
       // ---- per-person 6-bit indices (x4) ------------------------------
-      // row c enters with its code bits swapped (see the table layout above)
+      // rows a and b get row c's lo bits XORed into their lo bits; row c
+      // enters with its code bits swapped (see the table layout above)
+      const uint32_t ya = xa ^ (xc & 0x55555555u);
+      const uint32_t yb = xb ^ (xc & 0x55555555u);
       const uint32_t xs = ((xc >> 1) & 0x55555555u) | ((xc << 1) & 0xAAAAAAAAu);
-      const uint32_t E = (xa & 0x33333333u) | ((xb << 2) & 0xCCCCCCCCu);
-      const uint32_t O = ((xa >> 2) & 0x33333333u) | (xb & 0xCCCCCCCCu);
+      const uint32_t E = (ya & 0x33333333u) | ((yb << 2) & 0xCCCCCCCCu);
+      const uint32_t O = ((ya >> 2) & 0x33333333u) | (yb & 0xCCCCCCCCu);
       uint32_t ix[4];
       ix[0] = ((E << 2) & 0x3C3C3C3Cu) | ((xs << 6) & 0xC0C0C0C0u);
       ix[1] = ((O << 2) & 0x3C3C3C3Cu) | ((xs << 4) & 0xC0C0C0C0u);
       ix[2] = ((E >> 2) & 0x3C3C3C3Cu) | ((xs << 2) & 0xC0C0C0C0u);
       ix[3] = ((O >> 2) & 0x3C3C3C3Cu) | (xs & 0xC0C0C0C0u);
-      const uint8_t* lg = lbase + g * 256;
+      const uint32_t lg = lbase + g * 256;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         float v[4];
+        // address = table address with its low byte replaced by index byte j
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          v[j] = *reinterpret_cast<const float*>(lg + __byte_perm(ix[q], 0u, 0x4440u + j));
+        for (int j = 0; j < 4; ++j) v[j] = lds_f32(__byte_perm(ix[q], lg, 0x7650u + j));
         accp[2 * q] = add_f32x2(accp[2 * q], v[0], v[1]);
         accp[2 * q + 1] = add_f32x2(accp[2 * q + 1], v[2], v[3]);
       }
@@ -203,7 +254,7 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
       const uint32_t c3 = (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
       ev += c3 & 0x33333333u;
       od += (c3 >> 2) & 0x33333333u;
-      if ((g % 5) == 4 || g == kPlainRows / 3 - 1) {
+      if ((g % 5) == 4 || g == kPlainGroups - 1) {
         by[0] += ev & 0x0F0F0F0Fu;
         by[2] += (ev >> 4) & 0x0F0F0F0Fu;
         by[1] += od & 0x0F0F0F0Fu;
@@ -217,19 +268,39 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
     } else if (members == (uint64_t(1) << kPlainRows) - 1) {
       // every row of the stage is a member of this score (the common case)
 #pragma unroll
-      for (uint32_t g = 0; g < kPlainRows / 3; ++g) group(g, 0x55555555u, 0x55555555u, 0x55555555u);
+      for (uint32_t g = 0; g < kPlainGroups; ++g) group(g, 0x55555555u, 0x55555555u, 0x55555555u);
     } else {
 #pragma unroll
-      for (uint32_t g = 0; g < kPlainRows / 3; ++g) {
+      for (uint32_t g = 0; g < kPlainGroups; ++g) {
         const uint32_t ma = (0u - uint32_t((members >> (3 * g + 0)) & 1u)) & 0x55555555u;
         const uint32_t mb = (0u - uint32_t((members >> (3 * g + 1)) & 1u)) & 0x55555555u;
         const uint32_t mc = (0u - uint32_t((members >> (3 * g + 2)) & 1u)) & 0x55555555u;
         group(g, ma, mb, mc);
       }
     }
-    // FP32 sums and byte counters span two stages (96 variants, <= 96 calls
+
+    // Release the buffer.  __syncwarp orders this warp's reads before lane
+    // 0's release-add; the warp that completes the count acquires every
+    // warp's release, so all reads of the buffer are done before it hands the
+    // buffer to the async proxy for the stage four ahead.
+    __syncwarp();
+    if (lane == 0) {
+      const uint32_t old = atom_add_acq_rel(rel0 + 4 * buf, 1u);
+      if (old == PlainSmem::kWarps - 1) {
+        sts_u32(rel0 + 4 * buf, 0u);
+        const uint32_t nxt = st + PlainSmem::kStages;
+        if (nxt < nstages) {
+          last_issued[buf] = nxt;
+          fence_proxy_async_smem();
+          plain_issue_stage(&map, a.tables, sbase, buf, tile_x,
+                            int32_t(r_begin + uint64_t(nxt) * kPlainRows), stage0 + nxt);
+        }
+      }
+    }
+
+    // FP32 sums and byte counters span four stages (96 variants, <= 96 calls
     // per byte counter) before they are flushed to FP64 / 32-bit counts.
-    if ((st & 1u) || st + 1 == nstages) {
+    if ((st & 3u) == 3u || st + 1 == nstages) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
 #pragma unroll
@@ -246,14 +317,18 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
         accp[2 * q + 1] = 0ull;
       }
     }
+  }
 
-    __syncthreads();  // every thread is done with stage buffer `buf`
-    if (tid == 0 && st + 2 < nstages) {
-      fence_proxy_async_smem();
-      plain_issue_stage(&map, a.records, sbase, buf, tile_x,
-                        int32_t(r_begin + (st + 2) * kPlainRows),
-                        a.record_row0 + r_begin + (st + 2) * kPlainRows);
+  // A warp that gave up on a TMA wait leaves stages other warps may still
+  // wait for (bounded).  Once every warp is here, drain each buffer's last
+  // issued copy (bounded) so no TMA is in flight when the CTA exits.
+  if (__syncthreads_or(failed)) {
+    if (tid == 0) {
+      for (uint32_t b = 0; b < PlainSmem::kStages; ++b)
+        if (last_issued[b] != 0xFFFFFFFFu)
+          mbar_wait_bounded(bar0 + 8 * b, (last_issued[b] / PlainSmem::kStages) & 1u);
     }
+    return;
   }
 
   // FP64 partials for this (split, person) accumulate across calls.
@@ -295,9 +370,11 @@ __global__ void gnm_decode(const uint8_t* rows, uint64_t pitch, uint64_t nv, uin
 }
 
 // One thread per 32-bit word of a row (16 people).  Same generator as the
-// CPU oracle: key = mix64(seed) ^ v*C1 ^ i*C2, x = mix64(key).
+// CPU oracle: key = mix64(seed) ^ v*C1 ^ i*C2, x = mix64(key), with i the
+// cohort-wide person index i0 + local column (a person shard fills its own
+// column slice of the cohort).
 __global__ void gnm_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint64_t nv,
-                               uint64_t np, const uint32_t* thr, uint64_t seed) {
+                               uint64_t i0, uint64_t np, const uint32_t* thr, uint64_t seed) {
   const uint64_t words = pitch / 4;
   const uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const uint64_t j = blockIdx.y + uint64_t(blockIdx.z) * gridDim.y;
@@ -310,7 +387,7 @@ __global__ void gnm_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint6
   for (uint32_t q = 0; q < 16; ++q) {
     const uint64_t i = w * 16 + q;
     if (i < np) {
-      const uint64_t x = mix64(sk ^ (i * 0x8CB92BA72F3D8DD7ull));
+      const uint64_t x = mix64(sk ^ ((i0 + i) * 0x8CB92BA72F3D8DD7ull));
       const uint32_t um = uint32_t(x), ug = uint32_t(x >> 32);
       const uint32_t code = um < tm ? 1u : (ug < t0 ? 0u : (ug < t1 ? 2u : 3u));
       word |= code << (2 * q);
@@ -320,6 +397,14 @@ __global__ void gnm_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint6
 }
 
 // ---- host launchers --------------------------------------------------------
+
+cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s) {
+  const uint64_t stages = (a.num_rows + kPlainRows - 1) / kPlainRows;
+  if (stages == 0) return cudaSuccess;
+  if (stages > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+  gnm_plain_tables<<<uint32_t(stages), kPlainGroups * 64, 0, s>>>(a);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tiles,
                                     uint32_t splits, cudaStream_t s) {
@@ -360,11 +445,12 @@ cudaError_t launch_decode(const uint8_t* rows, uint64_t pitch, uint64_t nv, uint
 }
 
 cudaError_t launch_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint64_t nv,
-                              uint64_t np, const uint32_t* thr, uint64_t seed, cudaStream_t s) {
+                              uint64_t i0, uint64_t np, const uint32_t* thr, uint64_t seed,
+                              cudaStream_t s) {
   if (nv == 0) return cudaSuccess;
   const uint64_t words = pitch / 4;
-  gnm_synth_fill<<<rows_grid((words + 255) / 256, nv), 256, 0, s>>>(rows, pitch, v0, nv, np, thr,
-                                                                    seed);
+  gnm_synth_fill<<<rows_grid((words + 255) / 256, nv), 256, 0, s>>>(rows, pitch, v0, nv, i0, np,
+                                                                    thr, seed);
   return cudaGetLastError();
 }
 

@@ -46,6 +46,10 @@ struct gnm_plan {
   uint64_t part_stride = 0;    // people per partial slot (tiles * 4096)
   uint64_t rec_stride = 0;     // records per score (V + pad)
   float4* d_records = nullptr; // [K][rec_stride]
+  uint8_t* d_tables = nullptr;  // stage tables of every score, [K][tab_stages][kPlainTableBytes]
+  uint64_t tab_stages = 0;      // ceil(V / kPlainRows) when d_tables is cached, else 0
+  uint8_t* d_tab_scratch = nullptr;  // one score's tables for blocks the cache cannot serve
+  uint64_t tab_scratch_stages = 0;
   double* d_part_sum = nullptr;
   uint32_t* d_part_cnt = nullptr;
 

@@ -147,15 +147,18 @@ class DevicePlan:
 
 
 def synth_fill(rows: torch.Tensor, pitch: int, variant_begin: int, num_variants: int,
-               num_people: int, thresholds: np.ndarray, seed: int, stream=None):
-    """Fill device rows with the deterministic HWE generator (gnomon_b200.synth)."""
+               num_people: int, thresholds: np.ndarray, seed: int, stream=None,
+               person_begin: int = 0):
+    """Fill device rows with the deterministic HWE generator (gnomon_b200.synth).
+
+    Column c holds cohort person ``person_begin + c``."""
     lib = _lib.load()
     thr = torch.from_numpy(np.ascontiguousarray(thresholds, dtype=np.uint32).view(np.int32)).to(
         rows.device)
     e = _lib.gnm_error()
     _lib.check(lib.gnm_synth_fill_device(rows.data_ptr(), pitch, variant_begin, num_variants,
-                                         num_people, thr.data_ptr(), seed, _stream_ptr(stream),
-                                         C.byref(e)), e)
+                                         person_begin, num_people, thr.data_ptr(), seed,
+                                         _stream_ptr(stream), C.byref(e)), e)
     return thr
 
 

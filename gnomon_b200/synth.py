@@ -53,10 +53,12 @@ def variant_thresholds(seed: int, v0: int, n: int, p_lo: float, p_hi: float,
     return t
 
 
-def genotype_codes(seed: int, v0: int, n: int, num_people: int, thr: np.ndarray) -> np.ndarray:
-    """Reference numpy generator: uint8 codes [n, num_people] (0..3)."""
+def genotype_codes(seed: int, v0: int, n: int, num_people: int, thr: np.ndarray,
+                   person_begin: int = 0) -> np.ndarray:
+    """Reference numpy generator: uint8 codes [n, num_people] (0..3) of cohort
+    people person_begin .. person_begin + num_people - 1."""
     v = np.arange(v0, v0 + n, dtype=np.uint64)[:, None]
-    i = np.arange(num_people, dtype=np.uint64)[None, :]
+    i = np.arange(person_begin, person_begin + num_people, dtype=np.uint64)[None, :]
     with np.errstate(over="ignore"):
         key = mix64(np.uint64(seed)) ^ (v * np.uint64(0xD1B54A32D192ED03)) \
             ^ (i * np.uint64(0x8CB92BA72F3D8DD7))
@@ -93,8 +95,8 @@ def unpack_codes(rows: np.ndarray, num_people: int) -> np.ndarray:
 
 
 def synth_rows(seed: int, v0: int, n: int, num_people: int, thr: np.ndarray,
-               pitch: int | None = None) -> np.ndarray:
-    return pack_codes(genotype_codes(seed, v0, n, num_people, thr), pitch)
+               pitch: int | None = None, person_begin: int = 0) -> np.ndarray:
+    return pack_codes(genotype_codes(seed, v0, n, num_people, thr, person_begin), pitch)
 
 
 # ---------------------------------------------------------------------------

@@ -205,12 +205,14 @@ gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch,
                              gnm_error* err);
 
 /* Fill a device matrix with the deterministic synthetic HWE genotype
- * generator (see DESIGN.md "Synthetic data"): per-variant uint32 thresholds
- * {t_missing, T0, T1}, code = u_m < t_m ? 01 : u_g < T0 ? 00 : u_g < T1 ? 10 : 11
- * with (u_m, u_g) the two halves of mix64(key(seed, v, i)).  Padding people
- * (i >= num_people) are 00. */
+ * generator: per-variant uint32 thresholds {t_missing, T0, T1},
+ * code = u_m < t_m ? 01 : u_g < T0 ? 00 : u_g < T1 ? 10 : 11 with (u_m, u_g)
+ * the two halves of mix64(key(seed, v, i)).  Column c of the matrix holds
+ * cohort person i = person_begin + c, so a person shard can generate its own
+ * column slice of a larger cohort.  Padding columns (c >= num_people) are 00. */
 gnm_status gnm_synth_fill_device(uint8_t* d_rows, uint64_t pitch, uint64_t variant_begin,
-                                 uint64_t num_variants, uint64_t num_people,
+                                 uint64_t num_variants, uint64_t person_begin,
+                                 uint64_t num_people,
                                  const uint32_t* d_thresholds /* [num_variants][3] */,
                                  uint64_t seed, void* stream, gnm_error* err);
 

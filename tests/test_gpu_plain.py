@@ -181,6 +181,53 @@ def test_gpu_generator_matches_numpy(cuda, people):
     synth_fill(d, pitch, v0, n, people, thr, w.seed)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(d.cpu().numpy(), synth.synth_rows(w.seed, v0, n, people, thr, pitch))
+    # a person shard's columns: cohort people person_begin .. person_begin+people-1
+    synth_fill(d, pitch, v0, n, people, thr, w.seed, person_begin=40_000)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.cpu().numpy(), synth.synth_rows(w.seed, v0, n, people, thr, pitch,
+                                                                    person_begin=40_000))
+
+
+@pytest.mark.parametrize("engine", [PLAIN, _lib.ENGINE_TENSOR])
+@pytest.mark.parametrize("subset", [False, True])
+def test_person_shards_reassemble_cohort(cuda, engine, subset):
+    """The multi-GPU layout run shard by shard on one device: every shard's
+    rows are a byte-column slice, scored by its own plan; reassembled in output
+    order they match the unsharded run (counts exact, sums at the reference
+    tolerance; FP32 grouping may differ with the shard's launch shape)."""
+    import torch
+    from gnomon_b200 import sharding
+    from gnomon_b200.device import DevicePlan, row_pitch
+    _, prep, rows, _ = synth_case(9001, 700, scores=3, config="diff_20k_x_200k_k16")
+    if subset:
+        keep = np.random.default_rng(3).permutation(9001)[:6000].astype(np.uint32)
+        prep = PreparationResult(prep.sparse_weights, prep.sparse_missing_corrections,
+                                 prep.sparse_score_columns, prep.sparse_row_offsets,
+                                 list(prep.score_names), 9001, output_idx_to_fam_idx=keep)
+
+    def score(p, r):
+        pitch = row_pitch(p.bytes_per_variant)
+        dev = np.zeros((r.shape[0], pitch), np.uint8)
+        dev[:, :r.shape[1]] = r
+        plan = DevicePlan(p, engine=engine)
+        s, c = plan.score(torch.from_numpy(dev).cuda(), pitch)
+        plan.sync()
+        out = s.cpu().numpy(), c.cpu().numpy()
+        plan.close()
+        return out
+
+    s0, c0 = score(prep, rows)
+    K = prep.num_scores
+    world = 3
+    s = np.zeros((prep.num_people_to_score, K))
+    c = np.zeros((prep.num_people_to_score, K), np.uint32)
+    for r in range(world):
+        sh = sharding.make_shard(prep, r, world)
+        ss, cc = score(sh.prep, sharding.slice_rows(rows, sh.start, sh.stop))
+        s[sh.output_rows] = ss.reshape(-1, K)
+        c[sh.output_rows] = cc.reshape(-1, K)
+    np.testing.assert_array_equal(c.reshape(-1), c0.reshape(-1).astype(np.uint32))
+    assert oracle.within_reference_tolerance(s.reshape(-1), s0.reshape(-1)).all()
 
 
 @pytest.mark.parametrize("engine", [PLAIN, _lib.ENGINE_TENSOR])
