@@ -328,8 +328,9 @@ def gpu_arm(args, rank, world, local_rank):
     peak_hbm, peak_kind = peaks()
     if tensor:
         # executed tensor-core work: 8 limb MMAs (4 dosage, 3 correction, 1 count)
-        ptiles, kpad, vpad = -(-P // 128), -(-K // 128) * 128, -(-V // 64) * 64
-        flops = 2.0 * ptiles * 128 * vpad * kpad * 8
+        # over 256-person x 128-score tiles and 64-variant stages
+        ptiles, kpad, vpad = -(-P // 256), -(-K // 128) * 128, -(-V // 64) * 64
+        flops = 2.0 * ptiles * 256 * vpad * kpad * 8
         achieved = flops / (kernel_ms / 1e3) / 1e12
         pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"] \
             if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0

@@ -21,11 +21,17 @@
 // 1e-6 of the score) and 2^-25 for missing corrections (three limbs; they touch
 // only the ~1% missing calls).
 //
-// Kernel shape (one CTA per SM): M = 128 score rows (TMEM lanes), N = 128
-// people (TMEM columns), K = 64 variants per stage.  Warp 0 issues TMA (weight
-// limb planes, 3D map, 128-byte swizzle; packed rows, 2D map), warp 1 owns
-// TMEM and issues tcgen05.mma, warps 2-5 expand packed 2-bit genotypes into
-// the BF16 K-major operand in shared memory and drain TMEM at block ends.
+// Kernel shape (one CTA per SM): M = 128 score rows (TMEM lanes), N = 256
+// people (TMEM columns), K = 64 variants per stage, two limb planes per pass
+// (2 x 256 FP32 accumulator columns fill the 512 TMEM columns), three stages
+// of 68 KB in shared memory.  With 256 people per CTA every weight byte
+// staged from L2 feeds twice the MMA work of a 128-person tile; the four
+// passes (dosage limbs 0-1, dosage limbs 2-3, correction limbs 0-1,
+// correction limb 2 + member count) each re-expand the genotypes, which is
+// cheap CUDA-core work on separate warps.  Warp 0 issues TMA (weight limb
+// planes, 3D map, 128-byte swizzle; packed rows, 2D map), warp 1 owns TMEM
+// and issues tcgen05.mma, warps 2-5 expand packed 2-bit genotypes into the
+// BF16 K-major operand in shared memory and drain TMEM at block ends.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -44,10 +50,12 @@
 namespace gnm {
 
 constexpr uint32_t kTcM = 128;        // score rows per tile
-constexpr uint32_t kTcN = 128;        // people per tile
+constexpr uint32_t kTcN = 256;        // people per tile
 constexpr uint32_t kTcK = 64;         // variants per stage
 constexpr uint32_t kTcFlush = 256;    // stages per exact FP32 block (16384 variants)
 constexpr uint32_t kTcThreads = 192;  // 6 warps
+constexpr int kTcPlanes = 2;          // limb planes per pass (2 x 256 TMEM columns)
+constexpr int kTcStages = 3;          // pipeline stages (68 KB each)
 
 struct TensorPlan {
   uint64_t K_pad = 0, V_pad = 0, P_pad = 0;
@@ -67,14 +75,15 @@ struct TcArgs {
   uint64_t P_pad;
   uint32_t* err;
   uint32_t raster;         // 0: blockIdx.x = people tile, 1: blockIdx.x = score tile
+  int32_t z0;              // first limb plane of this pass (TMA z coordinate)
 };
 
 template <int NP, int ST>
 struct TcSmem {
   static constexpr uint32_t kPlane = kTcM * kTcK * 2;   // 16 KB
   static constexpr uint32_t kAStage = NP * kPlane;
-  static constexpr uint32_t kB = kTcN * kTcK * 2;       // 16 KB
-  static constexpr uint32_t kPk = kTcK * (kTcN / 4);    // 2 KB
+  static constexpr uint32_t kB = kTcN * kTcK * 2;       // 32 KB
+  static constexpr uint32_t kPk = kTcK * (kTcN / 4);    // 4 KB
   static constexpr uint32_t kAOff = 0;
   static constexpr uint32_t kBOff = kAOff + ST * kAStage;
   static constexpr uint32_t kPkOff = kBOff + ST * kB;
@@ -93,7 +102,10 @@ __device__ __forceinline__ uint32_t bf16_pair(uint32_t y16, uint32_t lo, uint32_
   return __byte_perm(lo, hi, y16 * 0x11u + 0x4040u);
 }
 
-template <int NP, int ST, bool MISSING>
+// MISSING: the B operand is the missing indicator (else the dosage).
+// COUNT_LAST: the pass's last plane is the member plane; its products are the
+// missing counts (else every plane is a limb of the pass's sum).
+template <int NP, int ST, bool MISSING, bool COUNT_LAST>
 __global__ void __launch_bounds__(kTcThreads, 1)
     gnm_tc_accumulate(const __grid_constant__ CUtensorMap amap,
                       const __grid_constant__ CUtensorMap pmap, TcArgs a) {
@@ -148,7 +160,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (*abort_flag) break;
         mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
         tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kTcK),
-                    int32_t(stile * kTcM), 0, full(s));
+                    int32_t(stile * kTcM), a.z0, full(s));
         tma_load_2d(sb + L::kPkOff + s * L::kPk, &pmap, int32_t(ptile * (kTcN / 4)),
                     int32_t(it * kTcK), full(s));
       }
@@ -211,27 +223,33 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint8_t* pk = smem + L::kPkOff + s * L::kPk;
       uint8_t* bt = smem + L::kBOff + s * L::kB;
 #pragma unroll
-      for (uint32_t cc = 0; cc < 2; ++cc) {
-        const uint32_t r0 = 16 * vg + 8 * cc;
-        uint32_t xl = 0, xh = 0;
+      for (uint32_t h = 0; h < kTcN / 128; ++h) {
+        const uint32_t bc = 32 * h + col;   // byte column: people 4bc..4bc+3
 #pragma unroll
-        for (uint32_t i = 0; i < 4; ++i) {
-          xl |= uint32_t(pk[(r0 + i) * (kTcN / 4) + col]) << (8 * i);
-          xh |= uint32_t(pk[(r0 + 4 + i) * (kTcN / 4) + col]) << (8 * i);
-        }
-        const uint32_t c = 2 * vg + cc;  // 16-byte chunk (8 variants) index
+        for (uint32_t cc = 0; cc < 2; ++cc) {
+          const uint32_t r0 = 16 * vg + 8 * cc;
+          uint32_t xl = 0, xh = 0;
 #pragma unroll
-        for (uint32_t q = 0; q < 4; ++q) {
-          const uint32_t yl = (xl >> (2 * q)) & 0x03030303u;
-          const uint32_t yh = (xh >> (2 * q)) & 0x03030303u;
-          const uint32_t lo = MISSING ? kMisLo : kDosLo, hi = MISSING ? kMisHi : kDosHi;
-          uint4 v;
-          v.x = bf16_pair(yl & 0xFFFFu, lo, hi);
-          v.y = bf16_pair(yl >> 16, lo, hi);
-          v.z = bf16_pair(yh & 0xFFFFu, lo, hi);
-          v.w = bf16_pair(yh >> 16, lo, hi);
-          const uint32_t n = 32 * q + col;  // operand row of person 4col+q
-          *reinterpret_cast<uint4*>(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4)) = v;
+          for (uint32_t i = 0; i < 4; ++i) {
+            xl |= uint32_t(pk[(r0 + i) * (kTcN / 4) + bc]) << (8 * i);
+            xh |= uint32_t(pk[(r0 + 4 + i) * (kTcN / 4) + bc]) << (8 * i);
+          }
+          const uint32_t c = 2 * vg + cc;  // 16-byte chunk (8 variants) index
+#pragma unroll
+          for (uint32_t q = 0; q < 4; ++q) {
+            const uint32_t yl = (xl >> (2 * q)) & 0x03030303u;
+            const uint32_t yh = (xh >> (2 * q)) & 0x03030303u;
+            const uint32_t lo = MISSING ? kMisLo : kDosLo, hi = MISSING ? kMisHi : kDosHi;
+            uint4 v;
+            v.x = bf16_pair(yl & 0xFFFFu, lo, hi);
+            v.y = bf16_pair(yl >> 16, lo, hi);
+            v.z = bf16_pair(yh & 0xFFFFu, lo, hi);
+            v.w = bf16_pair(yh >> 16, lo, hi);
+            // operand row of person 128h + 4col + q (conflict-free 16-byte stores)
+            const uint32_t n = 128 * h + 32 * q + col;
+            *reinterpret_cast<uint4*>(bt + (n >> 3) * 1024 + (n & 7) * 128 +
+                                      ((c ^ (n & 7)) << 4)) = v;
+          }
         }
       }
       fence_proxy_async_smem();
@@ -253,9 +271,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           double acc[32];
 #pragma unroll
           for (int i = 0; i < 32; ++i) acc[i] = 0.0;
-          // limb accumulators: all NP planes for dosage weights, the three
-          // correction limbs in the missing pass (its plane 3 is the count)
-          constexpr uint32_t kSum = MISSING ? 3u : uint32_t(NP);
+          // limb planes of this pass's sum (the member plane, when present, is last)
+          constexpr uint32_t kSum = COUNT_LAST ? uint32_t(NP) - 1u : uint32_t(NP);
 #pragma unroll
           for (uint32_t j = 0; j < kSum; ++j) {
             uint32_t r[32];
@@ -266,9 +283,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
 #pragma unroll
           for (int i = 0; i < 32; ++i) ps[32 * cb + i] += acc[i];
-          if (MISSING) {
+          if (COUNT_LAST) {
             uint32_t r[32];
-            tmem_ld32(lane_base + 3 * kTcN + 32 * cb, r);
+            tmem_ld32(lane_base + (NP - 1) * kTcN + 32 * cb, r);
             tmem_ld_wait();
 #pragma unroll
             for (int i = 0; i < 32; ++i) pc[32 * cb + i] += __float2uint_rn(__uint_as_float(r[i]));
@@ -323,7 +340,8 @@ __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uin
 }
 
 // out[o*K + k] = init[k] + part_sum[k][slot(fam(o))]; slot(f) is the operand
-// row of person f: tile (f / 128), row 32*(f%4) + (f%128)/4.
+// row of person f: tile (f / 256), row 128*h + 32*(r%4) + (r%128)/4 with
+// r = f % 256 and h = r / 128.
 __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt, uint64_t P_pad,
                                 const double* init, const uint32_t* out_to_fam, uint64_t P,
                                 uint64_t K, double* sums, uint32_t* counts) {
@@ -331,8 +349,8 @@ __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt
   if (x >= P * K) return;
   const uint64_t o = x / K, k = x % K;
   const uint64_t f = out_to_fam ? out_to_fam[o] : o;
-  const uint64_t r = f % kTcN;
-  const uint64_t slot = (f / kTcN) * kTcN + 32 * (r % 4) + r / 4;
+  const uint64_t r = f % kTcN, h = r / 128, rr = r % 128;
+  const uint64_t slot = (f / kTcN) * kTcN + 128 * h + 32 * (rr % 4) + rr / 4;
   sums[x] = init[k] + part_sum[k * P_pad + slot];
   counts[x] = part_cnt[k * P_pad + slot];
 }
@@ -450,23 +468,25 @@ __global__ void __launch_bounds__(kBwThreads)
 
 // ---- host ------------------------------------------------------------------------
 
-template <int NP, int ST, bool MISSING>
+template <int NP, int ST, bool MISSING, bool COUNT_LAST>
 static cudaError_t launch_tc(const CUtensorMap& amap, const CUtensorMap& pmap, const TcArgs& a,
                              uint32_t ptiles, uint32_t stiles, cudaStream_t s) {
   using L = TcSmem<NP, ST>;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(gnm_tc_accumulate<NP, ST, MISSING>,
+    cudaError_t e = cudaFuncSetAttribute(gnm_tc_accumulate<NP, ST, MISSING, COUNT_LAST>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(L::kTotal));
     if (e != cudaSuccess) return e;
     attr = true;
   }
   const dim3 grid = a.raster ? dim3(stiles, ptiles) : dim3(ptiles, stiles);
-  gnm_tc_accumulate<NP, ST, MISSING><<<grid, kTcThreads, L::kTotal, s>>>(amap, pmap, a);
+  gnm_tc_accumulate<NP, ST, MISSING, COUNT_LAST><<<grid, kTcThreads, L::kTotal, s>>>(amap, pmap,
+                                                                                     a);
   return cudaGetLastError();
 }
 
+// 4 limb planes [4][K_pad][V_pad]; a box holds `np` consecutive planes.
 static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, uint64_t K_pad,
                                   uint32_t np) {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -480,7 +500,7 @@ static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, u
     fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
   }
   CUtensorMap map;
-  cuuint64_t dims[3] = {V_pad, K_pad, np};
+  cuuint64_t dims[3] = {V_pad, K_pad, 4};
   cuuint64_t strides[2] = {V_pad * 2, K_pad * V_pad * 2};
   cuuint32_t box[3] = {kTcK, kTcM, np};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -554,8 +574,8 @@ void tensor_plan_create(gnm_plan* p) {
     check_cuda(cudaGetLastError(), "plane build launch");
   }
   check_cuda(cudaDeviceSynchronize(), "plane build");
-  t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, 4);
-  t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, 4);
+  t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcPlanes);
+  t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcPlanes);
 }
 
 void tensor_plan_destroy(gnm_plan* p) {
@@ -590,11 +610,24 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
   a.err = p->d_err;
   a.raster = p->raster;
   if (a.raster && t->ptiles > 65535u) a.raster = 0;  // grid.y limit
-  check_cuda((launch_tc<4, 2, false>(t->map_dos, pmap, a, t->ptiles, t->stiles, s)),
+  // dosage limbs 0-1 and 2-3, then correction limbs 0-1 and (limb 2, count)
+  a.z0 = 0;
+  check_cuda((launch_tc<kTcPlanes, kTcStages, false, false>(t->map_dos, pmap, a, t->ptiles,
+                                                            t->stiles, s)),
              "tensor dosage launch");
-  check_cuda((launch_tc<4, 2, true>(t->map_mis, pmap, a, t->ptiles, t->stiles, s)),
+  a.z0 = 2;
+  check_cuda((launch_tc<kTcPlanes, kTcStages, false, false>(t->map_dos, pmap, a, t->ptiles,
+                                                            t->stiles, s)),
+             "tensor dosage launch");
+  a.z0 = 0;
+  check_cuda((launch_tc<kTcPlanes, kTcStages, true, false>(t->map_mis, pmap, a, t->ptiles,
+                                                           t->stiles, s)),
              "tensor missing launch");
-  p->launches += 2;
+  a.z0 = 2;
+  check_cuda((launch_tc<kTcPlanes, kTcStages, true, true>(t->map_mis, pmap, a, t->ptiles,
+                                                          t->stiles, s)),
+             "tensor missing launch");
+  p->launches += 4;
 }
 
 void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_baseline,
