@@ -106,3 +106,49 @@ def test_tensor_matches_plain(cuda):
     p = run(PipelineContext(prep), rows.reshape(-1), engine=_lib.ENGINE_PLAIN)
     np.testing.assert_array_equal(t[1], p[1])
     assert oracle.rel_err(t[0], p[0]).max() < 1e-6
+
+
+def _condition(prep, rows):
+    """sum_v |w'_vk d_pv| + |corr_vk| m_pv per (p, k): the scale of each sum's terms."""
+    from gnomon_b200 import synth
+    P, K, V = prep.total_people_in_fam, prep.num_scores, prep.num_reconciled_variants
+    codes = synth.unpack_codes(rows, P).astype(np.int64)       # [V, P]
+    d = np.where(codes == 2, 1.0, np.where(codes == 3, 2.0, 0.0))
+    m = (codes == 1).astype(np.float64)
+    W = np.zeros((V, K))
+    C = np.zeros((V, K))
+    offs = prep.sparse_row_offsets.astype(np.int64)
+    vrow = np.repeat(np.arange(V), np.diff(offs))
+    W[vrow, prep.sparse_score_columns] = np.abs(prep.sparse_weights)
+    C[vrow, prep.sparse_score_columns] = np.abs(prep.sparse_missing_corrections)
+    return (d.T @ W + m.T @ C).reshape(-1)
+
+
+@pytest.mark.parametrize("config,people,variants", [("plain_2k_x_50k", 2000, 50_000),
+                                                    ("bandwidth_50k_x_1m", 4096, 100_000),
+                                                    ("batched_100k_x_500k_k512", 256, 40_000),
+                                                    ("diff_20k_x_200k_k16", 1024, 50_000),
+                                                    ("biobank_500k_x_1p2m_k64", 512, 60_000)])
+def test_error_report_workload_subsets(cuda, config, people, variants):
+    """Error report of both engines on the named workloads (the 2,000 x 50,000
+    one at full size, the others as subsets with all of their scores): max
+    relative error (the reference's metric) and, for the split-BF16 engine,
+    the error relative to the sum of |terms|, against the extended-precision
+    oracle.  Printed as one ERROR_REPORT line per workload (pytest -s)."""
+    import json
+    _, prep, rows, _ = synth_case(people, variants, scores=None, config=config)
+    s, c = host_run(prep, rows)
+    es, ec = oracle.score_extended(rows, prep)
+    np.testing.assert_array_equal(c, ec)
+    rel = oracle.rel_err(s, es)
+    cond = np.abs(s - es) / np.maximum(_condition(prep, rows), 1e-300)
+    ps, pc = run(PipelineContext(prep), np.ascontiguousarray(rows).reshape(-1),
+                 engine=_lib.ENGINE_PLAIN)
+    print("ERROR_REPORT " + json.dumps({
+        "workload": config, "people": people, "variants": variants,
+        "scores": prep.num_scores, "tensor_max_rel_err": float(rel.max()),
+        "tensor_max_err_over_sum_abs_terms": float(cond.max()),
+        "plain_max_rel_err": float(oracle.rel_err(ps, es).max())}))
+    assert rel.max() < TOL
+    np.testing.assert_array_equal(pc, ec)
+    assert oracle.within_reference_tolerance(ps, es).all()
