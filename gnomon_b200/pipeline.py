@@ -22,24 +22,31 @@ from typing import Callable, Optional, Union
 import numpy as np
 
 from . import _lib
+from .checkpoint import ScoreCheckpoint, ScoreCheckpointWriter
 from .prepare import PreparationResult
 
 PLINK_MAGIC = bytes([0x6C, 0x1B, 0x01])
 
 
 @dataclass
-class ScoreCheckpoint:
-    """Resume state (score/checkpoint.rs:293-340)."""
-
-    completed_variants: int
-    sum_scores: np.ndarray      # f64 [P*K]
-    missing_counts: np.ndarray  # u32 [P*K]
-
-
-@dataclass
 class PipelineContext:
+    """pipeline.rs:408-446: the prepared inputs, an optional checkpoint to
+    resume from, and where / under which fingerprint to write checkpoints
+    while scoring (``with_checkpoint``)."""
+
     prep_result: PreparationResult
     checkpoint: Optional[ScoreCheckpoint] = None
+    checkpoint_path: Optional[Path] = None
+    checkpoint_fingerprint: Optional[bytes] = None
+
+    @classmethod
+    def with_checkpoint(cls, prep_result: PreparationResult,
+                        checkpoint: Optional[ScoreCheckpoint], checkpoint_path,
+                        checkpoint_fingerprint: bytes) -> "PipelineContext":
+        return cls(prep_result, checkpoint, Path(checkpoint_path), checkpoint_fingerprint)
+
+    def checkpoint_completed_variants(self) -> int:
+        return self.checkpoint.completed_variants if self.checkpoint is not None else 0
 
 
 class PipelineError(RuntimeError):
@@ -136,13 +143,27 @@ def try_run_cuda(context: PipelineContext, bed, engine: int = _lib.ENGINE_AUTO,
     opts.engine = engine
     opts.device = device
     opts.block_variants = block_variants
-    if on_block is not None:
+    # checkpoints after each variant block, forced when the last one completes
+    # (cuda_backend.rs:1638-1648, 1969-2011, 2335-2352)
+    writer = None
+    if context.checkpoint_path is not None and context.checkpoint_fingerprint is not None:
+        writer = ScoreCheckpointWriter(context.checkpoint_path, context.checkpoint_fingerprint,
+                                       prep.num_reconciled_variants)
+    cb_errors = []
+    if on_block is not None or writer is not None:
+        V = prep.num_reconciled_variants
+
         def _cb(_ctx, done, s_ptr, c_ptr):
             s = np.ctypeslib.as_array(C.cast(s_ptr, C.POINTER(C.c_double)), shape=(P * K,))
             c = np.ctypeslib.as_array(C.cast(c_ptr, C.POINTER(C.c_uint32)), shape=(P * K,))
             try:
-                return 0 if on_block(int(done), s, c) is not False else 1
-            except Exception:
+                if writer is not None:
+                    writer.maybe_save(int(done), s, c, force=int(done) >= V)
+                if on_block is not None and on_block(int(done), s, c) is False:
+                    return 1
+                return 0
+            except Exception as e:  # noqa: BLE001 - reported after the call returns
+                cb_errors.append(e)
                 return 1
         opts.on_block = _lib.BLOCK_CB(_cb)
     err = _lib.gnm_error()
@@ -150,6 +171,9 @@ def try_run_cuda(context: PipelineContext, bed, engine: int = _lib.ENGINE_AUTO,
                               C.byref(opts), sums.ctypes.data, counts.ctypes.data, C.byref(err))
     if st == _lib.GNM_DECLINED:
         return None
+    if cb_errors and isinstance(cb_errors[0], OSError):
+        raise PipelineError("Io", f"Failed to write score checkpoint: {cb_errors[0]}",
+                            _lib.GNM_ERR_IO) from cb_errors[0]
     if st != _lib.GNM_OK:
         raise PipelineError(_KIND.get(st, "Compute"), err.message.decode(errors="replace"), st)
     return sums, counts

@@ -41,6 +41,10 @@ class PreparationResult:
     baseline: Optional[np.ndarray] = None               # f64 [K]
     score_variant_counts: Optional[np.ndarray] = None   # u32 [K]
     final_person_iids: Optional[list] = None
+    # read only by the checkpoint fingerprint (checkpoint.rs:83-121)
+    total_variants_in_bim: Optional[int] = None
+    required_is_complex: Optional[np.ndarray] = None        # u8 [V]
+    pipeline_kind: Optional[object] = None                  # .bed path or fileset boundaries
 
     def __post_init__(self):
         self.sparse_weights = np.ascontiguousarray(self.sparse_weights, dtype=np.float32)

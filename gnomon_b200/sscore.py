@@ -11,6 +11,7 @@ the header when score regions are given.
 from __future__ import annotations
 
 import os
+import time
 from pathlib import Path
 from typing import Optional, Sequence
 
@@ -31,38 +32,86 @@ def averages(sums: np.ndarray, missing: np.ndarray, score_variant_counts: np.nda
     return avg, pct
 
 
-def _fmt64(x: float) -> str:
-    r = repr(float(x))
-    return r.replace("e-0", "e-").replace("e+0", "e").replace("e+", "e")
+def _shortest(x, single: bool) -> tuple[str, int]:
+    """(digits, k) with |x| = int(digits) * 10**k and the fewest digits that
+    read back to the same float64 (float32 when ``single``)."""
+    t = np.float32(x) if single else np.float64(x)
+    m, e = np.format_float_scientific(abs(t), unique=True, exp_digits=1).split("e")
+    digits = m.replace(".", "").rstrip("0") or "0"
+    return digits, int(e) - (len(digits) - 1)
 
 
-def _fmt32(x: np.float32) -> str:
-    return _fmt64(float(np.format_float_positional(np.float32(x), unique=True, trim="0")
-                        if np.isfinite(x) else x))
+def _ryu(x, single: bool) -> str:
+    """Text of one value as the ryu crate (1.0.x) prints it: shortest
+    round-trip digits, laid out as ``d.0`` / ``dd.dd`` / ``0.000dd`` when the
+    decimal exponent is small (float64: point position -5 < kk <= 16; float32:
+    -6 < kk <= 13) and ``d.ddde<exp>`` otherwise."""
+    v = float(np.float32(x)) if single else float(x)
+    if v != v:
+        return "NaN"
+    if v in (float("inf"), float("-inf")):
+        return "inf" if v > 0 else "-inf"
+    sign = "-" if np.signbit(v) else ""
+    if v == 0.0:
+        return sign + "0.0"
+    digits, k = _shortest(v, single)
+    hi, lo = (13, -6) if single else (16, -5)
+    n = len(digits)
+    kk = n + k          # 10^(kk-1) <= |v| < 10^kk
+    if 0 <= k and kk <= hi:
+        body = digits + "0" * k + ".0"
+    elif 0 < kk <= hi:
+        body = digits[:kk] + "." + digits[kk:]
+    elif lo < kk <= 0:
+        body = "0." + "0" * (-kk) + digits
+    elif n == 1:
+        body = f"{digits}e{kk - 1}"
+    else:
+        body = f"{digits[0]}.{digits[1:]}e{kk - 1}"
+    return sign + body
+
+
+def format_f64(x: float) -> str:
+    return _ryu(x, single=False)
+
+
+def format_f32(x) -> str:
+    return _ryu(x, single=True)
 
 
 def write_sscore(path, person_iids: Sequence[str], score_names: Sequence[str],
                  score_variant_counts, sums, missing,
                  score_regions: Optional[dict] = None) -> None:
-    """Write the .sscore table atomically (temp file + rename, like the reference)."""
+    """Write the .sscore table atomically: a unique temporary file in the same
+    directory, fsynced, renamed over the target (main.rs:1398-1548)."""
     avg, pct = averages(sums, missing, score_variant_counts)
     path = Path(path)
-    tmp = path.with_name(f".{path.name}.{os.getpid()}.tmp")
-    with open(tmp, "w") as f:
-        if score_regions:
-            wrote = False
-            for name in score_names:
-                if name in score_regions:
-                    if not wrote:
-                        f.write("#REGION\tSCORE\tINTERVAL\n")
-                        wrote = True
-                    f.write(f"#REGION\t{name}\t{score_regions[name]}\n")
-        f.write("#IID" + "".join(f"\t{n}_AVG\t{n}_MISSING_PCT" for n in score_names) + "\n")
-        for p, iid in enumerate(person_iids):
-            cells = "".join(f"\t{_fmt64(avg[p, k])}\t{_fmt32(pct[p, k])}"
-                            for k in range(len(score_names)))
-            f.write(f"{iid}{cells}\n")
-    os.replace(tmp, path)
+    tmp = path.with_name(f".{path.name}.{os.getpid()}.{time.time_ns()}.tmp")
+    fd = os.open(tmp, os.O_WRONLY | os.O_CREAT | os.O_EXCL, 0o644)
+    try:
+        with os.fdopen(fd, "w") as f:
+            if score_regions:
+                wrote = False
+                for name in score_names:
+                    if name in score_regions:
+                        if not wrote:
+                            f.write("#REGION\tSCORE\tINTERVAL\n")
+                            wrote = True
+                        f.write(f"#REGION\t{name}\t{score_regions[name]}\n")
+            f.write("#IID" + "".join(f"\t{n}_AVG\t{n}_MISSING_PCT" for n in score_names) + "\n")
+            for p, iid in enumerate(person_iids):
+                cells = "".join(f"\t{format_f64(avg[p, k])}\t{format_f32(pct[p, k])}"
+                                for k in range(len(score_names)))
+                f.write(f"{iid}{cells}\n")
+            f.flush()
+            os.fsync(f.fileno())
+        os.replace(tmp, path)
+    except BaseException:
+        try:
+            os.unlink(tmp)
+        except OSError:
+            pass
+        raise
 
 
 def read_sscore(path):

@@ -260,3 +260,33 @@ def test_cuda_graph_replay_and_autotune(cuda, engine):
     np.testing.assert_array_equal(c1.cpu().numpy(), c0)
     assert oracle.rel_err(s1.cpu().numpy(), s0).max() < 1e-6
     plan.close()
+
+
+@pytest.mark.parametrize("engine", [PLAIN, _lib.ENGINE_TENSOR])
+def test_checkpoint_file_interrupt_and_resume(cuda, tmp_path, engine):
+    """A run with a checkpoint path writes gnomon-format checkpoints after its
+    variant blocks; a run aborted after the second block leaves the first
+    block's checkpoint on disk (saves are at most every 30 s), and resuming
+    from that file gives the uninterrupted result.  A completed run leaves a
+    final checkpoint equal to its output."""
+    from gnomon_b200 import checkpoint as ck
+    _, prep, rows, _ = synth_case(2500, 1000, scores=3, config="diff_20k_x_200k_k16")
+    flat = rows.reshape(-1)
+    full = run(PipelineContext(prep), flat, engine=engine, block_variants=320)
+    fp = ck.fingerprint_preparation(prep)
+    path = tmp_path / "cohort.sscore.gnomon-checkpoint.bin"
+
+    ctx = PipelineContext.with_checkpoint(prep, None, path, fp)
+    with pytest.raises(PipelineError):
+        run(ctx, flat, engine=engine, block_variants=320, on_block=lambda n, s, c: n < 640)
+    saved = ck.load_checkpoint(path, fp, prep.num_people_to_score * prep.num_scores, 1000)
+    assert saved.completed_variants == 320
+
+    resumed = run(PipelineContext.with_checkpoint(prep, saved, path, fp), flat, engine=engine,
+                  block_variants=320)
+    np.testing.assert_array_equal(resumed[1], full[1])
+    assert oracle.within_reference_tolerance(resumed[0], full[0]).all()
+    final = ck.load_checkpoint(path, fp, prep.num_people_to_score * prep.num_scores, 1000)
+    assert final.completed_variants == 1000
+    np.testing.assert_array_equal(final.sum_scores, resumed[0])
+    np.testing.assert_array_equal(final.missing_counts, resumed[1])
