@@ -787,6 +787,32 @@ gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv,
   });
 }
 
+gnm_status gnm_watchdog_selftest(int device, uint64_t wait_ns, uint64_t* waited_ns_out,
+                                 gnm_error* err) {
+  return guarded(err, [&] {
+    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
+    if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    DeviceGuard g(device);
+    void* d = nullptr;
+    check_cuda(cudaMalloc(&d, 16), "cudaMalloc(watchdog words)");
+    struct Free {
+      void* p;
+      ~Free() { cudaFree(p); }
+    } free_on_exit{d};
+    uint64_t* waited = static_cast<uint64_t*>(d);
+    uint32_t* word = reinterpret_cast<uint32_t*>(static_cast<char*>(d) + 8);
+    check_cuda(cudaMemset(d, 0, 16), "memset");
+    check_cuda(launch_watchdog_probe(wait_ns, word, waited, 0), "watchdog probe launch");
+    check_cuda(cudaDeviceSynchronize(), "watchdog probe");
+    uint64_t host[2] = {0, 0};
+    check_cuda(cudaMemcpy(host, d, 16, cudaMemcpyDeviceToHost), "D2H");
+    if (waited_ns_out) *waited_ns_out = host[0];
+    if (uint32_t(host[1]) & kErrTmaTimeout)
+      fail(GNM_ERR_TIMEOUT, "device watchdog: a bounded wait expired after " +
+                                std::to_string(host[0]) + " ns (self-test)");
+  });
+}
+
 gnm_status gnm_synth_fill_device(uint8_t* d_rows, uint64_t pitch, uint64_t v0, uint64_t nv,
                                  uint64_t i0, uint64_t np, const uint32_t* d_thr, uint64_t seed,
                                  void* stream, gnm_error* err) {

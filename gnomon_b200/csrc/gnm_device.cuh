@@ -10,8 +10,8 @@
 
 namespace gnm {
 
-// ~2^24 polls with a 32-256 ns back-off: several seconds before giving up.
-constexpr uint32_t kWaitPolls = 1u << 24;
+// Every device wait gives up after this long (measured on the global timer).
+constexpr uint64_t kWaitLimitNs = 2000000000ull;   // 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -50,17 +50,34 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait on phase `parity` of an mbarrier.  Returns false on expiry.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  uint32_t ns = 32;
-  for (uint32_t i = 0; i < kWaitPolls; ++i) {
+__device__ __forceinline__ uint64_t global_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait on phase `parity` of an mbarrier for at most `limit_ns`.  Returns false
+// on expiry.  The clock is read only after the first polls fail, so a wait that
+// is satisfied at once costs one try_wait.
+__device__ __forceinline__ bool mbar_wait_timed(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+  for (int i = 0; i < 8; ++i)
     if (mbar_try_wait(bar, parity)) return true;
-    if (i > 8) {
-      __nanosleep(ns);
-      if (ns < 256) ns <<= 1;
-    }
+  const uint64_t t0 = global_timer_ns();
+  uint32_t ns = 32;
+  // time is the limit; the iteration cap (2^26 polls, >= 2^26 x 32 ns) only
+  // guarantees an end should the clock not advance
+  for (uint32_t i = 0; i < (1u << 26); ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_timer_ns() - t0 > limit_ns) return false;
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
   }
   return false;
+}
+
+// Bounded wait with the kernels' watchdog limit.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  return mbar_wait_timed(bar, parity, kWaitLimitNs);
 }
 
 // 2D tiled TMA load global -> shared, completion counted on `bar` (bytes).

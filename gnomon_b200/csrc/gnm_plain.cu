@@ -396,7 +396,33 @@ __global__ void gnm_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint6
   reinterpret_cast<uint32_t*>(rows + j * pitch)[w] = word;
 }
 
+// Watchdog self-test: one warp waits on an mbarrier that nothing ever arrives
+// on, with the kernels' bounded-wait helper and a caller-chosen limit.  The
+// wait expires, the kernel records the timeout in the error word the way the
+// scoring kernels do and returns; the context stays usable.
+__global__ void gnm_watchdog_probe(uint64_t limit_ns, uint32_t* err, uint64_t* waited_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    mbar_init(b, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const uint64_t t0 = global_timer_ns();
+  const bool ok = mbar_wait_timed(b, 0, limit_ns);   // phase 0 never completes
+  if (threadIdx.x == 0) {
+    if (!ok) atomicOr(err, kErrTmaTimeout);
+    *waited_ns = global_timer_ns() - t0;
+  }
+}
+
 // ---- host launchers --------------------------------------------------------
+
+cudaError_t launch_watchdog_probe(uint64_t limit_ns, uint32_t* err, uint64_t* waited_ns,
+                                  cudaStream_t s) {
+  gnm_watchdog_probe<<<1, 32, 0, s>>>(limit_ns, err, waited_ns);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s) {
   const uint64_t stages = (a.num_rows + kPlainRows - 1) / kPlainRows;

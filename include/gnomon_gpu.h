@@ -175,6 +175,17 @@ gnm_status gnm_plan_finalize_device(gnm_plan* plan, double* d_sums_out,
 /* Synchronize `stream` and report any device-side watchdog / error flag. */
 gnm_status gnm_plan_sync(gnm_plan* plan, void* stream, gnm_error* err);
 
+/* Device watchdog self-test (no reference counterpart; the reference's GPU
+ * engine has no bounded device waits).  Every wait in this library's kernels
+ * gives up after 2 s, records the expiry in a device error word and returns,
+ * which the host turns into GNM_ERR_TIMEOUT with the context still usable.
+ * This runs that same bounded-wait code on an mbarrier that nothing ever
+ * signals, with a limit of `wait_ns`, on device `device` (-1 = current), and
+ * returns what a scoring call would: GNM_ERR_TIMEOUT once the wait expired.
+ * *waited_ns_out (may be NULL) receives the measured wait. */
+gnm_status gnm_watchdog_selftest(int device, uint64_t wait_ns, uint64_t* waited_ns_out,
+                                 gnm_error* err);
+
 /* One-shot device scoring: reset + accumulate(all V rows) + finalize. */
 gnm_status gnm_score_device(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
                             double* d_sums_out, uint32_t* d_missing_out,

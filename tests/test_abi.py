@@ -60,3 +60,13 @@ def test_declines_without_cuda_device():
     prep, rows = case_prep(known_answer_cases()["engine_cases"][0])
     st, msg = _run(prep, rows)
     assert st == _lib.GNM_DECLINED, msg
+
+
+def test_watchdog_selftest_declines_without_cuda_device():
+    import ctypes as C
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    e = _lib.gnm_error()
+    st = _lib.load().gnm_watchdog_selftest(-1, 1000, None, C.byref(e))
+    assert st == _lib.GNM_DECLINED
