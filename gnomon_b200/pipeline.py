@@ -176,6 +176,17 @@ def try_run_cuda(context: PipelineContext, bed, engine: int = _lib.ENGINE_AUTO,
                             _lib.GNM_ERR_IO) from cb_errors[0]
     if st != _lib.GNM_OK:
         raise PipelineError(_KIND.get(st, "Compute"), err.message.decode(errors="replace"), st)
+    if prep.complex_rules:
+        # multi-row loci, on the CPU after the engine (cuda_backend.rs:1465-1535)
+        from .complex import ComplexResolutionError, GenotypeSource, resolve_complex_variants
+        try:
+            resolve_complex_variants(prep.complex_rules,
+                                     GenotypeSource.single(src.rows, prep.bytes_per_variant),
+                                     prep.output_idx_to_fam_idx, P, prep.score_names, sums,
+                                     counts, prep.final_person_iids)
+        except ComplexResolutionError as e:
+            raise PipelineError(e.kind, str(e), _lib.GNM_ERR_IO if e.kind == "Io"
+                                else _lib.GNM_ERR_COMPUTE) from e
     return sums, counts
 
 

@@ -45,6 +45,8 @@ class PreparationResult:
     total_variants_in_bim: Optional[int] = None
     required_is_complex: Optional[np.ndarray] = None        # u8 [V]
     pipeline_kind: Optional[object] = None                  # .bed path or fileset boundaries
+    # multi-row loci resolved on the CPU after the GPU pass (gnomon_b200.complex)
+    complex_rules: list = field(default_factory=list)
 
     def __post_init__(self):
         self.sparse_weights = np.ascontiguousarray(self.sparse_weights, dtype=np.float32)

@@ -290,3 +290,31 @@ def test_checkpoint_file_interrupt_and_resume(cuda, tmp_path, engine):
     assert final.completed_variants == 1000
     np.testing.assert_array_equal(final.sum_scores, resumed[0])
     np.testing.assert_array_equal(final.missing_counts, resumed[1])
+
+
+@pytest.mark.parametrize("engine", [PLAIN, _lib.ENGINE_TENSOR])
+def test_complex_rules_after_the_engine(cuda, engine):
+    """Multi-row loci are resolved on the CPU after the GPU pass, onto the
+    engine's final sums (cuda_backend.rs:1465-1535): the result equals the
+    engine's output followed by the per-person restatement of the resolver."""
+    from gnomon_b200.complex import GroupedComplexRule, ScoreInfo
+    from test_complex import _per_person_loop
+    _, prep, rows, _ = synth_case(1500, 600, scores=3, config="diff_20k_x_200k_k16")
+    rng = np.random.default_rng(5)
+    rules = []
+    for r in range(12):
+        ctx_rows = rng.choice(600, 3, replace=False)
+        ctxs = [(int(ctx_rows[0]), "A", "G"), (int(ctx_rows[1]), "G", "A"),
+                (int(ctx_rows[2]), "A", "AT")]
+        apps = [ScoreInfo("A", "G", float(np.float32(rng.normal())), k) for k in range(3)]
+        rules.append(GroupedComplexRule(("2", 500 + r), ctxs, apps))
+    base = run(PipelineContext(prep), rows.reshape(-1), engine=engine)
+    p2 = PreparationResult(prep.sparse_weights, prep.sparse_missing_corrections,
+                           prep.sparse_score_columns, prep.sparse_row_offsets, prep.score_names,
+                           1500, complex_rules=rules)
+    got = run(PipelineContext(p2), rows.reshape(-1), engine=engine)
+    S, C = base[0].reshape(1500, 3).copy(), base[1].reshape(1500, 3).copy()
+    codes = synth.unpack_codes(rows, 1500)
+    _per_person_loop(rules, lambda v, f: int(codes[v, f]), np.arange(1500), 3, S, C)
+    np.testing.assert_array_equal(got[0].reshape(1500, 3), S)
+    np.testing.assert_array_equal(got[1].reshape(1500, 3), C)
