@@ -86,6 +86,7 @@ SIGNATURES = {
     "gnm_plan_tuned_shape": (C.c_uint32, [C.c_void_p]),
     "gnm_decode_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_uint64, C.c_void_p, C.POINTER(gnm_error)]),
+    "gnm_release_cached_memory": (C.c_int, [C.c_int, C.POINTER(gnm_error)]),
     "gnm_watchdog_selftest": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_uint64),
                                         C.POINTER(gnm_error)]),
     "gnm_synth_fill_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,

@@ -12,9 +12,12 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -77,11 +80,48 @@ CUtensorMap make_row_map(const uint8_t* d_rows, uint64_t bytes_per_row, uint64_t
   return map;
 }
 
+// Per-device memory pool for every device buffer of the library (plans and
+// gnm_score_run's row blocks, staging and outputs).  Freed buffers stay
+// reserved in the pool, so the next plan or run on the device allocates
+// without mapping memory again (mapping and unmapping a 12.5 GB row block
+// costs tens of milliseconds); gnm_release_cached_memory returns the reserve
+// to the device.
+static cudaMemPool_t run_pool(int dev) {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static cudaMemPool_t pools[kMaxDevices] = {};
+  if (dev < 0 || dev >= kMaxDevices) fail(GNM_ERR_INVALID, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    check_cuda(cudaMemPoolCreate(&pools[dev], &props), "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    check_cuda(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep),
+               "cudaMemPoolSetAttribute");
+  }
+  return pools[dev];
+}
+
+// Plan buffers: allocated on the default stream and made visible to every
+// stream at once; freed by gnm_plan_destroy after a device synchronize.
+void* pool_alloc(int dev, uint64_t bytes, const char* what) {
+  void* ptr = nullptr;
+  check_cuda(cudaMallocFromPoolAsync(&ptr, std::max<uint64_t>(1, bytes), run_pool(dev), 0), what);
+  check_cuda(cudaStreamSynchronize(0), what);
+  return ptr;
+}
+
+void pool_free(void* ptr) {
+  if (ptr) cudaFreeAsync(ptr, 0);
+}
+
 template <class T>
 static T* dalloc(gnm_plan* p, uint64_t n, const char* what) {
-  void* ptr = nullptr;
   const uint64_t bytes = std::max<uint64_t>(1, n * sizeof(T));
-  check_cuda(cudaMalloc(&ptr, bytes), what);
+  void* ptr = pool_alloc(p->device, bytes, what);
   p->device_bytes += bytes;
   return static_cast<T*>(ptr);
 }
@@ -152,14 +192,36 @@ static bool device_available(int device) {
   return device < n;
 }
 
+// Optional phase trace of plan creation and gnm_score_run / gnm_score_run_ex
+// on stderr (environment variable GNM_TRACE set and not "0"): host wall time
+// of each phase, after synchronising the streams it waited on.
+namespace {
+struct PhaseTrace {
+  bool on = false;
+  std::chrono::steady_clock::time_point t0, last;
+  PhaseTrace() {
+    const char* e = std::getenv("GNM_TRACE");
+    on = e && *e && std::strcmp(e, "0") != 0;
+    t0 = last = std::chrono::steady_clock::now();
+  }
+  void mark(const char* phase) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "gnm_trace %-22s %9.3f ms  (total %9.3f ms)\n", phase,
+                 std::chrono::duration<double, std::milli>(now - last).count(),
+                 std::chrono::duration<double, std::milli>(now - t0).count());
+    last = now;
+  }
+};
+}  // namespace
+
 // ---- plan --------------------------------------------------------------------
 static void plain_geometry(gnm_plan* p) {
   p->tiles = uint32_t(std::max<uint64_t>(1, (p->bpv + kPlainTileBytes - 1) / kPlainTileBytes));
   p->part_stride = uint64_t(p->tiles) * kPlainTileBytes * 4;
   int per_sm = 0;
-  cudaDeviceProp prop;
-  check_cuda(cudaGetDeviceProperties(&prop, p->device), "cudaGetDeviceProperties");
-  p->num_sms = prop.multiProcessorCount;
+  check_cuda(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device),
+             "cudaDeviceGetAttribute");
   per_sm = 2;  // __launch_bounds__(256, 2) with ~108 KB of shared memory
   const uint64_t slots = uint64_t(per_sm) * uint64_t(p->num_sms);
   const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
@@ -177,26 +239,48 @@ static void plain_geometry(gnm_plan* p) {
   p->splits_alloc = uint32_t(alloc);
 }
 
-static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep) {
+static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace& trace) {
   p->rec_stride = p->V + kRecordPad;
-  std::vector<float4> rec(p->K * p->rec_stride, make_float4(0.f, 0.f, 0.f, 0.f));
+  std::vector<float4> rec(p->K * p->rec_stride);
   const uint32_t member_bits = 0x55555555u;
   float member_f;
   std::memcpy(&member_f, &member_bits, 4);
-  for (uint64_t v = 0; v < p->V; ++v)
-    for (uint64_t e = prep->sparse_row_offsets[v]; e < prep->sparse_row_offsets[v + 1]; ++e) {
-      const uint32_t k = prep->sparse_score_columns[e];
-      const float w = prep->sparse_weights[e];
-      const float c = prep->sparse_missing_corrections[e];
-      rec[k * p->rec_stride + v] = make_float4(-c, w, 2.0f * w, member_f);
-    }
+  // Host threads over disjoint variant ranges: each clears its variants'
+  // records in every score row and writes their cells.
+  const uint64_t stride = p->rec_stride, V = p->V, K = p->K;
+  auto fill = [&](uint64_t v0, uint64_t v1) {
+    for (uint64_t k = 0; k < K; ++k)
+      std::fill(rec.begin() + k * stride + v0, rec.begin() + k * stride + v1,
+                make_float4(0.f, 0.f, 0.f, 0.f));
+    for (uint64_t v = v0; v < std::min(v1, V); ++v)
+      for (uint64_t e = prep->sparse_row_offsets[v]; e < prep->sparse_row_offsets[v + 1]; ++e) {
+        const uint32_t k = prep->sparse_score_columns[e];
+        const float w = prep->sparse_weights[e];
+        const float c = prep->sparse_missing_corrections[e];
+        rec[k * stride + v] = make_float4(-c, w, 2.0f * w, member_f);
+      }
+  };
+  const uint64_t nthreads = std::min<uint64_t>(
+      std::max(1u, std::thread::hardware_concurrency()), std::max<uint64_t>(1, stride / 65536));
+  if (nthreads <= 1) {
+    fill(0, stride);
+  } else {
+    std::vector<std::thread> pool;
+    const uint64_t per = (stride + nthreads - 1) / nthreads;
+    for (uint64_t t = 0; t < nthreads; ++t)
+      pool.emplace_back(fill, t * per, std::min(stride, (t + 1) * per));
+    for (auto& th : pool) th.join();
+  }
+  trace.mark("  plan: records (host)");
   p->d_records = dalloc<float4>(p, rec.size(), "cudaMalloc(records)");
   check_cuda(cudaMemcpy(p->d_records, rec.data(), rec.size() * sizeof(float4),
                         cudaMemcpyHostToDevice),
              "upload records");
+  trace.mark("  plan: records upload");
   const uint64_t part = p->K * uint64_t(p->splits_alloc) * p->part_stride;
   p->d_part_sum = dalloc<double>(p, part, "cudaMalloc(partial sums)");
   p->d_part_cnt = dalloc<uint32_t>(p, part, "cudaMalloc(partial counts)");
+  trace.mark("  plan: partials");
 
   // Stage tables (the 3-variant lookup tables) of every score, built once on
   // the device while they fit the cache budget; blocks that start on a
@@ -233,7 +317,7 @@ static const uint8_t* plain_tables_for(gnm_plan* p, uint64_t k, uint64_t v0, uin
                             "a multiple of 24 variants");
     check_cuda(cudaStreamSynchronize(s), "stream synchronize");
     if (p->d_tab_scratch) {
-      cudaFree(p->d_tab_scratch);
+      pool_free(p->d_tab_scratch);
       p->device_bytes -= p->tab_scratch_stages * kPlainTableBytes;
       p->d_tab_scratch = nullptr;
       p->tab_scratch_stages = 0;
@@ -252,7 +336,9 @@ static const uint8_t* plain_tables_for(gnm_plan* p, uint64_t k, uint64_t v0, uin
 }
 
 static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, int device) {
+  PhaseTrace trace;
   validate_prep(prep);
+  trace.mark("  plan: validate");
   if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
   if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
   DeviceGuard g(device);
@@ -291,6 +377,7 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
     p->d_err = dalloc<uint32_t>(p, 1, "cudaMalloc(error word)");
     check_cuda(cudaMemset(p->d_err, 0, 4), "memset");
 
+    trace.mark("  plan: baseline, maps");
     p->h_offs.assign(prep->sparse_row_offsets, prep->sparse_row_offsets + p->V + 1);
     if (nnz) {
       p->h_w.assign(prep->sparse_weights, prep->sparse_weights + nnz);
@@ -299,11 +386,15 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
     }
     if (p->engine == GNM_ENGINE_PLAIN) {
       plain_geometry(p);
-      build_plain_records(p, prep);
+      trace.mark("  plan: csr copy, geometry");
+      build_plain_records(p, prep, trace);
     } else {
       tensor_plan_create(p);
     }
-    check_cuda(cudaDeviceSynchronize(), "plan upload");
+    trace.mark("  plan: weights, tables");
+    // only the default stream: a concurrent run may be streaming rows
+    check_cuda(cudaStreamSynchronize(0), "plan upload");
+    trace.mark("  plan: device sync");
   } catch (...) {
     gnm_plan_destroy(p);
     throw;
@@ -446,7 +537,7 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
 
 // ---- host streaming run ------------------------------------------------------
 struct HostRun {
-  gnm_plan* p;
+  uint64_t bpv;
   const gnm_prep_view* prep;
   const gnm_bed_view* bed;
   uint64_t pitch;
@@ -464,7 +555,7 @@ static bool is_pinned(const void* ptr) {
 
 // Copy rows [v0, v0+n) into dst (pitch layout); zero the padding.
 static void gather_rows(const HostRun& r, uint64_t v0, uint64_t n, uint8_t* dst) {
-  const uint64_t bpv = r.p->bpv;
+  const uint64_t bpv = r.bpv;
   const uint64_t* map = r.prep->required_bim_indices;
   const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
   const unsigned nt = unsigned(std::min<uint64_t>(hw, std::max<uint64_t>(1, n / 256)));
@@ -501,6 +592,40 @@ static void gather_rows(const HostRun& r, uint64_t v0, uint64_t n, uint8_t* dst)
   if (bad == 2) fail(GNM_ERR_PRODUCER, "read_at callback failed");
 }
 
+// Streams and pool buffers of one host run.  Whatever way the run ends, the
+// streams are drained before the buffers go back to the pool.
+struct RunResources {
+  int dev = 0;
+  cudaStream_t cs = nullptr, xs = nullptr, rs = nullptr;   // compute, copy, repitch
+  std::vector<void*> bufs;
+  explicit RunResources(int d) : dev(d) {
+    check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+    check_cuda(cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking), "stream");
+    check_cuda(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking), "stream");
+  }
+  template <class T>
+  T* alloc(uint64_t bytes, const char* what) {
+    void* ptr = nullptr;
+    check_cuda(cudaMallocFromPoolAsync(&ptr, std::max<uint64_t>(1, bytes), run_pool(dev), cs),
+               what);
+    bufs.push_back(ptr);
+    return static_cast<T*>(ptr);
+  }
+  void release() {
+    for (cudaStream_t st : {cs, xs, rs})
+      if (st) cudaStreamSynchronize(st);
+    for (void* b : bufs) cudaFreeAsync(b, cs);
+    bufs.clear();
+    if (cs) cudaStreamSynchronize(cs);
+  }
+  ~RunResources() {
+    release();
+    for (cudaStream_t st : {cs, xs, rs})
+      if (st) cudaStreamDestroy(st);
+  }
+};
+
+
 static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
                           const gnm_resume* resume, const gnm_run_options* opts,
                           double* sums_out, uint32_t* missing_out) {
@@ -510,34 +635,31 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   o.engine = GNM_ENGINE_AUTO;
   o.device = -1;
   if (opts) o = *opts;
-  gnm_plan* p = plan_create_impl(prep, o.engine, o.device);
-  struct PlanOwner {
-    gnm_plan* p;
-    ~PlanOwner() { gnm_plan_destroy(p); }
-  } owner{p};
-  DeviceGuard g(p->device);
+  PhaseTrace trace;
+  validate_prep(prep);
+  int device = o.device;
+  if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
+  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  DeviceGuard g(device);
+  const gnm_engine engine =
+      o.engine == GNM_ENGINE_AUTO
+          ? (prep->num_scores > kTensorMinScores ? GNM_ENGINE_TENSOR : GNM_ENGINE_PLAIN)
+          : o.engine;
 
-  const uint64_t P = p->P, K = p->K, V = p->V;
+  const uint64_t P = prep->num_people, K = prep->num_scores, V = prep->num_variants;
+  const uint64_t bpv = prep->bytes_per_variant;
   const uint64_t v_start = resume ? resume->completed_variants : 0;
   if (v_start > V) fail(GNM_ERR_INVALID, "resume.completed_variants exceeds num_variants");
   if (resume && (!resume->sums || !resume->counts))
     fail(GNM_ERR_INVALID, "resume state has NULL buffers");
-  const uint64_t pitch = (p->bpv + 127) / 128 * 128;
+  const uint64_t pitch = (bpv + 127) / 128 * 128;
   // tensor-engine blocks start on 64-variant boundaries; rows between the
   // boundary and the resume point are staged as zeros (they contribute nothing)
-  const uint64_t v_first = p->engine == GNM_ENGINE_TENSOR ? v_start - v_start % 64 : v_start;
-  HostRun r{p, prep, bed, pitch, v_start};
+  const uint64_t v_first = engine == GNM_ENGINE_TENSOR ? v_start - v_start % 64 : v_start;
+  HostRun r{bpv, prep, bed, pitch, v_start};
 
-  cudaStream_t cs = nullptr, xs = nullptr;
-  check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
-  check_cuda(cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking), "stream");
-  struct Streams {
-    cudaStream_t a, b;
-    ~Streams() {
-      cudaStreamDestroy(a);
-      cudaStreamDestroy(b);
-    }
-  } st_owner{cs, xs};
+  RunResources res(device);
+  cudaStream_t cs = res.cs, xs = res.xs, rs = res.rs;
 
   // Block size: everything if it fits in ~60% of free memory, else two
   // alternating blocks of block_variants rows.
@@ -548,34 +670,29 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   const uint64_t cap_rows = std::max<uint64_t>(kPlainRows, uint64_t(0.6 * double(free_b)) / pitch);
   if (!o.block_variants && block > cap_rows) block = std::max<uint64_t>(kPlainRows, cap_rows / 2);
   block = std::max<uint64_t>(1, std::min<uint64_t>(block, std::max<uint64_t>(1, remaining)));
-  if (p->engine == GNM_ENGINE_TENSOR) block = (block + 63) / 64 * 64;
+  if (engine == GNM_ENGINE_TENSOR) block = (block + 63) / 64 * 64;
   const int nbuf = remaining > block ? 2 : 1;
 
   std::vector<uint8_t*> dbuf(nbuf, nullptr);
-  struct DevBufs {
-    std::vector<uint8_t*>& v;
-    ~DevBufs() {
-      for (auto* b : v) cudaFree(b);
-    }
-  } db_owner{dbuf};
-  for (int i = 0; i < nbuf; ++i)
-    check_cuda(cudaMalloc(&dbuf[i], block * pitch), "cudaMalloc(row block)");
-  double* d_sums = nullptr;
-  uint32_t* d_cnt = nullptr;
-  check_cuda(cudaMalloc(&d_sums, std::max<uint64_t>(1, P * K) * sizeof(double)), "cudaMalloc(sums)");
-  check_cuda(cudaMalloc(&d_cnt, std::max<uint64_t>(1, P * K) * sizeof(uint32_t)), "cudaMalloc(counts)");
-  struct OutBufs {
-    double* a;
-    uint32_t* b;
-    ~OutBufs() {
-      cudaFree(a);
-      cudaFree(b);
-    }
-  } ob_owner{d_sums, d_cnt};
+  for (int i = 0; i < nbuf; ++i) dbuf[i] = res.alloc<uint8_t>(block * pitch, "row block");
+  double* d_sums = res.alloc<double>(P * K * sizeof(double), "sums");
+  uint32_t* d_cnt = res.alloc<uint32_t>(P * K * sizeof(uint32_t), "counts");
 
-  // Direct path: identity rows from pinned memory -> one 2D copy per block.
+  // Direct path: identity rows from pinned memory, copied in 128 MB chunks
+  // with at most two in flight (so other copies, like the plan's weight
+  // upload, are not queued behind the whole matrix).  Rows whose length is
+  // not the device pitch go back to back into a device staging ring (the
+  // link's full rate; a pitched 2D copy runs ~5% slower) and are re-pitched
+  // on the device, each chunk's repitch overlapping the next chunk's copy.
   const bool identity = prep->required_bim_indices == nullptr;
   const bool direct = identity && bed->data && is_pinned(bed->data);
+  if (direct && V * bpv > bed->data_len)
+    fail(GNM_ERR_IO, "truncated .bed: a required row lies past the end of the data");
+  const bool repitch = direct && pitch != bpv;
+  const uint64_t rpc = std::max<uint64_t>(1, (uint64_t(128) << 20) / std::max<uint64_t>(1, bpv));
+  uint8_t* staging[2] = {nullptr, nullptr};
+  if (repitch)
+    for (int i = 0; i < 2; ++i) staging[i] = res.alloc<uint8_t>(rpc * bpv, "staging");
   const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(block, (uint64_t(128) << 20) / pitch));
   uint8_t* pinned[2] = {nullptr, nullptr};
   struct Pinned {
@@ -588,45 +705,65 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   if (!direct)
     for (int i = 0; i < 2; ++i)
       check_cuda(cudaHostAlloc(&pinned[i], chunk * pitch, cudaHostAllocDefault), "cudaHostAlloc");
-  cudaEvent_t copied[2], consumed[2], staged[2];
+  check_cuda(cudaStreamSynchronize(cs), "pool allocations");
+
+  // copied: block rows are in dbuf; consumed: compute done with dbuf;
+  // staged: host staging buffer free; landed / repitched: device staging
+  // buffer filled / drained
+  cudaEvent_t copied[2], consumed[2], staged[2], landed[2], repitched[2];
+  struct Events {
+    cudaEvent_t* e[5];
+    ~Events() {
+      for (auto* a : e)
+        for (int i = 0; i < 2; ++i)
+          if (a[i]) cudaEventDestroy(a[i]);
+    }
+  } ev_owner{{copied, consumed, staged, landed, repitched}};
+  for (auto* a : ev_owner.e) a[0] = a[1] = nullptr;
   for (int i = 0; i < 2; ++i) {
-    check_cuda(cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming), "event");
-    check_cuda(cudaEventCreateWithFlags(&consumed[i], cudaEventDisableTiming), "event");
-    check_cuda(cudaEventCreateWithFlags(&staged[i], cudaEventDisableTiming), "event");
+    for (auto* a : ev_owner.e)
+      check_cuda(cudaEventCreateWithFlags(&a[i], cudaEventDisableTiming), "event");
     check_cuda(cudaEventRecord(consumed[i], cs), "event");
     check_cuda(cudaEventRecord(staged[i], xs), "event");
+    check_cuda(cudaEventRecord(landed[i], xs), "event");
+    check_cuda(cudaEventRecord(repitched[i], rs), "event");
   }
-  struct Events {
-    cudaEvent_t* a;
-    cudaEvent_t* b;
-    cudaEvent_t* c;
-    ~Events() {
-      for (int i = 0; i < 2; ++i) {
-        cudaEventDestroy(a[i]);
-        cudaEventDestroy(b[i]);
-        cudaEventDestroy(c[i]);
-      }
-    }
-  } ev_owner{copied, consumed, staged};
+  trace.mark("buffers");
 
-  plan_reset_impl(p, cs);
+  // Rows of block [b0, b0 + nb) into dbuf[slot]; copied[slot] fires when they are in.
   uint64_t stage_idx = 0;
-  std::vector<double> cb_sums;
-  std::vector<uint32_t> cb_cnt;
-  for (uint64_t b0 = v_first, bi = 0; b0 < V; b0 += block, ++bi) {
-    const uint64_t nb = std::min(block, V - b0);
-    const int slot = int(bi % nbuf);
-    // the compute of the block that last used this device buffer must be done
-    check_cuda(cudaStreamWaitEvent(xs, consumed[slot], 0), "wait");
+  auto issue_block = [&](uint64_t b0, uint64_t nb, int slot) {
+    const uint64_t skip = b0 < v_start ? v_start - b0 : 0;
     if (direct) {
-      const uint64_t skip = b0 < v_start ? v_start - b0 : 0;
-      if (skip) check_cuda(cudaMemsetAsync(dbuf[slot], 0, skip * pitch, xs), "zero rows");
-      if (nb > skip)
-        check_cuda(cudaMemcpy2DAsync(dbuf[slot] + skip * pitch, pitch,
-                                     bed->data + (b0 + skip) * p->bpv, p->bpv, p->bpv, nb - skip,
+      cudaStream_t ws = repitch ? rs : xs;        // the stream that writes dbuf
+      check_cuda(cudaStreamWaitEvent(ws, consumed[slot], 0), "wait");
+      if (!repitch) check_cuda(cudaStreamWaitEvent(xs, consumed[slot], 0), "wait");
+      if (skip) check_cuda(cudaMemsetAsync(dbuf[slot], 0, skip * pitch, ws), "zero rows");
+      const uint64_t step = repitch ? rpc : chunk;
+      for (uint64_t c0 = skip; c0 < nb; c0 += step, ++stage_idx) {
+        const uint64_t nc = std::min(step, nb - c0);
+        const int sb = int(stage_idx & 1);
+        check_cuda(cudaEventSynchronize(landed[sb]), "pace copies");   // two chunks in flight
+        const uint8_t* src = bed->data + (b0 + c0) * bpv;
+        if (repitch) {
+          check_cuda(cudaStreamWaitEvent(xs, repitched[sb], 0), "wait");
+          check_cuda(cudaMemcpyAsync(staging[sb], src, nc * bpv, cudaMemcpyHostToDevice, xs),
+                     "H2D rows");
+          check_cuda(cudaEventRecord(landed[sb], xs), "event");
+          check_cuda(cudaStreamWaitEvent(rs, landed[sb], 0), "wait");
+          check_cuda(launch_repitch(staging[sb], bpv, nc, dbuf[slot] + c0 * pitch, pitch, rs),
+                     "repitch launch");
+          check_cuda(cudaEventRecord(repitched[sb], rs), "event");
+        } else {
+          check_cuda(cudaMemcpyAsync(dbuf[slot] + c0 * pitch, src, nc * bpv,
                                      cudaMemcpyHostToDevice, xs),
-                   "H2D rows");
+                     "H2D rows");
+          check_cuda(cudaEventRecord(landed[sb], xs), "event");
+        }
+      }
+      check_cuda(cudaEventRecord(copied[slot], repitch ? rs : xs), "event");
     } else {
+      check_cuda(cudaStreamWaitEvent(xs, consumed[slot], 0), "wait");
       for (uint64_t c0 = 0; c0 < nb; c0 += chunk, ++stage_idx) {
         const uint64_t nc = std::min(chunk, nb - c0);
         const int ps = int(stage_idx & 1);
@@ -637,8 +774,42 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
                    "H2D rows");
         check_cuda(cudaEventRecord(staged[ps], xs), "event");
       }
+      check_cuda(cudaEventRecord(copied[slot], xs), "event");
     }
-    check_cuda(cudaEventRecord(copied[slot], xs), "event");
+  };
+
+  // The plan (weights -> records / stage tables / limb planes on the device)
+  // is built on a helper thread while this thread streams the first block.
+  gnm_plan* p = nullptr;
+  std::exception_ptr plan_error;
+  std::thread planner([&] {
+    try {
+      DeviceGuard pg(device);
+      p = plan_create_impl(prep, engine, device);
+    } catch (...) {
+      plan_error = std::current_exception();
+    }
+  });
+  struct PlanOwner {
+    std::thread& t;
+    gnm_plan*& p;
+    ~PlanOwner() {
+      if (t.joinable()) t.join();
+      gnm_plan_destroy(p);
+    }
+  } owner{planner, p};
+  if (v_first < V) issue_block(v_first, std::min(block, V - v_first), 0);
+  planner.join();
+  if (plan_error) std::rethrow_exception(plan_error);
+  trace.mark("plan + first rows");
+
+  plan_reset_impl(p, cs);
+  std::vector<double> cb_sums;
+  std::vector<uint32_t> cb_cnt;
+  for (uint64_t b0 = v_first, bi = 0; b0 < V; b0 += block, ++bi) {
+    const uint64_t nb = std::min(block, V - b0);
+    const int slot = int(bi % nbuf);
+    if (bi > 0) issue_block(b0, nb, slot);
     check_cuda(cudaStreamWaitEvent(cs, copied[slot], 0), "wait");
     accumulate_impl(p, dbuf[slot], pitch, b0, nb, cs);
     check_cuda(cudaEventRecord(consumed[slot], cs), "event");
@@ -658,6 +829,13 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
         fail(GNM_ERR_PRODUCER, "block callback requested abort");
     }
   }
+  if (trace.on) {   // (tracing serialises the last block's copy and compute)
+    check_cuda(cudaStreamSynchronize(xs), "trace sync");
+    check_cuda(cudaStreamSynchronize(rs), "trace sync");
+    trace.mark("rows host->device");
+    check_cuda(cudaStreamSynchronize(cs), "trace sync");
+    trace.mark("accumulate");
+  }
   finalize_impl(p, d_sums, d_cnt, resume == nullptr, cs);
   check_cuda(cudaMemcpyAsync(sums_out, d_sums, P * K * sizeof(double), cudaMemcpyDeviceToHost, cs),
              "D2H sums");
@@ -665,11 +843,18 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
       cudaMemcpyAsync(missing_out, d_cnt, P * K * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs),
       "D2H counts");
   sync_impl(p, cs);
+  trace.mark("finalize + results");
   if (resume)
     for (uint64_t x = 0; x < P * K; ++x) {
       sums_out[x] += resume->sums[x];
       missing_out[x] += resume->counts[x];
     }
+  if (trace.on) {
+    res.release();
+    gnm_plan_destroy(p);
+    p = nullptr;
+    trace.mark("release");
+  }
 }
 
 }  // namespace gnm
@@ -704,17 +889,15 @@ void gnm_plan_destroy(gnm_plan* p) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(p->device);
+  cudaDeviceSynchronize();   // no kernel of any stream may still use the buffers
   if (p->tensor) tensor_plan_destroy(p);
-  cudaFree(p->d_records);
-  cudaFree(p->d_tables);
-  cudaFree(p->d_tab_scratch);
-  cudaFree(p->d_part_sum);
-  cudaFree(p->d_part_cnt);
-  cudaFree(p->d_baseline);
-  cudaFree(p->d_zero_base);
-  cudaFree(p->d_out_to_fam);
-  cudaFree(p->d_err);
-  cudaFree(p->d_grad_fam);
+  for (void* b : {static_cast<void*>(p->d_records), static_cast<void*>(p->d_tables),
+                  static_cast<void*>(p->d_tab_scratch), static_cast<void*>(p->d_part_sum),
+                  static_cast<void*>(p->d_part_cnt), static_cast<void*>(p->d_baseline),
+                  static_cast<void*>(p->d_zero_base), static_cast<void*>(p->d_out_to_fam),
+                  static_cast<void*>(p->d_err), static_cast<void*>(p->d_grad_fam)})
+    pool_free(b);
+  cudaStreamSynchronize(0);
   if (prev >= 0) cudaSetDevice(prev);
   delete p;
 }
@@ -784,6 +967,15 @@ gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv,
     check_cuda(launch_decode(d_rows, pitch, nv, np, d_out, out_pitch,
                              static_cast<cudaStream_t>(stream)),
                "decode launch");
+  });
+}
+
+gnm_status gnm_release_cached_memory(int device, gnm_error* err) {
+  return guarded(err, [&] {
+    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
+    if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    DeviceGuard g(device);
+    check_cuda(cudaMemPoolTrimTo(run_pool(device), 0), "cudaMemPoolTrimTo");
   });
 }
 

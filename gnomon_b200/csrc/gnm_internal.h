@@ -68,6 +68,8 @@ cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, 
                                     uint32_t splits, cudaStream_t s);
 uint32_t plain_smem_bytes();
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
+cudaError_t launch_repitch(const uint8_t* src, uint64_t bpv, uint64_t nrows, uint8_t* dst,
+                           uint64_t pitch, cudaStream_t s);
 cudaError_t launch_watchdog_probe(uint64_t limit_ns, uint32_t* err, uint64_t* waited_ns,
                                   cudaStream_t s);
 cudaError_t launch_decode(const uint8_t* rows, uint64_t pitch, uint64_t nv, uint64_t np,

@@ -396,6 +396,24 @@ __global__ void gnm_synth_fill(uint8_t* rows, uint64_t pitch, uint64_t v0, uint6
   reinterpret_cast<uint32_t*>(rows + j * pitch)[w] = word;
 }
 
+// Packed rows stored back to back (stride bpv, as in a .bed file) -> rows of
+// `pitch` bytes (a multiple of 16, as TMA needs), zero padded.  One thread
+// per 4-byte output word; byte loads keep unaligned source rows legal and
+// are coalesced across the warp.
+__global__ void gnm_repitch(const uint8_t* src, uint64_t bpv, uint64_t nrows, uint8_t* dst,
+                            uint64_t pitch) {
+  const uint64_t words = pitch / 4;
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nrows * words) return;
+  const uint64_t r = i / words, c = (i % words) * 4;
+  const uint8_t* s = src + r * bpv;
+  uint32_t v = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < 4; ++j)
+    if (c + j < bpv) v |= uint32_t(s[c + j]) << (8 * j);
+  reinterpret_cast<uint32_t*>(dst + r * pitch)[c / 4] = v;
+}
+
 // Watchdog self-test: one warp waits on an mbarrier that nothing ever arrives
 // on, with the kernels' bounded-wait helper and a caller-chosen limit.  The
 // wait expires, the kernel records the timeout in the error word the way the
@@ -417,6 +435,14 @@ __global__ void gnm_watchdog_probe(uint64_t limit_ns, uint32_t* err, uint64_t* w
 }
 
 // ---- host launchers --------------------------------------------------------
+
+cudaError_t launch_repitch(const uint8_t* src, uint64_t bpv, uint64_t nrows, uint8_t* dst,
+                           uint64_t pitch, cudaStream_t s) {
+  if (nrows == 0) return cudaSuccess;
+  const uint64_t n = nrows * (pitch / 4);
+  gnm_repitch<<<uint32_t((n + 255) / 256), 256, 0, s>>>(src, bpv, nrows, dst, pitch);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_watchdog_probe(uint64_t limit_ns, uint32_t* err, uint64_t* waited_ns,
                                   cudaStream_t s) {

@@ -27,6 +27,10 @@ struct DeviceGuard {
   ~DeviceGuard();
 };
 
+// Device buffers of plans come from the library's per-device memory pool.
+void* pool_alloc(int device, uint64_t bytes, const char* what);
+void pool_free(void* ptr);
+
 CUtensorMap make_row_map(const uint8_t* d_rows, uint64_t bytes_per_row, uint64_t num_rows,
                          uint64_t pitch, uint32_t box_x, uint32_t box_y);
 

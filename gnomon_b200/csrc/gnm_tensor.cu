@@ -536,7 +536,7 @@ void tensor_plan_create(gnm_plan* p) {
     }
   const uint64_t plane = t->K_pad * t->V_pad;
   auto alloc = [&](void** ptr, uint64_t bytes, const char* what) {
-    check_cuda(cudaMalloc(ptr, std::max<uint64_t>(1, bytes)), what);
+    *ptr = pool_alloc(p->device, bytes, what);
     p->device_bytes += bytes;
   };
   alloc(reinterpret_cast<void**>(&t->d_planes_dos), 4 * plane * 2, "cudaMalloc(limb planes)");
@@ -550,15 +550,20 @@ void tensor_plan_create(gnm_plan* p) {
   float *dw = nullptr, *dc = nullptr, *dq = nullptr;
   uint32_t* dcol = nullptr;
   uint64_t* doff = nullptr;
-  check_cuda(cudaMalloc(&dw, std::max<uint64_t>(1, nnz) * 4), "cudaMalloc");
-  check_cuda(cudaMalloc(&dc, std::max<uint64_t>(1, nnz) * 4), "cudaMalloc");
-  check_cuda(cudaMalloc(&dcol, std::max<uint64_t>(1, nnz) * 4), "cudaMalloc");
-  check_cuda(cudaMalloc(&doff, (p->V + 1) * 8), "cudaMalloc");
-  check_cuda(cudaMalloc(&dq, t->K_pad * 4), "cudaMalloc");
+  dw = static_cast<decltype(dw)>(
+      pool_alloc(p->device, std::max<uint64_t>(1, nnz) * 4, "plane build inputs"));
+  dc = static_cast<decltype(dc)>(
+      pool_alloc(p->device, std::max<uint64_t>(1, nnz) * 4, "plane build inputs"));
+  dcol = static_cast<decltype(dcol)>(
+      pool_alloc(p->device, std::max<uint64_t>(1, nnz) * 4, "plane build inputs"));
+  doff = static_cast<decltype(doff)>(
+      pool_alloc(p->device, (p->V + 1) * 8, "plane build inputs"));
+  dq = static_cast<decltype(dq)>(
+      pool_alloc(p->device, t->K_pad * 4, "plane build inputs"));
   struct Tmp {
     void* a[5];
     ~Tmp() {
-      for (void* x : a) cudaFree(x);
+      for (void* x : a) pool_free(x);
     }
   } tmp{{dw, dc, dcol, doff, dq}};
   if (nnz) {
@@ -573,7 +578,7 @@ void tensor_plan_create(gnm_plan* p) {
         dw, dc, dcol, doff, p->V, dq, t->d_planes_dos, t->d_planes_mis, t->K_pad, t->V_pad);
     check_cuda(cudaGetLastError(), "plane build launch");
   }
-  check_cuda(cudaDeviceSynchronize(), "plane build");
+  check_cuda(cudaStreamSynchronize(0), "plane build");
   t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcPlanes);
   t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcPlanes);
 }
@@ -581,10 +586,10 @@ void tensor_plan_create(gnm_plan* p) {
 void tensor_plan_destroy(gnm_plan* p) {
   TensorPlan* t = p->tensor;
   if (!t) return;
-  cudaFree(t->d_planes_dos);
-  cudaFree(t->d_planes_mis);
-  cudaFree(t->d_part_sum);
-  cudaFree(t->d_part_cnt);
+  pool_free(t->d_planes_dos);
+  pool_free(t->d_planes_mis);
+  pool_free(t->d_part_sum);
+  pool_free(t->d_part_cnt);
   delete t;
   p->tensor = nullptr;
 }
@@ -653,8 +658,8 @@ void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float
   if (p->d_out_to_fam || p->P != p->fam) {
     // dS rows in .bed person order: zero for people outside the keep set
     if (!p->d_grad_fam) {
-      check_cuda(cudaMalloc(&p->d_grad_fam, std::max<uint64_t>(1, p->fam * p->K) * 4),
-                 "cudaMalloc(fam-order gradient)");
+      p->d_grad_fam = static_cast<float*>(
+          pool_alloc(p->device, std::max<uint64_t>(1, p->fam * p->K) * 4, "fam-order gradient"));
       p->device_bytes += p->fam * p->K * 4;
     }
     check_cuda(cudaMemsetAsync(p->d_grad_fam, 0, p->fam * p->K * 4, s), "memset");

@@ -70,3 +70,12 @@ def test_watchdog_selftest_declines_without_cuda_device():
     e = _lib.gnm_error()
     st = _lib.load().gnm_watchdog_selftest(-1, 1000, None, C.byref(e))
     assert st == _lib.GNM_DECLINED
+
+
+def test_release_cached_memory_declines_without_cuda_device():
+    import ctypes as C
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    e = _lib.gnm_error()
+    assert _lib.load().gnm_release_cached_memory(-1, C.byref(e)) == _lib.GNM_DECLINED
