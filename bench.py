@@ -46,6 +46,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def peaks_tc():
+    """Sustained dense bf16 tensor-core peak (TFLOP/s) and its source."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["bf16_tflops_sustained"]), "measured"
+    return 1400.0, "fallback"
+
+
 def traffic_from_profile():
     """dram bytes per launch recorded from the ncu capture (profiles/), else None."""
     if not PROFILE.exists():
@@ -332,8 +340,7 @@ def gpu_arm(args, rank, world, local_rank):
         ptiles, kpad, vpad = -(-P // 256), -(-K // 128) * 128, -(-V // 64) * 64
         flops = 2.0 * ptiles * 256 * vpad * kpad * 8
         achieved = flops / (kernel_ms / 1e3) / 1e12
-        pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"] \
-            if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
+        pk = peaks_tc()[0]
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                 "frac": achieved / pk, "traffic": None,
                 "peak_kind": peak_kind + " (bf16 sustained)",
@@ -417,8 +424,19 @@ def gpu_arm(args, rank, world, local_rank):
             "clocks": clocks.summary(),
         }
         if bwd_ms is not None:
-            line["backward"] = {"ms": bwd_ms, "pairs_per_s": P * V * K / (bwd_ms / 1e3),
-                                "kernel": "gnm_backward_kernel"}
+            # tcgen05 GEMM: M = variants (tiles of 128), N = 4 limbs x 16 scores per
+            # score tile, K = people (stages of 64); executed work and packed-row bytes
+            v_pad = -(-V // 128) * 128
+            p_pad = -(-w.people // 64) * 64
+            k_pad = -(-K // 16) * 16
+            bw_flops = 2.0 * v_pad * p_pad * 4 * k_pad
+            bw_tflops = bw_flops / (bwd_ms / 1e3) / 1e12
+            line["backward"] = {
+                "ms": bwd_ms, "pairs_per_s": P * V * K / (bwd_ms / 1e3),
+                "kernel": "gnm_tc_backward (+ dS limb build)",
+                "executed_tflops": bw_tflops,
+                "tensor_frac_of_sustained": bw_tflops / peaks_tc()[0],
+                "row_bytes_gbs": V * bpv * (k_pad // 16) / (bwd_ms / 1e3) / 1e9}
         print(json.dumps(line), flush=True)
     plan.close()
 

@@ -895,7 +895,8 @@ void gnm_plan_destroy(gnm_plan* p) {
                   static_cast<void*>(p->d_tab_scratch), static_cast<void*>(p->d_part_sum),
                   static_cast<void*>(p->d_part_cnt), static_cast<void*>(p->d_baseline),
                   static_cast<void*>(p->d_zero_base), static_cast<void*>(p->d_out_to_fam),
-                  static_cast<void*>(p->d_err), static_cast<void*>(p->d_grad_fam)})
+                  static_cast<void*>(p->d_err), static_cast<void*>(p->d_grad_fam),
+                  static_cast<void*>(p->d_bw)})
     pool_free(b);
   cudaStreamSynchronize(0);
   if (prev >= 0) cudaSetDevice(prev);

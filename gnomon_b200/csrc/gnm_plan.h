@@ -63,6 +63,8 @@ struct gnm_plan {
   uint32_t* d_out_to_fam = nullptr;
   uint32_t* d_err = nullptr;
   float* d_grad_fam = nullptr;     // backward: dS in .bed person order (keep subsets)
+  uint8_t* d_bw = nullptr;         // backward: dS limb rows, FP32 dS, per-score maxima
+  uint64_t bw_bytes = 0;
   std::vector<double> h_baseline;
   uint64_t device_bytes = 0;
   uint64_t launches = 0;

@@ -356,26 +356,288 @@ __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt
 }
 
 // ---- backward: dW[v,k] = sum_p d(p,v) dS[p,k], dC[v,k] = -sum_{p missing} dS[p,k]
-// One thread per variant row, 16 score columns per CTA column block.  dS comes
-// in .bed (fam) person order, [fam][K] (scattered from output order when a keep
-// subset is used); 512-person chunks of the block's 16 columns are staged in
-// shared memory and read as broadcasts, genotypes come straight from the
-// packed row as 16-byte vectors (64 people), and the 16 products per person
-// are two-wide FMAs (fma.rn.f32x2).  FP32 sums per chunk, FP64 across chunks.
-constexpr uint32_t kBwThreads = 128;
-constexpr uint32_t kBwChunk = 512;
+//
+// A tcgen05 GEMM with the variants as M: D[v, n] = sum_p A[v, p] B[n, p].  A is
+// the allele-2 dosage (missing -> 0) re-expanded from the packed rows into BF16
+// by CUDA-core warps; a .bed row is already contiguous along people, so the
+// K-major operand row of a variant is its own row, expanded in place (no
+// transpose).  B holds dS split into four BF16 limbs per score (row
+// n = 16 * limb + score): the hi/mid/lo/lo2 split of the forward planes, each
+// limb an integer multiple of its quantum (q, q/2^8, q/2^16, q/2^24 with
+// 2^E = 256 q >= max_p |dS[p,k]|) with |integer| <= 256, so products with
+// d in {0,1,2} are exact and every partial sum stays exact in FP32 below
+// 32768 people, where the accumulators are flushed to FP64.  The only error
+// left is the limb residual (< 2^-33 of the score's largest |dS|).
+//
+// The missing-call term touches ~1% of the calls, so it is not a second GEMM:
+// the thread that expands a variant row finds the row's code-01 calls with
+// SWAR masks and adds that person's FP32 dS row (staged next to the limbs)
+// into FP32 registers, flushed to FP64 every 4096 people (about 41 terms at
+// 1% missing: the FP32 rounding stays below 3e-6 of the |dS| it sums, which
+// is itself ~1% of the score's sum of |dS|).  Converting every term to FP64
+// instead saturated the conversion pipe.
+//
+// CTA: 128 variants x 16 scores; people in stages of 64 (one 128-byte
+// K-major operand row per variant).  Warp 0 issues TMA (packed rows
+// [128 x 16 bytes], dS limbs [64 x 64] BF16 with 128-byte swizzle, FP32 dS
+// [64 people x 16 scores]), warp 1 owns 64 TMEM columns and issues
+// tcgen05.mma (M = 128, N = 64, K = 16), warps 2-5 expand genotypes (thread =
+// variant row 32 * (warp % 4) + lane, the TMEM lane it later drains) and run
+// the epilogue.  Two CTAs per SM.
+constexpr uint32_t kBwM = 128;                    // variants per CTA (TMEM lanes)
+constexpr uint32_t kBwScores = 16;                // scores per CTA
+constexpr uint32_t kBwN = 4 * kBwScores;          // limb rows = accumulator columns
+constexpr uint32_t kBwK = 64;                     // people per stage
+constexpr uint32_t kBwStages = 3;
+constexpr uint32_t kBwFlush = 512;                // stages per exact FP32 block (32768 people)
+constexpr uint32_t kBwMissFlush = 64;             // stages per FP32 missing-term sum (4096 people)
+constexpr uint32_t kBwThreads = 192;
 
-__device__ __forceinline__ uint64_t fma_f32x2(float d, uint64_t g, uint64_t acc) {
-  uint64_t r;
-  asm("{\n\t.reg .b64 dd;\n\tmov.b64 dd, {%1, %1};\n\tfma.rn.f32x2 %0, dd, %2, %3;\n\t}"
-      : "=l"(r)
-      : "f"(d), "l"(g), "l"(acc));
-  return r;
+struct BwSmem {
+  static constexpr uint32_t kA = kBwM * kBwK * 2;           // 16 KB dosage operand
+  static constexpr uint32_t kB = kBwN * kBwK * 2;           // 8 KB dS limbs
+  static constexpr uint32_t kPk = kBwM * (kBwK / 4);        // 2 KB packed rows
+  static constexpr uint32_t kDs = kBwK * kBwScores * 4;     // 4 KB FP32 dS
+  static constexpr uint32_t kAOff = 0;
+  static constexpr uint32_t kBOff = kAOff + kA;
+  static constexpr uint32_t kPkOff = kBOff + kB;
+  static constexpr uint32_t kDsOff = kPkOff + kPk;
+  static constexpr uint32_t kStage = kDsOff + kDs;           // 30 KB
+  static constexpr uint32_t kBarOff = kBwStages * kStage;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (3 * kBwStages + 2);
+  static constexpr uint32_t kTotal = kHolder + 16 + 1024;    // + alignment slack
+};
+static_assert(BwSmem::kStage % 1024 == 0 && BwSmem::kBOff % 1024 == 0, "operand alignment");
+
+struct BwArgs {
+  uint64_t V, K;
+  uint32_t nstages;   // people stages: P_pad / kBwK
+  float* gw;
+  float* gc;          // may be null
+  uint32_t* err;
+};
+
+// Two BF16 dosages from two codes held in bytes 0 and 1 of y (bytes 2-3 ignored).
+__device__ __forceinline__ uint32_t dos_pair(uint32_t y) {
+  return __byte_perm(kDosLo, kDosHi, y * 0x11u + 0x4040u);
 }
-__device__ __forceinline__ uint64_t sub_f32x2(uint64_t acc, uint64_t g) {
-  uint64_t r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(acc), "l"(g));
-  return r;
+
+__global__ void __launch_bounds__(kBwThreads, 2)
+    gnm_tc_backward(const __grid_constant__ CUtensorMap rmap,
+                    const __grid_constant__ CUtensorMap bmap,
+                    const __grid_constant__ CUtensorMap dmap, BwArgs a) {
+  using L = BwSmem;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sb = smem_u32(smem);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t vtile = blockIdx.x, stile = blockIdx.y;
+  const uint32_t nit = a.nstages;
+  constexpr uint32_t ST = kBwStages;
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
+  auto aready = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
+  auto empty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (2 * ST + s); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < ST; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(aready(s), 128);
+      mbar_init(empty(s), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, 128);
+    *abort_flag = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&rmap);
+    prefetch_tmap(&bmap);
+    prefetch_tmap(&dmap);
+  }
+  if (warp == 1) {
+    tmem_alloc(sb + L::kHolder, kBwN);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + L::kHolder);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        if (!mbar_wait_bounded(empty(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (*abort_flag) break;
+        const uint32_t st = sb + s * L::kStage;
+        mbar_arrive_expect_tx(full(s), L::kB + L::kPk + L::kDs);
+        tma_load_2d(st + L::kPkOff, &rmap, int32_t(it * (kBwK / 4)), int32_t(vtile * kBwM),
+                    full(s));
+        tma_load_2d(st + L::kBOff, &bmap, int32_t(it * kBwK), int32_t(stile * kBwN), full(s));
+        tma_load_2d(st + L::kDsOff, &dmap, int32_t(stile * kBwScores), int32_t(it * kBwK),
+                    full(s));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16_f32(kBwM, kBwN);
+      uint32_t blk = 0;
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        const bool first = (it % kBwFlush) == 0;
+        if (first && it > 0) {
+          if (!mbar_wait_bounded(accempty, (blk - 1) & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            break;
+          }
+        }
+        if (!mbar_wait_bounded(aready(s), ph)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (*abort_flag) break;
+        tc_fence_after();
+        const uint32_t a0 = sb + s * L::kStage + L::kAOff;
+        const uint32_t b0 = sb + s * L::kStage + L::kBOff;
+#pragma unroll
+        for (uint32_t kk = 0; kk < kBwK / 16; ++kk)
+          tc_mma_f16(tmem, desc_kmajor_sw128(a0 + kk * 32), desc_kmajor_sw128(b0 + kk * 32), idesc,
+                     (first && kk == 0) ? 0u : 1u);
+        tc_commit(empty(s));
+        if ((it % kBwFlush) == kBwFlush - 1 || it == nit - 1) {
+          tc_commit(accfull);
+          ++blk;
+        }
+      }
+    }
+  } else {
+    // ---------------- genotype expansion + epilogue (warps 2-5) ----------------
+    const uint32_t quad = warp & 3;
+    const uint32_t r = 32 * quad + lane;   // variant row of this thread and its TMEM lane
+    double gwd[kBwScores], gcd[kBwScores];
+    float gcf[kBwScores];   // missing term of the last <= kBwMissFlush stages
+#pragma unroll
+    for (uint32_t k = 0; k < kBwScores; ++k) {
+      gwd[k] = gcd[k] = 0.0;
+      gcf[k] = 0.0f;
+    }
+    bool ok = true;
+    uint32_t blk = 0;
+    for (uint32_t it = 0; it < nit; ++it) {
+      const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      if (!mbar_wait_bounded(full(s), ph)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrTmaTimeout);
+        ok = false;
+        break;
+      }
+      if (*abort_flag) {
+        ok = false;
+        break;
+      }
+      const uint32_t st = sb + s * L::kStage;
+      const uint4 x4 = lds_u128(st + L::kPkOff + r * (kBwK / 4));
+      const uint32_t xw[4] = {x4.x, x4.y, x4.z, x4.w};   // word w: people 16w..16w+15
+      uint8_t* arow = smem + s * L::kStage + L::kAOff + (r >> 3) * 1024 + (r & 7) * 128;
+#pragma unroll
+      for (uint32_t w = 0; w < 4; ++w) {
+        // byte j of s_q = code of person 4j + q of the word
+        const uint32_t x = xw[w];
+        const uint32_t s0 = x & 0x03030303u, s1 = (x >> 2) & 0x03030303u;
+        const uint32_t s2 = (x >> 4) & 0x03030303u, s3 = (x >> 6) & 0x03030303u;
+#pragma unroll
+        for (uint32_t h = 0; h < 2; ++h) {
+          // 16-byte chunk c = people 8c..8c+7 of the stage (bytes 2h, 2h+1 of x)
+          constexpr uint32_t kSel[2] = {0x40u, 0x51u};
+          const uint32_t sa = kSel[0] + 0x22u * h, sbb = kSel[1] + 0x22u * h;
+          uint4 v;
+          v.x = dos_pair(__byte_perm(s0, s1, sa));
+          v.y = dos_pair(__byte_perm(s2, s3, sa));
+          v.z = dos_pair(__byte_perm(s0, s1, sbb));
+          v.w = dos_pair(__byte_perm(s2, s3, sbb));
+          const uint32_t c = 2 * w + h;
+          *reinterpret_cast<uint4*>(arow + ((c ^ (r & 7)) << 4)) = v;
+        }
+      }
+      // missing calls (code 01): add the person's FP32 dS row
+#pragma unroll
+      for (uint32_t w = 0; w < 4; ++w) {
+        uint32_t m = xw[w] & ~(xw[w] >> 1) & 0x55555555u;
+        while (m) {
+          const uint32_t b = 31u - __clz(m);   // highest set bit: one find-leading-one
+          m ^= 1u << b;
+          const uint32_t drow = st + L::kDsOff + (16 * w + b / 2) * (kBwScores * 4);
+#pragma unroll
+          for (uint32_t q = 0; q < kBwScores / 4; ++q) {
+            const uint4 f = lds_u128(drow + 16 * q);
+            gcf[4 * q + 0] += __uint_as_float(f.x);
+            gcf[4 * q + 1] += __uint_as_float(f.y);
+            gcf[4 * q + 2] += __uint_as_float(f.z);
+            gcf[4 * q + 3] += __uint_as_float(f.w);
+          }
+        }
+      }
+      if ((it % kBwMissFlush) == kBwMissFlush - 1 || it == nit - 1) {
+#pragma unroll
+        for (uint32_t k = 0; k < kBwScores; ++k) {
+          gcd[k] += double(gcf[k]);
+          gcf[k] = 0.0f;
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(aready(s));
+
+      if ((it % kBwFlush) == kBwFlush - 1 || it == nit - 1) {
+        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t lane_base = tmem + ((32 * quad) << 16);
+#pragma unroll
+        for (uint32_t half = 0; half < 2; ++half) {   // limbs 0-1, then 2-3
+          uint32_t d[32];
+          tmem_ld32(lane_base + 32 * half, d);
+          tmem_ld_wait();
+#pragma unroll
+          for (uint32_t k = 0; k < kBwScores; ++k)
+            gwd[k] += double(__uint_as_float(d[k])) + double(__uint_as_float(d[16 + k]));
+        }
+        tc_fence_before();
+        mbar_arrive(accempty);
+        ++blk;
+      }
+    }
+    const uint64_t v = uint64_t(vtile) * kBwM + r;
+    if (ok && v < a.V) {
+#pragma unroll
+      for (uint32_t k = 0; k < kBwScores; ++k) {
+        const uint64_t kk = uint64_t(stile) * kBwScores + k;
+        if (kk < a.K) {
+          a.gw[v * a.K + kk] = float(gwd[k]);
+          if (a.gc) a.gc[v * a.K + kk] = float(-gcd[k]);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kBwN);
+  }
 }
 
 // dS in output order -> fam order (zero for people outside the keep set).
@@ -387,82 +649,49 @@ __global__ void gnm_scatter_grad(const float* gs, const uint32_t* out_to_fam, ui
   gsf[uint64_t(out_to_fam[o]) * K + k] = gs[x];
 }
 
-__global__ void __launch_bounds__(kBwThreads)
-    gnm_backward_kernel(const uint8_t* rows, uint64_t pitch, uint64_t bpv, uint64_t V,
-                        const float* gsf, uint64_t fam, uint32_t K, float* gw, float* gc) {
-  __shared__ __align__(16) float g_s[kBwChunk * 16];
-  const uint32_t t = threadIdx.x;
-  const uint64_t v = uint64_t(blockIdx.x) * kBwThreads + t;
-  const uint32_t k0 = blockIdx.y * 16;
-  const uint8_t* row = rows + (v < V ? v : 0) * pitch;
-  uint64_t aw[8], ac[8];
-  double dw[16];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) aw[j] = ac[j] = 0ull;
-#pragma unroll
-  for (int j = 0; j < 16; ++j) dw[j] = 0.0;
-  for (uint64_t p0 = 0; p0 < fam; p0 += kBwChunk) {
-    const uint32_t np = uint32_t(fam - p0 < kBwChunk ? fam - p0 : kBwChunk);
-    __syncthreads();
-    for (uint32_t i = t; i < kBwChunk * 16; i += kBwThreads) {
-      const uint32_t pp = i / 16, kk = i % 16;
-      g_s[i] = (pp < np && k0 + kk < K) ? __ldg(gsf + (p0 + pp) * K + k0 + kk) : 0.f;
-    }
-    __syncthreads();
-    if (v < V) {
-      for (uint32_t seg = 0; seg < kBwChunk / 64; ++seg) {
-        const uint64_t b0 = p0 / 4 + seg * 16;  // 16 bytes = 64 people
-        if (b0 >= bpv) break;
-        const uint4 x4 = *reinterpret_cast<const uint4*>(row + b0);
-        const uint32_t xw[4] = {x4.x, x4.y, x4.z, x4.w};
-#pragma unroll
-        for (int wi = 0; wi < 4; ++wi) {
-          const uint32_t x = xw[wi];
-          if (x == 0u) continue;   // 16 homozygous-reference calls
-#pragma unroll 4
-          for (int i = 0; i < 16; ++i) {
-            const uint32_t c = (x >> (2 * i)) & 3u;
-            const uint64_t* gp =
-                reinterpret_cast<const uint64_t*>(&g_s[(seg * 64 + wi * 16 + i) * 16]);
-            uint64_t g[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) g[j] = gp[j];
-            // dosage 0 for codes 00 and 01 (missing): one FMA path for everyone
-            const float d = c == 3u ? 2.f : (c == 2u ? 1.f : 0.f);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) aw[j] = fma_f32x2(d, g[j], aw[j]);
-            if (c == 1u) {
-#pragma unroll
-              for (int j = 0; j < 8; ++j) ac[j] = sub_f32x2(ac[j], g[j]);
-            }
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float lo, hi;
-      asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(aw[j]));
-      dw[2 * j] += double(lo);
-      dw[2 * j + 1] += double(hi);
-      aw[j] = 0ull;
+// Per-score max |dS| as float bit patterns (non-negative floats order like
+// their bits); thread = (64-person chunk, score), consecutive threads read
+// consecutive scores of a row.
+__global__ void gnm_bw_amax(const float* g, uint64_t rows, uint64_t K, uint32_t* amax_bits) {
+  const uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t k = x % K, p0 = (x / K) * 64;
+  if (p0 >= rows) return;
+  const uint64_t p1 = p0 + 64 < rows ? p0 + 64 : rows;
+  uint32_t m = 0;
+  for (uint64_t p = p0; p < p1; ++p) m = max(m, __float_as_uint(fabsf(g[p * K + k])));
+  atomicMax(amax_bits + k, m);
+}
+
+// dS [rows][K] -> limb rows (tile t = k / 16: rows 64t + 16j + k % 16, limb j)
+// of P_pad people each, and the FP32 copy [P_pad][K16] for the missing term;
+// zeros past the last person and the last score.
+__global__ void gnm_bw_build(const float* g, uint64_t rows, uint64_t K, uint64_t K16,
+                             uint64_t P_pad, const uint32_t* amax_bits, __nv_bfloat16* planes,
+                             float* ds) {
+  const uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (x >= K16 * P_pad) return;
+  const uint64_t p = x % P_pad, k = x / P_pad;
+  const bool in = p < rows && k < K;
+  const float val = in ? g[p * K + k] : 0.0f;
+  ds[p * K16 + k] = val;
+  // quantum q = 2^(E-8), 2^E > max |dS| of the score (no smaller than 2^-126)
+  float q = 1.0f;
+  if (k < K) {
+    const float am = __uint_as_float(amax_bits[k]);
+    if (am > 0.0f) {
+      int e = 0;
+      frexpf(am, &e);
+      q = ldexpf(1.0f, max(e - 8, -126));
     }
   }
-  if (v < V) {
+  const uint64_t row0 = (k / kBwScores) * kBwN + (k % kBwScores);
+  float rem = val;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float lo, hi;
-      asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(ac[j]));
-      const uint32_t k = k0 + 2 * j;
-      if (k < K) {
-        gw[v * K + k] = float(dw[2 * j]);
-        if (gc) gc[v * K + k] = lo;
-      }
-      if (k + 1 < K) {
-        gw[v * K + k + 1] = float(dw[2 * j + 1]);
-        if (gc) gc[v * K + k + 1] = hi;
-      }
-    }
+  for (uint32_t j = 0; j < 4; ++j) {
+    const float qj = q * ldexpf(1.0f, -8 * int(j));   // power of two: exact division
+    const float limb = qj > 0.0f ? rintf(rem / qj) * qj : 0.0f;
+    rem -= limb;
+    planes[(row0 + kBwScores * j) * P_pad + p] = __float2bfloat16_rn(limb);
   }
 }
 
@@ -486,9 +715,7 @@ static cudaError_t launch_tc(const CUtensorMap& amap, const CUtensorMap& pmap, c
   return cudaGetLastError();
 }
 
-// 4 limb planes [4][K_pad][V_pad]; a box holds `np` consecutive planes.
-static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, uint64_t K_pad,
-                                  uint32_t np) {
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
     void* p = nullptr;
@@ -499,16 +726,42 @@ static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, u
       fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled is not available from the driver");
     fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
   }
+  return fn;
+}
+
+// 4 limb planes [4][K_pad][V_pad]; a box holds `np` consecutive planes.
+static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, uint64_t K_pad,
+                                  uint32_t np) {
   CUtensorMap map;
   cuuint64_t dims[3] = {V_pad, K_pad, 4};
   cuuint64_t strides[2] = {V_pad * 2, K_pad * V_pad * 2};
   cuuint32_t box[3] = {kTcK, kTcM, np};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = fn(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(planes),
-                  dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = tensor_map_encoder()(
+      &map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(planes), dims,
+      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled failed for limb planes");
+  return map;
+}
+
+// Row-major 2D map [rows][cols] (cols innermost; the row stride is cols
+// elements, a multiple of 16 bytes).
+static CUtensorMap make_2d_map(CUtensorMapDataType type, uint32_t elem_bytes, const void* base,
+                               uint64_t cols, uint64_t rows, uint32_t box_cols,
+                               uint32_t box_rows, CUtensorMapSwizzle swizzle, const char* what) {
+  if ((cols * elem_bytes) % 16 != 0 || reinterpret_cast<uintptr_t>(base) % 16 != 0)
+    fail(GNM_ERR_COMPUTE, std::string(what) + ": rows are not 16-byte aligned");
+  CUtensorMap map;
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {cols * elem_bytes};
+  cuuint32_t box[2] = {box_cols, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = tensor_map_encoder()(&map, type, 2, const_cast<void*>(base), dims, strides, box,
+                                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(GNM_ERR_COMPUTE, std::string("cuTensorMapEncodeTiled failed for ") + what);
   return map;
 }
 
@@ -672,9 +925,61 @@ void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float
     }
     gsf = p->d_grad_fam;
   }
-  const dim3 grid(uint32_t((p->V + kBwThreads - 1) / kBwThreads), uint32_t((p->K + 15) / 16));
-  gnm_backward_kernel<<<grid, kBwThreads, 0, s>>>(d_rows, pitch, p->bpv, p->V, gsf, p->fam,
-                                                  uint32_t(p->K), d_grad_w, d_grad_corr);
+  // dS limb rows and the FP32 copy, re-derived on every call
+  const uint64_t K16 = (p->K + kBwScores - 1) / kBwScores * kBwScores;
+  const uint64_t P_pad = std::max<uint64_t>(kBwK, (p->fam + kBwK - 1) / kBwK * kBwK);
+  const uint64_t limb_rows = K16 / kBwScores * kBwN;
+  const uint64_t planes_bytes = (limb_rows * P_pad * 2 + 255) / 256 * 256;
+  const uint64_t ds_bytes = (P_pad * K16 * 4 + 255) / 256 * 256;
+  const uint64_t need = planes_bytes + ds_bytes + K16 * 4;
+  if (p->bw_bytes < need) {
+    check_cuda(cudaStreamSynchronize(s), "backward buffer resize");
+    pool_free(p->d_bw);
+    p->d_bw = nullptr;
+    p->device_bytes -= p->bw_bytes;
+    p->bw_bytes = 0;
+    p->d_bw = static_cast<uint8_t*>(pool_alloc(p->device, need, "backward dS limbs"));
+    p->bw_bytes = need;
+    p->device_bytes += need;
+  }
+  auto* planes = reinterpret_cast<__nv_bfloat16*>(p->d_bw);
+  auto* ds = reinterpret_cast<float*>(p->d_bw + planes_bytes);
+  auto* amax = reinterpret_cast<uint32_t*>(p->d_bw + planes_bytes + ds_bytes);
+  check_cuda(cudaMemsetAsync(amax, 0, K16 * 4, s), "memset");
+  const uint64_t na = (p->fam + 63) / 64 * p->K;
+  if (na) {
+    gnm_bw_amax<<<uint32_t((na + 255) / 256), 256, 0, s>>>(gsf, p->fam, p->K, amax);
+    check_cuda(cudaGetLastError(), "gradient maximum launch");
+    p->launches += 1;
+  }
+  const uint64_t nb = K16 * P_pad;
+  gnm_bw_build<<<uint32_t((nb + 255) / 256), 256, 0, s>>>(gsf, p->fam, p->K, K16, P_pad, amax,
+                                                          planes, ds);
+  check_cuda(cudaGetLastError(), "gradient limb launch");
+  p->launches += 1;
+
+  const CUtensorMap rmap = make_row_map(d_rows, p->bpv, p->V, pitch, kBwK / 4, kBwM);
+  const CUtensorMap bmap =
+      make_2d_map(CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, planes, P_pad, limb_rows, kBwK, kBwN,
+                  CU_TENSOR_MAP_SWIZZLE_128B, "gradient limbs");
+  const CUtensorMap dmap = make_2d_map(CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ds, K16, P_pad,
+                                       kBwScores, kBwK, CU_TENSOR_MAP_SWIZZLE_NONE, "gradient");
+  static bool attr = false;
+  if (!attr) {
+    check_cuda(cudaFuncSetAttribute(gnm_tc_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(BwSmem::kTotal)),
+               "backward shared memory");
+    attr = true;
+  }
+  BwArgs a;
+  a.V = p->V;
+  a.K = p->K;
+  a.nstages = uint32_t(P_pad / kBwK);
+  a.gw = d_grad_w;
+  a.gc = d_grad_corr;
+  a.err = p->d_err;
+  const dim3 grid(uint32_t((p->V + kBwM - 1) / kBwM), uint32_t(K16 / kBwScores));
+  gnm_tc_backward<<<grid, kBwThreads, BwSmem::kTotal, s>>>(rmap, bmap, dmap, a);
   check_cuda(cudaGetLastError(), "backward launch");
   p->launches += 1;
 }

@@ -90,3 +90,34 @@ def test_autograd_finite_differences_and_fp64_gradient(cuda):
         wm[v, k] -= h
         fd = (loss_of(wp)[0].item() - loss_of(wm)[0].item()) / (2 * h)
         assert abs(fd - g[v, k]) <= 1e-4 * max(1.0, abs(g[v, k])) + 1e-7, (v, k, fd, g[v, k])
+
+
+def test_backward_many_people_and_score_scales(cuda):
+    """More than 32768 people (two exact FP32 blocks of the tensor-core
+    backward), a ragged last variant tile, and scores whose dS magnitudes
+    differ by 60 orders (the per-score limb quantum), one all-zero."""
+    import torch
+    from gnomon_b200.device import DevicePlan, row_pitch
+    _, prep, rows, _ = synth_case(40001, 260, scores=5, config="diff_20k_x_200k_k16")
+    P, K = prep.num_people_to_score, prep.num_scores
+    rng = np.random.default_rng(7)
+    gs = rng.standard_normal((P, K)).astype(np.float32)
+    gs[:, 0] *= np.float32(1e-3)
+    gs[:, 1] *= np.float32(1e3)
+    gs[:, 2] = 0.0
+    gs[:, 3] *= np.float32(1e-30)
+    gs[::7, 4] = np.float32(0.0)
+    pitch = row_pitch(prep.bytes_per_variant)
+    plan = DevicePlan(prep, engine=_lib.ENGINE_PLAIN)
+    gw, gc = plan.backward(_device_rows(rows, pitch), pitch, torch.from_numpy(gs).cuda(),
+                           grad_corr=True)
+    plan.sync()
+    ew, ec = oracle.backward_extended(rows, prep, gs)
+    gw, gc = gw.cpu().numpy().astype(np.float64), gc.cpu().numpy().astype(np.float64)
+    for k in range(K):
+        scale = np.abs(gs[:, k].astype(np.float64)).sum()
+        if scale == 0:
+            assert not gw[:, k].any() and not gc[:, k].any()
+            continue
+        assert np.abs(gw[:, k] - ew[:, k]).max() / scale < 1e-6, k
+        assert np.abs(gc[:, k] - ec[:, k]).max() / scale < 1e-6, k
