@@ -35,6 +35,7 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "bandwidth_50k_x_1m"
 METRIC = "genotype*score pairs/s"
+NARROW_MAX_SCORES = 64   # the tensor engine's people-as-M kernel serves up to 64 scores
 PROFILE = ROOT / "profiles" / "plain_accumulate_bandwidth_50k_x_1m.md"
 
 
@@ -334,7 +335,22 @@ def gpu_arm(args, rank, world, local_rank):
     pairs = P * V * K
     value = world * pairs / (ms / 1e3)
     peak_hbm, peak_kind = peaks()
-    if tensor:
+    if tensor and K <= NARROW_MAX_SCORES:
+        # narrow engine: M = 128 people, N = 4 limb planes x 16 scores, two MMAs
+        # (dosage, missing) per 16-variant slice; one launch per block
+        ptiles, k16, vpad = -(-P // 128), -(-K // 16) * 16, -(-V // 64) * 64
+        flops = 2.0 * ptiles * 128 * vpad * (4 * k16) * 2
+        achieved = flops / (kernel_ms / 1e3) / 1e12
+        pk = peaks_tc()[0]
+        roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
+                "frac": achieved / pk, "traffic": None,
+                "peak_kind": peak_kind + " (bf16 sustained)",
+                "kernel": "gnm_tc_narrow (dosage + missing MMAs, one pass)",
+                "kernel_ms": kernel_ms, "algorithmic_flops_per_launch": flops,
+                "row_bytes_gbs": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9,
+                "row_bytes_frac_of_hbm": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9
+                / peak_hbm}
+    elif tensor:
         # executed tensor-core work: 8 limb MMAs (4 dosage, 3 correction, 1 count)
         # over 256-person x 128-score tiles and 64-variant stages
         ptiles, kpad, vpad = -(-P // 256), -(-K // 128) * 128, -(-V // 64) * 64

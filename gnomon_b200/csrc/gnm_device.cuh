@@ -57,20 +57,18 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 }
 
 // Wait on phase `parity` of an mbarrier for at most `limit_ns`.  Returns false
-// on expiry.  The clock is read only after the first polls fail, so a wait that
-// is satisfied at once costs one try_wait.
+// on expiry.  mbarrier.try_wait itself suspends the thread until the phase
+// completes or a hardware time limit passes, so the loop polls without a
+// software back-off (a sleep between polls delays every pipeline hand-off by
+// up to the sleep); the clock is read every 64 polls.
 __device__ __forceinline__ bool mbar_wait_timed(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
-  for (int i = 0; i < 8; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
+  if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
-  uint32_t ns = 32;
-  // time is the limit; the iteration cap (2^26 polls, >= 2^26 x 32 ns) only
-  // guarantees an end should the clock not advance
-  for (uint32_t i = 0; i < (1u << 26); ++i) {
+  // time is the limit; the iteration cap (2^28 polls) only guarantees an end
+  // should the clock not advance
+  for (uint32_t i = 1; i < (1u << 28); ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (global_timer_ns() - t0 > limit_ns) return false;
-    __nanosleep(ns);
-    if (ns < 256) ns <<= 1;
+    if ((i & 63u) == 0 && global_timer_ns() - t0 > limit_ns) return false;
   }
   return false;
 }
@@ -123,6 +121,24 @@ __device__ __forceinline__ uint4 lds_u128(uint32_t addr) {
                : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
                : "r"(addr));
   return v;
+}
+
+__device__ __forceinline__ uint32_t lds_u8(uint32_t addr) {
+  uint32_t v;
+  asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(addr));
+  return v;
+}
+
+__device__ __forceinline__ uint2 lds_u64(uint32_t addr) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
+  return v;
+}
+
+__device__ __forceinline__ void sts_u128(uint32_t addr, uint4 v) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y),
+               "r"(v.z), "r"(v.w)
+               : "memory");
 }
 
 // SplitMix64 finaliser (Steele, Lea, Flood 2014); shared with the CPU oracle.

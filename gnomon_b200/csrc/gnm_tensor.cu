@@ -56,15 +56,21 @@ constexpr uint32_t kTcFlush = 256;    // stages per exact FP32 block (16384 vari
 constexpr uint32_t kTcThreads = 192;  // 6 warps
 constexpr int kTcPlanes = 2;          // limb planes per pass (2 x 256 TMEM columns)
 constexpr int kTcStages = 3;          // pipeline stages (68 KB each)
+constexpr uint64_t kNarrowMaxScores = 64;   // up to 4 narrow score tiles
 
 struct TensorPlan {
   uint64_t K_pad = 0, V_pad = 0, P_pad = 0;
   uint32_t ptiles = 0, stiles = 0;
   __nv_bfloat16* d_planes_dos = nullptr;  // [4][K_pad][V_pad] W' limbs
   __nv_bfloat16* d_planes_mis = nullptr;  // [4][K_pad][V_pad] -corr limbs, member
-  double* d_part_sum = nullptr;           // [K_pad][P_pad]
-  uint32_t* d_part_cnt = nullptr;         // [K_pad][P_pad]
+  double* d_part_sum = nullptr;           // wide: [K_pad][P_pad]; narrow: [nsplits][K16][P_pad]
+  uint32_t* d_part_cnt = nullptr;
+  uint64_t part_elems = 0;                // elements of d_part_sum / d_part_cnt
+  uint32_t nsplits = 1;                   // narrow: variant splits (grid z)
+  uint64_t nslot = 0;                     // narrow: elements per split slot (K16 * P_pad)
   CUtensorMap map_dos, map_mis;
+  bool narrow = false;                    // few scores: gnm_tc_narrow (people as M)
+  CUtensorMap nmap_dos, nmap_mis;         // narrow boxes: 16 scores x 4 planes
 };
 
 struct TcArgs {
@@ -220,8 +226,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         break;
       }
       if (*abort_flag) break;
-      const uint8_t* pk = smem + L::kPkOff + s * L::kPk;
-      uint8_t* bt = smem + L::kBOff + s * L::kB;
+      // explicit shared-space accesses: the realigned base is a generic pointer
+      const uint32_t pk = sb + L::kPkOff + s * L::kPk;
+      const uint32_t bt = sb + L::kBOff + s * L::kB;
 #pragma unroll
       for (uint32_t h = 0; h < kTcN / 128; ++h) {
         const uint32_t bc = 32 * h + col;   // byte column: people 4bc..4bc+3
@@ -231,8 +238,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           uint32_t xl = 0, xh = 0;
 #pragma unroll
           for (uint32_t i = 0; i < 4; ++i) {
-            xl |= uint32_t(pk[(r0 + i) * (kTcN / 4) + bc]) << (8 * i);
-            xh |= uint32_t(pk[(r0 + 4 + i) * (kTcN / 4) + bc]) << (8 * i);
+            xl |= lds_u8(pk + (r0 + i) * (kTcN / 4) + bc) << (8 * i);
+            xh |= lds_u8(pk + (r0 + 4 + i) * (kTcN / 4) + bc) << (8 * i);
           }
           const uint32_t c = 2 * vg + cc;  // 16-byte chunk (8 variants) index
 #pragma unroll
@@ -247,8 +254,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             v.w = bf16_pair(yh >> 16, lo, hi);
             // operand row of person 128h + 4col + q (conflict-free 16-byte stores)
             const uint32_t n = 128 * h + 32 * q + col;
-            *reinterpret_cast<uint4*>(bt + (n >> 3) * 1024 + (n & 7) * 128 +
-                                      ((c ^ (n & 7)) << 4)) = v;
+            sts_u128(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4), v);
           }
         }
       }
@@ -305,6 +311,261 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
+// ---- narrow tensor engine (few score columns) ---------------------------------
+// For a handful of scores the M = 128 score rows of gnm_tc_accumulate would be
+// mostly empty, so the roles turn: M = 128 PEOPLE (TMEM lanes), N = 64 = the
+// four limb planes of 16 scores (row n = 16 * plane + score, one 3D TMA box of
+// the same limb planes), K = 64 variants per stage.  Each stage runs two MMAs
+// per 16-variant slice: the dosage operand against the W' limbs and the
+// missing-indicator operand against the -C limbs and the member plane, into
+// 2 x 64 accumulator columns, so ONE pass produces sums and missing counts.
+// The genotype expansion is the transposing one of gnm_tc_accumulate (operand
+// row n = 32 q + col holds person 4 col + q), writing both operands, spread
+// over eight warps (one 8-variant chunk per thread): with fewer, each warp's
+// chain of dependent byte loads and permutes set the stage time.  Sums of a
+// 16384-variant block are exact in FP32 (same limb argument) and are added to
+// the FP64 partials of the CTA's variant split in natural person order at
+// block ends; gnm_tc_finalize adds the split slots in a fixed order.
+constexpr uint32_t kNrM = 128;                // people per CTA
+constexpr uint32_t kNrScores = 16;            // scores per CTA
+constexpr uint32_t kNrN = 4 * kNrScores;      // accumulator columns per operand
+constexpr uint32_t kNrStages = 4;
+constexpr uint32_t kNrExpand = 256;           // expansion threads (warps 2-9)
+constexpr uint32_t kNrThreads = 64 + kNrExpand;
+
+struct NrSmem {
+  static constexpr uint32_t kA = kNrM * kTcK * 2;          // 16 KB per operand
+  static constexpr uint32_t kB = kNrN * kTcK * 2;          // 8 KB per limb set
+  static constexpr uint32_t kPk = kTcK * (kNrM / 4);       // 2 KB packed rows
+  static constexpr uint32_t kADos = 0;
+  static constexpr uint32_t kAMis = kADos + kA;
+  static constexpr uint32_t kBDos = kAMis + kA;
+  static constexpr uint32_t kBMis = kBDos + kB;
+  static constexpr uint32_t kPkOff = kBMis + kB;
+  static constexpr uint32_t kStage = kPkOff + kPk;          // 50 KB
+  static constexpr uint32_t kBarOff = kNrStages * kStage;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (3 * kNrStages + 2);
+  static constexpr uint32_t kTotal = kHolder + 16 + 1024;   // + alignment slack
+};
+static_assert(NrSmem::kStage % 1024 == 0 && NrSmem::kBDos % 1024 == 0 &&
+                  NrSmem::kBMis % 1024 == 0,
+              "operand alignment");
+
+struct NrArgs {
+  uint64_t num_rows;          // rows of this block
+  int32_t a_x0;               // absolute variant index of block row 0 (multiple of 64)
+  uint32_t stages_per_split;  // 64-variant stages per blockIdx.z split
+  double* part_sum;           // [split][K_pad][P_pad], natural person order
+  uint32_t* part_cnt;
+  uint64_t P_pad;
+  uint64_t slot_stride;       // K_pad * P_pad
+  uint32_t* err;
+};
+
+__global__ void __launch_bounds__(kNrThreads, 1)
+    gnm_tc_narrow(const __grid_constant__ CUtensorMap dmap,
+                  const __grid_constant__ CUtensorMap mmap,
+                  const __grid_constant__ CUtensorMap pmap, NrArgs a) {
+  using L = NrSmem;
+  constexpr uint32_t ST = kNrStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sb = smem_u32(smem);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ptile = blockIdx.x, stile = blockIdx.y, split = blockIdx.z;
+  const uint32_t nall = uint32_t((a.num_rows + kTcK - 1) / kTcK);
+  const uint32_t it0 = split * a.stages_per_split;
+  const uint32_t nit = it0 < nall ? min(a.stages_per_split, nall - it0) : 0u;
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
+  auto bready = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
+  auto empty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (2 * ST + s); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  if (nit == 0) return;   // a split past the block's last stage (uniform per CTA)
+
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < ST; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(bready(s), kNrExpand);
+      mbar_init(empty(s), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, kNrExpand);
+    *abort_flag = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&dmap);
+    prefetch_tmap(&mmap);
+    prefetch_tmap(&pmap);
+  }
+  if (warp == 1) {
+    tmem_alloc(sb + L::kHolder, 2 * kNrN);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + L::kHolder);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        if (!mbar_wait_bounded(empty(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (*abort_flag) break;
+        const uint32_t st = sb + s * L::kStage;
+        mbar_arrive_expect_tx(full(s), 2 * L::kB + L::kPk);
+        const int32_t x = a.a_x0 + int32_t((it0 + it) * kTcK);
+        tma_load_3d(st + L::kBDos, &dmap, x, int32_t(stile * kNrScores), 0, full(s));
+        tma_load_3d(st + L::kBMis, &mmap, x, int32_t(stile * kNrScores), 0, full(s));
+        tma_load_2d(st + L::kPkOff, &pmap, int32_t(ptile * (kNrM / 4)),
+                    int32_t((it0 + it) * kTcK), full(s));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16_f32(kNrM, kNrN);
+      uint32_t blk = 0;
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        const bool first = (it % kTcFlush) == 0;
+        if (first && it > 0) {
+          if (!mbar_wait_bounded(accempty, (blk - 1) & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            break;
+          }
+        }
+        if (!mbar_wait_bounded(bready(s), ph)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (*abort_flag) break;
+        tc_fence_after();
+        const uint32_t st = sb + s * L::kStage;
+#pragma unroll
+        for (uint32_t kk = 0; kk < kTcK / 16; ++kk) {
+          const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+          tc_mma_f16(tmem, desc_kmajor_sw128(st + L::kADos + kk * 32),
+                     desc_kmajor_sw128(st + L::kBDos + kk * 32), idesc, acc);
+          tc_mma_f16(tmem + kNrN, desc_kmajor_sw128(st + L::kAMis + kk * 32),
+                     desc_kmajor_sw128(st + L::kBMis + kk * 32), idesc, acc);
+        }
+        tc_commit(empty(s));
+        if ((it % kTcFlush) == kTcFlush - 1 || it == nit - 1) {
+          tc_commit(accfull);
+          ++blk;
+        }
+      }
+    }
+  } else {
+    // ---------------- genotype expansion + epilogue (warps 2-9) ----------------
+    const uint32_t pt = threadIdx.x - 64;   // 0..255
+    const uint32_t col = pt & 31;           // byte column: people 4col..4col+3
+    const uint32_t c = pt >> 5;             // 16-byte chunk: variants 8c..8c+7 of the stage
+    const uint32_t quad = warp & 3;         // TMEM lane quadrant of this warp
+    const uint32_t half = (warp - 2) >> 2;  // epilogue: scores 8 half .. 8 half + 7
+    double* ps = a.part_sum + uint64_t(split) * a.slot_stride;
+    uint32_t* pc = a.part_cnt + uint64_t(split) * a.slot_stride;
+    uint32_t blk = 0;
+    for (uint32_t it = 0; it < nit; ++it) {
+      const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      if (!mbar_wait_bounded(full(s), ph)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrTmaTimeout);
+        break;
+      }
+      if (*abort_flag) break;
+      // explicit shared-space accesses: the realigned base is a generic pointer
+      const uint32_t pk = sb + s * L::kStage + L::kPkOff;
+      const uint32_t ad = sb + s * L::kStage + L::kADos;
+      const uint32_t am = sb + s * L::kStage + L::kAMis;
+      {
+        const uint32_t r0 = 8 * c;
+        uint32_t xl = 0, xh = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < 4; ++i) {
+          xl |= lds_u8(pk + (r0 + i) * (kNrM / 4) + col) << (8 * i);
+          xh |= lds_u8(pk + (r0 + 4 + i) * (kNrM / 4) + col) << (8 * i);
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+          const uint32_t yl = (xl >> (2 * q)) & 0x03030303u;
+          const uint32_t yh = (xh >> (2 * q)) & 0x03030303u;
+          uint4 vd, vm;
+          vd.x = bf16_pair(yl & 0xFFFFu, kDosLo, kDosHi);
+          vd.y = bf16_pair(yl >> 16, kDosLo, kDosHi);
+          vd.z = bf16_pair(yh & 0xFFFFu, kDosLo, kDosHi);
+          vd.w = bf16_pair(yh >> 16, kDosLo, kDosHi);
+          vm.x = bf16_pair(yl & 0xFFFFu, kMisLo, kMisHi);
+          vm.y = bf16_pair(yl >> 16, kMisLo, kMisHi);
+          vm.z = bf16_pair(yh & 0xFFFFu, kMisLo, kMisHi);
+          vm.w = bf16_pair(yh >> 16, kMisLo, kMisHi);
+          // operand row of person 4col + q (conflict-free 16-byte stores)
+          const uint32_t n = 32 * q + col;
+          const uint32_t off = (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4);
+          sts_u128(ad + off, vd);
+          sts_u128(am + off, vm);
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(bready(s));
+
+      if ((it % kTcFlush) == kTcFlush - 1 || it == nit - 1) {
+        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        tc_fence_after();
+        // TMEM lane 32 quad + lane = operand row n -> person 4 (n % 32) + n / 32.
+        // Column group g (16 columns): dosage limbs 0-3, -C limbs 0-2, member;
+        // this thread reads its 8 scores of every group.
+        const uint64_t person = uint64_t(ptile) * kNrM + 4 * lane + quad;
+        const uint32_t lane_base = tmem + ((32 * quad) << 16) + 8 * half;
+        double acc[8];
+        uint32_t cnt[8];
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) acc[k] = 0.0;
+#pragma unroll
+        for (uint32_t g = 0; g < 8; ++g) {
+          uint32_t d[8];
+          tmem_ld8(lane_base + 16 * g, d);
+          tmem_ld_wait();
+#pragma unroll
+          for (uint32_t k = 0; k < 8; ++k) {
+            if (g < 7) acc[k] += double(__uint_as_float(d[k]));
+            else cnt[k] = __float2uint_rn(__uint_as_float(d[k]));
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(accempty);
+        ++blk;
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) {
+          const uint64_t at = (uint64_t(stile) * kNrScores + 8 * half + k) * a.P_pad + person;
+          ps[at] += acc[k];
+          pc[at] += cnt[k];
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 2 * kNrN);
+  }
+}
+
 // Limb planes from the CSR: one thread per variant.
 __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uint32_t* cols,
                                     const uint64_t* offs, uint64_t V, const float* qhi,
@@ -341,18 +602,32 @@ __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uin
 
 // out[o*K + k] = init[k] + part_sum[k][slot(fam(o))]; slot(f) is the operand
 // row of person f: tile (f / 256), row 128*h + 32*(r%4) + (r%128)/4 with
-// r = f % 256 and h = r / 128.
+// r = f % 256 and h = r / 128.  The narrow engine's epilogue writes in person
+// order, one slot per variant split: those slots are added in split order.
 __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt, uint64_t P_pad,
                                 const double* init, const uint32_t* out_to_fam, uint64_t P,
-                                uint64_t K, double* sums, uint32_t* counts) {
+                                uint64_t K, uint32_t nslots, uint64_t slot_stride,
+                                double* sums, uint32_t* counts) {
   const uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (x >= P * K) return;
   const uint64_t o = x / K, k = x % K;
   const uint64_t f = out_to_fam ? out_to_fam[o] : o;
-  const uint64_t r = f % kTcN, h = r / 128, rr = r % 128;
-  const uint64_t slot = (f / kTcN) * kTcN + 128 * h + 32 * (rr % 4) + rr / 4;
-  sums[x] = init[k] + part_sum[k * P_pad + slot];
-  counts[x] = part_cnt[k * P_pad + slot];
+  if (nslots == 0) {   // wide engine: one slot, operand-row order
+    const uint64_t r = f % kTcN, h = r / 128, rr = r % 128;
+    const uint64_t slot = (f / kTcN) * kTcN + 128 * h + 32 * (rr % 4) + rr / 4;
+    sums[x] = init[k] + part_sum[k * P_pad + slot];
+    counts[x] = part_cnt[k * P_pad + slot];
+    return;
+  }
+  // narrow engine: natural order, variant-split slots added in split order
+  double s = 0.0;
+  uint32_t c = 0;
+  for (uint32_t z = 0; z < nslots; ++z) {
+    s += part_sum[z * slot_stride + k * P_pad + f];
+    c += part_cnt[z * slot_stride + k * P_pad + f];
+  }
+  sums[x] = init[k] + s;
+  counts[x] = c;
 }
 
 // ---- backward: dW[v,k] = sum_p d(p,v) dS[p,k], dC[v,k] = -sum_{p missing} dS[p,k]
@@ -381,17 +656,20 @@ __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt
 // K-major operand row per variant).  Warp 0 issues TMA (packed rows
 // [128 x 16 bytes], dS limbs [64 x 64] BF16 with 128-byte swizzle, FP32 dS
 // [64 people x 16 scores]), warp 1 owns 64 TMEM columns and issues
-// tcgen05.mma (M = 128, N = 64, K = 16), warps 2-5 expand genotypes (thread =
-// variant row 32 * (warp % 4) + lane, the TMEM lane it later drains) and run
-// the epilogue.  Two CTAs per SM.
+// tcgen05.mma (M = 128, N = 64, K = 16), warps 2-9 expand genotypes: two
+// threads per variant row (row 32 * (warp % 4) + lane, the TMEM lane the pair
+// later drains; people 32 * half ..), each draining 8 of the 16 scores.  With
+// one expanding warp per scheduler the chain of dependent permutes and stores
+// set the stage time; with two, their latencies overlap.
 constexpr uint32_t kBwM = 128;                    // variants per CTA (TMEM lanes)
 constexpr uint32_t kBwScores = 16;                // scores per CTA
 constexpr uint32_t kBwN = 4 * kBwScores;          // limb rows = accumulator columns
 constexpr uint32_t kBwK = 64;                     // people per stage
-constexpr uint32_t kBwStages = 3;
+constexpr uint32_t kBwStages = 6;
 constexpr uint32_t kBwFlush = 512;                // stages per exact FP32 block (32768 people)
 constexpr uint32_t kBwMissFlush = 64;             // stages per FP32 missing-term sum (4096 people)
-constexpr uint32_t kBwThreads = 192;
+constexpr uint32_t kBwExpand = 256;               // expansion threads (warps 2-9)
+constexpr uint32_t kBwThreads = 64 + kBwExpand;
 
 struct BwSmem {
   static constexpr uint32_t kA = kBwM * kBwK * 2;           // 16 KB dosage operand
@@ -406,8 +684,11 @@ struct BwSmem {
   static constexpr uint32_t kBarOff = kBwStages * kStage;
   static constexpr uint32_t kHolder = kBarOff + 8 * (3 * kBwStages + 2);
   static constexpr uint32_t kTotal = kHolder + 16 + 1024;    // + alignment slack
+  // end of kernel: both halves' FP64 missing sums [2][128][16], over stage 0-1
+  static constexpr uint32_t kSwap = 2 * kBwM * kBwScores * 8;
 };
 static_assert(BwSmem::kStage % 1024 == 0 && BwSmem::kBOff % 1024 == 0, "operand alignment");
+static_assert(BwSmem::kSwap <= BwSmem::kBarOff, "swap area");
 
 struct BwArgs {
   uint64_t V, K;
@@ -422,7 +703,7 @@ __device__ __forceinline__ uint32_t dos_pair(uint32_t y) {
   return __byte_perm(kDosLo, kDosHi, y * 0x11u + 0x4040u);
 }
 
-__global__ void __launch_bounds__(kBwThreads, 2)
+__global__ void __launch_bounds__(kBwThreads, 1)
     gnm_tc_backward(const __grid_constant__ CUtensorMap rmap,
                     const __grid_constant__ CUtensorMap bmap,
                     const __grid_constant__ CUtensorMap dmap, BwArgs a) {
@@ -445,11 +726,11 @@ __global__ void __launch_bounds__(kBwThreads, 2)
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < ST; ++s) {
       mbar_init(full(s), 1);
-      mbar_init(aready(s), 128);
+      mbar_init(aready(s), kBwExpand);
       mbar_init(empty(s), 1);
     }
     mbar_init(accfull, 1);
-    mbar_init(accempty, 128);
+    mbar_init(accempty, kBwExpand);
     *abort_flag = 0u;
     fence_mbar_init();
     prefetch_tmap(&rmap);
@@ -521,16 +802,19 @@ __global__ void __launch_bounds__(kBwThreads, 2)
       }
     }
   } else {
-    // ---------------- genotype expansion + epilogue (warps 2-5) ----------------
+    // ---------------- genotype expansion + epilogue (warps 2-9) ----------------
     const uint32_t quad = warp & 3;
-    const uint32_t r = 32 * quad + lane;   // variant row of this thread and its TMEM lane
-    double gwd[kBwScores], gcd[kBwScores];
+    const uint32_t half = (warp - 2) >> 2;  // people 32 half .. of each stage; scores 8 half ..
+    const uint32_t r = 32 * quad + lane;    // variant row of this thread and its TMEM lane
+    double gwd[8], gcd[kBwScores];
     float gcf[kBwScores];   // missing term of the last <= kBwMissFlush stages
 #pragma unroll
     for (uint32_t k = 0; k < kBwScores; ++k) {
-      gwd[k] = gcd[k] = 0.0;
+      gcd[k] = 0.0;
       gcf[k] = 0.0f;
     }
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) gwd[k] = 0.0;
     bool ok = true;
     uint32_t blk = 0;
     for (uint32_t it = 0; it < nit; ++it) {
@@ -546,11 +830,13 @@ __global__ void __launch_bounds__(kBwThreads, 2)
         break;
       }
       const uint32_t st = sb + s * L::kStage;
-      const uint4 x4 = lds_u128(st + L::kPkOff + r * (kBwK / 4));
-      const uint32_t xw[4] = {x4.x, x4.y, x4.z, x4.w};   // word w: people 16w..16w+15
-      uint8_t* arow = smem + s * L::kStage + L::kAOff + (r >> 3) * 1024 + (r & 7) * 128;
+      // words 2 half, 2 half + 1 of the row: people 32 half + 16 w' ..
+      // explicit shared-space accesses: the realigned base is a generic pointer
+      const uint2 x2 = lds_u64(st + L::kPkOff + r * (kBwK / 4) + 8 * half);
+      const uint32_t xw[2] = {x2.x, x2.y};
+      const uint32_t arow = st + L::kAOff + (r >> 3) * 1024 + (r & 7) * 128;
 #pragma unroll
-      for (uint32_t w = 0; w < 4; ++w) {
+      for (uint32_t w = 0; w < 2; ++w) {
         // byte j of s_q = code of person 4j + q of the word
         const uint32_t x = xw[w];
         const uint32_t s0 = x & 0x03030303u, s1 = (x >> 2) & 0x03030303u;
@@ -558,33 +844,31 @@ __global__ void __launch_bounds__(kBwThreads, 2)
 #pragma unroll
         for (uint32_t h = 0; h < 2; ++h) {
           // 16-byte chunk c = people 8c..8c+7 of the stage (bytes 2h, 2h+1 of x)
-          constexpr uint32_t kSel[2] = {0x40u, 0x51u};
-          const uint32_t sa = kSel[0] + 0x22u * h, sbb = kSel[1] + 0x22u * h;
+          const uint32_t sa = 0x40u + 0x22u * h, sbb = 0x51u + 0x22u * h;
           uint4 v;
           v.x = dos_pair(__byte_perm(s0, s1, sa));
           v.y = dos_pair(__byte_perm(s2, s3, sa));
           v.z = dos_pair(__byte_perm(s0, s1, sbb));
           v.w = dos_pair(__byte_perm(s2, s3, sbb));
-          const uint32_t c = 2 * w + h;
-          *reinterpret_cast<uint4*>(arow + ((c ^ (r & 7)) << 4)) = v;
+          const uint32_t c = 4 * half + 2 * w + h;
+          sts_u128(arow + ((c ^ (r & 7)) << 4), v);
         }
       }
-      // missing calls (code 01): add the person's FP32 dS row
+      // missing calls (code 01): add the person's FP32 dS row; bit 2i of m
+      // is person 32 half + i
+      uint64_t m = (uint64_t(xw[1] & ~(xw[1] >> 1) & 0x55555555u) << 32) |
+                   (xw[0] & ~(xw[0] >> 1) & 0x55555555u);
+      while (m) {
+        const uint32_t b = 63u - __clzll(m);   // highest set bit: one find-leading-one
+        m ^= uint64_t(1) << b;
+        const uint32_t drow = st + L::kDsOff + (32 * half + b / 2) * (kBwScores * 4);
 #pragma unroll
-      for (uint32_t w = 0; w < 4; ++w) {
-        uint32_t m = xw[w] & ~(xw[w] >> 1) & 0x55555555u;
-        while (m) {
-          const uint32_t b = 31u - __clz(m);   // highest set bit: one find-leading-one
-          m ^= 1u << b;
-          const uint32_t drow = st + L::kDsOff + (16 * w + b / 2) * (kBwScores * 4);
-#pragma unroll
-          for (uint32_t q = 0; q < kBwScores / 4; ++q) {
-            const uint4 f = lds_u128(drow + 16 * q);
-            gcf[4 * q + 0] += __uint_as_float(f.x);
-            gcf[4 * q + 1] += __uint_as_float(f.y);
-            gcf[4 * q + 2] += __uint_as_float(f.z);
-            gcf[4 * q + 3] += __uint_as_float(f.w);
-          }
+        for (uint32_t q = 0; q < kBwScores / 4; ++q) {
+          const uint4 f = lds_u128(drow + 16 * q);
+          gcf[4 * q + 0] += __uint_as_float(f.x);
+          gcf[4 * q + 1] += __uint_as_float(f.y);
+          gcf[4 * q + 2] += __uint_as_float(f.z);
+          gcf[4 * q + 3] += __uint_as_float(f.w);
         }
       }
       if ((it % kBwMissFlush) == kBwMissFlush - 1 || it == nit - 1) {
@@ -605,29 +889,40 @@ __global__ void __launch_bounds__(kBwThreads, 2)
           break;
         }
         tc_fence_after();
-        const uint32_t lane_base = tmem + ((32 * quad) << 16);
+        // columns 16 j + 8 half + k: limb j of score 8 half + k
+        const uint32_t lane_base = tmem + ((32 * quad) << 16) + 8 * half;
 #pragma unroll
-        for (uint32_t half = 0; half < 2; ++half) {   // limbs 0-1, then 2-3
-          uint32_t d[32];
-          tmem_ld32(lane_base + 32 * half, d);
+        for (uint32_t j = 0; j < 4; ++j) {
+          uint32_t d[8];
+          tmem_ld8(lane_base + 16 * j, d);
           tmem_ld_wait();
 #pragma unroll
-          for (uint32_t k = 0; k < kBwScores; ++k)
-            gwd[k] += double(__uint_as_float(d[k])) + double(__uint_as_float(d[16 + k]));
+          for (uint32_t k = 0; k < 8; ++k) gwd[k] += double(__uint_as_float(d[k]));
         }
         tc_fence_before();
         mbar_arrive(accempty);
         ++blk;
       }
     }
-    const uint64_t v = uint64_t(vtile) * kBwM + r;
-    if (ok && v < a.V) {
+    // The two halves of a row hold the missing term of different people: add
+    // them in a fixed order through shared memory (stage buffers are idle: the
+    // last accumulator commit followed every MMA, and every TMA was consumed).
+    named_barrier(1, kBwExpand);
+    double* swap = reinterpret_cast<double*>(smem);
 #pragma unroll
-      for (uint32_t k = 0; k < kBwScores; ++k) {
-        const uint64_t kk = uint64_t(stile) * kBwScores + k;
+    for (uint32_t k = 0; k < kBwScores; ++k) swap[(half * kBwM + r) * kBwScores + k] = gcd[k];
+    named_barrier(1, kBwExpand);
+    const uint64_t v = uint64_t(vtile) * kBwM + r;
+    if (ok && !*abort_flag && v < a.V) {
+#pragma unroll
+      for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t kl = 8 * half + k;
+        const uint64_t kk = uint64_t(stile) * kBwScores + kl;
         if (kk < a.K) {
           a.gw[v * a.K + kk] = float(gwd[k]);
-          if (a.gc) a.gc[v * a.K + kk] = float(-gcd[k]);
+          if (a.gc)
+            a.gc[v * a.K + kk] =
+                float(-(swap[r * kBwScores + kl] + swap[(kBwM + r) * kBwScores + kl]));
         }
       }
     }
@@ -731,11 +1026,11 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // 4 limb planes [4][K_pad][V_pad]; a box holds `np` consecutive planes.
 static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, uint64_t K_pad,
-                                  uint32_t np) {
+                                  uint32_t box_scores, uint32_t np) {
   CUtensorMap map;
   cuuint64_t dims[3] = {V_pad, K_pad, 4};
   cuuint64_t strides[2] = {V_pad * 2, K_pad * V_pad * 2};
-  cuuint32_t box[3] = {kTcK, kTcM, np};
+  cuuint32_t box[3] = {kTcK, box_scores, np};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = tensor_map_encoder()(
       &map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(planes), dims,
@@ -765,6 +1060,24 @@ static CUtensorMap make_2d_map(CUtensorMapDataType type, uint32_t elem_bytes, co
   return map;
 }
 
+// Variant splits of the narrow engine: enough CTAs for about four waves, then
+// the count whose last wave is fullest (at most 16 splits, one stage each).
+static uint32_t narrow_splits(uint64_t base_ctas, uint64_t stages, int sms) {
+  uint32_t best = 1;
+  double best_score = -1.0;
+  for (uint32_t s = 1; s <= 16 && s <= std::max<uint64_t>(1, stages); ++s) {
+    const uint64_t ctas = base_ctas * s;
+    const uint64_t waves = (ctas + sms - 1) / sms;
+    const double tail = double(ctas) / double(waves * uint64_t(sms));
+    const double score = tail * std::min(1.0, double(ctas) / (4.0 * sms));
+    if (score > best_score + 1e-9) {
+      best_score = score;
+      best = s;
+    }
+  }
+  return best;
+}
+
 void tensor_plan_create(gnm_plan* p) {
   auto* t = new TensorPlan();
   p->tensor = t;
@@ -773,6 +1086,7 @@ void tensor_plan_create(gnm_plan* p) {
   t->ptiles = uint32_t(std::max<uint64_t>(1, (p->fam + kTcN - 1) / kTcN));
   t->stiles = uint32_t(t->K_pad / kTcM);
   t->P_pad = uint64_t(t->ptiles) * kTcN;
+  t->narrow = p->K <= kNarrowMaxScores;
   if (t->V_pad > (uint64_t(1) << 31)) fail(GNM_ERR_INVALID, "too many variants for the tensor engine");
 
   // per-score quantum q = 2^(E-8), 2^E >= max |x| over the score's values
@@ -794,8 +1108,20 @@ void tensor_plan_create(gnm_plan* p) {
   };
   alloc(reinterpret_cast<void**>(&t->d_planes_dos), 4 * plane * 2, "cudaMalloc(limb planes)");
   alloc(reinterpret_cast<void**>(&t->d_planes_mis), 4 * plane * 2, "cudaMalloc(limb planes)");
-  alloc(reinterpret_cast<void**>(&t->d_part_sum), t->K_pad * t->P_pad * 8, "cudaMalloc(partials)");
-  alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->K_pad * t->P_pad * 4, "cudaMalloc(partials)");
+  if (t->narrow) {
+    const uint64_t k16 = (p->K + kNrScores - 1) / kNrScores * kNrScores;
+    const uint64_t base = ((p->fam + kNrM - 1) / kNrM) * (k16 / kNrScores);
+    int sms = 0;
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device),
+               "cudaDeviceGetAttribute");
+    t->nsplits = narrow_splits(base, t->V_pad / kTcK, std::max(1, sms));
+    t->nslot = k16 * t->P_pad;
+    t->part_elems = uint64_t(t->nsplits) * t->nslot;
+  } else {
+    t->part_elems = t->K_pad * t->P_pad;
+  }
+  alloc(reinterpret_cast<void**>(&t->d_part_sum), t->part_elems * 8, "cudaMalloc(partials)");
+  alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->part_elems * 4, "cudaMalloc(partials)");
   check_cuda(cudaMemset(t->d_planes_dos, 0, 4 * plane * 2), "memset planes");
   check_cuda(cudaMemset(t->d_planes_mis, 0, 4 * plane * 2), "memset planes");
 
@@ -832,8 +1158,12 @@ void tensor_plan_create(gnm_plan* p) {
     check_cuda(cudaGetLastError(), "plane build launch");
   }
   check_cuda(cudaStreamSynchronize(0), "plane build");
-  t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcPlanes);
-  t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcPlanes);
+  t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcM, kTcPlanes);
+  t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcM, kTcPlanes);
+  if (t->narrow) {
+    t->nmap_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kNrScores, 4);
+    t->nmap_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kNrScores, 4);
+  }
 }
 
 void tensor_plan_destroy(gnm_plan* p) {
@@ -849,8 +1179,8 @@ void tensor_plan_destroy(gnm_plan* p) {
 
 void tensor_reset(gnm_plan* p, cudaStream_t s) {
   TensorPlan* t = p->tensor;
-  check_cuda(cudaMemsetAsync(t->d_part_sum, 0, t->K_pad * t->P_pad * 8, s), "reset partials");
-  check_cuda(cudaMemsetAsync(t->d_part_cnt, 0, t->K_pad * t->P_pad * 4, s), "reset partials");
+  check_cuda(cudaMemsetAsync(t->d_part_sum, 0, t->part_elems * 8, s), "reset partials");
+  check_cuda(cudaMemsetAsync(t->d_part_cnt, 0, t->part_elems * 4, s), "reset partials");
 }
 
 void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,
@@ -858,6 +1188,32 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
   TensorPlan* t = p->tensor;
   if (v0 % kTcK != 0)
     fail(GNM_ERR_INVALID, "tensor engine blocks must start at a multiple of 64 variants");
+  if (t->narrow) {
+    const CUtensorMap pmap = make_row_map(d_rows, p->bpv, nv, pitch, kNrM / 4, kTcK);
+    static bool attr = false;
+    if (!attr) {
+      check_cuda(cudaFuncSetAttribute(gnm_tc_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(NrSmem::kTotal)),
+                 "narrow shared memory");
+      attr = true;
+    }
+    NrArgs a;
+    a.num_rows = nv;
+    a.a_x0 = int32_t(v0);
+    const uint32_t nall = uint32_t((nv + kTcK - 1) / kTcK);
+    a.stages_per_split = (nall + t->nsplits - 1) / t->nsplits;
+    a.part_sum = t->d_part_sum;
+    a.part_cnt = t->d_part_cnt;
+    a.P_pad = t->P_pad;
+    a.slot_stride = t->nslot;
+    a.err = p->d_err;
+    const dim3 grid(uint32_t((p->fam + kNrM - 1) / kNrM),
+                    uint32_t((p->K + kNrScores - 1) / kNrScores), t->nsplits);
+    gnm_tc_narrow<<<grid, kNrThreads, NrSmem::kTotal, s>>>(t->nmap_dos, t->nmap_mis, pmap, a);
+    check_cuda(cudaGetLastError(), "narrow tensor launch");
+    p->launches += 1;
+    return;
+  }
   const CUtensorMap pmap = make_row_map(d_rows, p->bpv, nv, pitch, kTcN / 4, kTcK);
   TcArgs a;
   a.num_rows = nv;
@@ -895,7 +1251,7 @@ void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_b
   if (n == 0) return;
   gnm_tc_finalize<<<uint32_t((n + 255) / 256), 256, 0, s>>>(
       t->d_part_sum, t->d_part_cnt, t->P_pad, add_baseline ? p->d_baseline : p->d_zero_base,
-      p->d_out_to_fam, p->P, p->K, d_sums, d_counts);
+      p->d_out_to_fam, p->P, p->K, t->narrow ? t->nsplits : 0u, t->nslot, d_sums, d_counts);
   check_cuda(cudaGetLastError(), "tensor finalize launch");
   p->launches += 1;
 }

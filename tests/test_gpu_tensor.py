@@ -53,8 +53,9 @@ def test_ragged_tiles(cuda, people, variants, scores):
     check(prep, rows, host_run(prep, rows))
 
 
-def test_block_flush_past_16k_variants(cuda):
-    _, prep, rows, _ = synth_case(300, 40_000, scores=130, config="batched_100k_x_500k_k512")
+@pytest.mark.parametrize("scores", [130, 20])   # wide (score rows as M) and narrow engines
+def test_block_flush_past_16k_variants(cuda, scores):
+    _, prep, rows, _ = synth_case(300, 40_000, scores=scores, config="batched_100k_x_500k_k512")
     check(prep, rows, host_run(prep, rows))
 
 
