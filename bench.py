@@ -235,7 +235,7 @@ def _engine(args, K):
         return _lib.ENGINE_PLAIN
     if args.engine == "tensor":
         return _lib.ENGINE_TENSOR
-    return _lib.ENGINE_PLAIN if K < 32 else _lib.ENGINE_TENSOR
+    return _lib.ENGINE_PLAIN if K < 8 else _lib.ENGINE_TENSOR   # the library's AUTO rule
 
 
 def gpu_arm(args, rank, world, local_rank):

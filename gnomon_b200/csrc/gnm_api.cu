@@ -350,7 +350,7 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
     p->bpv = prep->bytes_per_variant;
     p->K = prep->num_scores;
     p->V = prep->num_variants;
-    if (engine == GNM_ENGINE_AUTO) engine = p->K > kTensorMinScores ? GNM_ENGINE_TENSOR : GNM_ENGINE_PLAIN;
+    if (engine == GNM_ENGINE_AUTO) engine = p->K >= kTensorMinScores ? GNM_ENGINE_TENSOR : GNM_ENGINE_PLAIN;
     p->engine = engine;
 
     // baseline (prepare.rs:644-646), f64 in CSR order
@@ -643,7 +643,7 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   DeviceGuard g(device);
   const gnm_engine engine =
       o.engine == GNM_ENGINE_AUTO
-          ? (prep->num_scores > kTensorMinScores ? GNM_ENGINE_TENSOR : GNM_ENGINE_PLAIN)
+          ? (prep->num_scores >= kTensorMinScores ? GNM_ENGINE_TENSOR : GNM_ENGINE_PLAIN)
           : o.engine;
 
   const uint64_t P = prep->num_people, K = prep->num_scores, V = prep->num_variants;

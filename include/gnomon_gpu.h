@@ -60,7 +60,7 @@ typedef struct gnm_error {
 
 /* Engine selection for gnm_score_run_ex. */
 typedef enum gnm_engine {
-  GNM_ENGINE_AUTO = 0,     /* plain for small K, split-BF16 tensor cores for large K */
+  GNM_ENGINE_AUTO = 0,     /* plain below 8 score columns, split-BF16 tensor cores from 8 */
   GNM_ENGINE_PLAIN = 1,    /* FP32 CUDA-core LUT kernel, FP64 cross-block reduce */
   GNM_ENGINE_TENSOR = 2    /* split-BF16 (hi/mid/lo) tcgen05 GEMM, FP32 TMEM accum */
 } gnm_engine;
