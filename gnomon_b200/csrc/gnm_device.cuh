@@ -123,6 +123,14 @@ __device__ __forceinline__ uint4 lds_u128(uint32_t addr) {
   return v;
 }
 
+// Shared-memory flag read that is never cached in a register (explicit shared
+// space: a generic load of the same word waits on the global-memory pipeline).
+__device__ __forceinline__ uint32_t lds_volatile_u32(uint32_t addr) {
+  uint32_t v;
+  asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ uint32_t lds_u8(uint32_t addr) {
   uint32_t v;
   asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(addr));

@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
   const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
   volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  const uint32_t abort_addr = sb + L::kHolder + 8;
 
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < ST; ++s) {
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           atomicOr(a.err, kErrMmaTimeout);
           break;
         }
-        if (*abort_flag) break;
+        if (lds_volatile_u32(abort_addr)) break;
         mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
         tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kTcK),
                     int32_t(stile * kTcM), a.z0, full(s));
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           atomicOr(a.err, kErrMmaTimeout);
           break;
         }
-        if (*abort_flag) break;
+        if (lds_volatile_u32(abort_addr)) break;
         tc_fence_after();
         const uint32_t a0 = sb + L::kAOff + s * L::kAStage;
         const uint32_t b0 = sb + L::kBOff + s * L::kB;
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         atomicOr(a.err, kErrTmaTimeout);
         break;
       }
-      if (*abort_flag) break;
+      if (lds_volatile_u32(abort_addr)) break;
       // explicit shared-space accesses: the realigned base is a generic pointer
       const uint32_t pk = sb + L::kPkOff + s * L::kPk;
       const uint32_t bt = sb + L::kBOff + s * L::kB;
@@ -383,6 +384,7 @@ __global__ void __launch_bounds__(kNrThreads, 1)
   const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
   const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
   volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  const uint32_t abort_addr = sb + L::kHolder + 8;
   if (nit == 0) return;   // a split past the block's last stage (uniform per CTA)
 
   if (threadIdx.x == 0) {
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(kNrThreads, 1)
           atomicOr(a.err, kErrMmaTimeout);
           break;
         }
-        if (*abort_flag) break;
+        if (lds_volatile_u32(abort_addr)) break;
         const uint32_t st = sb + s * L::kStage;
         mbar_arrive_expect_tx(full(s), 2 * L::kB + L::kPk);
         const int32_t x = a.a_x0 + int32_t((it0 + it) * kTcK);
@@ -448,7 +450,7 @@ __global__ void __launch_bounds__(kNrThreads, 1)
           atomicOr(a.err, kErrMmaTimeout);
           break;
         }
-        if (*abort_flag) break;
+        if (lds_volatile_u32(abort_addr)) break;
         tc_fence_after();
         const uint32_t st = sb + s * L::kStage;
 #pragma unroll
@@ -483,7 +485,7 @@ __global__ void __launch_bounds__(kNrThreads, 1)
         atomicOr(a.err, kErrTmaTimeout);
         break;
       }
-      if (*abort_flag) break;
+      if (lds_volatile_u32(abort_addr)) break;
       // explicit shared-space accesses: the realigned base is a generic pointer
       const uint32_t pk = sb + s * L::kStage + L::kPkOff;
       const uint32_t ad = sb + s * L::kStage + L::kADos;
@@ -722,6 +724,7 @@ __global__ void __launch_bounds__(kBwThreads, 1)
   const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
   const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
   volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  const uint32_t abort_addr = sb + L::kHolder + 8;
 
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < ST; ++s) {
@@ -756,7 +759,7 @@ __global__ void __launch_bounds__(kBwThreads, 1)
           atomicOr(a.err, kErrMmaTimeout);
           break;
         }
-        if (*abort_flag) break;
+        if (lds_volatile_u32(abort_addr)) break;
         const uint32_t st = sb + s * L::kStage;
         mbar_arrive_expect_tx(full(s), L::kB + L::kPk + L::kDs);
         tma_load_2d(st + L::kPkOff, &rmap, int32_t(it * (kBwK / 4)), int32_t(vtile * kBwM),
@@ -786,7 +789,7 @@ __global__ void __launch_bounds__(kBwThreads, 1)
           atomicOr(a.err, kErrMmaTimeout);
           break;
         }
-        if (*abort_flag) break;
+        if (lds_volatile_u32(abort_addr)) break;
         tc_fence_after();
         const uint32_t a0 = sb + s * L::kStage + L::kAOff;
         const uint32_t b0 = sb + s * L::kStage + L::kBOff;
@@ -825,7 +828,7 @@ __global__ void __launch_bounds__(kBwThreads, 1)
         ok = false;
         break;
       }
-      if (*abort_flag) {
+      if (lds_volatile_u32(abort_addr)) {
         ok = false;
         break;
       }
@@ -913,7 +916,7 @@ __global__ void __launch_bounds__(kBwThreads, 1)
     for (uint32_t k = 0; k < kBwScores; ++k) swap[(half * kBwM + r) * kBwScores + k] = gcd[k];
     named_barrier(1, kBwExpand);
     const uint64_t v = uint64_t(vtile) * kBwM + r;
-    if (ok && !*abort_flag && v < a.V) {
+    if (ok && !lds_volatile_u32(abort_addr) && v < a.V) {
 #pragma unroll
       for (uint32_t k = 0; k < 8; ++k) {
         const uint32_t kl = 8 * half + k;
