@@ -150,6 +150,45 @@ static gnm_status guarded(gnm_error* err, F&& f) {
 }
 
 // ---- validation (prepare.rs:760-790 invariants) ----------------------------
+// Runs f(begin, end, chunk) over [0, n) on up to 16 host threads (chunks of at
+// least `min_chunk`); f must not throw.
+template <class F>
+static void parallel_chunks(uint64_t n, uint64_t min_chunk, F f) {
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const uint64_t nt =
+      std::max<uint64_t>(1, std::min<uint64_t>(hw, n / std::max<uint64_t>(1, min_chunk)));
+  if (nt == 1) {
+    f(uint64_t(0), n, uint64_t(0));
+    return;
+  }
+  std::vector<std::thread> th;
+  for (uint64_t i = 0; i < nt; ++i) th.emplace_back(f, n * i / nt, n * (i + 1) / nt, i);
+  for (auto& x : th) x.join();
+}
+
+// First failure over parallel chunks (lowest index wins, as a serial scan).
+struct ChunkErrors {
+  std::vector<uint64_t> at;
+  std::vector<const char*> what;
+  ChunkErrors() : at(16, UINT64_MAX), what(16, nullptr) {}
+  void set(uint64_t chunk, uint64_t index, const char* msg) {
+    if (index < at[chunk]) {
+      at[chunk] = index;
+      what[chunk] = msg;
+    }
+  }
+  void raise() const {
+    uint64_t best = UINT64_MAX;
+    const char* msg = nullptr;
+    for (size_t i = 0; i < at.size(); ++i)
+      if (at[i] < best) {
+        best = at[i];
+        msg = what[i];
+      }
+    if (msg) fail(GNM_ERR_INVALID, msg);
+  }
+};
+
 static void validate_prep(const gnm_prep_view* p) {
   if (!p) fail(GNM_ERR_INVALID, "prep is NULL");
   if (p->num_scores == 0) fail(GNM_ERR_INVALID, "num_scores must be > 0");
@@ -162,25 +201,49 @@ static void validate_prep(const gnm_prep_view* p) {
   if (p->num_people > 0 && !p->output_idx_to_fam_idx && p->num_people > p->total_people_in_fam)
     fail(GNM_ERR_INVALID, "num_people exceeds total_people_in_fam with identity mapping");
   const uint64_t* offs = p->sparse_row_offsets;
-  if (p->num_variants > 0) {
+  const uint64_t V = p->num_variants;
+  if (V > 0) {
     if (offs[0] != 0) fail(GNM_ERR_INVALID, "sparse_row_offsets[0] must be 0");
-    for (uint64_t v = 0; v < p->num_variants; ++v)
-      if (offs[v + 1] < offs[v]) fail(GNM_ERR_INVALID, "sparse_row_offsets not monotone");
-    const uint64_t nnz = offs[p->num_variants];
+    ChunkErrors mono;
+    parallel_chunks(V, 1 << 16, [&](uint64_t b, uint64_t e, uint64_t c) {
+      for (uint64_t v = b; v < e; ++v)
+        if (offs[v + 1] < offs[v]) {
+          mono.set(c, v, "sparse_row_offsets not monotone");
+          return;
+        }
+    });
+    mono.raise();
+    const uint64_t nnz = offs[V];
     if (nnz && (!p->sparse_weights || !p->sparse_missing_corrections || !p->sparse_score_columns))
       fail(GNM_ERR_INVALID, "CSR arrays are NULL");
-    for (uint64_t v = 0; v < p->num_variants; ++v)
-      for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
-        if (p->sparse_score_columns[e] >= p->num_scores)
-          fail(GNM_ERR_INVALID, "CSR score column out of range");
-        if (e > offs[v] && p->sparse_score_columns[e] <= p->sparse_score_columns[e - 1])
-          fail(GNM_ERR_INVALID, "CSR columns must be strictly ascending within a row");
-      }
+    const uint32_t* cols = p->sparse_score_columns;
+    ChunkErrors col;
+    parallel_chunks(V, 1 << 14, [&](uint64_t b, uint64_t e, uint64_t c) {
+      for (uint64_t v = b; v < e; ++v)
+        for (uint64_t x = offs[v]; x < offs[v + 1]; ++x) {
+          if (cols[x] >= p->num_scores) {
+            col.set(c, v, "CSR score column out of range");
+            return;
+          }
+          if (x > offs[v] && cols[x] <= cols[x - 1]) {
+            col.set(c, v, "CSR columns must be strictly ascending within a row");
+            return;
+          }
+        }
+    });
+    col.raise();
   }
-  if (p->output_idx_to_fam_idx)
-    for (uint64_t o = 0; o < p->num_people; ++o)
-      if (p->output_idx_to_fam_idx[o] >= p->total_people_in_fam)
-        fail(GNM_ERR_INVALID, "output_idx_to_fam_idx entry out of range");
+  if (p->output_idx_to_fam_idx) {
+    ChunkErrors map;
+    parallel_chunks(p->num_people, 1 << 16, [&](uint64_t b, uint64_t e, uint64_t c) {
+      for (uint64_t o = b; o < e; ++o)
+        if (p->output_idx_to_fam_idx[o] >= p->total_people_in_fam) {
+          map.set(c, o, "output_idx_to_fam_idx entry out of range");
+          return;
+        }
+    });
+    map.raise();
+  }
 }
 
 static bool device_available(int device) {
@@ -192,28 +255,6 @@ static bool device_available(int device) {
   return device < n;
 }
 
-// Optional phase trace of plan creation and gnm_score_run / gnm_score_run_ex
-// on stderr (environment variable GNM_TRACE set and not "0"): host wall time
-// of each phase, after synchronising the streams it waited on.
-namespace {
-struct PhaseTrace {
-  bool on = false;
-  std::chrono::steady_clock::time_point t0, last;
-  PhaseTrace() {
-    const char* e = std::getenv("GNM_TRACE");
-    on = e && *e && std::strcmp(e, "0") != 0;
-    t0 = last = std::chrono::steady_clock::now();
-  }
-  void mark(const char* phase) {
-    if (!on) return;
-    const auto now = std::chrono::steady_clock::now();
-    std::fprintf(stderr, "gnm_trace %-22s %9.3f ms  (total %9.3f ms)\n", phase,
-                 std::chrono::duration<double, std::milli>(now - last).count(),
-                 std::chrono::duration<double, std::milli>(now - t0).count());
-    last = now;
-  }
-};
-}  // namespace
 
 // ---- plan --------------------------------------------------------------------
 static void plain_geometry(gnm_plan* p) {
@@ -335,9 +376,10 @@ static const uint8_t* plain_tables_for(gnm_plan* p, uint64_t k, uint64_t v0, uin
   return p->d_tab_scratch;
 }
 
-static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, int device) {
+static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, int device,
+                                  bool validated = false) {
   PhaseTrace trace;
-  validate_prep(prep);
+  if (!validated) validate_prep(prep);
   trace.mark("  plan: validate");
   if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
   if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
@@ -378,18 +420,12 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
     check_cuda(cudaMemset(p->d_err, 0, 4), "memset");
 
     trace.mark("  plan: baseline, maps");
-    p->h_offs.assign(prep->sparse_row_offsets, prep->sparse_row_offsets + p->V + 1);
-    if (nnz) {
-      p->h_w.assign(prep->sparse_weights, prep->sparse_weights + nnz);
-      p->h_corr.assign(prep->sparse_missing_corrections, prep->sparse_missing_corrections + nnz);
-      p->h_cols.assign(prep->sparse_score_columns, prep->sparse_score_columns + nnz);
-    }
     if (p->engine == GNM_ENGINE_PLAIN) {
       plain_geometry(p);
       trace.mark("  plan: csr copy, geometry");
       build_plain_records(p, prep, trace);
     } else {
-      tensor_plan_create(p);
+      tensor_plan_create(p, prep, &trace);
     }
     trace.mark("  plan: weights, tables");
     // only the default stream: a concurrent run may be streaming rows
@@ -553,6 +589,104 @@ static bool is_pinned(const void* ptr) {
   return at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeManaged;
 }
 
+// Device -> host copy of a result array.  Large copies into pageable memory go
+// through a cached pinned ring (two 64 MB chunks): the DMA fills one chunk at
+// the link rate while host threads copy the other out (a direct pageable copy
+// of the batched workload's 0.6 GB of results ran at ~4 GB/s).
+namespace {
+std::mutex g_ring_mu;
+uint8_t* g_ring[2] = {nullptr, nullptr};
+constexpr uint64_t kRingChunk = uint64_t(64) << 20;
+}  // namespace
+
+static void release_result_ring() {
+  std::lock_guard<std::mutex> lock(g_ring_mu);
+  for (auto*& r : g_ring) {
+    if (r) cudaFreeHost(r);
+    r = nullptr;
+  }
+}
+
+static void copy_to_host(void* dst, const void* src, uint64_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  if (bytes < 2 * kRingChunk || is_pinned(dst)) {
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "D2H results");
+    check_cuda(cudaStreamSynchronize(s), "D2H results");
+    return;
+  }
+  std::lock_guard<std::mutex> lock(g_ring_mu);
+  for (auto*& r : g_ring)
+    if (!r) check_cuda(cudaHostAlloc(&r, kRingChunk, cudaHostAllocDefault), "cudaHostAlloc");
+  cudaEvent_t landed[2] = {nullptr, nullptr};
+  struct Ev {
+    cudaEvent_t* e;
+    ~Ev() {
+      for (int i = 0; i < 2; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } ev{landed};
+  for (auto& e : landed) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  const uint64_t n = (bytes + kRingChunk - 1) / kRingChunk;
+  auto issue = [&](uint64_t i) {
+    const uint64_t off = i * kRingChunk, len = std::min(kRingChunk, bytes - off);
+    check_cuda(cudaMemcpyAsync(g_ring[i % 2], static_cast<const uint8_t*>(src) + off, len,
+                               cudaMemcpyDeviceToHost, s),
+               "D2H results");
+    check_cuda(cudaEventRecord(landed[i % 2], s), "event");
+  };
+  issue(0);
+  for (uint64_t i = 0; i < n; ++i) {
+    check_cuda(cudaEventSynchronize(landed[i % 2]), "D2H results");
+    if (i + 1 < n) issue(i + 1);   // the other chunk was copied out last iteration
+    const uint64_t off = i * kRingChunk, len = std::min(kRingChunk, bytes - off);
+    const uint8_t* from = g_ring[i % 2];
+    uint8_t* to = static_cast<uint8_t*>(dst) + off;
+    parallel_chunks(len, uint64_t(4) << 20, [&](uint64_t b, uint64_t e, uint64_t) {
+      std::memcpy(to + b, from + b, e - b);
+    });
+  }
+}
+
+// Host -> device copy of a large pageable array (the tensor plan's CSR)
+// through the same pinned ring: host threads fill one chunk while the DMA
+// sends the other (a direct pageable copy of the batched workload's 1.6 GB
+// CSR ran at ~10 GB/s).
+void copy_to_device(void* dst, const void* src, uint64_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  if (bytes < 2 * kRingChunk || is_pinned(src)) {
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "H2D upload");
+    check_cuda(cudaStreamSynchronize(s), "H2D upload");
+    return;
+  }
+  std::lock_guard<std::mutex> lock(g_ring_mu);
+  for (auto*& r : g_ring)
+    if (!r) check_cuda(cudaHostAlloc(&r, kRingChunk, cudaHostAllocDefault), "cudaHostAlloc");
+  cudaEvent_t sent[2] = {nullptr, nullptr};
+  struct Ev {
+    cudaEvent_t* e;
+    ~Ev() {
+      for (int i = 0; i < 2; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } ev{sent};
+  for (auto& e : sent) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  const uint64_t n = (bytes + kRingChunk - 1) / kRingChunk;
+  for (uint64_t i = 0; i < n; ++i) {
+    const int slot = int(i % 2);
+    if (i >= 2) check_cuda(cudaEventSynchronize(sent[slot]), "H2D upload");
+    const uint64_t off = i * kRingChunk, len = std::min(kRingChunk, bytes - off);
+    const uint8_t* from = static_cast<const uint8_t*>(src) + off;
+    uint8_t* to = g_ring[slot];
+    parallel_chunks(len, uint64_t(4) << 20, [&](uint64_t b, uint64_t e, uint64_t) {
+      std::memcpy(to + b, from + b, e - b);
+    });
+    check_cuda(cudaMemcpyAsync(static_cast<uint8_t*>(dst) + off, to, len, cudaMemcpyHostToDevice, s),
+               "H2D upload");
+    check_cuda(cudaEventRecord(sent[slot], s), "event");
+  }
+  check_cuda(cudaStreamSynchronize(s), "H2D upload");
+}
+
 // Copy rows [v0, v0+n) into dst (pitch layout); zero the padding.
 static void gather_rows(const HostRun& r, uint64_t v0, uint64_t n, uint8_t* dst) {
   const uint64_t bpv = r.bpv;
@@ -669,6 +803,12 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   uint64_t block = o.block_variants ? o.block_variants : remaining;
   const uint64_t cap_rows = std::max<uint64_t>(kPlainRows, uint64_t(0.6 * double(free_b)) / pitch);
   if (!o.block_variants && block > cap_rows) block = std::max<uint64_t>(kPlainRows, cap_rows / 2);
+  // The tensor engine's accumulate takes about as long as the copy of the
+  // rows (batched workload: 365 ms against ~230 ms), so its rows go in four
+  // blocks and each block's accumulate overlaps the next block's copy; the
+  // plain engine's accumulate is ~2% of the copy, one block is best there.
+  if (!o.block_variants && engine == GNM_ENGINE_TENSOR && remaining >= 4 * kTensorMinBlock)
+    block = std::min(block, (remaining + 3) / 4);
   block = std::max<uint64_t>(1, std::min<uint64_t>(block, std::max<uint64_t>(1, remaining)));
   if (engine == GNM_ENGINE_TENSOR) block = (block + 63) / 64 * 64;
   const int nbuf = remaining > block ? 2 : 1;
@@ -785,7 +925,7 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   std::thread planner([&] {
     try {
       DeviceGuard pg(device);
-      p = plan_create_impl(prep, engine, device);
+      p = plan_create_impl(prep, engine, device, true);
     } catch (...) {
       plan_error = std::current_exception();
     }
@@ -837,12 +977,9 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
     trace.mark("accumulate");
   }
   finalize_impl(p, d_sums, d_cnt, resume == nullptr, cs);
-  check_cuda(cudaMemcpyAsync(sums_out, d_sums, P * K * sizeof(double), cudaMemcpyDeviceToHost, cs),
-             "D2H sums");
-  check_cuda(
-      cudaMemcpyAsync(missing_out, d_cnt, P * K * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs),
-      "D2H counts");
   sync_impl(p, cs);
+  copy_to_host(sums_out, d_sums, P * K * sizeof(double), cs);
+  copy_to_host(missing_out, d_cnt, P * K * sizeof(uint32_t), cs);
   trace.mark("finalize + results");
   if (resume)
     for (uint64_t x = 0; x < P * K; ++x) {
@@ -977,6 +1114,7 @@ gnm_status gnm_release_cached_memory(int device, gnm_error* err) {
     if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
     DeviceGuard g(device);
     check_cuda(cudaMemPoolTrimTo(run_pool(device), 0), "cudaMemPoolTrimTo");
+    release_result_ring();
   });
 }
 

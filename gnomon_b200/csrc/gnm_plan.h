@@ -1,6 +1,10 @@
 // gnm_plan.h — the plan object behind the C ABI (host side).
 #pragma once
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -30,6 +34,31 @@ struct DeviceGuard {
 // Device buffers of plans come from the library's per-device memory pool.
 void* pool_alloc(int device, uint64_t bytes, const char* what);
 void pool_free(void* ptr);
+
+// Optional phase trace of plan creation and gnm_score_run / gnm_score_run_ex
+// on stderr (environment variable GNM_TRACE set and not "0"): host wall time
+// of each phase, after synchronising the streams it waited on.
+struct PhaseTrace {
+  bool on = false;
+  std::chrono::steady_clock::time_point t0, last;
+  PhaseTrace() {
+    const char* e = std::getenv("GNM_TRACE");
+    on = e && *e && std::strcmp(e, "0") != 0;
+    t0 = last = std::chrono::steady_clock::now();
+  }
+  void mark(const char* phase) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "gnm_trace %-22s %9.3f ms  (total %9.3f ms)\n", phase,
+                 std::chrono::duration<double, std::milli>(now - last).count(),
+                 std::chrono::duration<double, std::milli>(now - t0).count());
+    last = now;
+  }
+};
+
+// Synchronous host -> device copy on stream s; large pageable sources go
+// through a pinned ring with threaded host copies.
+void copy_to_device(void* dst, const void* src, uint64_t bytes, cudaStream_t s);
 
 CUtensorMap make_row_map(const uint8_t* d_rows, uint64_t bytes_per_row, uint64_t num_rows,
                          uint64_t pitch, uint32_t box_x, uint32_t box_y);
@@ -70,10 +99,6 @@ struct gnm_plan {
   uint64_t launches = 0;
   double last_spotcheck = 0.0;
 
-  // CSR kept on host for the tensor engine / backward
-  std::vector<float> h_w, h_corr;
-  std::vector<uint32_t> h_cols;
-  std::vector<uint64_t> h_offs;
 
   gnm::TensorPlan* tensor = nullptr;
 };

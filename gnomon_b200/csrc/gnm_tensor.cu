@@ -569,8 +569,35 @@ __global__ void __launch_bounds__(kNrThreads, 1)
 }
 
 // Limb planes from the CSR: one thread per variant.
+// Per-score max(|w|, |corr|) as float bit patterns (non-negative floats order
+// like their bits): shared-memory maxima per block, then one global atomic per
+// score and block (global atomics only when the scores do not fit).
+constexpr uint64_t kAmaxSharedScores = 8192;
+__global__ void gnm_tc_amax(const float* w, const float* corr, const uint32_t* cols, uint64_t nnz,
+                            uint64_t K_pad, uint32_t* amax_bits) {
+  extern __shared__ uint32_t s_max[];
+  const bool shared = K_pad <= kAmaxSharedScores;
+  if (shared) {
+    for (uint64_t k = threadIdx.x; k < K_pad; k += blockDim.x) s_max[k] = 0u;
+    __syncthreads();
+  }
+  for (uint64_t e = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < nnz;
+       e += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t m = __float_as_uint(fmaxf(fabsf(w[e]), fabsf(corr[e])));
+    if (shared)
+      atomicMax(s_max + cols[e], m);
+    else
+      atomicMax(amax_bits + cols[e], m);
+  }
+  if (shared) {
+    __syncthreads();
+    for (uint64_t k = threadIdx.x; k < K_pad; k += blockDim.x)
+      if (s_max[k]) atomicMax(amax_bits + k, s_max[k]);
+  }
+}
+
 __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uint32_t* cols,
-                                    const uint64_t* offs, uint64_t V, const float* qhi,
+                                    const uint64_t* offs, uint64_t V, const uint32_t* amax_bits,
                                     __nv_bfloat16* dos, __nv_bfloat16* mis, uint64_t K_pad,
                                     uint64_t V_pad) {
   const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -578,9 +605,17 @@ __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uin
   const uint64_t plane = K_pad * V_pad;
   for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
     const uint32_t k = cols[e];
-    // quanta q, q/2^8, q/2^16, q/2^24 (powers of two: the divisions are exact and
-    // every residual below is exact in FP32)
-    const float q = qhi[k], qm = q * (1.0f / 256.0f), ql = q * (1.0f / 65536.0f),
+    // quantum q = 2^(E-8) with amax = f 2^E, f in [0.5, 1); then q/2^8, q/2^16,
+    // q/2^24 (powers of two: the divisions are exact and every residual below
+    // is exact in FP32)
+    float q = 1.0f;
+    const float am = __uint_as_float(amax_bits[k]);
+    if (am > 0.0f) {
+      int ex = 0;
+      frexpf(am, &ex);
+      q = ldexpf(1.0f, max(ex - 8, -125));   // q / 2^24 stays a (subnormal) FP32 value
+    }
+    const float qm = q * (1.0f / 256.0f), ql = q * (1.0f / 65536.0f),
                 ql2 = q * (1.0f / 16777216.0f);
     const uint64_t at = uint64_t(k) * V_pad + v;
     const float xs[2] = {w[e], -corr[e]};
@@ -1081,7 +1116,10 @@ static uint32_t narrow_splits(uint64_t base_ctas, uint64_t stages, int sms) {
   return best;
 }
 
-void tensor_plan_create(gnm_plan* p) {
+void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trace) {
+  auto mark = [&](const char* what) {
+    if (trace) trace->mark(what);
+  };
   auto* t = new TensorPlan();
   p->tensor = t;
   t->K_pad = (p->K + kTcM - 1) / kTcM * kTcM;
@@ -1092,18 +1130,6 @@ void tensor_plan_create(gnm_plan* p) {
   t->narrow = p->K <= kNarrowMaxScores;
   if (t->V_pad > (uint64_t(1) << 31)) fail(GNM_ERR_INVALID, "too many variants for the tensor engine");
 
-  // per-score quantum q = 2^(E-8), 2^E >= max |x| over the score's values
-  std::vector<float> amax(t->K_pad, 0.f), qhi(t->K_pad, 1.f);
-  for (size_t e = 0; e < p->h_cols.size(); ++e) {
-    const uint32_t k = p->h_cols[e];
-    amax[k] = std::max(amax[k], std::max(std::fabs(p->h_w[e]), std::fabs(p->h_corr[e])));
-  }
-  for (uint64_t k = 0; k < t->K_pad; ++k)
-    if (amax[k] > 0.f) {
-      int ex = 0;
-      std::frexp(amax[k], &ex);  // amax = f * 2^ex, f in [0.5, 1)
-      qhi[k] = std::ldexp(1.0f, ex - 8);
-    }
   const uint64_t plane = t->K_pad * t->V_pad;
   auto alloc = [&](void** ptr, uint64_t bytes, const char* what) {
     *ptr = pool_alloc(p->device, bytes, what);
@@ -1127,9 +1153,11 @@ void tensor_plan_create(gnm_plan* p) {
   alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->part_elems * 4, "cudaMalloc(partials)");
   check_cuda(cudaMemset(t->d_planes_dos, 0, 4 * plane * 2), "memset planes");
   check_cuda(cudaMemset(t->d_planes_mis, 0, 4 * plane * 2), "memset planes");
+  mark("  tensor: planes alloc");
 
-  const uint64_t nnz = p->h_cols.size();
-  float *dw = nullptr, *dc = nullptr, *dq = nullptr;
+  const uint64_t nnz = p->V ? prep->sparse_row_offsets[p->V] : 0;
+  float *dw = nullptr, *dc = nullptr;
+  uint32_t* dq = nullptr;
   uint32_t* dcol = nullptr;
   uint64_t* doff = nullptr;
   dw = static_cast<decltype(dw)>(
@@ -1140,8 +1168,7 @@ void tensor_plan_create(gnm_plan* p) {
       pool_alloc(p->device, std::max<uint64_t>(1, nnz) * 4, "plane build inputs"));
   doff = static_cast<decltype(doff)>(
       pool_alloc(p->device, (p->V + 1) * 8, "plane build inputs"));
-  dq = static_cast<decltype(dq)>(
-      pool_alloc(p->device, t->K_pad * 4, "plane build inputs"));
+  dq = static_cast<uint32_t*>(pool_alloc(p->device, t->K_pad * 4, "plane build inputs"));
   struct Tmp {
     void* a[5];
     ~Tmp() {
@@ -1149,18 +1176,27 @@ void tensor_plan_create(gnm_plan* p) {
     }
   } tmp{{dw, dc, dcol, doff, dq}};
   if (nnz) {
-    check_cuda(cudaMemcpy(dw, p->h_w.data(), nnz * 4, cudaMemcpyHostToDevice), "upload");
-    check_cuda(cudaMemcpy(dc, p->h_corr.data(), nnz * 4, cudaMemcpyHostToDevice), "upload");
-    check_cuda(cudaMemcpy(dcol, p->h_cols.data(), nnz * 4, cudaMemcpyHostToDevice), "upload");
+    copy_to_device(dw, prep->sparse_weights, nnz * 4, 0);
+    copy_to_device(dc, prep->sparse_missing_corrections, nnz * 4, 0);
+    copy_to_device(dcol, prep->sparse_score_columns, nnz * 4, 0);
   }
-  check_cuda(cudaMemcpy(doff, p->h_offs.data(), (p->V + 1) * 8, cudaMemcpyHostToDevice), "upload");
-  check_cuda(cudaMemcpy(dq, qhi.data(), t->K_pad * 4, cudaMemcpyHostToDevice), "upload");
+  copy_to_device(doff, prep->sparse_row_offsets, (p->V + 1) * 8, 0);
+  mark("  tensor: csr upload");
+  // per-score quantum from max |x| over the score's values (on the device)
+  check_cuda(cudaMemset(dq, 0, t->K_pad * 4), "memset");
+  if (nnz) {
+    const uint32_t smem = t->K_pad <= kAmaxSharedScores ? uint32_t(t->K_pad * 4) : 0u;
+    const uint64_t blocks = std::min<uint64_t>((nnz + 255) / 256, 4096);
+    gnm_tc_amax<<<uint32_t(blocks), 256, smem>>>(dw, dc, dcol, nnz, t->K_pad, dq);
+    check_cuda(cudaGetLastError(), "weight maximum launch");
+  }
   if (p->V) {
     gnm_tc_build_planes<<<uint32_t((p->V + 255) / 256), 256>>>(
         dw, dc, dcol, doff, p->V, dq, t->d_planes_dos, t->d_planes_mis, t->K_pad, t->V_pad);
     check_cuda(cudaGetLastError(), "plane build launch");
   }
   check_cuda(cudaStreamSynchronize(0), "plane build");
+  mark("  tensor: plane build");
   t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcM, kTcPlanes);
   t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcM, kTcPlanes);
   if (t->narrow) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 struct gnm_plan;
+struct gnm_prep_view;
 
 namespace gnm {
 
@@ -13,7 +14,12 @@ namespace gnm {
 // 2.25 ms against 16 x 0.33 ms).
 constexpr uint64_t kTensorMinScores = 8;
 
-void tensor_plan_create(gnm_plan* p);
+// Smallest row block the end-to-end call splits the tensor engine's rows into.
+constexpr uint64_t kTensorMinBlock = 16384;
+
+struct PhaseTrace;
+// Builds the limb planes from the caller's CSR (read during the call only).
+void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trace);
 void tensor_plan_destroy(gnm_plan* p);
 void tensor_reset(gnm_plan* p, cudaStream_t s);
 void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,

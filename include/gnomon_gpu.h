@@ -177,10 +177,12 @@ gnm_status gnm_plan_sync(gnm_plan* plan, void* stream, gnm_error* err);
 
 /* gnm_score_run / gnm_score_run_ex allocate their row blocks, staging and
  * output buffers from a per-device memory pool that keeps freed memory
- * reserved, so repeated runs on a device skip mapping and unmapping it.  This
- * returns that reserve to the device (-1 = current device); it is safe to
- * call at any time and frees nothing a running call holds.  No reference
- * counterpart (the reference's engine allocates and frees per call). */
+ * reserved, so repeated runs on a device skip mapping and unmapping it, and
+ * copy large results back through a cached 128 MB pinned host ring.  This
+ * returns that reserve to the device (-1 = current device) and frees the
+ * ring; it is safe to call at any time and frees nothing a running call
+ * holds.  No reference counterpart (the reference's engine allocates and
+ * frees per call). */
 gnm_status gnm_release_cached_memory(int device, gnm_error* err);
 
 /* Device watchdog self-test (no reference counterpart; the reference's GPU
