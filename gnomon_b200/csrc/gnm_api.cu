@@ -325,7 +325,7 @@ static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep, PhaseTra
 
   // Stage tables (the 3-variant lookup tables) of every score, built once on
   // the device while they fit the cache budget; blocks that start on a
-  // 24-variant boundary read them directly.  Otherwise each accumulate call
+  // kPlainRows-variant boundary read them directly.  Otherwise each accumulate call
   // builds the tables of its block into a one-score scratch.
   const uint64_t stages = (p->V + kPlainRows - 1) / kPlainRows;
   if (p->K * stages * kPlainTableBytes <= kTableCacheBytes) {
@@ -355,7 +355,7 @@ static const uint8_t* plain_tables_for(gnm_plan* p, uint64_t k, uint64_t v0, uin
     if (cs != cudaStreamCaptureStatusNone)
       fail(GNM_ERR_INVALID, "stage-table scratch must grow during stream capture: run one "
                             "uncaptured pass over the same block first, or start blocks on "
-                            "a multiple of 24 variants");
+                            "a multiple of " + std::to_string(kPlainRows) + " variants");
     check_cuda(cudaStreamSynchronize(s), "stream synchronize");
     if (p->d_tab_scratch) {
       pool_free(p->d_tab_scratch);

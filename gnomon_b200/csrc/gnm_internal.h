@@ -19,11 +19,11 @@ enum : uint32_t {
 constexpr uint32_t kPlainThreads = 256;      // one 32-bit word column (16 people) each
 constexpr uint32_t kPlainTileBytes = 1024;   // bytes of a row per CTA (4096 people)
 constexpr uint32_t kPlainBoxBytes = 256;     // TMA box inner extent (max 256 elements)
-constexpr uint32_t kPlainRows = 24;          // variant rows per pipeline stage (8 groups of 3)
+constexpr uint32_t kPlainRows = 30;          // variant rows per pipeline stage (10 groups of 3)
 constexpr uint32_t kPlainGroups = kPlainRows / 3;
-// One stage table: 8 group tables of 64 FP32 entries (256 B each) + the
+// One stage table: 10 group tables of 64 FP32 entries (256 B each) + the
 // stage's membership word, padded to a multiple of 16 bytes (bulk copies).
-constexpr uint32_t kPlainTableBytes = kPlainGroups * 256 + 16;   // 2064
+constexpr uint32_t kPlainTableBytes = kPlainGroups * 256 + 16;   // 2576
 constexpr uint32_t kRecordPad = 64;          // zero records past the last variant
 constexpr uint64_t kTableCacheBytes = uint64_t(4) << 30;  // per-plan stage-table cache budget
 
