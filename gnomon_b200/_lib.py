@@ -92,7 +92,6 @@ SIGNATURES = {
     "gnm_synth_fill_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,
                                         C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,
                                         C.POINTER(gnm_error)]),
-    "gnm_plan_last_spotcheck": (C.c_double, [C.c_void_p]),
     "gnm_backward_dw_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.POINTER(gnm_error)]),

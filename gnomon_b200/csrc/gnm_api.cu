@@ -1043,7 +1043,6 @@ void gnm_plan_destroy(gnm_plan* p) {
 gnm_engine gnm_plan_engine(const gnm_plan* p) { return p ? p->engine : GNM_ENGINE_AUTO; }
 uint64_t gnm_plan_device_bytes(const gnm_plan* p) { return p ? p->device_bytes : 0; }
 uint64_t gnm_plan_launch_count(const gnm_plan* p) { return p ? p->launches : 0; }
-double gnm_plan_last_spotcheck(const gnm_plan* p) { return p ? p->last_spotcheck : 0.0; }
 
 gnm_status gnm_plan_reset(gnm_plan* p, void* stream, gnm_error* err) {
   if (!p) return GNM_ERR_INVALID;

@@ -97,7 +97,6 @@ struct gnm_plan {
   std::vector<double> h_baseline;
   uint64_t device_bytes = 0;
   uint64_t launches = 0;
-  double last_spotcheck = 0.0;
 
 
   gnm::TensorPlan* tensor = nullptr;

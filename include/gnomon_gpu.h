@@ -207,9 +207,10 @@ uint64_t gnm_plan_launch_count(const gnm_plan* plan);
 /* Autotuner (no reference counterpart; the reference sizes its tiles from free
  * memory only, score/cuda_backend.rs:803-975): times the plan's accumulate on
  * the first `variant_count` resident rows for each candidate launch shape —
- * plain engine: variant-split count (1x/2x/4x of the default); tensor engine:
- * CTA raster order — keeps the fastest, and leaves the plan reset.  Blocks
- * until done. */
+ * plain engine: variant-split count (1x/2x/4x of the default); tensor engine
+ * with more than 64 scores: CTA raster order (the narrow kernel used up to 64
+ * scores has a single order) — keeps the fastest, and leaves the plan reset.
+ * Blocks until done. */
 gnm_status gnm_plan_autotune(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
                              uint64_t variant_count, void* stream, gnm_error* err);
 
@@ -236,12 +237,6 @@ gnm_status gnm_synth_fill_device(uint8_t* d_rows, uint64_t pitch, uint64_t varia
                                  uint64_t num_people,
                                  const uint32_t* d_thresholds /* [num_variants][3] */,
                                  uint64_t seed, void* stream, gnm_error* err);
-
-/* ---- Split-BF16 tensor-core batched scoring ------------------------------ */
-
-/* Max relative error report of the last tensor-engine run versus its own
- * FP64 spot check (0 if none). */
-double gnm_plan_last_spotcheck(const gnm_plan* plan);
 
 /* ---- Backward: dW = G^T dS by re-unpacking genotypes -------------------- */
 
