@@ -153,3 +153,21 @@ def test_error_report_workload_subsets(cuda, config, people, variants):
     assert rel.max() < TOL
     np.testing.assert_array_equal(pc, ec)
     assert oracle.within_reference_tolerance(ps, es).all()
+
+
+@pytest.mark.parametrize("scores,engine", [(7, _lib.ENGINE_PLAIN), (8, _lib.ENGINE_TENSOR)])
+def test_auto_engine_rule(cuda, scores, engine):
+    """Default options: plain kernel below 8 score columns, tensor engine from
+    8.  Either way the drop-in call's counts are exact and its sums are within
+    the reference's tolerance of the restated reference engine."""
+    from gnomon_b200.device import DevicePlan
+    _, prep, rows, _ = synth_case(1500, 900, scores=scores, config="batched_100k_x_500k_k512")
+    plan = DevicePlan(prep)   # AUTO
+    try:
+        assert plan.engine == engine
+    finally:
+        plan.close()
+    s, c = run(PipelineContext(prep), np.ascontiguousarray(rows).reshape(-1))
+    rs, rc = oracle.score_reference(rows, prep, threads=4)
+    np.testing.assert_array_equal(c, rc)
+    assert oracle.within_reference_tolerance(s, rs).all()
