@@ -11,7 +11,7 @@
 //     code 00 contributes 0), so decode, effect-allele flip and the
 //     missing-call rule become ONE lookup per person per 3 variants; eight
 //     group tables and a membership word make one 2064-byte stage table;
-//   * packed .bed rows are TMA-staged (cp.async.bulk.tensor, no multicast) in
+//   * packed .bed rows are TMA-staged (cp.async.bulk.tensor into this CTA only) in
 //     [30 rows x 1024 bytes] stages together with their stage table (a 1D bulk
 //     copy on the same mbarrier), three buffers deep (30 x 3 ran 4% faster
 //     than 24 x 4, 18 x 5 and 12 x 8 slower: the per-stage wait, release and
