@@ -397,8 +397,21 @@ def gpu_arm(args, rank, world, local_rank):
     # end-to-end through the public C ABI from pinned host memory; every rank
     # runs its shard in lockstep and a step takes the slowest rank's time
     e2e = None
+    host, pin_error = None, None
     if not args.no_e2e:
-        host = torch.empty((V, bpv), dtype=torch.uint8, pin_memory=True)
+        try:
+            host = torch.empty((V, bpv), dtype=torch.uint8, pin_memory=True)
+        except RuntimeError as exc:   # pinned host memory exhausted on this rank
+            pin_error = str(exc).splitlines()[0][:160]
+        if world > 1:   # every rank takes the e2e leg's collectives, or none does
+            ok = torch.tensor([0 if host is None else 1], dtype=torch.int32, device=dev)
+            dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+            if int(ok.item()) == 0:
+                host = None
+                pin_error = pin_error or "pinned host allocation failed on another rank"
+        if host is None:
+            e2e = {"unavailable": f"pinned host rows ({V * bpv / 1e9:.1f} GB per rank): {pin_error}"}
+    if host is not None:
         host.copy_(rows[:, :bpv])
         src = BedSource(host.numpy().reshape(-1))
         ctx = PipelineContext(prep)
