@@ -79,3 +79,33 @@ def test_release_cached_memory_declines_without_cuda_device():
         pytest.skip("a CUDA device is present")
     e = _lib.gnm_error()
     assert _lib.load().gnm_release_cached_memory(-1, C.byref(e)) == _lib.GNM_DECLINED
+
+
+def test_parallel_validation_reports_the_first_bad_row():
+    """The CSR is checked on several host threads; the error reported is the
+    one a serial scan would meet first (lowest variant), not whichever thread
+    finishes first."""
+    from gnomon_b200.prepare import PreparationResult
+    V = 200_000
+    offs = np.arange(V + 1, dtype=np.uint64)              # one cell per variant
+    w = np.zeros(V, np.float32)
+    prep = PreparationResult(w, w.copy(), np.zeros(V, np.uint32), offs, ["S0", "S1"], 8)
+    rows = np.zeros((V, 2), np.uint8)
+    # variant 100,000 gets a second cell with the same column (not ascending);
+    # variant 150,000 a column past the last score
+    offs2 = offs.copy()
+    offs2[100_001:] += 1
+    cols = np.zeros(V + 1, np.uint32)
+    cols[150_001] = 7
+    prep.sparse_row_offsets = offs2
+    prep.sparse_score_columns = cols
+    prep.sparse_weights = np.zeros(V + 1, np.float32)
+    prep.sparse_missing_corrections = np.zeros(V + 1, np.float32)
+    st, msg = _run(prep, rows)
+    assert st == _lib.GNM_ERR_INVALID and "ascending" in msg, msg
+    # with the early error fixed, the later one is reported
+    cols = cols.copy()
+    cols[100_001] = 1
+    prep.sparse_score_columns = cols
+    st, msg = _run(prep, rows)
+    assert st == _lib.GNM_ERR_INVALID and "out of range" in msg, msg
