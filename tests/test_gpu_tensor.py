@@ -171,3 +171,24 @@ def test_auto_engine_rule(cuda, scores, engine):
     rs, rc = oracle.score_reference(rows, prep, threads=4)
     np.testing.assert_array_equal(c, rc)
     assert oracle.within_reference_tolerance(s, rs).all()
+
+
+def test_large_csr_and_results_through_pinned_ring(cuda):
+    """The end-to-end call uploads a CSR above 128 MB per array, and copies
+    results above 128 MB back, through its pinned host ring (host threads
+    fill or drain one 64 MB chunk while the DMA moves the other). Both
+    directions are checked against the restated reference engine."""
+    # 256 people x 131,072 variants x 256 dense scores: 33.5 M cells, 134 MB per CSR array
+    _, prep, rows, _ = synth_case(256, 131_072, scores=256, config="diff_20k_x_200k_k16")
+    assert prep.sparse_weights.nbytes >= (128 << 20)   # the ring is used from 128 MiB
+    s, c = host_run(prep, rows)
+    rs, rc = oracle.score_reference(rows, prep, threads=8)
+    np.testing.assert_array_equal(c, rc)
+    assert oracle.within_reference_tolerance(s, rs).all()
+    # 131,072 people x 256 variants x 128 scores: 134 MB of FP64 sums
+    _, prep, rows, _ = synth_case(131_072, 256, scores=128, config="diff_20k_x_200k_k16")
+    s, c = host_run(prep, rows)
+    assert s.nbytes >= (128 << 20)
+    rs, rc = oracle.score_reference(rows, prep, threads=8)
+    np.testing.assert_array_equal(c, rc)
+    assert oracle.within_reference_tolerance(s, rs).all()
