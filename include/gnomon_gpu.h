@@ -114,7 +114,10 @@ typedef int (*gnm_block_callback)(void* user_ctx, uint64_t completed_variants,
 typedef struct gnm_run_options {
   gnm_engine engine;
   int device;                     /* CUDA ordinal; -1 = current device            */
-  uint64_t block_variants;        /* streaming block; 0 = whole matrix if it fits */
+  uint64_t block_variants;        /* streaming block; 0 = default: the whole matrix
+                                     if it fits (tensor engine: four blocks of at
+                                     least 16,384 variants, each block's compute
+                                     overlapping the next block's copy)           */
   gnm_block_callback on_block;    /* may be NULL                                  */
   void* on_block_ctx;
 } gnm_run_options;
