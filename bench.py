@@ -588,6 +588,102 @@ def stream_arm(args, rank, world, local_rank):
     plan.close()
 
 
+def pgen_arm(args, rank, world, local_rank):
+    """PLINK 2 .pgen -> .bed rows on the device (gnm_pgen_*): a synthetic
+    50,000-sample .pgen of ``--pgen`` variants with linkage (runs of 17
+    variants, 2% of calls redrawn per step, REF/ALT swaps), so the file mixes
+    2-bit, 1-bit, fill and LD-compressed records as real cohorts do.  2048
+    distinct variants are encoded and repeated (each repeat keeps its LD
+    anchors).  ``value``: variants/s of device-timed decodes with the file
+    resident in HBM; ``e2e``: the one-shot ``gnm_pgen_decode_device`` from host
+    bytes, upload of the file included."""
+    import torch
+    from gnomon_b200 import synth
+    from gnomon_b200.device import row_pitch
+    from gnomon_b200.pgen import PgenFile, pgen_dims
+    from gnomon_b200 import _lib
+    import ctypes as C
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = synth.WORKLOADS[args.workload]
+    distinct = 2048
+    reps = max(1, args.pgen // distinct)
+    cats = synth.pgen_ld_categories(w.seed, distinct, w.people)
+    data = np.frombuffer(synth.encode_pgen(cats, repeats=reps), np.uint8)
+    V, n = pgen_dims(data)
+    bpv = (n + 3) // 4
+    pitch = row_pitch(bpv)
+    rows = torch.empty(V * pitch, dtype=torch.uint8, device=dev)
+    from oracle import pgen_oracle   # header counts for the byte accounting only
+    h = pgen_oracle.parse_header(data.tobytes())
+    kinds = np.bincount(h["types"] & 7, minlength=8)
+    record_bytes = int(h["lens"].astype(np.int64).sum())
+    n_ld = int(kinds[2] + kinds[3])
+    algo_bytes = record_bytes + V * bpv                   # records read + rows written
+    s = torch.cuda.Stream(dev)
+    pg = PgenFile(data, device=local_rank)
+    for _ in range(args.warmup):
+        pg.decode(rows, pitch, stream=s)
+    pg.check(s)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        for a, b in ev:
+            a.record(s)
+            pg.decode(rows, pitch, stream=s)
+            b.record(s)
+        s.synchronize()
+    pg.check(s)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = statistics.mean(step_ms)
+    # end to end: host bytes -> rows through the one-shot C ABI call
+    lib = _lib.load()
+    e2e_s = []
+    for i in range(max(1, args.e2e_steps) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e = _lib.gnm_error()
+        _lib.check(lib.gnm_pgen_decode_device(data.ctypes.data, data.nbytes, local_rank,
+                                              rows.data_ptr(), pitch, s.cuda_stream, C.byref(e)), e)
+        if i:
+            e2e_s.append(time.perf_counter() - t0)
+    e2e = statistics.median(e2e_s)
+    hbm, src = peaks()
+    achieved = algo_bytes / (ms / 1e3) / 1e9
+    line = {"metric": "pgen variants decoded/s", "value": V / (ms / 1e3), "unit": "variants/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded HWE categories with linkage, 2048 distinct variants "
+                    "repeated)",
+            "config": {"workload": f"pgen_decode_{n}_x_{V}", "samples": n, "variants": V,
+                       "file_bytes": int(data.nbytes), "record_bytes": record_bytes,
+                       "rows_bytes": V * bpv, "ld_records": n_ld,
+                       "record_types": {str(k): int(c) for k, c in enumerate(kinds) if c},
+                       "l2": "rows written per step exceed L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_source": src,
+                         "algorithmic_bytes_per_step": algo_bytes,
+                         "kernels": "gnm_pgen_direct + gnm_pgen_ld (one decode = both)",
+                         "traffic": None},
+            "e2e": {"value": V / e2e, "unit": "variants/s", "h2d_bytes_per_step": int(data.nbytes),
+                    "d2h_bytes_per_step": 8, "seconds": e2e},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks.summary()}
+    if rank == 0 and not args.no_cpu:
+        k = 64
+        sub = synth.encode_pgen(cats[:k])
+        t0 = time.perf_counter()
+        pgen_oracle.decode_to_bed(sub)
+        t = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": k / t, "unit": "variants/s", "cores": 1, "kind": "port",
+                                "sample": f"oracle decode of the first {k} variants x {n} "
+                                          f"samples, {t:.2f} s"}
+    pg.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -606,6 +702,8 @@ def main():
                     help="stream rows from pinned host memory in blocks of this many variants")
     ap.add_argument("--variants", type=int, default=0,
                     help="override the variant count (small cases for profiler captures)")
+    ap.add_argument("--pgen", type=int, default=0,
+                    help="time .pgen -> .bed decoding of this many variants instead")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -615,6 +713,9 @@ def main():
         return
     if args.stream_block:
         stream_arm(args, rank, world, local_rank)
+        return
+    if args.pgen:
+        pgen_arm(args, rank, world, local_rank)
         return
     if world > 1:
         import datetime

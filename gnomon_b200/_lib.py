@@ -95,6 +95,17 @@ SIGNATURES = {
     "gnm_backward_dw_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.POINTER(gnm_error)]),
+    "gnm_pgen_dims": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
+                                C.POINTER(C.c_uint64), C.POINTER(gnm_error)]),
+    "gnm_pgen_decode_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_void_p, C.c_uint64,
+                                         C.c_void_p, C.POINTER(gnm_error)]),
+    "gnm_pgen_open": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(C.c_void_p),
+                                C.POINTER(gnm_error)]),
+    "gnm_pgen_close": (None, [C.c_void_p]),
+    "gnm_pgen_device_bytes": (C.c_uint64, [C.c_void_p]),
+    "gnm_pgen_decode": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint64,
+                                  C.c_void_p, C.POINTER(gnm_error)]),
+    "gnm_pgen_check": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(gnm_error)]),
     "gnm_score_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.POINTER(gnm_error)]),

@@ -15,7 +15,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libgnomon_gpu.so"
-SOURCES = ["gnm_api.cu", "gnm_plain.cu", "gnm_tensor.cu", "gnm_noalloc.cu"]
+SOURCES = ["gnm_api.cu", "gnm_plain.cu", "gnm_tensor.cu", "gnm_noalloc.cu", "gnm_pgen.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

@@ -126,29 +126,6 @@ static T* dalloc(gnm_plan* p, uint64_t n, const char* what) {
   return static_cast<T*>(ptr);
 }
 
-static void set_error(gnm_error* err, const std::string& m) {
-  if (!err) return;
-  std::snprintf(err->message, sizeof(err->message), "%s", m.c_str());
-}
-
-template <class F>
-static gnm_status guarded(gnm_error* err, F&& f) {
-  try {
-    f();
-    if (err) err->message[0] = '\0';
-    return GNM_OK;
-  } catch (const Failure& e) {
-    set_error(err, e.message);
-    return e.status;
-  } catch (const std::exception& e) {
-    set_error(err, std::string("internal error: ") + e.what());
-    return GNM_ERR_COMPUTE;
-  } catch (...) {
-    set_error(err, "internal error");
-    return GNM_ERR_COMPUTE;
-  }
-}
-
 // ---- validation (prepare.rs:760-790 invariants) ----------------------------
 // Runs f(begin, end, chunk) over [0, n) on up to 16 host threads (chunks of at
 // least `min_chunk`); f must not throw.
@@ -246,14 +223,6 @@ static void validate_prep(const gnm_prep_view* p) {
   }
 }
 
-static bool device_available(int device) {
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
-    cudaGetLastError();
-    return false;
-  }
-  return device < n;
-}
 
 
 // ---- plan --------------------------------------------------------------------

@@ -1,6 +1,7 @@
 // gnm_plan.h — the plan object behind the C ABI (host side).
 #pragma once
 #include <chrono>
+#include <exception>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -30,6 +31,41 @@ struct DeviceGuard {
   explicit DeviceGuard(int dev);
   ~DeviceGuard();
 };
+
+// Runs f at the C-ABI edge: a Failure becomes its status and message, any
+// other exception GNM_ERR_COMPUTE; nothing is thrown across the ABI.
+inline void set_error(gnm_error* err, const std::string& m) {
+  if (!err) return;
+  std::snprintf(err->message, sizeof(err->message), "%s", m.c_str());
+}
+
+template <class F>
+gnm_status guarded(gnm_error* err, F&& f) {
+  try {
+    f();
+    if (err) err->message[0] = '\0';
+    return GNM_OK;
+  } catch (const Failure& e) {
+    set_error(err, e.message);
+    return e.status;
+  } catch (const std::exception& e) {
+    set_error(err, std::string("internal error: ") + e.what());
+    return GNM_ERR_COMPUTE;
+  } catch (...) {
+    set_error(err, "internal error");
+    return GNM_ERR_COMPUTE;
+  }
+}
+
+// A CUDA device with this ordinal exists (clears the error of a failed query).
+inline bool device_available(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return false;
+  }
+  return device < n;
+}
 
 // Device buffers of plans come from the library's per-device memory pool.
 void* pool_alloc(int device, uint64_t bytes, const char* what);

@@ -1,0 +1,165 @@
+"""PLINK 2 ``.pgen`` hard calls decoded on the GPU into ``.bed`` rows.
+
+gnomon scores a ``.pgen`` fileset by presenting it to the scoring engine as a
+virtual ``.bed`` (shared/adapt_plink2.rs:1093-1158): each variant's hard
+calls are decoded (:2108-2666) and packed as the ``.bed`` codes of the
+A1 = ALT dosage.  Here that decode runs on the device
+(``gnm_pgen_decode_device``), writing rows straight into HBM where
+``DevicePlan`` reads them; the file's bytes cross PCIe once, compressed.
+
+Supported: storage modes 0x02 and 0x10 / 0x11 with biallelic hard-call
+records (main-track types 0-4, 6, 7; phase tracks are skipped).  Records
+with multiallelic or dosage tracks are rejected with ``GNM_ERR_INVALID``,
+truncated or malformed files with ``GNM_ERR_IO``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple, Union
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import DevicePlan, _stream_ptr, row_pitch
+from .prepare import PreparationResult
+
+PgenSource = Union[str, os.PathLike, bytes, bytearray, np.ndarray]
+
+
+def _bytes(data: PgenSource) -> np.ndarray:
+    if isinstance(data, (str, os.PathLike)):
+        return np.fromfile(data, dtype=np.uint8)
+    if isinstance(data, (bytes, bytearray)):
+        return np.frombuffer(bytes(data), dtype=np.uint8)
+    return np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+
+
+def pgen_dims(data: PgenSource) -> Tuple[int, int]:
+    """(variants, samples) from a ``.pgen`` header."""
+    buf = _bytes(data)
+    lib = _lib.load()
+    m, n = C.c_uint64(), C.c_uint64()
+    e = _lib.gnm_error()
+    _lib.check(lib.gnm_pgen_dims(buf.ctypes.data, buf.nbytes, C.byref(m), C.byref(n),
+                                 C.byref(e)), e)
+    return int(m.value), int(n.value)
+
+
+def decode_to_device(data: PgenSource, device: Optional[int] = None,
+                     rows: Optional[torch.Tensor] = None, pitch: Optional[int] = None,
+                     stream: Optional[torch.cuda.Stream] = None) -> Tuple[torch.Tensor, int]:
+    """Decode every variant into device ``.bed`` rows; returns (rows, pitch).
+
+    ``rows`` (uint8, 16-byte aligned, at least variants x pitch bytes) may be
+    supplied; otherwise it is allocated with a 128-byte pitch.  Row ``v`` holds
+    ``.pgen`` variant ``v``; bytes past ``ceil(samples / 4)`` are left as
+    they were.  Returns after the decode has finished on ``stream``."""
+    buf = _bytes(data)
+    m, n = pgen_dims(buf)
+    bpv = (n + 3) // 4
+    dev = torch.cuda.current_device() if device is None else device
+    if pitch is None:
+        pitch = row_pitch(bpv)
+    if rows is None:
+        rows = torch.zeros(max(m, 1) * pitch, dtype=torch.uint8, device=torch.device("cuda", dev))
+    if not (rows.is_cuda and rows.dtype == torch.uint8 and rows.numel() >= m * pitch):
+        raise ValueError("rows must be a CUDA uint8 tensor of at least variants x pitch bytes")
+    lib = _lib.load()
+    e = _lib.gnm_error()
+    _lib.check(lib.gnm_pgen_decode_device(buf.ctypes.data, buf.nbytes, dev, rows.data_ptr(),
+                                          pitch, _stream_ptr(stream), C.byref(e)), e)
+    return rows, pitch
+
+
+class PgenFile:
+    """A ``.pgen`` resident on one device (``gnm_pgen_open``): decode any
+    variant range on demand, asynchronously, e.g. block by block into a
+    streaming buffer.  Use from one stream at a time."""
+
+    def __init__(self, data: PgenSource, device: Optional[int] = None):
+        self.lib = _lib.load()
+        buf = _bytes(data)
+        self.variants, self.samples = pgen_dims(buf)
+        self.bytes_per_variant = (self.samples + 3) // 4
+        self.device = torch.cuda.current_device() if device is None else device
+        handle = C.c_void_p()
+        e = _lib.gnm_error()
+        _lib.check(self.lib.gnm_pgen_open(buf.ctypes.data, buf.nbytes, self.device,
+                                          C.byref(handle), C.byref(e)), e)
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.gnm_pgen_close(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.gnm_pgen_device_bytes(self.handle))
+
+    def decode(self, rows: torch.Tensor, pitch: int, variant_begin: int = 0,
+               variant_count: Optional[int] = None, stream=None):
+        """Enqueue the decode of a variant range into ``rows`` (row 0 = ``variant_begin``)."""
+        n = self.variants - variant_begin if variant_count is None else variant_count
+        if not (rows.is_cuda and rows.dtype == torch.uint8 and rows.numel() >= n * pitch):
+            raise ValueError("rows must be a CUDA uint8 tensor of at least count x pitch bytes")
+        e = _lib.gnm_error()
+        _lib.check(self.lib.gnm_pgen_decode(self.handle, variant_begin, n, rows.data_ptr(), pitch,
+                                            _stream_ptr(stream), C.byref(e)), e)
+
+    def check(self, stream=None):
+        """Wait for ``stream``; raise if any record decoded so far was malformed."""
+        e = _lib.gnm_error()
+        _lib.check(self.lib.gnm_pgen_check(self.handle, _stream_ptr(stream), C.byref(e)), e)
+
+
+def score_pgen(prep: PreparationResult, data: PgenSource, engine: int = _lib.ENGINE_AUTO,
+               device: Optional[int] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """Score a ``.pgen`` whose variants are the ``.bim``-order rows ``prep`` indexes.
+
+    Decodes on the device, gathers the reconciled variants' rows
+    (``required_bim_indices``) and scores them; returns host (sums f64,
+    missing counts u32), person-major like ``gnm_score_run``.  Multi-row
+    loci (``prep.complex_rules``) are resolved on the CPU afterwards from the
+    decoded rows, as ``try_run_cuda`` does for a ``.bed``."""
+    buf = _bytes(data)
+    m, n = pgen_dims(buf)
+    if n != prep.total_people_in_fam:
+        raise ValueError(f".pgen has {n} samples, the preparation {prep.total_people_in_fam}")
+    rows, pitch = decode_to_device(buf, device=device)
+    scored = rows
+    if prep.required_bim_indices is not None:
+        req = torch.from_numpy(prep.required_bim_indices.astype(np.int64)).to(rows.device)
+        if len(req) and int(req.max()) >= m:
+            raise ValueError("required_bim_indices point past the .pgen's variants")
+        scored = rows[:m * pitch].view(m, pitch).index_select(0, req).reshape(-1)
+    plan = DevicePlan(prep, engine=engine, device=rows.device.index)
+    try:
+        sums, counts = plan.score(scored, pitch)
+        torch.cuda.synchronize(rows.device)
+        sums = sums.cpu().numpy()
+        counts = counts.cpu().numpy().view(np.uint32)
+    finally:
+        plan.close()
+    if prep.complex_rules:
+        from .complex import GenotypeSource, resolve_complex_variants
+        bpv = (n + 3) // 4
+        host = rows[:m * pitch].view(m, pitch)[:, :bpv].cpu().numpy().reshape(-1)
+        resolve_complex_variants(prep.complex_rules, GenotypeSource.single(host, bpv),
+                                 prep.output_idx_to_fam_idx, prep.num_people_to_score,
+                                 prep.score_names, sums, counts, prep.final_person_iids)
+    return sums, counts

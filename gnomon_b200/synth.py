@@ -187,3 +187,183 @@ def score_cells(w: Workload, chunk: int = 1 << 16):
     weight = (rng.standard_normal(nnz) * w.sigma).astype(np.float32)
     flipped = rng.random(nnz) < w.flip_frac
     return offs, cols, weight, flipped
+
+
+# ---- synthetic PLINK 2 .pgen files ------------------------------------------------
+
+# PGEN genotype category (0 hom REF, 1 het, 2 hom ALT, 3 missing) <-> .bed
+# code.  gnomon's virtual .bed writes category c as the .bed code of the
+# A1 = ALT dosage: 2 -> 00, 1 -> 10, 0 -> 11, missing -> 01.
+PGEN_CAT_TO_BED = np.array([0b11, 0b10, 0b00, 0b01], np.uint8)
+BED_TO_PGEN_CAT = np.array([2, 3, 1, 0], np.uint8)   # inverse of PGEN_CAT_TO_BED
+
+
+def _varint_bytes(x: int) -> bytes:
+    out = bytearray()
+    while True:
+        b = x & 0x7F
+        x >>= 7
+        if x:
+            out.append(b | 0x80)
+        else:
+            out.append(b)
+            return bytes(out)
+
+
+def _varints(d: np.ndarray):
+    """Base-128 varints of an array -> (bytes as uint8 array, bytes per value)."""
+    d = np.asarray(d, np.uint64)
+    nb = np.ones(len(d), np.int64)
+    for k in range(1, 10):
+        nb += d >= np.uint64(1) << np.uint64(7 * k)
+    out = np.empty(int(nb.sum()), np.uint8)
+    starts = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(np.int64)
+    for k in range(int(nb.max()) if len(d) else 0):
+        sel = nb > k
+        byte = ((d[sel] >> np.uint64(7 * k)) & np.uint64(0x7F)).astype(np.uint8)
+        out[starts[sel] + k] = byte | ((nb[sel] > k + 1).astype(np.uint8) << 7)
+    return out, nb
+
+
+def _difflist_bytes(ids: np.ndarray, cats: np.ndarray, n: int) -> bytes:
+    """A PLINK 2 difflist of (sample id, category) pairs, ids ascending."""
+    ids = np.asarray(ids, np.int64)
+    length = len(ids)
+    out = bytearray(_varint_bytes(length))
+    if length == 0:
+        return bytes(out)
+    wid = 1 if n <= 1 << 8 else 2 if n <= 1 << 16 else 3 if n <= 1 << 24 else 4
+    groups = (length + 63) // 64
+    first = ids[::64]
+    out += b"".join(int(f).to_bytes(wid, "little") for f in first)
+    # deltas inside each group (the first id of a group carries no delta)
+    in_group = np.arange(length) % 64 != 0
+    deltas = np.diff(ids, prepend=0)[in_group]
+    vbytes, nb = _varints(deltas)
+    group_of = (np.arange(length) // 64)[in_group]
+    gbytes = np.bincount(group_of, weights=nb, minlength=groups).astype(np.int64)
+    out += (gbytes[:groups - 1] - 63).astype(np.uint8).tobytes()
+    vals = np.zeros((length + 3) // 4 * 4, np.uint8)
+    vals[:length] = cats
+    q = vals.reshape(-1, 4)
+    out += (q[:, 0] | (q[:, 1] << 2) | (q[:, 2] << 4) | (q[:, 3] << 6)).astype(np.uint8).tobytes()
+    out += vbytes.tobytes()
+    return bytes(out)
+
+
+def _pgen_records(cats: np.ndarray):
+    """Genotype categories [V][N] -> (record types, record bodies), each variant
+    in the smallest of the encodings ``encode_pgen`` lists."""
+    cats = np.asarray(cats, np.uint8)
+    V, n = cats.shape
+    pair_code = {(0, 1): 1, (0, 2): 2, (0, 3): 3, (1, 2): 5, (1, 3): 6, (2, 3): 9}
+    recs, types = [], []
+    anchor = None
+    for v in range(V):
+        c = cats[v]
+        if v % (1 << 16) == 0:
+            anchor = None
+        options = []
+        q = np.zeros((n + 3) // 4 * 4, np.uint8)
+        q[:n] = c
+        q = q.reshape(-1, 4)
+        options.append((0, (q[:, 0] | (q[:, 1] << 2) | (q[:, 2] << 4) | (q[:, 3] << 6))
+                        .astype(np.uint8).tobytes()))
+        counts = np.bincount(c, minlength=4)
+        top = np.argsort(-counts, kind="stable")[:2]
+        low, high = int(min(top)), int(max(top))
+        if counts[low] > 0 and counts[high] > 0:
+            bits = np.zeros((n + 7) // 8 * 8, np.uint8)
+            bits[:n] = c == high
+            rest = np.nonzero((c != low) & (c != high))[0]
+            body = bytes([pair_code[(low, high)]]) + np.packbits(bits, bitorder="little").tobytes()
+            options.append((1, body + _difflist_bytes(rest, c[rest], n)))
+        for kind, fill in ((4, 0), (6, 2), (7, 3)):
+            diff = np.nonzero(c != fill)[0]
+            if len(diff) < n // 8:
+                options.append((kind, _difflist_bytes(diff, c[diff], n)))
+        if anchor is not None:
+            diff = np.nonzero(c != anchor)[0]
+            options.append((2, _difflist_bytes(diff, c[diff], n)))
+            swapped = np.where(c == 0, 2, np.where(c == 2, 0, c)).astype(np.uint8)
+            diff = np.nonzero(swapped != anchor)[0]
+            options.append((3, _difflist_bytes(diff, swapped[diff], n)))
+        kind, body = min(options, key=lambda o: len(o[1]))
+        recs.append(body)
+        types.append(kind)
+        if kind not in (2, 3):
+            anchor = c
+    return types, recs
+
+
+def _pgen_file(n: int, types, recs) -> bytes:
+    V = len(recs)
+    blocks = (V + 0xFFFF) >> 16
+    head = bytearray(b"\x6c\x1b\x10")
+    head += np.array([V, n], "<u4").tobytes()
+    head.append(0x07)                       # 8-bit types, 4-byte lengths, no allele counts
+    index_len = 8 * blocks + sum(min(V - (b << 16), 1 << 16) * 5 for b in range(blocks))
+    off = len(head) + index_len
+    block_offs, pos = [], off
+    for b in range(blocks):
+        block_offs.append(pos)
+        pos += sum(len(r) for r in recs[b << 16:(b + 1) << 16])
+    head += np.array(block_offs, "<u8").tobytes()
+    for b in range(blocks):
+        lo, hi = b << 16, min(V, (b + 1) << 16)
+        head += np.array(types[lo:hi], np.uint8).tobytes()
+        head += np.array([len(r) for r in recs[lo:hi]], "<u4").tobytes()
+    assert len(head) == off
+    return bytes(head) + b"".join(recs)
+
+
+def encode_pgen(cats: np.ndarray, repeats: int = 1) -> bytes:
+    """Genotype categories [V][N] (0 hom REF, 1 het, 2 hom ALT, 3 missing) ->
+    a variable-width (mode 0x10) .pgen, 8-bit record types, 4-byte lengths.
+
+    Each variant takes the smallest of these encodings: a 2-bit array (type 0);
+    two categories as a bit array plus a difflist (type 1); all hom REF / hom
+    ALT / missing plus a difflist (types 4 / 6 / 7); a difflist against the
+    most recent non-LD record of its 2^16-variant block (type 2), or against
+    that record with REF and ALT homozygotes swapped (type 3).
+
+    ``repeats`` > 1 writes the V records that many times over (variant
+    ``r * V + v`` holds the genotypes of variant ``v``); V must then divide
+    2^16 so that no repeat straddles a block and every LD record keeps its
+    anchor.  Large files are built that way in seconds.
+    """
+    cats = np.asarray(cats, np.uint8)
+    V, n = cats.shape
+    if repeats > 1 and (1 << 16) % V:
+        raise ValueError("a repeated .pgen needs a variant count that divides 2^16")
+    types, recs = _pgen_records(cats)
+    return _pgen_file(n, types * repeats, recs * repeats)
+
+
+def pgen_ld_categories(seed: int, num_variants: int, num_people: int, run: int = 17,
+                       change: float = 0.02, swap_every: int = 5) -> np.ndarray:
+    """Seeded categories with linkage: within runs of ``run`` variants each one
+    copies its predecessor (REF/ALT homozygotes swapped every ``swap_every``-th
+    variant) and redraws a ``change`` fraction of people, so the encoder picks
+    LD-compressed records (types 2 and 3) as real cohorts do."""
+    base = pgen_categories(seed, num_variants, num_people)
+    rng = np.random.default_rng(seed ^ 0x5EED)
+    c = base.copy()
+    for v in range(1, num_variants):
+        if v % run == 0:
+            continue
+        prev = c[v - 1]
+        if v % swap_every == 0:
+            prev = np.where(prev == 0, 2, np.where(prev == 2, 0, prev))
+        redraw = rng.random(num_people) < change
+        c[v] = np.where(redraw, base[v], prev)
+    return c.astype(np.uint8)
+
+
+def pgen_categories(seed: int, num_variants: int, num_people: int, p_lo: float = 0.01,
+                    p_hi: float = 0.5, missing_rate: float = 0.01) -> np.ndarray:
+    """Seeded HWE genotype categories [V][N] for synthetic .pgen files (the same
+    generator as synth_rows, read back as PGEN categories)."""
+    thr = variant_thresholds(seed, 0, num_variants, p_lo, p_hi, missing_rate)
+    codes = genotype_codes(seed, 0, num_variants, num_people, thr)
+    return BED_TO_PGEN_CAT[codes]

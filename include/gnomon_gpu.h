@@ -252,6 +252,63 @@ gnm_status gnm_backward_dw_device(gnm_plan* plan, const uint8_t* d_rows, uint64_
                                   const float* d_grad_s, float* d_grad_w,
                                   float* d_grad_corr, void* stream, gnm_error* err);
 
+/* ---- PLINK 2 .pgen input ---------------------------------------------------
+ * gnomon scores a .pgen through a virtual .bed (shared/adapt_plink2.rs:1093-
+ * 1158, 2108-2666): each variant's hard calls are decoded and packed as the
+ * .bed codes of the A1 = ALT dosage.  These entry points do that decode on the
+ * GPU, straight into device rows the scoring plans read (gnm_plan_accumulate /
+ * gnm_score_device), one row per .pgen variant in file order.
+ *
+ * Supported: storage modes 0x02 and 0x10 / 0x11, biallelic hard-call records
+ * (main-track types 0-4, 6, 7, optionally followed by a phase track).
+ * Records with multiallelic or dosage tracks, external-index modes, and more
+ * than 2^31 samples are rejected with GNM_ERR_INVALID; truncated or
+ * malformed files give GNM_ERR_IO.  The reference additionally projects
+ * multiallelic records, coerces dosages to hard calls and applies
+ * sex-chromosome ploidy from the .pvar / .psam; callers handle those. */
+
+/* Variant and sample counts from a .pgen header (host bytes). */
+gnm_status gnm_pgen_dims(const uint8_t* pgen, uint64_t pgen_len, uint64_t* num_variants,
+                         uint64_t* num_samples, gnm_error* err);
+
+/* Decode every variant of the .pgen (host bytes) into d_rows[v * pitch ..]
+ * on `device` (-1 = current): ceil(samples / 4) bytes per row, padding fields
+ * of the last byte set to 01 as the reference packs them; the other bytes of
+ * each row keep their values.  d_rows 16-byte aligned, pitch a multiple of 16.
+ * Synchronous on `stream` (NULL = default stream).  Same as gnm_pgen_open +
+ * gnm_pgen_decode of every variant + gnm_pgen_check + gnm_pgen_close. */
+gnm_status gnm_pgen_decode_device(const uint8_t* pgen, uint64_t pgen_len, int device,
+                                  uint8_t* d_rows, uint64_t pitch, void* stream,
+                                  gnm_error* err);
+
+/* A .pgen resident on one device: the file's bytes and its record index are
+ * copied to HBM once (the reference's reader keeps the same index,
+ * shared/adapt_plink2.rs:1512-1716), then any variant range is decoded on
+ * demand, e.g. block by block into a streaming buffer.  Use a handle from one
+ * stream at a time. */
+typedef struct gnm_pgen gnm_pgen;
+
+/* Parse and validate the header, upload the file; GNM_DECLINED without a
+ * device. */
+gnm_status gnm_pgen_open(const uint8_t* pgen, uint64_t pgen_len, int device, gnm_pgen** out,
+                         gnm_error* err);
+void gnm_pgen_close(gnm_pgen* pg);
+
+/* Bytes of device memory the handle holds (file, index, one scratch row). */
+uint64_t gnm_pgen_device_bytes(const gnm_pgen* pg);
+
+/* Decode variants [variant_begin, variant_begin + variant_count) into
+ * d_rows[(v - variant_begin) * pitch ..], asynchronously on `stream`.  An
+ * LD-compressed record whose anchor precedes the range is decoded from that
+ * anchor, which the call decodes into the handle's scratch row.  Malformed
+ * records set the handle's sticky error word; gnm_pgen_check reports it. */
+gnm_status gnm_pgen_decode(gnm_pgen* pg, uint64_t variant_begin, uint64_t variant_count,
+                           uint8_t* d_rows, uint64_t pitch, void* stream, gnm_error* err);
+
+/* Wait for `stream`, then GNM_ERR_IO if any record decoded so far was
+ * malformed (the message names the first such variant). */
+gnm_status gnm_pgen_check(gnm_pgen* pg, void* stream, gnm_error* err);
+
 /* ---- Allocation-free scoring ---------------------------------------------
  * No counterpart in the reference: an extra entry point of this library.
  *

@@ -1,0 +1,198 @@
+"""CPU oracle for PGEN hard-call decoding — TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/`` and ``bench.py``'s CPU-baseline leg import this module, and
+only as the checker. The product (``gnomon_b200``) never imports it.
+
+It restates, in plain Python/numpy, how gnomon turns a PLINK 2 ``.pgen``
+into the PLINK 1 ``.bed`` rows its scoring engine reads (the "virtual .bed"
+of shared/adapt_plink2.rs). The restated steps are:
+
+* the header (shared/adapt_plink2.rs:1512-1716): modes 0x02 (fixed-width
+  hard calls) and 0x10 / 0x11 (variable-width). Record types are 4- or 8-bit
+  per variant and record lengths 1-4 bytes, in 2^16-variant blocks, skipping
+  the allele-count and reference-flag arrays;
+* base-128 varints (:1721-1741), bit arrays (:1753-1777), sample-id widths
+  (:1812-1822) and difflists (:1920-2040);
+* the LD anchor, i.e. the most recent record in the same 2^16 block whose
+  main track is not LD-compressed (:2237-2257);
+* main-track types 0, 1, 2, 3, 4, 6 and 7, and the REF/ALT swap of type 3
+  after its patch (:2574-2666);
+* categories to A1 (= ALT, :927-935) dosage (:2682-2692);
+* packing into .bed codes, with padding fields set to the missing code
+  (:1136-1158).
+
+Records with multiallelic (vrtype bit 3) or dosage (bits 5-6) tracks are
+rejected. The reference also reads those tracks; this decoder does not.
+Phase tracks (bit 4) follow the main track and do not change hard calls.
+Parity is pinned by the reference's own fixture pair data/testdata/ld.bed
+and ld_p.pgen, which hold the same genotypes.
+"""
+from __future__ import annotations
+
+import struct
+
+import numpy as np
+
+# genotype category (0 hom REF, 1 het, 2 hom ALT, 3 missing) -> .bed code of
+# the A1 = ALT dosage (2 -> 00, 1 -> 10, 0 -> 11, missing -> 01)
+CAT_TO_BED = np.array([0b11, 0b10, 0b00, 0b01], np.uint8)
+
+
+class PgenError(ValueError):
+    pass
+
+
+def _varint(buf, cur):
+    out, shift = 0, 0
+    while True:
+        if cur >= len(buf):
+            raise PgenError("EOF in varint")
+        b = buf[cur]
+        cur += 1
+        out |= (b & 0x7F) << shift
+        if not b & 0x80:
+            return out, cur
+        shift += 7
+        if shift > 63:
+            raise PgenError("varint too large")
+
+
+def _sid_bytes(n):
+    return 1 if n <= 1 << 8 else 2 if n <= 1 << 16 else 3 if n <= 1 << 24 else 4
+
+
+def _difflist(buf, cur, n):
+    """-> (ids, cats, cursor after the list)."""
+    length, cur = _varint(buf, cur)
+    if length == 0:
+        return [], [], cur
+    groups = (length + 63) // 64
+    w = _sid_bytes(n)
+    first = []
+    for _ in range(groups):
+        first.append(int.from_bytes(buf[cur:cur + w], "little"))
+        cur += w
+    glen = [b + 63 for b in buf[cur:cur + groups - 1]]
+    cur += groups - 1
+    nvb = (length + 3) // 4
+    vals = [(buf[cur + i // 4] >> (2 * (i % 4))) & 3 for i in range(length)]
+    cur += nvb
+    ids = []
+    for g in range(groups):
+        count = 64 if g < groups - 1 else length - 64 * (groups - 1)
+        start = cur
+        ids.append(first[g])
+        for _ in range(count - 1):
+            d, cur = _varint(buf, cur)
+            ids.append(ids[-1] + d)
+        if g < groups - 1 and cur - start != glen[g]:
+            raise PgenError("difflist group byte-length mismatch")
+    return ids, vals, cur
+
+
+def parse_header(data: bytes):
+    """-> dict(mode, variants, samples, offsets[V], types[V], lens[V])."""
+    if len(data) < 12 or data[0] != 0x6C or data[1] != 0x1B:
+        raise PgenError("not a PGEN (bad magic)")
+    mode = data[2]
+    m, n = struct.unpack_from("<II", data, 3)
+    if mode == 0x02:
+        rec = (n + 3) // 4
+        offs = 12 + rec * np.arange(m, dtype=np.uint64)
+        return dict(mode=mode, variants=m, samples=n, offsets=offs,
+                    types=np.zeros(m, np.uint8), lens=np.full(m, rec, np.uint32))
+    if mode not in (0x10, 0x11):
+        raise PgenError(f"unsupported PGEN mode 0x{mode:02x}")
+    fmt = data[11]
+    type_bits = 4 if (fmt & 0x0F) <= 3 else 8
+    len_bytes = (fmt & 0x07) % 4 + 1
+    ac_bytes = {0: 0, 1: 1, 2: 2, 3: 4}[(fmt >> 4) & 3]
+    ref_flag_mode = (fmt >> 6) & 3
+    blocks = (m + 0xFFFF) >> 16
+    off = 12
+    block_offs = list(struct.unpack_from(f"<{blocks}Q", data, off))
+    off += 8 * blocks
+    types = np.zeros(m, np.uint8)
+    lens = np.zeros(m, np.uint32)
+    idx = 0
+    for _ in range(blocks):
+        cnt = min(m - idx, 1 << 16)
+        if type_bits == 4:
+            raw = np.frombuffer(data, np.uint8, (cnt + 1) // 2, off)
+            t = np.empty(2 * len(raw), np.uint8)
+            t[0::2], t[1::2] = raw & 15, raw >> 4
+            types[idx:idx + cnt] = t[:cnt]
+            off += (cnt + 1) // 2
+        else:
+            types[idx:idx + cnt] = np.frombuffer(data, np.uint8, cnt, off)
+            off += cnt
+        raw = np.frombuffer(data, np.uint8, cnt * len_bytes, off).reshape(cnt, len_bytes)
+        lens[idx:idx + cnt] = sum(raw[:, j].astype(np.uint32) << (8 * j) for j in range(len_bytes))
+        off += cnt * len_bytes + cnt * ac_bytes
+        if ref_flag_mode == 3:
+            off += (cnt + 7) // 8
+        idx += cnt
+    offsets = np.zeros(m, np.uint64)
+    for b in range(blocks):
+        lo, hi = b << 16, min(m, (b + 1) << 16)
+        offsets[lo] = block_offs[b]
+        offsets[lo + 1:hi] = block_offs[b] + np.cumsum(lens[lo:hi - 1].astype(np.uint64))
+    return dict(mode=mode, variants=m, samples=n, offsets=offsets, types=types, lens=lens)
+
+
+def _main_track(rec, kind, n, anchor):
+    cats = np.full(n, 3, np.uint8)
+    cur = 0
+    if kind == 0:
+        raw = np.frombuffer(rec, np.uint8, (n + 3) // 4)
+        c = np.stack([(raw >> (2 * s)) & 3 for s in range(4)], 1).reshape(-1)[:n]
+        return c.astype(np.uint8)
+    if kind == 1:
+        pairs = {1: (0, 1), 2: (0, 2), 3: (0, 3), 5: (1, 2), 6: (1, 3), 9: (2, 3)}
+        if rec[0] not in pairs:
+            raise PgenError("invalid 1-bit pair code")
+        low, high = pairs[rec[0]]
+        bits = np.unpackbits(np.frombuffer(rec, np.uint8, (n + 7) // 8, 1),
+                             bitorder="little")[:n]
+        cats = np.where(bits == 1, high, low).astype(np.uint8)
+        cur = 1 + (n + 7) // 8
+    elif kind in (2, 3):
+        cats = anchor.copy()
+    elif kind in (4, 6, 7):
+        cats[:] = {4: 0, 6: 2, 7: 3}[kind]
+    else:
+        raise PgenError(f"unsupported main-track type {kind}")
+    ids, vals, _ = _difflist(rec, cur, n)
+    for i, v in zip(ids, vals):
+        if i < n:
+            cats[i] = v
+    if kind == 3:
+        cats = np.where(cats == 0, 2, np.where(cats == 2, 0, cats)).astype(np.uint8)
+    return cats
+
+
+def decode_to_bed(data: bytes) -> np.ndarray:
+    """Decode every variant -> [V][ceil(N/4)] .bed rows (padding fields = 01)."""
+    h = parse_header(data)
+    m, n = h["variants"], h["samples"]
+    bpv = (n + 3) // 4
+    out = np.zeros((m, bpv), np.uint8)
+    anchor, anchor_idx = None, -1
+    for v in range(m):
+        t = int(h["types"][v])
+        if t & 0b1110_1000:
+            raise PgenError(f"variant {v}: multiallelic or dosage tracks are not supported")
+        kind = t & 7
+        rec = data[int(h["offsets"][v]):int(h["offsets"][v]) + int(h["lens"][v])]
+        if kind in (2, 3):
+            if anchor is None or (anchor_idx >> 16) != (v >> 16):
+                raise PgenError(f"variant {v}: LD-compressed record without an anchor in its block")
+            cats = _main_track(rec, kind, n, anchor)
+        else:
+            cats = _main_track(rec, kind, n, None)
+            anchor, anchor_idx = cats, v
+        codes = np.full(bpv * 4, 0b01, np.uint8)
+        codes[:n] = CAT_TO_BED[cats]
+        q = codes.reshape(bpv, 4)
+        out[v] = q[:, 0] | (q[:, 1] << 2) | (q[:, 2] << 4) | (q[:, 3] << 6)
+    return out

@@ -21,6 +21,9 @@ Sources (SauersML/gnomon, read as text; the Rust code cannot run here):
 * ld_fixture.npz — the packed rows of data/testdata/ld.bed (200 samples x
   1500 variants, real PLINK bytes), for decode parity.  Copied only when the
   reference tree is present at generation time.
+* ld_pgen_fixture.npz — the bytes of data/testdata/ld_p.pgen, the same
+  genotypes as a PLINK 2 variable-width .pgen (LD-compressed and 1-bit
+  records), for PGEN decode parity against ld_fixture.npz.
 
 Run: python tests/golden/make_golden.py [--reference /root/reference]
 """
@@ -141,6 +144,10 @@ def main():
         bpv = (n_people + 3) // 4
         rows = raw[3:].reshape(n_var, bpv)
         np.savez_compressed(HERE / "ld_fixture.npz", rows=rows, num_people=n_people)
+    pg = Path(a.reference) / "data" / "testdata" / "ld_p.pgen"
+    if pg.exists():
+        np.savez_compressed(HERE / "ld_pgen_fixture.npz",
+                            pgen=np.frombuffer(pg.read_bytes(), dtype=np.uint8))
     print("golden fixtures written to", HERE)
 
 

@@ -1,0 +1,178 @@
+"""PLINK 2 .pgen decode on the GPU (gnm_pgen_decode_device) against the oracle,
+and scoring from decoded rows against scoring the same genotypes as a .bed."""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from gnomon_b200 import _lib, synth
+from gnomon_b200.pgen import decode_to_device, score_pgen
+from gnomon_b200.pipeline import PipelineContext, run
+from helpers import synth_case
+from oracle import oracle, pgen_oracle
+from test_pgen import corrupt, encode_fixed_width, expected_rows, ld_pgen, GOLDEN
+
+pytestmark = pytest.mark.gpu
+SENTINEL = 0xA7
+
+
+def device_rows(data, n):
+    """Decode into sentinel-filled rows; the bytes past each row must survive."""
+    m = pgen_oracle.parse_header(data)["variants"]
+    bpv = (n + 3) // 4
+    pitch = (bpv + 127) // 128 * 128
+    rows = torch.full((max(m, 1) * pitch,), SENTINEL, dtype=torch.uint8, device="cuda")
+    rows, pitch = decode_to_device(data, rows=rows, pitch=pitch)
+    host = rows[:m * pitch].view(m, pitch).cpu().numpy()
+    assert (host[:, bpv:] == SENTINEL).all(), "bytes past the row were changed"
+    return host[:, :bpv]
+
+
+def test_reference_fixture(cuda):
+    z = np.load(GOLDEN / "ld_fixture.npz")
+    np.testing.assert_array_equal(device_rows(ld_pgen(), 200), z["rows"])
+
+
+@pytest.mark.parametrize("n", [1, 3, 4, 5, 64, 203, 256, 257, 300, 4097, 65537, 70001])
+def test_synthetic_every_record_type(cuda, n):
+    V = 120 if n < 10_000 else 40
+    cats = synth.pgen_ld_categories(n, V, n)
+    for j, fill in enumerate((0, 2, 3)):          # near-constant variants: fill types 4 / 6 / 7
+        cats[V - 3 + j] = fill
+        cats[V - 3 + j, ::37] = (fill + 1) % 4
+    data = synth.encode_pgen(cats)
+    got = device_rows(data, n)
+    np.testing.assert_array_equal(got, pgen_oracle.decode_to_bed(data))
+    np.testing.assert_array_equal(got, expected_rows(cats))
+
+
+def test_long_difflists(cuda):
+    """A difflist longer than one shared-memory chunk of 2048 groups (131,072
+    entries) is laid out in rounds: a fill record (type 4) with 200,000
+    exceptions, then an LD record against it and a shorter fill record."""
+    n = 400_000
+    ids = np.arange(0, n, 2, dtype=np.int64)
+    rng = np.random.default_rng(1)
+    vals = rng.integers(1, 4, len(ids)).astype(np.uint8)
+    cats = np.zeros((3, n), np.uint8)
+    cats[0, ids] = vals
+    cats[1] = cats[0]
+    flip = ids[::3] + 1
+    cats[1, flip] = 1
+    cats[2] = 0
+    cats[2, 1::5] = 2
+    recs = [synth._difflist_bytes(ids, vals, n),
+            synth._difflist_bytes(flip, cats[1, flip], n),
+            synth._difflist_bytes(np.arange(1, n, 5), cats[2, 1::5], n)]
+    data = synth._pgen_file(n, [4, 2, 4], recs)
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(cats))
+    np.testing.assert_array_equal(device_rows(data, n), expected_rows(cats))
+
+
+def test_two_blocks_of_repeated_records(cuda):
+    cats = synth.pgen_ld_categories(7, 256, 203)
+    data = synth.encode_pgen(cats, repeats=300)   # 76,800 variants: LD anchors per block
+    np.testing.assert_array_equal(device_rows(data, 203), expected_rows(cats, 300))
+
+
+def test_fixed_width_mode(cuda):
+    cats = synth.pgen_categories(4, 50, 301)
+    data = encode_fixed_width(cats)
+    np.testing.assert_array_equal(device_rows(data, 301), expected_rows(cats))
+
+
+def _find(data, kinds):
+    h = pgen_oracle.parse_header(data)
+    v = next(i for i, t in enumerate(h["types"].tolist()) if t in kinds)
+    return int(h["offsets"][v])
+
+
+def test_malformed_records_are_reported(cuda):
+    cats = synth.pgen_ld_categories(2, 64, 100)
+    data = synth.encode_pgen(cats)
+    # an LD difflist claiming more entries than samples
+    bad = corrupt(data, _find(data, (2, 3)), 0x7F)
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        device_rows(bad, 100)
+    assert ei.value.status == _lib.GNM_ERR_IO and "overruns" in str(ei.value)
+    # a 1-bit record with an invalid pair code
+    cats[5] = 0
+    cats[5, ::3] = 1
+    data = synth.encode_pgen(cats)
+    bad = corrupt(data, _find(data, (1,)), 4)
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        device_rows(bad, 100)
+    assert ei.value.status == _lib.GNM_ERR_IO and "pair code" in str(ei.value)
+    # the device is still usable
+    np.testing.assert_array_equal(device_rows(ld_pgen(), 200),
+                                  np.load(GOLDEN / "ld_fixture.npz")["rows"])
+
+
+def _as_pgen(rows, people):
+    codes = synth.unpack_codes(rows, people)
+    return synth.BED_TO_PGEN_CAT[codes].astype(np.uint8)
+
+
+@pytest.mark.parametrize("people,variants,scores", [(1001, 300, 1), (2003, 257, 16)])
+def test_score_from_pgen_equals_bed(cuda, people, variants, scores):
+    w, prep, rows, _ = synth_case(people, variants, scores)
+    data = synth.encode_pgen(_as_pgen(rows, people))
+    s, c = score_pgen(prep, data)
+    bs, bc = run(PipelineContext(prep), rows.reshape(-1))
+    np.testing.assert_array_equal(c, bc)
+    np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)
+    es, ec = oracle.score_extended(rows, prep)
+    np.testing.assert_array_equal(c, ec)
+
+
+def test_score_from_pgen_gathers_required_variants(cuda):
+    people, V = 777, 200
+    w, prep, rows, _ = synth_case(people, V, 4)
+    other = synth.pgen_ld_categories(5, V, people)
+    cats = np.empty((2 * V, people), np.uint8)
+    cats[1::2] = _as_pgen(rows, people)          # the scored variants at odd rows
+    cats[0::2] = other
+    data = synth.encode_pgen(cats)
+    prep2 = dataclasses.replace(prep, required_bim_indices=np.arange(1, 2 * V, 2, dtype=np.uint64))
+    s, c = score_pgen(prep2, data)
+    bs, bc = run(PipelineContext(prep), rows.reshape(-1))
+    np.testing.assert_array_equal(c, bc)
+    np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("block", [1, 7, 17, 100, 4096])
+def test_range_decode_matches_whole_file(cuda, block):
+    """Blocks that start inside a run of LD records decode their anchor into
+    the scratch row; every block equals the same rows of a whole-file decode."""
+    from gnomon_b200.pgen import PgenFile
+    cats = synth.pgen_ld_categories(21, 128, 203)
+    data = synth.encode_pgen(cats, repeats=2)
+    want = expected_rows(cats, 2)
+    V, bpv = want.shape
+    pitch = 64
+    buf = torch.full((block * pitch,), SENTINEL, dtype=torch.uint8, device="cuda")
+    with PgenFile(data) as pg:
+        assert (pg.variants, pg.samples) == (V, 203)
+        assert pg.device_bytes >= len(data)
+        for b0 in range(0, V, block):
+            n = min(block, V - b0)
+            pg.decode(buf, pitch, b0, n)
+            pg.check()
+            got = buf[:n * pitch].view(n, pitch).cpu().numpy()
+            np.testing.assert_array_equal(got[:, :bpv], want[b0:b0 + n], err_msg=f"block {b0}")
+            assert (got[:, bpv:] == SENTINEL).all()
+
+
+def test_range_errors(cuda):
+    from gnomon_b200.pgen import PgenFile
+    with PgenFile(ld_pgen()) as pg:
+        buf = torch.zeros(64 * 10, dtype=torch.uint8, device="cuda")
+        with pytest.raises(_lib.GnomonGpuError) as ei:
+            pg.decode(buf, 64, 1495, 10)              # past the last variant
+        assert ei.value.status == _lib.GNM_ERR_INVALID
+        with pytest.raises(_lib.GnomonGpuError) as ei:
+            pg.decode(buf, 56, 0, 10)                 # pitch not a multiple of 16
+        assert ei.value.status == _lib.GNM_ERR_INVALID
+        pg.decode(buf, 64, 0, 0)                      # empty range: nothing to do
+        pg.check()

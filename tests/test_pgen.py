@@ -1,0 +1,153 @@
+"""PLINK 2 .pgen input, CPU side: the oracle against the reference's fixture
+pair, the synthetic encoder, and the C ABI's header parse (no GPU work)."""
+import collections
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gnomon_b200 import _lib, synth
+from gnomon_b200.pgen import pgen_dims
+from oracle import pgen_oracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def ld_pgen():
+    return np.load(GOLDEN / "ld_pgen_fixture.npz")["pgen"].tobytes()
+
+
+def expected_rows(cats, repeats=1):
+    """.bed rows of A1 = ALT dosage codes, padding fields 01."""
+    V, n = cats.shape
+    codes = np.full((V, (n + 3) // 4 * 4), 0b01, np.uint8)
+    codes[:, :n] = synth.PGEN_CAT_TO_BED[cats]
+    q = codes.reshape(V, -1, 4)
+    rows = (q[..., 0] | (q[..., 1] << 2) | (q[..., 2] << 4) | (q[..., 3] << 6)).astype(np.uint8)
+    return np.tile(rows, (repeats, 1))
+
+
+def test_oracle_matches_reference_bed_twin():
+    """ld_p.pgen and ld.bed hold the same genotypes (the reference's fixture pair)."""
+    z = np.load(GOLDEN / "ld_fixture.npz")
+    got = pgen_oracle.decode_to_bed(ld_pgen())
+    np.testing.assert_array_equal(got, z["rows"])
+
+
+def test_reference_fixture_uses_ld_records():
+    h = pgen_oracle.parse_header(ld_pgen())
+    assert (h["variants"], h["samples"]) == (1500, 200)
+    kinds = collections.Counter((h["types"] & 7).tolist())
+    assert kinds[2] + kinds[3] > 0 and kinds[0] + kinds[1] > 0
+
+
+@pytest.mark.parametrize("n", [1, 5, 203, 257, 300, 70001])
+def test_encoder_round_trip_through_oracle(n):
+    V = 96 if n < 1000 else 24
+    cats = synth.pgen_ld_categories(11, V, n)
+    data = synth.encode_pgen(cats)
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(cats))
+
+
+def test_encoder_covers_every_record_type():
+    seen = collections.Counter()
+    for n in (203, 300, 5000):
+        cats = synth.pgen_ld_categories(3, 64, n)
+        # constant variants with a few exceptions -> fill types 4 / 6 / 7
+        for j, fill in enumerate((0, 2, 3)):
+            cats[60 + j] = fill
+            cats[60 + j, ::97] = (fill + 1) % 4
+        seen.update(pgen_oracle.parse_header(synth.encode_pgen(cats))["types"].tolist())
+    assert {0, 1, 2, 3, 4, 6, 7} <= set(seen), seen
+
+
+def test_repeated_records_keep_their_anchors():
+    cats = synth.pgen_ld_categories(7, 256, 9)
+    data = synth.encode_pgen(cats, repeats=300)     # 76,800 variants over two blocks
+    h = pgen_oracle.parse_header(data)
+    assert h["variants"] == 76_800
+    rows = pgen_oracle.decode_to_bed(data)
+    np.testing.assert_array_equal(rows, expected_rows(cats, 300))
+
+
+def test_abi_dims():
+    assert pgen_dims(ld_pgen()) == (1500, 200)
+    data = synth.encode_pgen(synth.pgen_ld_categories(1, 32, 70001))
+    assert pgen_dims(data) == (32, 70001)
+
+
+def corrupt(data: bytes, at: int, value: int) -> bytes:
+    b = bytearray(data)
+    b[at] = value
+    return bytes(b)
+
+
+def _status(data):
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        pgen_dims(data)
+    return ei.value.status
+
+
+def test_abi_rejects_bad_files():
+    cats = synth.pgen_ld_categories(2, 40, 300)
+    data = synth.encode_pgen(cats)
+    types_at = 12 + 8                    # one block: 8-byte offset, then the 8-bit types
+    assert _status(data[:5]) == _lib.GNM_ERR_IO                        # no header
+    assert _status(b"\x6c\x1c" + data[2:]) == _lib.GNM_ERR_IO          # bad magic
+    assert _status(data[:-1]) == _lib.GNM_ERR_IO                       # last record cut
+    assert _status(corrupt(data, 2, 0x03)) == _lib.GNM_ERR_INVALID     # unsupported mode
+    kind = data[types_at]
+    assert _status(corrupt(data, types_at, kind | 0x08)) == _lib.GNM_ERR_INVALID  # multiallelic
+    assert _status(corrupt(data, types_at, kind | 0x20)) == _lib.GNM_ERR_INVALID  # dosage
+    assert _status(corrupt(data, types_at, 5)) == _lib.GNM_ERR_INVALID           # type 5
+    # the oracle rejects the same files
+    with pytest.raises(pgen_oracle.PgenError):
+        pgen_oracle.decode_to_bed(corrupt(data, types_at, kind | 0x08))
+
+
+def test_abi_phase_bit_is_accepted():
+    cats = synth.pgen_ld_categories(2, 40, 300)
+    data = synth.encode_pgen(cats)
+    types_at = 12 + 8
+    assert pgen_dims(corrupt(data, types_at, data[types_at] | 0x10)) == (40, 300)
+
+
+def test_decode_declines_without_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    lib = _lib.load()
+    data = np.frombuffer(ld_pgen(), np.uint8)
+    e = _lib.gnm_error()
+    st = lib.gnm_pgen_decode_device(data.ctypes.data, data.nbytes, 0, None, 64, None,
+                                    C.byref(e))
+    assert st == _lib.GNM_DECLINED
+
+
+def encode_fixed_width(cats):
+    """A storage-mode 0x02 .pgen: 2-bit category arrays, no index."""
+    V, n = cats.shape
+    q = np.zeros((V, (n + 3) // 4 * 4), np.uint8)
+    q[:, :n] = cats
+    q = q.reshape(V, -1, 4)
+    body = (q[..., 0] | (q[..., 1] << 2) | (q[..., 2] << 4) | (q[..., 3] << 6)).astype(np.uint8)
+    return b"\x6c\x1b\x02" + np.array([V, n], "<u4").tobytes() + b"\x00" + body.tobytes()
+
+
+def test_fixed_width_mode_oracle_and_dims():
+    cats = synth.pgen_categories(4, 50, 301)
+    data = encode_fixed_width(cats)
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(cats))
+    assert pgen_dims(data) == (50, 301)
+    assert _status(data[:-1]) == _lib.GNM_ERR_IO
+
+
+def test_long_difflist_oracle():
+    n = 400_000
+    ids = np.arange(0, n, 2, dtype=np.int64)
+    vals = np.random.default_rng(1).integers(1, 4, len(ids)).astype(np.uint8)
+    data = synth._pgen_file(n, [4], [synth._difflist_bytes(ids, vals, n)])
+    cats = np.zeros((1, n), np.uint8)
+    cats[0, ids] = vals
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(cats))
