@@ -19,15 +19,17 @@
 // coerces them; this decoder does not).
 //
 // Layout of the work: the bijection category -> .bed code lets every step
-// run on .bed codes directly.  Kernel 1 decodes the non-LD records (one CTA
-// per variant: a LUT pass over the 2-bit or 1-bit array, or a fill), kernel 2
-// the LD-compressed ones from their anchors' rows.  A record's difflist is
-// parsed once (thread 0: length, first sample ids, group byte lengths), then
-// its groups of 64 entries are applied in parallel, one thread per group,
-// each walking its base-128 sample-id deltas and patching 2-bit fields with
-// 32-bit atomics (fields of one word may belong to different groups).
-// Every byte read is bounded by the record's length; a malformed record sets
-// the error word and its row is left incomplete.
+// run on .bed codes directly.  One warp decodes one record, so an SM keeps up
+// to 64 records in flight (the work per record is a chain of dependent byte
+// reads, bound by latency rather than bandwidth).  Kernel 1 decodes the
+// non-LD records (a table pass over the 2-bit or 1-bit array, or a fill),
+// kernel 2 the LD-compressed ones from their anchors' rows.  A difflist's
+// groups of 64 entries go one per lane: a shuffle scan over the group byte
+// lengths places each lane at its group's deltas, then the lane walks its
+// base-128 sample-id deltas and patches 2-bit fields with 32-bit atomics
+// (fields of one word may belong to different groups).  Every byte read is
+// bounded by the record's length; a malformed record sets the error word and
+// its row is left incomplete.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,7 +44,7 @@ namespace gnm {
 namespace {
 
 constexpr uint32_t kPgThreads = 256;
-constexpr uint32_t kPgChunk = 2048;               // difflist groups laid out per round
+constexpr uint32_t kPgWarps = kPgThreads / 32;     // one record per warp
 constexpr uint64_t kPgMaxSamples = uint64_t(1) << 31;
 
 enum : uint32_t { kPgErrBounds = 1u, kPgErrPair = 2u };
@@ -65,6 +67,10 @@ struct PgArgs {
 };
 
 __constant__ uint8_t kCatToBed[4] = {0x3, 0x2, 0x0, 0x1};
+// 1-bit record pair codes (shared/adapt_plink2.rs:2600-2608): the category of
+// a clear bit and of a set bit; -1 = invalid code
+__constant__ int8_t kPairLow[16] = {-1, 0, 0, 0, -1, 1, 1, -1, -1, 2, -1, -1, -1, -1, -1, -1};
+__constant__ int8_t kPairHigh[16] = {-1, 1, 2, 3, -1, 2, 3, -1, -1, 3, -1, -1, -1, -1, -1, -1};
 
 __device__ __forceinline__ void flag(const PgArgs& a, uint32_t bit, uint32_t v) {
   atomicOr(a.err, bit);
@@ -92,105 +98,124 @@ struct Rec {
   }
 };
 
-// Set the 2-bit .bed code of sample `id` in a row (other fields untouched).
-__device__ __forceinline__ void put_code(uint8_t* row, uint64_t id, uint32_t code) {
-  uint32_t* w = reinterpret_cast<uint32_t*>(row) + id / 16;
-  const uint32_t sh = 2 * uint32_t(id % 16);
-  atomicAnd(w, ~(3u << sh));
-  atomicOr(w, code << sh);
+// SWAR REF/ALT swap of sixteen .bed fields: 00 <-> 11, 01 and 10 kept.
+__device__ __forceinline__ uint32_t swap_homs(uint32_t x) {
+  const uint32_t same = ~(x ^ (x >> 1)) & 0x55555555u;
+  return x ^ (same | (same << 1));
 }
 
-// Apply the difflist that starts at `cur` (all threads of the CTA call this).
+// Apply the difflist that starts at `cur`; one warp, all lanes call this.
 // Layout (shared/adapt_plink2.rs:1920-2040): length (varint); one first sample
 // id per group of 64 entries (1-4 bytes by sample count); the byte lengths of
 // all but the last group's deltas, minus 63; the 2-bit values; the groups'
-// base-128 id deltas.  Thread 0 lays out up to kPgChunk groups at a time, the
-// CTA applies them, one thread per group.
-__device__ void apply_difflist(const PgArgs& a, const Rec& r, uint32_t cur, uint8_t* row,
-                               uint32_t v) {
-  __shared__ uint32_t s_len, s_groups, s_wid, s_first_at, s_glen_at, s_vals, s_next, s_ok;
-  __shared__ uint32_t s_start[kPgChunk];   // byte offset of a group's deltas
-  __shared__ uint32_t s_first[kPgChunk];   // a group's first sample id
-  if (threadIdx.x == 0) {
-    s_ok = 1u;
-    uint64_t l = 0;
-    if (!r.varint(cur, l) || l > a.n) {
-      s_ok = 0u;
-      flag(a, kPgErrBounds, v);
-    } else {
-      const uint32_t groups = uint32_t((l + 63) / 64);
-      const uint32_t wid = a.n <= (1u << 8) ? 1 : a.n <= (1u << 16) ? 2 : a.n <= (1u << 24) ? 3 : 4;
-      s_len = uint32_t(l);
-      s_groups = groups;
-      s_wid = wid;
-      s_first_at = cur;
-      s_glen_at = cur + groups * wid;
-      s_vals = s_glen_at + (groups > 0 ? groups - 1 : 0);
-      s_next = s_vals + uint32_t((l + 3) / 4);
-      if (s_next > r.len) {
-        s_ok = 0u;
-        flag(a, kPgErrBounds, v);
-      }
-    }
+// base-128 id deltas.  Groups go 32 at a time, one lane each: a shuffle scan
+// over the group byte lengths places each lane at its group's deltas, then
+// the lane walks its group.
+//
+// Sample ids rise strictly (a record that breaks this is malformed), so a
+// group owns every 32-bit word of the row between its first and last id
+// except those two, which a neighbouring group may share.  A lane merges its
+// patches per word in registers and writes each word once: the final value
+// computed from `base` (the row before patching: the anchor row for an LD
+// record, with `swap` = type 3's REF/ALT swap applied to it and to the
+// patched values, or the row itself) with a plain store, or for the two end
+// words and the row's last partial word an atomicXor of the patched bits.
+__device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uint32_t cur,
+                                              uint8_t* row, const uint8_t* base, uint32_t v,
+                                              bool swap) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint64_t l = 0;
+  if (!r.varint(cur, l) || l > a.n) {
+    if (lane == 0) flag(a, kPgErrBounds, v);
+    return;
   }
-  __syncthreads();
-  if (!s_ok) return;
-  const uint32_t len = s_len, groups = s_groups;
-  for (uint32_t c0 = 0; c0 < groups; c0 += kPgChunk) {
-    const uint32_t cn = min(kPgChunk, groups - c0);
-    if (threadIdx.x == 0) {
-      uint32_t at = s_next;
-      for (uint32_t i = 0; i < cn && s_ok; ++i) {
-        const uint32_t g = c0 + i;
-        uint32_t id = 0;
-        for (uint32_t k = 0; k < s_wid; ++k) {
-          uint32_t b;
-          if (!r.byte(s_first_at + g * s_wid + k, b)) {
-            s_ok = 0u;
-            break;
-          }
-          id |= b << (8 * k);
-        }
-        s_first[i] = id;
-        s_start[i] = at;
-        if (g + 1 < groups) {
-          uint32_t b = 0;
-          if (!r.byte(s_glen_at + g, b)) s_ok = 0u;
-          at += b + 63;
-        }
-      }
-      s_next = at;
-      if (!s_ok) flag(a, kPgErrBounds, v);
-    }
-    __syncthreads();
-    if (!s_ok) return;
-    for (uint32_t i = threadIdx.x; i < cn; i += blockDim.x) {
-      const uint32_t g = c0 + i;
-      const uint32_t count = g + 1 < groups ? 64u : len - 64u * (groups - 1);
-      uint64_t id = s_first[i];
-      uint32_t at = s_start[i];
-      for (uint32_t e = 0; e < count; ++e) {
-        if (e > 0) {
-          uint64_t d;
-          if (!r.varint(at, d)) {
-            flag(a, kPgErrBounds, v);
-            break;
-          }
-          id += d;
-        }
-        const uint32_t idx = 64 * g + e;
-        const uint32_t val = (r.p[s_vals + idx / 4] >> (2 * (idx % 4))) & 3u;
-        if (id < a.n) put_code(row, id, kCatToBed[val]);
-      }
-    }
-    __syncthreads();   // before thread 0 lays out the next chunk
+  if (l == 0) return;
+  const uint32_t len = uint32_t(l);
+  const uint32_t groups = (len + 63) / 64;
+  const uint32_t wid = a.n <= (1u << 8) ? 1 : a.n <= (1u << 16) ? 2 : a.n <= (1u << 24) ? 3 : 4;
+  const uint32_t first_at = cur;
+  const uint32_t glen_at = first_at + groups * wid;
+  const uint32_t vals_at = glen_at + groups - 1;
+  uint32_t deltas = vals_at + (len + 3) / 4;   // the first group's deltas
+  if (deltas > r.len) {
+    if (lane == 0) flag(a, kPgErrBounds, v);
+    return;
   }
+  const uint64_t bpv = (a.n + 3) / 4;
+  // a word holding bytes past the row's end is only ever xor-patched
+  const uint64_t partial_word = bpv % 4 ? bpv / 4 : ~uint64_t(0);
+  uint32_t* row32 = reinterpret_cast<uint32_t*>(row);
+  const uint32_t* base32 = reinterpret_cast<const uint32_t*>(base);
+  auto first_id = [&](uint32_t g) {
+    uint64_t id = 0;
+    for (uint32_t k = 0; k < wid; ++k) id |= uint64_t(r.p[first_at + g * wid + k]) << (8 * k);
+    return id;
+  };
+  bool bad = false;
+  for (uint32_t c0 = 0; c0 < groups; c0 += 32) {
+    const uint32_t g = c0 + lane;
+    // bytes of group g's deltas (all groups but the last carry a length)
+    const uint32_t mine = g + 1 < groups ? uint32_t(r.p[glen_at + g]) + 63u : 0u;
+    uint32_t incl = mine;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+      if (lane >= d) incl += y;
+    }
+    uint32_t at = deltas + incl - mine;
+    deltas += __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (g >= groups) continue;
+    uint64_t id = first_id(g);
+    const uint32_t count = g + 1 < groups ? 64u : len - 64u * (groups - 1);
+    const uint32_t start = at;
+    uint64_t cw = ~uint64_t(0);      // word being patched
+    uint32_t pm = 0, pv = 0;         // its patched bits and their new values
+    bool edge = true;                // the group's first word
+    auto flush = [&](bool last) {
+      uint32_t old = base32[cw];
+      if (swap) old = swap_homs(old);
+      if (edge || last || cw == partial_word)
+        atomicXor(row32 + cw, (old & pm) ^ pv);
+      else
+        row32[cw] = (old & ~pm) | pv;
+      edge = false;
+    };
+    for (uint32_t e = 0; e < count; ++e) {
+      if (e > 0) {
+        uint64_t d;
+        if (!r.varint(at, d) || d == 0) {
+          bad = true;
+          break;
+        }
+        id += d;
+      }
+      if (id >= a.n) continue;
+      const uint32_t idx = 64 * g + e;
+      uint32_t val = (r.p[vals_at + idx / 4] >> (2 * (idx % 4))) & 3u;
+      if (swap && !(val & 1u)) val ^= 2u;
+      const uint64_t w = id / 16;
+      const uint32_t sh = 2 * uint32_t(id % 16);
+      if (w != cw) {
+        if (cw != ~uint64_t(0)) flush(false);
+        cw = w;
+        pm = pv = 0;
+      }
+      pm |= 3u << sh;
+      pv = (pv & ~(3u << sh)) | (uint32_t(kCatToBed[val]) << sh);
+    }
+    if (cw != ~uint64_t(0)) flush(true);
+    if (!bad && g + 1 < groups && (at != start + mine || id >= first_id(g + 1)))
+      bad = true;   // group length mismatch, or ids not rising into the next group
+  }
+  if (bad) flag(a, kPgErrBounds, v);
 }
 
-// Padding fields of the last byte -> 01 (missing), as the reference packs them.
-__device__ __forceinline__ void fix_tail(const PgArgs& a, uint8_t* row) {
+// Padding fields of the last byte -> 01 (missing), as the reference packs
+// them; lane 0, after the warp's writes to the row.
+__device__ __forceinline__ void warp_fix_tail(const PgArgs& a, uint8_t* row) {
+  __syncwarp();
   const uint32_t rem = uint32_t(a.n % 4);
-  if (threadIdx.x == 0 && rem) {
+  if ((threadIdx.x & 31u) == 0 && rem) {
     const uint64_t last = (a.n + 3) / 4 - 1;
     uint32_t b = row[last];
     for (uint32_t k = rem; k < 4; ++k) b = (b & ~(3u << (2 * k))) | (1u << (2 * k));
@@ -198,118 +223,143 @@ __device__ __forceinline__ void fix_tail(const PgArgs& a, uint8_t* row) {
   }
 }
 
-// One CTA per variant of the range (LD-compressed ones return at once), plus
-// one CTA for `extra` when the range's first LD records anchor before it.
+// Fill bpv bytes of a row with one byte value: 16-byte stores, then the tail.
+__device__ __forceinline__ void warp_fill(uint8_t* row, uint64_t bpv, uint32_t byte) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t w = byte * 0x01010101u;
+  const uint4 q = make_uint4(w, w, w, w);
+  const uint64_t vecs = bpv / 16;
+  for (uint64_t j = lane; j < vecs; j += 32) reinterpret_cast<uint4*>(row)[j] = q;
+  for (uint64_t j = 16 * vecs + lane; j < bpv; j += 32) row[j] = uint8_t(byte);
+}
+
+// One warp per non-LD record of the range (LD-compressed ones return at once),
+// plus one for `extra` when the range's first LD records anchor before it.
 __global__ void __launch_bounds__(kPgThreads) gnm_pgen_direct(PgArgs a) {
-  __shared__ uint8_t lut[256];
-  const bool in_range = blockIdx.x < a.count;
-  const uint32_t v = in_range ? a.begin + blockIdx.x : a.extra;
+  __shared__ uint8_t lut[256];     // byte of four PGEN categories -> byte of .bed codes
+  __shared__ uint8_t nlut[kPgWarps][16];
+  for (uint32_t x = threadIdx.x; x < 256; x += blockDim.x) {
+    uint32_t o = 0;
+    for (uint32_t k = 0; k < 4; ++k) o |= uint32_t(kCatToBed[(x >> (2 * k)) & 3u]) << (2 * k);
+    lut[x] = uint8_t(o);
+  }
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t wi = uint64_t(blockIdx.x) * kPgWarps + threadIdx.x / 32;
+  const bool in_range = wi < a.count;
+  if (!in_range && (wi != a.count || a.extra == kNoAnchor)) return;
+  const uint32_t v = in_range ? a.begin + uint32_t(wi) : a.extra;
   if (a.anchor_of[v] != kNoAnchor) return;
   const Rec r{a.pgen + a.offsets[v], a.lens[v]};
   const uint32_t kind = a.types[v] & 7u;
-  uint8_t* row = in_range ? a.rows + uint64_t(blockIdx.x) * a.pitch : a.scratch;
+  uint8_t* row = in_range ? a.rows + wi * a.pitch : a.scratch;
   const uint64_t bpv = (a.n + 3) / 4;
+  const uint64_t words = bpv / 4;
+  uint32_t* d32 = reinterpret_cast<uint32_t*>(row);
   uint32_t cur = 0;
   if (kind == 0) {
-    // byte of four PGEN 2-bit categories -> byte of four .bed codes
-    for (uint32_t x = threadIdx.x; x < 256; x += blockDim.x) {
-      uint32_t o = 0;
-      for (uint32_t k = 0; k < 4; ++k) o |= uint32_t(kCatToBed[(x >> (2 * k)) & 3u]) << (2 * k);
-      lut[x] = uint8_t(o);
-    }
-    __syncthreads();
     if (r.len < bpv) {
-      if (threadIdx.x == 0) flag(a, kPgErrBounds, v);
+      if (lane == 0) flag(a, kPgErrBounds, v);
       return;
     }
-    for (uint64_t j = threadIdx.x; j < bpv; j += blockDim.x) row[j] = lut[r.p[j]];
-    __syncthreads();
-    fix_tail(a, row);
+    // whole output words from funnel-shifted aligned input words (the record
+    // starts at any byte; an aligned word holding a needed byte lies inside
+    // the file's 16-byte-padded buffer)
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(r.p);
+    const uint32_t* al = reinterpret_cast<const uint32_t*>(addr & ~uintptr_t(3));
+    const uint32_t sh = uint32_t(addr & 3u) * 8u;
+    for (uint64_t j = lane; j < words; j += 32) {
+      const uint32_t x = __funnelshift_r(al[j], sh ? al[j + 1] : 0u, sh);
+      d32[j] = uint32_t(lut[x & 255u]) | uint32_t(lut[(x >> 8) & 255u]) << 8 |
+               uint32_t(lut[(x >> 16) & 255u]) << 16 | uint32_t(lut[x >> 24]) << 24;
+    }
+    for (uint64_t j = 4 * words + lane; j < bpv; j += 32) row[j] = lut[r.p[j]];
+    warp_fix_tail(a, row);
     return;
   }
   if (kind == 1) {
     // pair code -> (low, high) categories; bit set = high
     uint32_t pc = 0;
     const bool okb = r.byte(0, pc);
-    int low = -1, high = -1;
-    switch (pc) {
-      case 1: low = 0; high = 1; break;
-      case 2: low = 0; high = 2; break;
-      case 3: low = 0; high = 3; break;
-      case 5: low = 1; high = 2; break;
-      case 6: low = 1; high = 3; break;
-      case 9: low = 2; high = 3; break;
-      default: break;
-    }
+    const int low = okb && pc < 16 ? kPairLow[pc] : -1;
+    const int high = okb && pc < 16 ? kPairHigh[pc] : -1;
     if (!okb || low < 0) {
-      if (threadIdx.x == 0) flag(a, kPgErrPair, v);
+      if (lane == 0) flag(a, kPgErrPair, v);
       return;
     }
     const uint32_t nb = uint32_t((a.n + 7) / 8);
     if (r.len < 1 + nb) {
-      if (threadIdx.x == 0) flag(a, kPgErrBounds, v);
+      if (lane == 0) flag(a, kPgErrBounds, v);
       return;
     }
-    // nibble of four bits -> byte of four .bed codes
-    for (uint32_t x = threadIdx.x; x < 16; x += blockDim.x) {
+    // nibble of four bits -> byte of four .bed codes (a table per warp)
+    uint8_t* nib = nlut[threadIdx.x / 32];
+    if (lane < 16) {
       uint32_t o = 0;
       for (uint32_t k = 0; k < 4; ++k)
-        o |= uint32_t(kCatToBed[((x >> k) & 1u) ? high : low]) << (2 * k);
-      lut[x] = uint8_t(o);
+        o |= uint32_t(kCatToBed[((lane >> k) & 1u) ? high : low]) << (2 * k);
+      nib[lane] = uint8_t(o);
     }
-    __syncthreads();
-    for (uint64_t j = threadIdx.x; j < bpv; j += blockDim.x)
-      row[j] = lut[(r.p[1 + j / 2] >> (4 * (j % 2))) & 15u];
+    __syncwarp();
+    const uint8_t* bits = r.p + 1;
+    for (uint64_t j = lane; j < words; j += 32) {
+      const uint32_t b0 = bits[2 * j], b1 = bits[2 * j + 1];
+      d32[j] = uint32_t(nib[b0 & 15u]) | uint32_t(nib[b0 >> 4]) << 8 |
+               uint32_t(nib[b1 & 15u]) << 16 | uint32_t(nib[b1 >> 4]) << 24;
+    }
+    for (uint64_t j = 4 * words + lane; j < bpv; j += 32)
+      row[j] = nib[(bits[j / 2] >> (4 * (j % 2))) & 15u];
     cur = 1 + nb;
   } else if (kind == 4 || kind == 6 || kind == 7) {
-    const uint32_t c = kCatToBed[kind == 4 ? 0 : kind == 6 ? 2 : 3];
-    for (uint64_t j = threadIdx.x; j < bpv; j += blockDim.x) row[j] = uint8_t(c * 0x55u);
+    warp_fill(row, bpv, kCatToBed[kind == 4 ? 0 : kind == 6 ? 2 : 3] * 0x55u);
   } else {
-    if (threadIdx.x == 0) flag(a, kPgErrPair, v);
+    if (lane == 0) flag(a, kPgErrPair, v);
     return;
   }
-  __syncthreads();
-  apply_difflist(a, r, cur, row, v);
-  __syncthreads();
-  fix_tail(a, row);
+  __syncwarp();
+  warp_difflist(a, r, cur, row, row, v, false);
+  warp_fix_tail(a, row);
 }
 
-// One CTA per variant of the range (non-LD ones return at once).  The anchor
-// row is in the range's rows, or in `scratch` when it precedes the range.
+// One warp per LD-compressed record of the range (others return at once):
+// copy the anchor row (16-byte vectors; type 3 swaps REF and ALT homozygotes
+// on the way), then patch it with the record's difflist.  The anchor row is in
+// the range's rows, or in `scratch` when it precedes the range.
 __global__ void __launch_bounds__(kPgThreads) gnm_pgen_ld(PgArgs a) {
-  const uint32_t v = a.begin + blockIdx.x;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t wi = uint64_t(blockIdx.x) * kPgWarps + threadIdx.x / 32;
+  if (wi >= a.count) return;
+  const uint32_t v = a.begin + uint32_t(wi);
   const uint32_t anchor = a.anchor_of[v];
   if (anchor == kNoAnchor) return;
   const Rec r{a.pgen + a.offsets[v], a.lens[v]};
-  const uint32_t kind = a.types[v] & 7u;
-  uint8_t* row = a.rows + uint64_t(blockIdx.x) * a.pitch;
+  const bool swap = (a.types[v] & 7u) == 3u;
+  uint8_t* row = a.rows + wi * a.pitch;
   const uint8_t* src =
       anchor >= a.begin ? a.rows + uint64_t(anchor - a.begin) * a.pitch : a.scratch;
   const uint64_t bpv = (a.n + 3) / 4;
-  const uint64_t words = bpv / 4;   // whole 32-bit words; the rest byte by byte
-  const uint32_t* s32 = reinterpret_cast<const uint32_t*>(src);
-  uint32_t* d32 = reinterpret_cast<uint32_t*>(row);
-  for (uint64_t j = threadIdx.x; j < words; j += blockDim.x) d32[j] = s32[j];
-  for (uint64_t j = 4 * words + threadIdx.x; j < bpv; j += blockDim.x) row[j] = src[j];
-  __syncthreads();
-  apply_difflist(a, r, 0, row, v);
-  __syncthreads();
-  if (kind == 3) {
-    // swap hom REF (11) and hom ALT (00): flip both bits of fields whose bits agree
-    for (uint64_t j = threadIdx.x; j < words; j += blockDim.x) {
-      const uint32_t x = d32[j];
-      const uint32_t same = ~(x ^ (x >> 1)) & 0x55555555u;
-      d32[j] = x ^ (same | (same << 1));
+  const uint64_t vecs = bpv / 16;
+  const uint4* s16 = reinterpret_cast<const uint4*>(src);
+  uint4* d16 = reinterpret_cast<uint4*>(row);
+  if (swap) {
+    for (uint64_t j = lane; j < vecs; j += 32) {
+      uint4 q = s16[j];
+      q.x = swap_homs(q.x);
+      q.y = swap_homs(q.y);
+      q.z = swap_homs(q.z);
+      q.w = swap_homs(q.w);
+      d16[j] = q;
     }
-    for (uint64_t j = 4 * words + threadIdx.x; j < bpv; j += blockDim.x) {
-      const uint32_t x = row[j];
-      const uint32_t same = ~(x ^ (x >> 1)) & 0x55u;
-      row[j] = uint8_t(x ^ (same | (same << 1)));
-    }
-    __syncthreads();
+    for (uint64_t j = 16 * vecs + lane; j < bpv; j += 32) row[j] = uint8_t(swap_homs(src[j]));
+  } else {
+    for (uint64_t j = lane; j < vecs; j += 32) d16[j] = s16[j];
+    for (uint64_t j = 16 * vecs + lane; j < bpv; j += 32) row[j] = src[j];
   }
-  fix_tail(a, row);
+  __syncwarp();
+  warp_difflist(a, r, 0, row, src, v, swap);
+  warp_fix_tail(a, row);
 }
+
 
 // ---- host ----------------------------------------------------------------------
 
@@ -406,6 +456,9 @@ struct gnm_pgen {
   std::vector<void*> bufs;
   gnm::PgArgs base{};
   ~gnm_pgen() {
+    // decodes in flight on any stream may still read the buffers
+    gnm::DeviceGuard g(device);
+    cudaDeviceSynchronize();
     for (void* x : bufs) gnm::pool_free(x);
   }
 };
@@ -487,9 +540,10 @@ static void pgen_decode_impl(gnm_pgen* pg, uint64_t begin, uint64_t count, uint8
       break;
     }
   DeviceGuard g(pg->device);
-  gnm_pgen_direct<<<a.count + (a.extra != kNoAnchor ? 1u : 0u), kPgThreads, 0, s>>>(a);
+  const uint64_t direct_warps = uint64_t(a.count) + (a.extra != kNoAnchor ? 1u : 0u);
+  gnm_pgen_direct<<<uint32_t((direct_warps + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen decode launch");
-  gnm_pgen_ld<<<a.count, kPgThreads, 0, s>>>(a);
+  gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen LD decode launch");
 }
 

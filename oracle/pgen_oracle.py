@@ -23,6 +23,9 @@ of shared/adapt_plink2.rs). The restated steps are:
 
 Records with multiallelic (vrtype bit 3) or dosage (bits 5-6) tracks are
 rejected. The reference also reads those tracks; this decoder does not.
+Difflists whose sample ids do not rise strictly are rejected as malformed
+(PLINK 2 writes strictly rising ids; the reference would apply such a list in
+order, later entries winning).
 Phase tracks (bit 4) follow the main track and do not change hard calls.
 Parity is pinned by the reference's own fixture pair data/testdata/ld.bed
 and ld_p.pgen, which hold the same genotypes.
@@ -84,9 +87,13 @@ def _difflist(buf, cur, n):
         ids.append(first[g])
         for _ in range(count - 1):
             d, cur = _varint(buf, cur)
+            if d == 0:
+                raise PgenError("difflist sample ids do not rise")
             ids.append(ids[-1] + d)
         if g < groups - 1 and cur - start != glen[g]:
             raise PgenError("difflist group byte-length mismatch")
+        if g < groups - 1 and ids[-1] >= first[g + 1]:
+            raise PgenError("difflist sample ids do not rise")
     return ids, vals, cur
 
 

@@ -11,7 +11,8 @@ from gnomon_b200.pgen import decode_to_device, score_pgen
 from gnomon_b200.pipeline import PipelineContext, run
 from helpers import synth_case
 from oracle import oracle, pgen_oracle
-from test_pgen import corrupt, encode_fixed_width, expected_rows, ld_pgen, GOLDEN
+from test_pgen import (GOLDEN, corrupt, encode_fixed_width, expected_rows, ld_pgen,
+                       non_rising_pgens)
 
 pytestmark = pytest.mark.gpu
 SENTINEL = 0xA7
@@ -104,6 +105,13 @@ def test_malformed_records_are_reported(cuda):
     with pytest.raises(_lib.GnomonGpuError) as ei:
         device_rows(bad, 100)
     assert ei.value.status == _lib.GNM_ERR_IO and "pair code" in str(ei.value)
+    # sample ids that repeat or fall back
+    ok, dup, back = non_rising_pgens()
+    np.testing.assert_array_equal(device_rows(ok, 1000), pgen_oracle.decode_to_bed(ok))
+    for bad in (dup, back):
+        with pytest.raises(_lib.GnomonGpuError) as ei:
+            device_rows(bad, 1000)
+        assert ei.value.status == _lib.GNM_ERR_IO
     # the device is still usable
     np.testing.assert_array_equal(device_rows(ld_pgen(), 200),
                                   np.load(GOLDEN / "ld_fixture.npz")["rows"])

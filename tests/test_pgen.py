@@ -151,3 +151,26 @@ def test_long_difflist_oracle():
     cats = np.zeros((1, n), np.uint8)
     cats[0, ids] = vals
     np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(cats))
+
+
+def non_rising_pgens(n=1000):
+    """A valid fill record with a two-group difflist, and copies whose ids
+    repeat inside a group or fall back across the group boundary."""
+    ids = np.arange(0, 200, 2, dtype=np.int64)
+    vals = np.ones(len(ids), np.uint8)
+    rec = bytes(synth._difflist_bytes(ids, vals, n))
+    # length (1 byte), two 2-byte first ids, one group-length byte, 25 value bytes
+    deltas_at = 1 + 4 + 1 + 25
+    dup = bytearray(rec)
+    dup[deltas_at] = 0                       # a zero delta inside group 0
+    back = bytearray(rec)
+    back[3:5] = (100).to_bytes(2, "little")  # group 1 starts below group 0's last id
+    return [synth._pgen_file(n, [4], [r]) for r in (rec, bytes(dup), bytes(back))]
+
+
+def test_non_rising_difflist_ids_are_malformed():
+    ok, dup, back = non_rising_pgens()
+    pgen_oracle.decode_to_bed(ok)
+    for bad in (dup, back):
+        with pytest.raises(pgen_oracle.PgenError, match="rise"):
+            pgen_oracle.decode_to_bed(bad)
