@@ -120,9 +120,13 @@ __device__ __forceinline__ uint32_t swap_homs(uint32_t x) {
 // record, with `swap` = type 3's REF/ALT swap applied to it and to the
 // patched values, or the row itself) with a plain store, or for the two end
 // words and the row's last partial word an atomicXor of the patched bits.
+//
+// `warps` warps may share one difflist: warp `wi` takes the chunks of 32
+// groups numbered wi, wi + warps, ...; a strided sum over the group byte
+// lengths it skips gives its next chunk's first delta.
 __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uint32_t cur,
                                               uint8_t* row, const uint8_t* base, uint32_t v,
-                                              bool swap) {
+                                              bool swap, uint32_t wi = 0, uint32_t warps = 1) {
   const uint32_t lane = threadIdx.x & 31u;
   uint64_t l = 0;
   if (!r.varint(cur, l) || l > a.n) {
@@ -143,7 +147,7 @@ __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uin
   }
   const uint64_t bpv = (a.n + 3) / 4;
   // a word holding bytes past the row's end is only ever xor-patched
-  const uint64_t partial_word = bpv % 4 ? bpv / 4 : ~uint64_t(0);
+  const uint32_t partial_word = bpv % 4 ? uint32_t(bpv / 4) : 0xFFFFFFFFu;
   uint32_t* row32 = reinterpret_cast<uint32_t*>(row);
   const uint32_t* base32 = reinterpret_cast<const uint32_t*>(base);
   auto first_id = [&](uint32_t g) {
@@ -151,11 +155,24 @@ __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uin
     for (uint32_t k = 0; k < wid; ++k) id |= uint64_t(r.p[first_at + g * wid + k]) << (8 * k);
     return id;
   };
+  const uint8_t* p = r.p;
+  const uint32_t rlen = r.len;
+  const uint32_t n32 = uint32_t(a.n);      // samples <= 2^31: ids fit in 32 bits
+  // bytes of the deltas of groups [g0, g1), all of which carry a length
+  auto skip = [&](uint32_t g0, uint32_t g1) {
+    uint32_t s = 0;
+    for (uint32_t g = g0 + lane; g < g1; g += 32) s += uint32_t(p[glen_at + g]) + 63u;
+#pragma unroll
+    for (uint32_t d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, d);
+    return s;
+  };
   bool bad = false;
-  for (uint32_t c0 = 0; c0 < groups; c0 += 32) {
+  if (wi > 0 && 32 * wi < groups) deltas += skip(0, 32 * wi);
+  for (uint32_t c0 = 32 * wi; c0 < groups; c0 += 32 * warps) {
+    if (warps > 1 && c0 != 32 * wi) deltas += skip(c0 - 32 * (warps - 1), c0);
     const uint32_t g = c0 + lane;
     // bytes of group g's deltas (all groups but the last carry a length)
-    const uint32_t mine = g + 1 < groups ? uint32_t(r.p[glen_at + g]) + 63u : 0u;
+    const uint32_t mine = g + 1 < groups ? uint32_t(p[glen_at + g]) + 63u : 0u;
     uint32_t incl = mine;
 #pragma unroll
     for (uint32_t d = 1; d < 32; d <<= 1) {
@@ -165,46 +182,74 @@ __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uin
     uint32_t at = deltas + incl - mine;
     deltas += __shfl_sync(0xFFFFFFFFu, incl, 31);
     if (g >= groups) continue;
-    uint64_t id = first_id(g);
+    // ids saturate at 2^32 - 1; those >= the sample count are skipped, as
+    // the reference skips them
+    uint32_t id = uint32_t(min(first_id(g), uint64_t(0xFFFFFFFFu)));
     const uint32_t count = g + 1 < groups ? 64u : len - 64u * (groups - 1);
     const uint32_t start = at;
-    uint64_t cw = ~uint64_t(0);      // word being patched
-    uint32_t pm = 0, pv = 0;         // its patched bits and their new values
-    bool edge = true;                // the group's first word
-    auto flush = [&](bool last) {
-      uint32_t old = base32[cw];
-      if (swap) old = swap_homs(old);
-      if (edge || last || cw == partial_word)
-        atomicXor(row32 + cw, (old & pm) ^ pv);
-      else
-        row32[cw] = (old & ~pm) | pv;
-      edge = false;
-    };
+    const uint8_t* vals = p + vals_at + 16 * g;          // 64 entries = 16 value bytes
+    uint32_t cw = 0xFFFFFFFFu;    // word being patched
+    uint32_t old = 0;             // its value in `base` (loaded when the word starts)
+    uint32_t pm = 0, pv = 0;      // its patched bits and their new values
+    bool edge = true;             // the group's first word
+    uint32_t vb = 0;
+    // category -> .bed code as a packed 2-bit table (no divergent lookups):
+    // {11, 10, 00, 01}, or with the REF/ALT swap {00, 10, 11, 01}
+    const uint32_t code_of = swap ? 0x78u : 0x4Bu;
     for (uint32_t e = 0; e < count; ++e) {
       if (e > 0) {
-        uint64_t d;
-        if (!r.varint(at, d) || d == 0) {
+        if (at >= rlen) {
           bad = true;
           break;
         }
-        id += d;
+        uint32_t d = p[at++];
+        if (d & 0x80u) {   // multi-byte delta
+          uint64_t d64 = d & 0x7Fu;
+          uint32_t b, shift = 7;
+          do {
+            if (at >= rlen || shift > 56) {
+              bad = true;
+              break;
+            }
+            b = p[at++];
+            d64 |= uint64_t(b & 0x7Fu) << shift;
+            shift += 7;
+          } while (b & 0x80u);
+          if (bad) break;
+          d = uint32_t(min(d64, uint64_t(0xFFFFFFFFu)));
+        }
+        if (d == 0) {
+          bad = true;
+          break;
+        }
+        id = id > 0xFFFFFFFFu - d ? 0xFFFFFFFFu : id + d;
       }
-      if (id >= a.n) continue;
-      const uint32_t idx = 64 * g + e;
-      uint32_t val = (r.p[vals_at + idx / 4] >> (2 * (idx % 4))) & 3u;
-      if (swap && !(val & 1u)) val ^= 2u;
-      const uint64_t w = id / 16;
-      const uint32_t sh = 2 * uint32_t(id % 16);
+      if ((e & 3u) == 0) vb = vals[e / 4];
+      if (id >= n32) continue;
+      const uint32_t code = (code_of >> (2 * ((vb >> (2 * (e & 3u))) & 3u))) & 3u;
+      const uint32_t w = id >> 4;
+      const uint32_t sh = 2 * (id & 15u);
       if (w != cw) {
-        if (cw != ~uint64_t(0)) flush(false);
+        if (cw != 0xFFFFFFFFu) {
+          const uint32_t o = swap ? swap_homs(old) : old;
+          if (edge || cw == partial_word)
+            atomicXor(row32 + cw, (o & pm) ^ pv);
+          else
+            row32[cw] = (o & ~pm) | pv;
+          edge = false;
+        }
         cw = w;
+        old = base32[w];
         pm = pv = 0;
       }
-      pm |= 3u << sh;
-      pv = (pv & ~(3u << sh)) | (uint32_t(kCatToBed[val]) << sh);
+      pm |= 3u << sh;   // ids rise strictly: a field is patched once
+      pv |= code << sh;
     }
-    if (cw != ~uint64_t(0)) flush(true);
-    if (!bad && g + 1 < groups && (at != start + mine || id >= first_id(g + 1)))
+    if (cw != 0xFFFFFFFFu && !bad) {
+      if (swap) old = swap_homs(old);
+      atomicXor(row32 + cw, (old & pm) ^ pv);   // the group's last word
+    }
+    if (!bad && g + 1 < groups && (at != start + mine || uint64_t(id) >= first_id(g + 1)))
       bad = true;   // group length mismatch, or ids not rising into the next group
   }
   if (bad) flag(a, kPgErrBounds, v);
@@ -223,58 +268,74 @@ __device__ __forceinline__ void warp_fix_tail(const PgArgs& a, uint8_t* row) {
   }
 }
 
-// Fill bpv bytes of a row with one byte value: 16-byte stores, then the tail.
-__device__ __forceinline__ void warp_fill(uint8_t* row, uint64_t bpv, uint32_t byte) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t w = byte * 0x01010101u;
-  const uint4 q = make_uint4(w, w, w, w);
-  const uint64_t vecs = bpv / 16;
-  for (uint64_t j = lane; j < vecs; j += 32) reinterpret_cast<uint4*>(row)[j] = q;
-  for (uint64_t j = 16 * vecs + lane; j < bpv; j += 32) row[j] = uint8_t(byte);
+// Padding fields of the last byte -> 01 (missing), after a barrier over the
+// CTA's writes to the row.
+__device__ __forceinline__ void cta_fix_tail(const PgArgs& a, uint8_t* row) {
+  __syncthreads();
+  const uint32_t rem = uint32_t(a.n % 4);
+  if (threadIdx.x == 0 && rem) {
+    const uint64_t last = (a.n + 3) / 4 - 1;
+    uint32_t b = row[last];
+    for (uint32_t k = rem; k < 4; ++k) b = (b & ~(3u << (2 * k))) | (1u << (2 * k));
+    row[last] = uint8_t(b);
+  }
 }
 
-// One warp per non-LD record of the range (LD-compressed ones return at once),
+// One CTA per non-LD record of the range (LD-compressed ones return at once),
 // plus one for `extra` when the range's first LD records anchor before it.
+// Non-LD records are few and long (whole 2-bit or 1-bit arrays), so all eight
+// warps share one: the array pass strided over the CTA, the difflist's
+// chunks of 32 groups dealt out across the warps.
 __global__ void __launch_bounds__(kPgThreads) gnm_pgen_direct(PgArgs a) {
   __shared__ uint8_t lut[256];     // byte of four PGEN categories -> byte of .bed codes
-  __shared__ uint8_t nlut[kPgWarps][16];
-  for (uint32_t x = threadIdx.x; x < 256; x += blockDim.x) {
-    uint32_t o = 0;
-    for (uint32_t k = 0; k < 4; ++k) o |= uint32_t(kCatToBed[(x >> (2 * k)) & 3u]) << (2 * k);
-    lut[x] = uint8_t(o);
-  }
-  __syncthreads();
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint64_t wi = uint64_t(blockIdx.x) * kPgWarps + threadIdx.x / 32;
-  const bool in_range = wi < a.count;
-  if (!in_range && (wi != a.count || a.extra == kNoAnchor)) return;
-  const uint32_t v = in_range ? a.begin + uint32_t(wi) : a.extra;
+  __shared__ uint8_t nib[16];      // nibble of four bits -> byte of .bed codes (type 1)
+  const uint32_t tid = threadIdx.x;
+  const bool in_range = blockIdx.x < a.count;
+  const uint32_t v = in_range ? a.begin + blockIdx.x : a.extra;
   if (a.anchor_of[v] != kNoAnchor) return;
   const Rec r{a.pgen + a.offsets[v], a.lens[v]};
   const uint32_t kind = a.types[v] & 7u;
-  uint8_t* row = in_range ? a.rows + wi * a.pitch : a.scratch;
+  uint8_t* row = in_range ? a.rows + uint64_t(blockIdx.x) * a.pitch : a.scratch;
   const uint64_t bpv = (a.n + 3) / 4;
   const uint64_t words = bpv / 4;
   uint32_t* d32 = reinterpret_cast<uint32_t*>(row);
   uint32_t cur = 0;
   if (kind == 0) {
     if (r.len < bpv) {
-      if (lane == 0) flag(a, kPgErrBounds, v);
+      if (tid == 0) flag(a, kPgErrBounds, v);
       return;
     }
+    for (uint32_t x = tid; x < 256; x += blockDim.x) {
+      uint32_t o = 0;
+      for (uint32_t k = 0; k < 4; ++k) o |= uint32_t(kCatToBed[(x >> (2 * k)) & 3u]) << (2 * k);
+      lut[x] = uint8_t(o);
+    }
+    __syncthreads();
     // whole output words from funnel-shifted aligned input words (the record
     // starts at any byte; an aligned word holding a needed byte lies inside
-    // the file's 16-byte-padded buffer)
+    // the file's 16-byte-padded buffer); four consecutive words per thread and
+    // step, five input loads in flight
     const uintptr_t addr = reinterpret_cast<uintptr_t>(r.p);
     const uint32_t* al = reinterpret_cast<const uint32_t*>(addr & ~uintptr_t(3));
     const uint32_t sh = uint32_t(addr & 3u) * 8u;
-    for (uint64_t j = lane; j < words; j += 32) {
-      const uint32_t x = __funnelshift_r(al[j], sh ? al[j + 1] : 0u, sh);
-      d32[j] = uint32_t(lut[x & 255u]) | uint32_t(lut[(x >> 8) & 255u]) << 8 |
-               uint32_t(lut[(x >> 16) & 255u]) << 16 | uint32_t(lut[x >> 24]) << 24;
+    for (uint64_t j0 = 4 * uint64_t(tid); j0 < words; j0 += 4 * kPgThreads) {
+      uint32_t in[5];
+#pragma unroll
+      for (uint32_t k = 0; k < 5; ++k) {
+        // word j0 + k is needed by output k (k < 4) or by output k - 1's high half
+        const bool need = (k < 4 && j0 + k < words) || (sh && k > 0 && j0 + k - 1 < words);
+        in[k] = need ? al[j0 + k] : 0u;
+      }
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        if (j0 + k >= words) break;
+        const uint32_t x = __funnelshift_r(in[k], in[k + 1], sh);
+        d32[j0 + k] = uint32_t(lut[x & 255u]) | uint32_t(lut[(x >> 8) & 255u]) << 8 |
+                      uint32_t(lut[(x >> 16) & 255u]) << 16 | uint32_t(lut[x >> 24]) << 24;
+      }
     }
-    for (uint64_t j = 4 * words + lane; j < bpv; j += 32) row[j] = lut[r.p[j]];
-    warp_fix_tail(a, row);
+    for (uint64_t j = 4 * words + tid; j < bpv; j += blockDim.x) row[j] = lut[r.p[j]];
+    cta_fix_tail(a, row);
     return;
   }
   if (kind == 1) {
@@ -284,48 +345,51 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_direct(PgArgs a) {
     const int low = okb && pc < 16 ? kPairLow[pc] : -1;
     const int high = okb && pc < 16 ? kPairHigh[pc] : -1;
     if (!okb || low < 0) {
-      if (lane == 0) flag(a, kPgErrPair, v);
+      if (tid == 0) flag(a, kPgErrPair, v);
       return;
     }
     const uint32_t nb = uint32_t((a.n + 7) / 8);
     if (r.len < 1 + nb) {
-      if (lane == 0) flag(a, kPgErrBounds, v);
+      if (tid == 0) flag(a, kPgErrBounds, v);
       return;
     }
-    // nibble of four bits -> byte of four .bed codes (a table per warp)
-    uint8_t* nib = nlut[threadIdx.x / 32];
-    if (lane < 16) {
+    if (tid < 16) {
       uint32_t o = 0;
       for (uint32_t k = 0; k < 4; ++k)
-        o |= uint32_t(kCatToBed[((lane >> k) & 1u) ? high : low]) << (2 * k);
-      nib[lane] = uint8_t(o);
+        o |= uint32_t(kCatToBed[((tid >> k) & 1u) ? high : low]) << (2 * k);
+      nib[tid] = uint8_t(o);
     }
-    __syncwarp();
+    __syncthreads();
     const uint8_t* bits = r.p + 1;
-    for (uint64_t j = lane; j < words; j += 32) {
+    for (uint64_t j = tid; j < words; j += blockDim.x) {
       const uint32_t b0 = bits[2 * j], b1 = bits[2 * j + 1];
       d32[j] = uint32_t(nib[b0 & 15u]) | uint32_t(nib[b0 >> 4]) << 8 |
                uint32_t(nib[b1 & 15u]) << 16 | uint32_t(nib[b1 >> 4]) << 24;
     }
-    for (uint64_t j = 4 * words + lane; j < bpv; j += 32)
+    for (uint64_t j = 4 * words + tid; j < bpv; j += blockDim.x)
       row[j] = nib[(bits[j / 2] >> (4 * (j % 2))) & 15u];
     cur = 1 + nb;
   } else if (kind == 4 || kind == 6 || kind == 7) {
-    warp_fill(row, bpv, kCatToBed[kind == 4 ? 0 : kind == 6 ? 2 : 3] * 0x55u);
+    const uint32_t byte = kCatToBed[kind == 4 ? 0 : kind == 6 ? 2 : 3] * 0x55u;
+    const uint32_t w = byte * 0x01010101u;
+    const uint4 q = make_uint4(w, w, w, w);
+    const uint64_t vecs = bpv / 16;
+    for (uint64_t j = tid; j < vecs; j += blockDim.x) reinterpret_cast<uint4*>(row)[j] = q;
+    for (uint64_t j = 16 * vecs + tid; j < bpv; j += blockDim.x) row[j] = uint8_t(byte);
   } else {
-    if (lane == 0) flag(a, kPgErrPair, v);
+    if (tid == 0) flag(a, kPgErrPair, v);
     return;
   }
-  __syncwarp();
-  warp_difflist(a, r, cur, row, row, v, false);
-  warp_fix_tail(a, row);
+  __syncthreads();   // the row is complete before its words are patched
+  warp_difflist(a, r, cur, row, row, v, false, tid / 32, kPgWarps);
+  cta_fix_tail(a, row);
 }
 
-// One warp per LD-compressed record of the range (others return at once):
-// copy the anchor row (16-byte vectors; type 3 swaps REF and ALT homozygotes
+// One warp per LD-compressed record of the range (others return at once;
+// eight CTAs, 64 warps, per SM): copy the anchor row (16-byte vectors; type 3 swaps REF and ALT homozygotes
 // on the way), then patch it with the record's difflist.  The anchor row is in
 // the range's rows, or in `scratch` when it precedes the range.
-__global__ void __launch_bounds__(kPgThreads) gnm_pgen_ld(PgArgs a) {
+__global__ void __launch_bounds__(kPgThreads, 8) gnm_pgen_ld(PgArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t wi = uint64_t(blockIdx.x) * kPgWarps + threadIdx.x / 32;
   if (wi >= a.count) return;
@@ -341,20 +405,35 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_ld(PgArgs a) {
   const uint64_t vecs = bpv / 16;
   const uint4* s16 = reinterpret_cast<const uint4*>(src);
   uint4* d16 = reinterpret_cast<uint4*>(row);
-  if (swap) {
-    for (uint64_t j = lane; j < vecs; j += 32) {
-      uint4 q = s16[j];
+  // four 16-byte loads in flight per lane before their stores
+  uint64_t j = lane;
+  for (; j + 96 < vecs; j += 128) {
+    uint4 q[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] = s16[j + 32 * k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (swap) {
+        q[k].x = swap_homs(q[k].x);
+        q[k].y = swap_homs(q[k].y);
+        q[k].z = swap_homs(q[k].z);
+        q[k].w = swap_homs(q[k].w);
+      }
+      d16[j + 32 * k] = q[k];
+    }
+  }
+  for (; j < vecs; j += 32) {
+    uint4 q = s16[j];
+    if (swap) {
       q.x = swap_homs(q.x);
       q.y = swap_homs(q.y);
       q.z = swap_homs(q.z);
       q.w = swap_homs(q.w);
-      d16[j] = q;
     }
-    for (uint64_t j = 16 * vecs + lane; j < bpv; j += 32) row[j] = uint8_t(swap_homs(src[j]));
-  } else {
-    for (uint64_t j = lane; j < vecs; j += 32) d16[j] = s16[j];
-    for (uint64_t j = 16 * vecs + lane; j < bpv; j += 32) row[j] = src[j];
+    d16[j] = q;
   }
+  for (uint64_t b = 16 * vecs + lane; b < bpv; b += 32)
+    row[b] = uint8_t(swap ? swap_homs(src[b]) : src[b]);
   __syncwarp();
   warp_difflist(a, r, 0, row, src, v, swap);
   warp_fix_tail(a, row);
@@ -540,8 +619,7 @@ static void pgen_decode_impl(gnm_pgen* pg, uint64_t begin, uint64_t count, uint8
       break;
     }
   DeviceGuard g(pg->device);
-  const uint64_t direct_warps = uint64_t(a.count) + (a.extra != kNoAnchor ? 1u : 0u);
-  gnm_pgen_direct<<<uint32_t((direct_warps + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
+  gnm_pgen_direct<<<a.count + (a.extra != kNoAnchor ? 1u : 0u), kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen decode launch");
   gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen LD decode launch");
