@@ -116,10 +116,11 @@ __device__ __forceinline__ uint32_t swap_homs(uint32_t x) {
 // group owns every 32-bit word of the row between its first and last id
 // except those two, which a neighbouring group may share.  A lane merges its
 // patches per word in registers and writes each word once: the final value
-// computed from `base` (the row before patching: the anchor row for an LD
-// record, with `swap` = type 3's REF/ALT swap applied to it and to the
-// patched values, or the row itself) with a plain store, or for the two end
-// words and the row's last partial word an atomicXor of the patched bits.
+// computed from `base` (the row before patching: the anchor row of an LD
+// record, still in L1 from the copy, with `swap` = type 3's REF/ALT swap
+// applied to it and to the patched values; or the row itself) with a plain
+// store, or for the two end words and the row's last partial word an
+// atomicXor of the patched bits.
 //
 // `warps` warps may share one difflist: warp `wi` takes the chunks of 32
 // groups numbered wi, wi + warps, ...; a strided sum over the group byte
@@ -198,11 +199,9 @@ __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uin
     const uint32_t code_of = swap ? 0x78u : 0x4Bu;
     for (uint32_t e = 0; e < count; ++e) {
       if (e > 0) {
-        if (at >= rlen) {
-          bad = true;
-          break;
-        }
-        uint32_t d = p[at++];
+        // a read past the record gives 0, which ends the walk as a zero delta
+        uint32_t d = at < rlen ? p[at] : 0u;
+        ++at;
         if (d & 0x80u) {   // multi-byte delta
           uint64_t d64 = d & 0x7Fu;
           uint32_t b, shift = 7;
@@ -245,9 +244,9 @@ __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uin
       pm |= 3u << sh;   // ids rise strictly: a field is patched once
       pv |= code << sh;
     }
-    if (cw != 0xFFFFFFFFu && !bad) {
-      if (swap) old = swap_homs(old);
-      atomicXor(row32 + cw, (old & pm) ^ pv);   // the group's last word
+    if (cw != 0xFFFFFFFFu && !bad) {   // the group's last word
+      const uint32_t o = swap ? swap_homs(old) : old;
+      atomicXor(row32 + cw, (o & pm) ^ pv);
     }
     if (!bad && g + 1 < groups && (at != start + mine || uint64_t(id) >= first_id(g + 1)))
       bad = true;   // group length mismatch, or ids not rising into the next group
