@@ -55,12 +55,12 @@ def peaks_tc():
     return 1400.0, "fallback"
 
 
-def traffic_from_profile():
-    """dram bytes per launch recorded from the ncu capture (profiles/), else None."""
-    if not PROFILE.exists():
+def traffic_from_profile(path=PROFILE, key="traffic_bytes_per_launch"):
+    """A DRAM-bytes figure recorded from an ncu capture (profiles/), else None."""
+    if not path.exists():
         return None
-    for line in PROFILE.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+    for line in path.read_text().splitlines():
+        if line.strip().startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -652,6 +652,8 @@ def pgen_arm(args, rank, world, local_rank):
     e2e = statistics.median(e2e_s)
     hbm, src = peaks()
     achieved = algo_bytes / (ms / 1e3) / 1e9
+    traffic_pv = traffic_from_profile(ROOT / "profiles" / "pgen_decode_50k_x_16k.md",
+                                      "traffic_bytes_per_variant")
     line = {"metric": "pgen variants decoded/s", "value": V / (ms / 1e3), "unit": "variants/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
@@ -666,7 +668,9 @@ def pgen_arm(args, rank, world, local_rank):
                          "frac": achieved / hbm, "peak_source": src,
                          "algorithmic_bytes_per_step": algo_bytes,
                          "kernels": "gnm_pgen_direct + gnm_pgen_ld (one decode = both)",
-                         "traffic": None},
+                         "traffic": traffic_pv * V if traffic_pv else None,
+                         "traffic_source": "ncu DRAM bytes per variant of the 16,384-variant "
+                                           "case, times this case's variants"},
             "e2e": {"value": V / e2e, "unit": "variants/s", "h2d_bytes_per_step": int(data.nbytes),
                     "d2h_bytes_per_step": 8, "seconds": e2e},
             "gpu_launches": 2 * args.steps,

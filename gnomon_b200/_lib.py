@@ -106,6 +106,11 @@ SIGNATURES = {
     "gnm_pgen_decode": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint64,
                                   C.c_void_p, C.POINTER(gnm_error)]),
     "gnm_pgen_check": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(gnm_error)]),
+    "gnm_pgen_decode_list": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                       C.c_uint64, C.c_void_p, C.POINTER(gnm_error)]),
+    "gnm_score_pgen": (C.c_int, [C.POINTER(gnm_prep_view), C.c_void_p, C.c_uint64,
+                                 C.POINTER(gnm_run_options), C.c_void_p, C.c_void_p,
+                                 C.POINTER(gnm_error)]),
     "gnm_score_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.POINTER(gnm_error)]),

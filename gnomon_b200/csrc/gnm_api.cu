@@ -12,6 +12,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <memory>
 #include <chrono>
 #include <cstdlib>
 #include <atomic>
@@ -975,6 +976,82 @@ gnm_status gnm_score_run(const gnm_prep_view* prep, const gnm_bed_view* bed,
                          const gnm_resume* resume, double* sums_out, uint32_t* missing_out,
                          gnm_error* err) {
   return gnm_score_run_ex(prep, bed, resume, nullptr, sums_out, missing_out, err);
+}
+
+// The .pgen counterpart of the end-to-end run: the file is uploaded once, the
+// reconciled variants (required_bim_indices) are decoded on the device block
+// by block into one row buffer, and each block is accumulated as it lands.
+static void score_pgen_impl(const gnm_prep_view* prep, const uint8_t* pgen, uint64_t pgen_len,
+                            const gnm_run_options* opts, double* sums_out,
+                            uint32_t* missing_out) {
+  if (!prep) fail(GNM_ERR_INVALID, "prep is NULL");
+  if (!sums_out || !missing_out) fail(GNM_ERR_INVALID, "output buffers are NULL");
+  const gnm_engine engine = opts ? opts->engine : GNM_ENGINE_AUTO;
+  int device = opts ? opts->device : -1;
+  if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
+  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  validate_prep(prep);
+  std::unique_ptr<gnm_pgen, void (*)(gnm_pgen*)> pg(pgen_open_impl(pgen, pgen_len, device),
+                                                     gnm_pgen_close);
+  const uint64_t n = pgen_samples(pg.get()), m = pgen_variants(pg.get());
+  if (n != prep->total_people_in_fam || (n + 3) / 4 != prep->bytes_per_variant)
+    fail(GNM_ERR_INVALID, "the .pgen has " + std::to_string(n) + " samples, the preparation " +
+                              std::to_string(prep->total_people_in_fam));
+  const uint64_t V = prep->num_variants;
+  std::vector<uint64_t> req(V);
+  for (uint64_t v = 0; v < V; ++v) {
+    req[v] = prep->required_bim_indices ? prep->required_bim_indices[v] : v;
+    if (req[v] >= m)
+      fail(GNM_ERR_INVALID, "required variant " + std::to_string(req[v]) +
+                                " is past the .pgen's " + std::to_string(m) + " variants");
+  }
+  std::unique_ptr<gnm_plan, void (*)(gnm_plan*)> plan(plan_create_impl(prep, engine, device, true),
+                                                      gnm_plan_destroy);
+  DeviceGuard g(device);
+  struct Stream {
+    cudaStream_t s = nullptr;
+    ~Stream() {
+      if (s) cudaStreamDestroy(s);
+    }
+  } st;
+  check_cuda(cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking), "cudaStreamCreate");
+  const uint64_t pitch = (prep->bytes_per_variant + 127) / 128 * 128;
+  // default block: every reconciled variant if its rows take at most 4 GiB
+  uint64_t B = opts && opts->block_variants ? opts->block_variants
+                                            : std::max<uint64_t>(1, (uint64_t(4) << 30) / pitch);
+  B = std::max<uint64_t>(1, std::min<uint64_t>(B, std::max<uint64_t>(V, 1)));
+  struct Pool {
+    std::vector<void*> p;
+    ~Pool() {
+      for (void* x : p) pool_free(x);
+    }
+    void* get(int dev, uint64_t bytes, const char* what) {
+      p.push_back(pool_alloc(dev, bytes, what));
+      return p.back();
+    }
+  } pool;
+  auto* rows = static_cast<uint8_t*>(pool.get(device, B * pitch, ".pgen row block"));
+  const uint64_t PK = prep->num_people * prep->num_scores;
+  auto* d_sums = static_cast<double*>(pool.get(device, std::max<uint64_t>(PK, 1) * 8, "sums"));
+  auto* d_counts = static_cast<uint32_t*>(pool.get(device, std::max<uint64_t>(PK, 1) * 4, "counts"));
+  plan_reset_impl(plan.get(), st.s);
+  for (uint64_t b0 = 0; b0 < V; b0 += B) {
+    const uint64_t nb = std::min(B, V - b0);
+    pgen_decode_list_impl(pg.get(), req.data() + b0, nb, rows, pitch, st.s);
+    accumulate_impl(plan.get(), rows, pitch, b0, nb, st.s);
+  }
+  finalize_impl(plan.get(), d_sums, d_counts, true, st.s);
+  check_cuda(cudaMemcpyAsync(sums_out, d_sums, PK * 8, cudaMemcpyDeviceToHost, st.s), "sums");
+  check_cuda(cudaMemcpyAsync(missing_out, d_counts, PK * 4, cudaMemcpyDeviceToHost, st.s),
+             "counts");
+  pgen_check_impl(pg.get(), st.s);
+  sync_impl(plan.get(), st.s);
+}
+
+gnm_status gnm_score_pgen(const gnm_prep_view* prep, const uint8_t* pgen, uint64_t pgen_len,
+                          const gnm_run_options* opts, double* sums_out, uint32_t* missing_out,
+                          gnm_error* err) {
+  return guarded(err, [&] { score_pgen_impl(prep, pgen, pgen_len, opts, sums_out, missing_out); });
 }
 
 gnm_status gnm_score_run_ex(const gnm_prep_view* prep, const gnm_bed_view* bed,

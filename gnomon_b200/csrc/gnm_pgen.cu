@@ -62,9 +62,27 @@ struct PgArgs {
   uint64_t n;                  // samples
   uint8_t* rows;               // [count][pitch] .bed rows
   uint64_t pitch;
-  uint8_t* scratch;            // one row: the anchor of the range's first LD records
+  uint8_t* scratch;            // anchor rows outside the output: [extra_rows][spitch]
+  uint64_t spitch;
+  uint32_t extra_rows;         // scratch rows the direct kernel decodes
+  // list mode (null in range mode): the variant of output row i (rows count ..
+  // count + extra_rows - 1 are scratch rows) and the row holding its anchor
+  const uint32_t* vids;
+  const uint32_t* arow;
   uint32_t* err;               // [0] error bits, [1] first bad variant (atomicMin)
 };
+
+// Row i of a decode: an output row, or a scratch row past the output's end.
+__device__ __forceinline__ uint8_t* row_at(const PgArgs& a, uint32_t i) {
+  return i < a.count ? a.rows + uint64_t(i) * a.pitch
+                     : a.scratch + uint64_t(i - a.count) * a.spitch;
+}
+
+// The variant decoded into row i: listed, or the range's (the scratch row of
+// a range holds `extra`).
+__device__ __forceinline__ uint32_t variant_at(const PgArgs& a, uint32_t i) {
+  return a.vids ? a.vids[i] : i < a.count ? a.begin + i : a.extra;
+}
 
 __constant__ uint8_t kCatToBed[4] = {0x3, 0x2, 0x0, 0x1};
 // 1-bit record pair codes (shared/adapt_plink2.rs:2600-2608): the category of
@@ -280,8 +298,8 @@ __device__ __forceinline__ void cta_fix_tail(const PgArgs& a, uint8_t* row) {
   }
 }
 
-// One CTA per non-LD record of the range (LD-compressed ones return at once),
-// plus one for `extra` when the range's first LD records anchor before it.
+// One CTA per non-LD record of the range or list (LD-compressed ones return
+// at once), plus one per scratch row: anchors outside the output.
 // Non-LD records are few and long (whole 2-bit or 1-bit arrays), so all eight
 // warps share one: the array pass strided over the CTA, the difflist's
 // chunks of 32 groups dealt out across the warps.
@@ -289,12 +307,11 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_direct(PgArgs a) {
   __shared__ uint8_t lut[256];     // byte of four PGEN categories -> byte of .bed codes
   __shared__ uint8_t nib[16];      // nibble of four bits -> byte of .bed codes (type 1)
   const uint32_t tid = threadIdx.x;
-  const bool in_range = blockIdx.x < a.count;
-  const uint32_t v = in_range ? a.begin + blockIdx.x : a.extra;
+  const uint32_t v = variant_at(a, blockIdx.x);
   if (a.anchor_of[v] != kNoAnchor) return;
   const Rec r{a.pgen + a.offsets[v], a.lens[v]};
   const uint32_t kind = a.types[v] & 7u;
-  uint8_t* row = in_range ? a.rows + uint64_t(blockIdx.x) * a.pitch : a.scratch;
+  uint8_t* row = row_at(a, blockIdx.x);
   const uint64_t bpv = (a.n + 3) / 4;
   const uint64_t words = bpv / 4;
   uint32_t* d32 = reinterpret_cast<uint32_t*>(row);
@@ -384,22 +401,22 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_direct(PgArgs a) {
   cta_fix_tail(a, row);
 }
 
-// One warp per LD-compressed record of the range (others return at once;
-// eight CTAs, 64 warps, per SM): copy the anchor row (16-byte vectors; type 3 swaps REF and ALT homozygotes
-// on the way), then patch it with the record's difflist.  The anchor row is in
-// the range's rows, or in `scratch` when it precedes the range.
+// One warp per LD-compressed record of the range or list (others return at
+// once; eight CTAs, 64 warps, per SM): copy the anchor row (16-byte vectors; type 3 swaps REF and ALT homozygotes
+// on the way), then patch it with the record's difflist.  The anchor row is an
+// output row, or a scratch row when it is outside the output.
 __global__ void __launch_bounds__(kPgThreads, 8) gnm_pgen_ld(PgArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t wi = uint64_t(blockIdx.x) * kPgWarps + threadIdx.x / 32;
   if (wi >= a.count) return;
-  const uint32_t v = a.begin + uint32_t(wi);
+  const uint32_t v = variant_at(a, uint32_t(wi));
   const uint32_t anchor = a.anchor_of[v];
   if (anchor == kNoAnchor) return;
   const Rec r{a.pgen + a.offsets[v], a.lens[v]};
   const bool swap = (a.types[v] & 7u) == 3u;
   uint8_t* row = a.rows + wi * a.pitch;
-  const uint8_t* src =
-      anchor >= a.begin ? a.rows + uint64_t(anchor - a.begin) * a.pitch : a.scratch;
+  const uint32_t ar = a.arow ? a.arow[wi] : anchor >= a.begin ? anchor - a.begin : a.count;
+  const uint8_t* src = row_at(a, ar);
   const uint64_t bpv = (a.n + 3) / 4;
   const uint64_t vecs = bpv / 16;
   const uint4* s16 = reinterpret_cast<const uint4*>(src);
@@ -530,20 +547,28 @@ PgenIndex parse_pgen(const uint8_t* d, uint64_t len) {
 struct gnm_pgen {
   int device = 0;
   uint64_t variants = 0, samples = 0, file_bytes = 0, device_bytes = 0;
-  std::vector<uint32_t> anchor_of;   // host copy: the range's out-of-range anchor
+  std::vector<uint32_t> anchor_of;   // host copy: which anchors a decode needs
   std::vector<void*> bufs;
   gnm::PgArgs base{};
+  // list-mode buffers, grown on demand (device and host copies)
+  uint8_t* scratch = nullptr;
+  uint64_t scratch_rows = 0;
+  uint32_t* d_list = nullptr;        // [vids | arow]
+  uint64_t list_cap = 0;
+  std::vector<uint32_t> h_list;
   ~gnm_pgen() {
     // decodes in flight on any stream may still read the buffers
     gnm::DeviceGuard g(device);
     cudaDeviceSynchronize();
     for (void* x : bufs) gnm::pool_free(x);
+    gnm::pool_free(scratch);
+    gnm::pool_free(d_list);
   }
 };
 
 namespace gnm {
 
-static gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device) {
+gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device) {
   PgenIndex ix = parse_pgen(pgen, pgen_len);
   const uint64_t m = ix.variants;
   // one CTA per variant: the grid's x extent bounds the variant count
@@ -586,26 +611,120 @@ static gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int devi
   a.anchor_of = static_cast<const uint32_t*>(up(anchor_of.data(), m * 4, ".pgen index"));
   const uint32_t init_err[2] = {0u, 0xFFFFFFFFu};
   a.err = static_cast<uint32_t*>(up(init_err, 8, ".pgen error word"));
-  a.scratch = static_cast<uint8_t*>(up(nullptr, (ix.samples + 3) / 4, ".pgen anchor row"));
+  a.spitch = ((ix.samples + 3) / 4 + 15) / 16 * 16;
+  pg->scratch = static_cast<uint8_t*>(pool_alloc(device, a.spitch, ".pgen anchor rows"));
+  pg->scratch_rows = 1;
+  pg->device_bytes += a.spitch;
+  a.scratch = pg->scratch;
   a.n = ix.samples;
   pg->anchor_of = std::move(anchor_of);
   return pg.release();
 }
 
+// Grow a handle buffer; work in flight may read the old one, so the device
+// is synchronised before it is freed (growth is rare: the first large list).
+template <class T>
+static void grow(gnm_pgen* pg, T*& buf, uint64_t& cap, uint64_t need, uint64_t unit,
+                 const char* what) {
+  if (need <= cap) return;
+  check_cuda(cudaDeviceSynchronize(), what);
+  pool_free(buf);
+  pg->device_bytes -= cap * unit;
+  buf = nullptr;
+  cap = 0;
+  buf = static_cast<T*>(pool_alloc(pg->device, need * unit, what));
+  cap = need;
+  pg->device_bytes += need * unit;
+}
+
+static void check_rows(const gnm_pgen* pg, const uint8_t* d_rows, uint64_t pitch) {
+  const uint64_t bpv = (pg->samples + 3) / 4;
+  if (!d_rows) fail(GNM_ERR_INVALID, "d_rows is NULL");
+  if (pitch < bpv || pitch % 16 != 0 || reinterpret_cast<uintptr_t>(d_rows) % 16 != 0)
+    fail(GNM_ERR_INVALID, "rows must be 16-byte aligned with a pitch >= ceil(samples/4), "
+                          "a multiple of 16");
+}
+
+static void launch_decode(const PgArgs& a, cudaStream_t s) {
+  gnm_pgen_direct<<<a.count + a.extra_rows, kPgThreads, 0, s>>>(a);
+  check_cuda(cudaGetLastError(), "pgen decode launch");
+  gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
+  check_cuda(cudaGetLastError(), "pgen LD decode launch");
+}
+
+// Decode the listed variants (any order) into consecutive rows.  An LD
+// record whose anchor is not listed reads it from a scratch row the same
+// launch decodes; every such anchor is decoded once.
+void pgen_decode_list_impl(gnm_pgen* pg, const uint64_t* list, uint64_t count,
+                                  uint8_t* d_rows, uint64_t pitch, cudaStream_t s) {
+  if (!pg) fail(GNM_ERR_INVALID, "pgen handle is NULL");
+  if (count == 0) return;
+  if (!list) fail(GNM_ERR_INVALID, "variant list is NULL");
+  check_rows(pg, d_rows, pitch);
+  if (count > 0x3FFFFFFFull) fail(GNM_ERR_INVALID, "more than 2^30 - 1 listed variants");
+  std::vector<std::pair<uint32_t, uint32_t>> sorted(count);   // (variant, row)
+  for (uint64_t i = 0; i < count; ++i) {
+    if (list[i] >= pg->variants)
+      fail(GNM_ERR_INVALID, "listed variant " + std::to_string(list[i]) + " is past the .pgen's " +
+                                std::to_string(pg->variants) + " variants");
+    sorted[i] = {uint32_t(list[i]), uint32_t(i)};
+  }
+  std::sort(sorted.begin(), sorted.end());
+  std::vector<uint32_t>& h = pg->h_list;
+  h.assign(2 * count, 0u);   // vids (+ scratch variants appended), then arow
+  std::vector<uint32_t> extra;
+  std::vector<std::pair<uint32_t, uint32_t>> slot;             // (anchor, scratch row)
+  for (uint64_t i = 0; i < count; ++i) {
+    const uint32_t a = pg->anchor_of[list[i]];
+    h[i] = uint32_t(list[i]);
+    if (a == kNoAnchor) continue;
+    auto it = std::lower_bound(sorted.begin(), sorted.end(), std::make_pair(a, 0u));
+    if (it != sorted.end() && it->first == a) {
+      h[count + i] = it->second;
+    } else {
+      auto sl = std::lower_bound(slot.begin(), slot.end(), std::make_pair(a, 0u));
+      if (sl == slot.end() || sl->first != a) {
+        sl = slot.insert(sl, {a, uint32_t(extra.size())});
+        extra.push_back(a);
+      }
+      h[count + i] = uint32_t(count) + sl->second;
+    }
+  }
+  // layout on the device: vids [count + extra], arow [count]
+  std::vector<uint32_t> dev(2 * count + extra.size());
+  std::copy(h.begin(), h.begin() + count, dev.begin());
+  std::copy(extra.begin(), extra.end(), dev.begin() + count);
+  std::copy(h.begin() + count, h.end(), dev.begin() + count + extra.size());
+  pg->h_list.swap(dev);   // kept alive by the handle until the next call
+  DeviceGuard g(pg->device);
+  grow(pg, pg->d_list, pg->list_cap, pg->h_list.size(), sizeof(uint32_t), ".pgen variant list");
+  grow(pg, pg->scratch, pg->scratch_rows, std::max<uint64_t>(1, extra.size()), pg->base.spitch,
+       ".pgen anchor rows");
+  check_cuda(cudaMemcpyAsync(pg->d_list, pg->h_list.data(), pg->h_list.size() * 4,
+                             cudaMemcpyHostToDevice, s),
+             "upload .pgen variant list");
+  PgArgs a = pg->base;
+  a.scratch = pg->scratch;
+  a.count = uint32_t(count);
+  a.rows = d_rows;
+  a.pitch = pitch;
+  a.extra_rows = uint32_t(extra.size());
+  a.vids = pg->d_list;
+  a.arow = pg->d_list + count + extra.size();
+  launch_decode(a, s);
+}
+
 static void pgen_decode_impl(gnm_pgen* pg, uint64_t begin, uint64_t count, uint8_t* d_rows,
                              uint64_t pitch, cudaStream_t s) {
   if (!pg) fail(GNM_ERR_INVALID, "pgen handle is NULL");
-  const uint64_t bpv = (pg->samples + 3) / 4;
   if (begin > pg->variants || count > pg->variants - begin)
     fail(GNM_ERR_INVALID, "variant range [" + std::to_string(begin) + ", " +
                               std::to_string(begin + count) + ") exceeds the .pgen's " +
                               std::to_string(pg->variants) + " variants");
   if (count == 0) return;
-  if (!d_rows) fail(GNM_ERR_INVALID, "d_rows is NULL");
-  if (pitch < bpv || pitch % 16 != 0 || reinterpret_cast<uintptr_t>(d_rows) % 16 != 0)
-    fail(GNM_ERR_INVALID, "rows must be 16-byte aligned with a pitch >= ceil(samples/4), "
-                          "a multiple of 16");
+  check_rows(pg, d_rows, pitch);
   PgArgs a = pg->base;
+  a.scratch = pg->scratch;
   a.begin = uint32_t(begin);
   a.count = uint32_t(count);
   a.rows = d_rows;
@@ -617,14 +736,15 @@ static void pgen_decode_impl(gnm_pgen* pg, uint64_t begin, uint64_t count, uint8
       a.extra = pg->anchor_of[v];
       break;
     }
+  a.extra_rows = a.extra != kNoAnchor ? 1u : 0u;
   DeviceGuard g(pg->device);
-  gnm_pgen_direct<<<a.count + (a.extra != kNoAnchor ? 1u : 0u), kPgThreads, 0, s>>>(a);
-  check_cuda(cudaGetLastError(), "pgen decode launch");
-  gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
-  check_cuda(cudaGetLastError(), "pgen LD decode launch");
+  launch_decode(a, s);
 }
 
-static void pgen_check_impl(gnm_pgen* pg, cudaStream_t s) {
+uint64_t pgen_samples(const gnm_pgen* pg) { return pg->samples; }
+uint64_t pgen_variants(const gnm_pgen* pg) { return pg->variants; }
+
+void pgen_check_impl(gnm_pgen* pg, cudaStream_t s) {
   if (!pg) fail(GNM_ERR_INVALID, "pgen handle is NULL");
   DeviceGuard g(pg->device);
   uint32_t err[2] = {0, 0};
@@ -673,6 +793,13 @@ gnm_status gnm_pgen_decode(gnm_pgen* pg, uint64_t variant_begin, uint64_t varian
   return guarded(err, [&] {
     pgen_decode_impl(pg, variant_begin, variant_count, d_rows, pitch,
                      static_cast<cudaStream_t>(stream));
+  });
+}
+
+gnm_status gnm_pgen_decode_list(gnm_pgen* pg, const uint64_t* variants, uint64_t count,
+                                uint8_t* d_rows, uint64_t pitch, void* stream, gnm_error* err) {
+  return guarded(err, [&] {
+    pgen_decode_list_impl(pg, variants, count, d_rows, pitch, static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -96,6 +96,14 @@ struct PhaseTrace {
 // through a pinned ring with threaded host copies.
 void copy_to_device(void* dst, const void* src, uint64_t bytes, cudaStream_t s);
 
+// PLINK 2 .pgen decoding (gnm_pgen.cu), for the end-to-end .pgen run.
+gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device);
+void pgen_decode_list_impl(gnm_pgen* pg, const uint64_t* list, uint64_t count, uint8_t* d_rows,
+                           uint64_t pitch, cudaStream_t s);
+void pgen_check_impl(gnm_pgen* pg, cudaStream_t s);
+uint64_t pgen_samples(const gnm_pgen* pg);
+uint64_t pgen_variants(const gnm_pgen* pg);
+
 CUtensorMap make_row_map(const uint8_t* d_rows, uint64_t bytes_per_row, uint64_t num_rows,
                          uint64_t pitch, uint32_t box_x, uint32_t box_y);
 

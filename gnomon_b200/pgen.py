@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import DevicePlan, _stream_ptr, row_pitch
+from .device import _stream_ptr, row_pitch
 from .prepare import PreparationResult
 
 PgenSource = Union[str, os.PathLike, bytes, bytearray, np.ndarray]
@@ -121,6 +121,16 @@ class PgenFile:
         _lib.check(self.lib.gnm_pgen_decode(self.handle, variant_begin, n, rows.data_ptr(), pitch,
                                             _stream_ptr(stream), C.byref(e)), e)
 
+    def decode_list(self, rows: torch.Tensor, pitch: int, variants, stream=None):
+        """Enqueue the decode of the listed variants (any order) into consecutive rows."""
+        lst = np.ascontiguousarray(variants, dtype=np.uint64).reshape(-1)
+        if not (rows.is_cuda and rows.dtype == torch.uint8 and rows.numel() >= len(lst) * pitch):
+            raise ValueError("rows must be a CUDA uint8 tensor of at least count x pitch bytes")
+        e = _lib.gnm_error()
+        _lib.check(self.lib.gnm_pgen_decode_list(self.handle, lst.ctypes.data, len(lst),
+                                                 rows.data_ptr(), pitch, _stream_ptr(stream),
+                                                 C.byref(e)), e)
+
     def check(self, stream=None):
         """Wait for ``stream``; raise if any record decoded so far was malformed."""
         e = _lib.gnm_error()
@@ -128,38 +138,36 @@ class PgenFile:
 
 
 def score_pgen(prep: PreparationResult, data: PgenSource, engine: int = _lib.ENGINE_AUTO,
-               device: Optional[int] = None) -> Tuple[np.ndarray, np.ndarray]:
-    """Score a ``.pgen`` whose variants are the ``.bim``-order rows ``prep`` indexes.
-
-    Decodes on the device, gathers the reconciled variants' rows
-    (``required_bim_indices``) and scores them; returns host (sums f64,
-    missing counts u32), person-major like ``gnm_score_run``.  Multi-row
-    loci (``prep.complex_rules``) are resolved on the CPU afterwards from the
-    decoded rows, as ``try_run_cuda`` does for a ``.bed``."""
+               device: Optional[int] = None,
+               block_variants: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """Score a ``.pgen`` whose variants are the ``.bim``-order rows ``prep`` indexes
+    (``gnm_score_pgen``): the reconciled variants (``required_bim_indices``)
+    are decoded on the device block by block and scored as they land.
+    Returns host (sums f64, missing counts u32), person-major like
+    ``gnm_score_run``.  Multi-row loci (``prep.complex_rules``) are resolved on
+    the CPU afterwards from the decoded rows, as ``try_run_cuda`` does for a
+    ``.bed``."""
+    from .pipeline import prep_view
     buf = _bytes(data)
-    m, n = pgen_dims(buf)
-    if n != prep.total_people_in_fam:
-        raise ValueError(f".pgen has {n} samples, the preparation {prep.total_people_in_fam}")
-    rows, pitch = decode_to_device(buf, device=device)
-    scored = rows
-    if prep.required_bim_indices is not None:
-        req = torch.from_numpy(prep.required_bim_indices.astype(np.int64)).to(rows.device)
-        if len(req) and int(req.max()) >= m:
-            raise ValueError("required_bim_indices point past the .pgen's variants")
-        scored = rows[:m * pitch].view(m, pitch).index_select(0, req).reshape(-1)
-    plan = DevicePlan(prep, engine=engine, device=rows.device.index)
-    try:
-        sums, counts = plan.score(scored, pitch)
-        torch.cuda.synchronize(rows.device)
-        sums = sums.cpu().numpy()
-        counts = counts.cpu().numpy().view(np.uint32)
-    finally:
-        plan.close()
+    lib = _lib.load()
+    P, K = prep.num_people_to_score, prep.num_scores
+    sums = np.empty(P * K, dtype=np.float64)
+    counts = np.empty(P * K, dtype=np.uint32)
+    pv = prep_view(prep)
+    opts = _lib.gnm_run_options()
+    opts.engine = engine
+    opts.device = -1 if device is None else device
+    opts.block_variants = block_variants
+    e = _lib.gnm_error()
+    _lib.check(lib.gnm_score_pgen(C.byref(pv), buf.ctypes.data, buf.nbytes, C.byref(opts),
+                                  sums.ctypes.data, counts.ctypes.data, C.byref(e)), e)
     if prep.complex_rules:
         from .complex import GenotypeSource, resolve_complex_variants
+        m, n = pgen_dims(buf)
+        rows, pitch = decode_to_device(buf, device=device)
         bpv = (n + 3) // 4
         host = rows[:m * pitch].view(m, pitch)[:, :bpv].cpu().numpy().reshape(-1)
         resolve_complex_variants(prep.complex_rules, GenotypeSource.single(host, bpv),
-                                 prep.output_idx_to_fam_idx, prep.num_people_to_score,
-                                 prep.score_names, sums, counts, prep.final_person_iids)
+                                 prep.output_idx_to_fam_idx, P, prep.score_names, sums,
+                                 counts, prep.final_person_iids)
     return sums, counts

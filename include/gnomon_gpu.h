@@ -305,9 +305,29 @@ uint64_t gnm_pgen_device_bytes(const gnm_pgen* pg);
 gnm_status gnm_pgen_decode(gnm_pgen* pg, uint64_t variant_begin, uint64_t variant_count,
                            uint8_t* d_rows, uint64_t pitch, void* stream, gnm_error* err);
 
+/* Decode the listed variants (`count` indices, any order, each below the
+ * variant count) into d_rows[i * pitch ..] = variant variants[i],
+ * asynchronously on `stream`: e.g. the reconciled variants of a preparation
+ * (required_bim_indices), which the reference's virtual .bed serves.  LD
+ * anchors that are not listed are decoded into the handle's scratch rows. */
+gnm_status gnm_pgen_decode_list(gnm_pgen* pg, const uint64_t* variants, uint64_t count,
+                                uint8_t* d_rows, uint64_t pitch, void* stream, gnm_error* err);
+
 /* Wait for `stream`, then GNM_ERR_IO if any record decoded so far was
  * malformed (the message names the first such variant). */
 gnm_status gnm_pgen_check(gnm_pgen* pg, void* stream, gnm_error* err);
+
+/* gnm_score_run_ex with a .pgen (host bytes) as the genotype source: the
+ * reference's virtual-.bed route (shared/adapt_plink2.rs:1093-1158), with the
+ * decode on the device.  The .pgen's variants are the .bim rows
+ * required_bim_indices point at; its sample count must equal
+ * total_people_in_fam.  The reconciled variants are decoded and scored in
+ * blocks of opts->block_variants (0 = as many as 4 GiB of rows hold);
+ * opts->on_block is not called.  Same outputs and statuses as
+ * gnm_score_run. */
+gnm_status gnm_score_pgen(const gnm_prep_view* prep, const uint8_t* pgen, uint64_t pgen_len,
+                          const gnm_run_options* opts, double* sums_out, uint32_t* missing_out,
+                          gnm_error* err);
 
 /* ---- Allocation-free scoring ---------------------------------------------
  * No counterpart in the reference: an extra entry point of this library.

@@ -122,16 +122,22 @@ def _as_pgen(rows, people):
     return synth.BED_TO_PGEN_CAT[codes].astype(np.uint8)
 
 
-@pytest.mark.parametrize("people,variants,scores", [(1001, 300, 1), (2003, 257, 16)])
-def test_score_from_pgen_equals_bed(cuda, people, variants, scores):
+@pytest.mark.parametrize("people,variants,scores,block", [(1001, 300, 1, 0), (2003, 257, 16, 0),
+                                                          (1001, 300, 1, 37)])
+def test_score_from_pgen_equals_bed(cuda, people, variants, scores, block):
     w, prep, rows, _ = synth_case(people, variants, scores)
     data = synth.encode_pgen(_as_pgen(rows, people))
-    s, c = score_pgen(prep, data)
+    s, c = score_pgen(prep, data, block_variants=block)
     bs, bc = run(PipelineContext(prep), rows.reshape(-1))
     np.testing.assert_array_equal(c, bc)
-    np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)
+    if block == 0:   # same blocks as the .bed run: same sums
+        np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)
+    else:            # other FP32 block sums: the reference's 1e-6 metric
+        assert oracle.within_reference_tolerance(s, bs).all()
     es, ec = oracle.score_extended(rows, prep)
     np.testing.assert_array_equal(c, ec)
+    rs, _ = oracle.score_reference(rows, prep, threads=4)
+    assert oracle.within_reference_tolerance(s, rs).all()
 
 
 def test_score_from_pgen_gathers_required_variants(cuda):
@@ -143,10 +149,10 @@ def test_score_from_pgen_gathers_required_variants(cuda):
     cats[0::2] = other
     data = synth.encode_pgen(cats)
     prep2 = dataclasses.replace(prep, required_bim_indices=np.arange(1, 2 * V, 2, dtype=np.uint64))
-    s, c = score_pgen(prep2, data)
+    s, c = score_pgen(prep2, data, block_variants=23)
     bs, bc = run(PipelineContext(prep), rows.reshape(-1))
     np.testing.assert_array_equal(c, bc)
-    np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)
+    assert oracle.within_reference_tolerance(s, bs).all()   # 23-variant FP32 blocks
 
 
 @pytest.mark.parametrize("block", [1, 7, 17, 100, 4096])
@@ -184,3 +190,29 @@ def test_range_errors(cuda):
         assert ei.value.status == _lib.GNM_ERR_INVALID
         pg.decode(buf, 64, 0, 0)                      # empty range: nothing to do
         pg.check()
+
+
+def test_list_decode(cuda):
+    """Any order; LD records whose anchors are not listed read them from
+    scratch rows (decoded once each); listed anchors are read from the output."""
+    from gnomon_b200.pgen import PgenFile
+    cats = synth.pgen_ld_categories(31, 256, 203)
+    data = synth.encode_pgen(cats, repeats=2)
+    want = expected_rows(cats, 2)
+    kinds = pgen_oracle.parse_header(data)["types"] & 7
+    ld = np.nonzero((kinds == 2) | (kinds == 3))[0]
+    rng = np.random.default_rng(0)
+    lists = [rng.permutation(len(want))[:100], ld[::3], np.array([ld[-1]]),
+             np.arange(len(want))[::-1]]
+    pitch = 64
+    with PgenFile(data) as pg:
+        for lst in lists:
+            buf = torch.full((len(lst) * pitch,), SENTINEL, dtype=torch.uint8, device="cuda")
+            pg.decode_list(buf, pitch, lst)
+            pg.check()
+            got = buf.view(len(lst), pitch).cpu().numpy()
+            np.testing.assert_array_equal(got[:, :want.shape[1]], want[lst])
+            assert (got[:, want.shape[1]:] == SENTINEL).all()
+        with pytest.raises(_lib.GnomonGpuError) as ei:
+            pg.decode_list(buf, pitch, [len(want)])          # past the last variant
+        assert ei.value.status == _lib.GNM_ERR_INVALID

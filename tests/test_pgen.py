@@ -174,3 +174,16 @@ def test_non_rising_difflist_ids_are_malformed():
     for bad in (dup, back):
         with pytest.raises(pgen_oracle.PgenError, match="rise"):
             pgen_oracle.decode_to_bed(bad)
+
+
+def test_score_pgen_declines_without_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from helpers import synth_case
+    from gnomon_b200.pgen import score_pgen
+    w, prep, rows, _ = synth_case(101, 20, 1)
+    cats = synth.BED_TO_PGEN_CAT[synth.unpack_codes(rows, 101)].astype(np.uint8)
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        score_pgen(prep, synth.encode_pgen(cats))
+    assert ei.value.status == _lib.GNM_DECLINED
