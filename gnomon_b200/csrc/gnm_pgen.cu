@@ -211,41 +211,16 @@ __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uin
     uint32_t old = 0;             // its value in `base` (loaded when the word starts)
     uint32_t pm = 0, pv = 0;      // its patched bits and their new values
     bool edge = true;             // the group's first word
-    uint32_t vb = 0;
     // category -> .bed code as a packed 2-bit table (no divergent lookups):
     // {11, 10, 00, 01}, or with the REF/ALT swap {00, 10, 11, 01}
     const uint32_t code_of = swap ? 0x78u : 0x4Bu;
-    for (uint32_t e = 0; e < count; ++e) {
-      if (e > 0) {
-        // a read past the record gives 0, which ends the walk as a zero delta
-        uint32_t d = at < rlen ? p[at] : 0u;
-        ++at;
-        if (d & 0x80u) {   // multi-byte delta
-          uint64_t d64 = d & 0x7Fu;
-          uint32_t b, shift = 7;
-          do {
-            if (at >= rlen || shift > 56) {
-              bad = true;
-              break;
-            }
-            b = p[at++];
-            d64 |= uint64_t(b & 0x7Fu) << shift;
-            shift += 7;
-          } while (b & 0x80u);
-          if (bad) break;
-          d = uint32_t(min(d64, uint64_t(0xFFFFFFFFu)));
-        }
-        if (d == 0) {
-          bad = true;
-          break;
-        }
-        id = id > 0xFFFFFFFFu - d ? 0xFFFFFFFFu : id + d;
-      }
-      if ((e & 3u) == 0) vb = vals[e / 4];
-      if (id >= n32) continue;
-      const uint32_t code = (code_of >> (2 * ((vb >> (2 * (e & 3u))) & 3u))) & 3u;
-      const uint32_t w = id >> 4;
-      const uint32_t sh = 2 * (id & 15u);
+    // merge the patch of sample `pid` into the word being patched; flush that
+    // word when the id moves past it
+    auto patch = [&](uint32_t pid, uint32_t val) {
+      if (pid >= n32) return;
+      const uint32_t code = (code_of >> (2 * val)) & 3u;
+      const uint32_t w = pid >> 4;
+      const uint32_t sh = 2 * (pid & 15u);
       if (w != cw) {
         if (cw != 0xFFFFFFFFu) {
           const uint32_t o = swap ? swap_homs(old) : old;
@@ -261,6 +236,59 @@ __device__ __forceinline__ void warp_difflist(const PgArgs& a, const Rec& r, uin
       }
       pm |= 3u << sh;   // ids rise strictly: a field is patched once
       pv |= code << sh;
+    };
+    patch(id, vals[0] & 3u);   // entry 0: the group's first id
+    uint32_t e = 1;
+    while (e < count) {
+      // four one-byte deltas at once: read as one word (funnel-shifted from
+      // aligned words; the record's bytes sit in the file's 16-byte-padded
+      // buffer), taken when no byte carries a continuation bit or is zero
+      if (e + 4 <= count && at + 4 <= rlen && id < 0xFFFFFE00u) {
+        const uintptr_t addr = reinterpret_cast<uintptr_t>(p + at);
+        const uint32_t* al = reinterpret_cast<const uint32_t*>(addr & ~uintptr_t(3));
+        const uint32_t s8 = uint32_t(addr & 3u) * 8u;
+        const uint32_t x = __funnelshift_r(al[0], s8 ? al[1] : 0u, s8);
+        if (((x & 0x80808080u) | ((x - 0x01010101u) & ~x & 0x80808080u)) == 0u) {
+          // the values of entries e .. e + 3 (a second value byte unless e % 4 == 0)
+          const uint32_t lo = vals[e / 4];
+          const uint32_t hi = (e & 3u) ? uint32_t(vals[e / 4 + 1]) : 0u;
+          const uint32_t vw = (lo | (hi << 8)) >> (2 * (e & 3u));
+#pragma unroll
+          for (uint32_t k = 0; k < 4; ++k) {
+            id += (x >> (8 * k)) & 0xFFu;
+            patch(id, (vw >> (2 * k)) & 3u);
+          }
+          at += 4;
+          e += 4;
+          continue;
+        }
+      }
+      // one delta, any length; a read past the record gives 0, which ends
+      // the walk as a zero delta
+      uint32_t d = at < rlen ? p[at] : 0u;
+      ++at;
+      if (d & 0x80u) {   // multi-byte delta
+        uint64_t d64 = d & 0x7Fu;
+        uint32_t b, shift = 7;
+        do {
+          if (at >= rlen || shift > 56) {
+            bad = true;
+            break;
+          }
+          b = p[at++];
+          d64 |= uint64_t(b & 0x7Fu) << shift;
+          shift += 7;
+        } while (b & 0x80u);
+        if (bad) break;
+        d = uint32_t(min(d64, uint64_t(0xFFFFFFFFu)));
+      }
+      if (d == 0) {
+        bad = true;
+        break;
+      }
+      id = id > 0xFFFFFFFFu - d ? 0xFFFFFFFFu : id + d;
+      patch(id, (vals[e / 4] >> (2 * (e & 3u))) & 3u);
+      ++e;
     }
     if (cw != 0xFFFFFFFFu && !bad) {   // the group's last word
       const uint32_t o = swap ? swap_homs(old) : old;
