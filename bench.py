@@ -719,7 +719,9 @@ def main():
         stream_arm(args, rank, world, local_rank)
         return
     if args.pgen:
-        pgen_arm(args, rank, world, local_rank)
+        # a one-GPU measurement of the decoder: under torchrun only rank 0 runs it
+        if rank == 0:
+            pgen_arm(args, rank, 1, local_rank)
         return
     if world > 1:
         import datetime
