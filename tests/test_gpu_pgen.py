@@ -216,3 +216,20 @@ def test_list_decode(cuda):
         with pytest.raises(_lib.GnomonGpuError) as ei:
             pg.decode_list(buf, pitch, [len(want)])          # past the last variant
         assert ei.value.status == _lib.GNM_ERR_INVALID
+
+
+def test_zero_variants_and_missing_anchor(cuda):
+    from gnomon_b200.pgen import PgenFile
+    data = synth._pgen_file(7, [], [])
+    rows, pitch = decode_to_device(data)
+    with PgenFile(data) as pg:
+        assert (pg.variants, pg.samples) == (0, 7)
+        pg.decode(rows, pitch, 0, 0)
+        pg.check()
+    cats = synth.pgen_ld_categories(3, 8, 100)
+    types, recs = synth._pgen_records(cats)
+    first_ld = next(i for i, k in enumerate(types) if k in (2, 3))
+    bad = synth._pgen_file(100, types[first_ld:], recs[first_ld:])
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        PgenFile(bad)
+    assert ei.value.status == _lib.GNM_ERR_IO and "anchor" in str(ei.value)

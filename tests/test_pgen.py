@@ -187,3 +187,19 @@ def test_score_pgen_declines_without_a_device():
     with pytest.raises(_lib.GnomonGpuError) as ei:
         score_pgen(prep, synth.encode_pgen(cats))
     assert ei.value.status == _lib.GNM_DECLINED
+
+
+def test_zero_variant_file():
+    data = synth._pgen_file(7, [], [])
+    assert pgen_dims(data) == (0, 7)
+    assert pgen_oracle.decode_to_bed(data).shape == (0, 2)
+
+
+def test_ld_record_without_anchor_is_rejected_by_the_oracle():
+    cats = synth.pgen_ld_categories(3, 8, 100)
+    types, recs = synth._pgen_records(cats)
+    first_ld = next(i for i, k in enumerate(types) if k in (2, 3))
+    # drop the records before the first LD one: it now opens the block
+    data = synth._pgen_file(100, types[first_ld:], recs[first_ld:])
+    with pytest.raises(pgen_oracle.PgenError, match="anchor"):
+        pgen_oracle.decode_to_bed(data)
