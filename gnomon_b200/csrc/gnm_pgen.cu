@@ -19,17 +19,18 @@
 // coerces them; this decoder does not).
 //
 // Layout of the work: the bijection category -> .bed code lets every step
-// run on .bed codes directly.  One warp decodes one record, so an SM keeps up
-// to 64 records in flight (the work per record is a chain of dependent byte
-// reads, bound by latency rather than bandwidth).  Kernel 1 decodes the
-// non-LD records (a table pass over the 2-bit or 1-bit array, or a fill),
-// kernel 2 the LD-compressed ones from their anchors' rows.  A difflist's
-// groups of 64 entries go one per lane: a shuffle scan over the group byte
-// lengths places each lane at its group's deltas, then the lane walks its
-// base-128 sample-id deltas and patches 2-bit fields with 32-bit atomics
-// (fields of one word may belong to different groups).  Every byte read is
-// bounded by the record's length; a malformed record sets the error word and
-// its row is left incomplete.
+// run on .bed codes directly.  A decode is two launches over the same
+// records.  Kernel 1 decodes the non-LD records, one CTA each: they are few
+// and long (a table pass over a whole 2-bit or 1-bit array, or a fill), so
+// eight warps share one.  Kernel 2 decodes the LD-compressed records from
+// their anchors' rows, one warp each: they are many, and their work is a
+// chain of dependent byte reads, so 64 records per SM stay in flight.  A
+// difflist's groups of 64 entries go one per lane: a shuffle scan over the
+// group byte lengths places each lane at its group's deltas, and the lane
+// walks its base-128 sample-id deltas, four one-byte deltas per step where it
+// can.  A lane merges its patches per 32-bit word and writes each word once.
+// Every byte read is bounded by the record's length; a malformed record sets
+// the error word and its row is left incomplete.
 #include <cuda_runtime.h>
 
 #include <algorithm>
