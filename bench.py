@@ -688,6 +688,73 @@ def pgen_arm(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def project_arm(args, rank, world, local_rank):
+    """HWE-PCA projection blocks (gnm_project_*): 50,000 samples onto 20 axes,
+    ``--project`` variants in blocks of 32,768 (rows, coefficients and
+    loadings staged from host memory per block, as the reference stages
+    them).  ``value`` is genotype x component pairs/s through the host call;
+    the per-block host->device copy of the rows is inside the timed region."""
+    import torch
+    from gnomon_b200 import synth
+    from gnomon_b200.device import row_pitch, synth_fill
+    from gnomon_b200.project import Projector, hwe_coefficients
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = synth.WORKLOADS[args.workload]
+    n, k, B = w.people, 20, 32768
+    nblk = max(1, args.project // B)
+    bpv = (n + 3) // 4
+    pitch = row_pitch(bpv)
+    thr = synth.variant_thresholds(w.seed, 0, B, w.p_lo, w.p_hi, w.missing_rate)
+    d = torch.empty(B * pitch, dtype=torch.uint8, device=dev)
+    synth_fill(d, pitch, 0, B, n, thr, w.seed)
+    rows = np.ascontiguousarray(d.view(B, pitch)[:, :bpv].cpu().numpy())
+    rng = np.random.default_rng(w.seed)
+    freqs = rng.uniform(w.p_lo, w.p_hi, B)
+    coeffs = hwe_coefficients(freqs, np.sqrt(2 * freqs * (1 - freqs)))
+    loadings = (rng.standard_normal((B, k)) / np.sqrt(B * nblk)).astype(np.float32)
+    with Projector(n, k, device=local_rank) as pj:
+        for _ in range(max(1, args.warmup)):
+            pj.block(rows, coeffs, loadings)
+    secs = []
+    with ClockSampler(local_rank) as clocks:
+        for _ in range(args.steps):
+            with Projector(n, k, device=local_rank) as pj:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for _ in range(nblk):
+                    pj.block(rows, coeffs, loadings)
+                out = pj.scores()
+                secs.append(time.perf_counter() - t0)
+    s = statistics.median(secs)
+    pairs = n * B * nblk * k
+    line = {"metric": "projection genotype*component pairs/s", "value": pairs / s,
+            "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 tables, f64 sums",
+            "data": "synthetic HWE genotypes (one 32,768-variant block repeated)",
+            "config": {"workload": f"project_{n}_x_{B * nblk}_k{k}", "samples": n,
+                       "variants": B * nblk, "components": k, "block_variants": B,
+                       "blocks": nblk},
+            "e2e": {"value": pairs / s, "unit": "pairs/s",
+                    "h2d_bytes_per_step": nblk * B * (bpv + 4 * (3 + k)),
+                    "d2h_bytes_per_step": nblk * n * k * 8, "seconds": s},
+            "gpu_launches": nblk * (3 * k + 1),   # per block: repitch; per axis: tables, accumulate, finalize
+            "clocks": clocks.summary()}
+    if rank == 0 and not args.no_cpu:
+        from oracle import project_oracle
+        m = 512
+        t0 = time.perf_counter()
+        project_oracle.project_block(rows[:m], n, coeffs[:m], loadings[:m])
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n * m * k / tc, "unit": "pairs/s",
+                                "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"numpy float64 oracle (unpack + matmul) on the first {m} "
+                                          f"variants x {n} samples x {k} axes, {tc:.2f} s"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -708,6 +775,8 @@ def main():
                     help="override the variant count (small cases for profiler captures)")
     ap.add_argument("--pgen", type=int, default=0,
                     help="time .pgen -> .bed decoding of this many variants instead")
+    ap.add_argument("--project", type=int, default=0,
+                    help="time HWE-PCA projection blocks over this many variants instead")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -722,6 +791,10 @@ def main():
         # a one-GPU measurement of the decoder: under torchrun only rank 0 runs it
         if rank == 0:
             pgen_arm(args, rank, 1, local_rank)
+        return
+    if args.project:
+        if rank == 0:
+            project_arm(args, rank, 1, local_rank)
         return
     if world > 1:
         import datetime

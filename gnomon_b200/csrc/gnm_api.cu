@@ -27,6 +27,13 @@
 #include "gnm_plan.h"
 #include "gnm_tensor.h"
 
+// A projection in progress (gnm_project_*): its scores so far.
+struct gnm_projector {
+  int device = 0;
+  uint64_t n = 0, K = 0;
+  std::vector<double> acc;   // [n][K] row-major, every block so far
+};
+
 namespace gnm {
 
 void fail(gnm_status s, const std::string& msg) { throw Failure{s, msg}; }
@@ -250,6 +257,8 @@ static void plain_geometry(gnm_plan* p) {
   p->splits_alloc = uint32_t(alloc);
 }
 
+static void upload_plain_records(gnm_plan* p, const std::vector<float4>& rec, PhaseTrace& trace);
+
 static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace& trace) {
   p->rec_stride = p->V + kRecordPad;
   std::vector<float4> rec(p->K * p->rec_stride);
@@ -283,6 +292,12 @@ static void build_plain_records(gnm_plan* p, const gnm_prep_view* prep, PhaseTra
     for (auto& th : pool) th.join();
   }
   trace.mark("  plan: records (host)");
+  upload_plain_records(p, rec, trace);
+}
+
+// Upload a plain plan's cell records, allocate its partials and build the
+// stage tables while they fit the cache.
+static void upload_plain_records(gnm_plan* p, const std::vector<float4>& rec, PhaseTrace& trace) {
   p->d_records = dalloc<float4>(p, rec.size(), "cudaMalloc(records)");
   check_cuda(cudaMemcpy(p->d_records, rec.data(), rec.size() * sizeof(float4),
                         cudaMemcpyHostToDevice),
@@ -964,18 +979,99 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   }
 }
 
-}  // namespace gnm
+// ---- HWE-PCA projection blocks (map/project.rs) --------------------------------
+// The reference's GPU projection unpacks each variant block into a dense f32
+// matrix, code 00 -> coeffs[0], 10 -> coeffs[1], 11 -> coeffs[2], missing -> 0
+// (unpack_weighted_plink, map/project.rs:322-370), multiplies it by the
+// block's loadings with an SGEMM accumulating into f32 [P][k]
+// (compute_scores_block, :547-667) and adds that into f64 row-major scores
+// (:669-733).  Here a block is a plain-engine plan whose cell records are the
+// lookup values themselves: per (variant v, component c) baseline c0*L,
+// code 01 -> -c0*L, 10 -> (c1 - c0)*L, 11 -> (c2 - c0)*L (FP64, rounded to
+// FP32 records), so the 3-variant stage tables give exactly
+// sum_v coeff(code) * L for any coefficients, accumulated in FP32 over 120
+// variants and in FP64 beyond.
+static gnm_plan* plan_create_projection(int device, uint64_t n, uint64_t K, uint64_t V,
+                                        const float* coeffs, const float* loadings_cm) {
+  PhaseTrace trace;
+  DeviceGuard g(device);
+  auto* p = new gnm_plan();
+  try {
+    p->device = device;
+    p->P = n;
+    p->fam = n;
+    p->bpv = (n + 3) / 4;
+    p->K = K;
+    p->V = V;
+    p->engine = GNM_ENGINE_PLAIN;
+    p->h_baseline.assign(K, 0.0);
+    for (uint64_t k = 0; k < K; ++k) {
+      double b = 0.0;
+      for (uint64_t v = 0; v < V; ++v) b += double(coeffs[3 * v]) * double(loadings_cm[k * V + v]);
+      p->h_baseline[k] = b;
+    }
+    p->d_baseline = dalloc<double>(p, K, "cudaMalloc(baseline)");
+    check_cuda(cudaMemcpy(p->d_baseline, p->h_baseline.data(), K * sizeof(double),
+                          cudaMemcpyHostToDevice),
+               "upload baseline");
+    p->d_zero_base = dalloc<double>(p, K, "cudaMalloc(zero baseline)");
+    check_cuda(cudaMemset(p->d_zero_base, 0, K * sizeof(double)), "memset");
+    p->d_err = dalloc<uint32_t>(p, 1, "cudaMalloc(error word)");
+    check_cuda(cudaMemset(p->d_err, 0, 4), "memset");
+    plain_geometry(p);
+    p->rec_stride = V + kRecordPad;
+    std::vector<float4> rec(K * p->rec_stride, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (uint64_t k = 0; k < K; ++k)
+      for (uint64_t v = 0; v < V; ++v) {
+        const double l = loadings_cm[k * V + v];
+        const double c0 = coeffs[3 * v], c1 = coeffs[3 * v + 1], c2 = coeffs[3 * v + 2];
+        // member bits 0: the projection keeps no missing counts
+        rec[k * p->rec_stride + v] =
+            make_float4(float(-c0 * l), float((c1 - c0) * l), float((c2 - c0) * l), 0.f);
+      }
+    upload_plain_records(p, rec, trace);
+    check_cuda(cudaStreamSynchronize(0), "plan upload");
+  } catch (...) {
+    gnm_plan_destroy(p);
+    throw;
+  }
+  return p;
+}
 
-using namespace gnm;
-
-extern "C" {
-
-int gnm_abi_version(void) { return GNM_ABI_VERSION; }
-
-gnm_status gnm_score_run(const gnm_prep_view* prep, const gnm_bed_view* bed,
-                         const gnm_resume* resume, double* sums_out, uint32_t* missing_out,
-                         gnm_error* err) {
-  return gnm_score_run_ex(prep, bed, resume, nullptr, sums_out, missing_out, err);
+static void project_block_impl(gnm_projector* pj, const uint8_t* packed, uint64_t filled,
+                               const float* coeffs, const float* loadings_cm) {
+  if (!pj) fail(GNM_ERR_INVALID, "projector is NULL");
+  if (filled == 0) return;
+  if (!packed || !coeffs || !loadings_cm) fail(GNM_ERR_INVALID, "block buffers are NULL");
+  std::unique_ptr<gnm_plan, void (*)(gnm_plan*)> plan(
+      plan_create_projection(pj->device, pj->n, pj->K, filled, coeffs, loadings_cm),
+      gnm_plan_destroy);
+  DeviceGuard g(pj->device);
+  const uint64_t bpv = (pj->n + 3) / 4, pitch = (bpv + 127) / 128 * 128;
+  struct Bufs {
+    std::vector<void*> p;
+    ~Bufs() {
+      for (void* x : p) pool_free(x);
+    }
+  } b;
+  b.p.push_back(pool_alloc(pj->device, filled * pitch, "projection rows"));
+  auto* rows = static_cast<uint8_t*>(b.p.back());
+  b.p.push_back(pool_alloc(pj->device, pj->n * pj->K * 8, "projection sums"));
+  auto* d_sums = static_cast<double*>(b.p.back());
+  b.p.push_back(pool_alloc(pj->device, pj->n * pj->K * 4, "projection counts"));
+  auto* d_counts = static_cast<uint32_t*>(b.p.back());
+  // rows back to back through the pinned ring, then to the kernel pitch on the device
+  b.p.push_back(pool_alloc(pj->device, filled * bpv, "projection staging"));
+  auto* staging = static_cast<uint8_t*>(b.p.back());
+  copy_to_device(staging, packed, filled * bpv, 0);
+  check_cuda(launch_repitch(staging, bpv, filled, rows, pitch, 0), "repitch launch");
+  plan_reset_impl(plan.get(), 0);
+  accumulate_impl(plan.get(), rows, pitch, 0, filled, 0);
+  finalize_impl(plan.get(), d_sums, d_counts, true, 0);
+  std::vector<double> s(pj->n * pj->K);
+  check_cuda(cudaMemcpy(s.data(), d_sums, s.size() * 8, cudaMemcpyDeviceToHost), "sums");
+  sync_impl(plan.get(), 0);
+  for (uint64_t i = 0; i < s.size(); ++i) pj->acc[i] += s[i];
 }
 
 // The .pgen counterpart of the end-to-end run: the file is uploaded once, the
@@ -1048,10 +1144,57 @@ static void score_pgen_impl(const gnm_prep_view* prep, const uint8_t* pgen, uint
   sync_impl(plan.get(), st.s);
 }
 
+}  // namespace gnm
+
+using namespace gnm;
+
+extern "C" {
+
+int gnm_abi_version(void) { return GNM_ABI_VERSION; }
+
+gnm_status gnm_score_run(const gnm_prep_view* prep, const gnm_bed_view* bed,
+                         const gnm_resume* resume, double* sums_out, uint32_t* missing_out,
+                         gnm_error* err) {
+  return gnm_score_run_ex(prep, bed, resume, nullptr, sums_out, missing_out, err);
+}
+
 gnm_status gnm_score_pgen(const gnm_prep_view* prep, const uint8_t* pgen, uint64_t pgen_len,
                           const gnm_run_options* opts, double* sums_out, uint32_t* missing_out,
                           gnm_error* err) {
   return guarded(err, [&] { score_pgen_impl(prep, pgen, pgen_len, opts, sums_out, missing_out); });
+}
+
+gnm_status gnm_project_create(uint64_t n_samples, uint64_t components, int device,
+                              gnm_projector** out, gnm_error* err) {
+  return guarded(err, [&] {
+    if (!out) fail(GNM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (n_samples == 0 || components == 0)
+      fail(GNM_ERR_INVALID, "a projection needs samples and components");
+    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
+    if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    auto* pj = new gnm_projector;
+    pj->device = device;
+    pj->n = n_samples;
+    pj->K = components;
+    pj->acc.assign(n_samples * components, 0.0);
+    *out = pj;
+  });
+}
+
+void gnm_project_destroy(gnm_projector* pj) { delete pj; }
+
+gnm_status gnm_project_block(gnm_projector* pj, const uint8_t* packed, uint64_t filled,
+                             const float* coeffs, const float* loadings_col_major,
+                             gnm_error* err) {
+  return guarded(err, [&] { project_block_impl(pj, packed, filled, coeffs, loadings_col_major); });
+}
+
+gnm_status gnm_project_scores(const gnm_projector* pj, double* scores_row_major, gnm_error* err) {
+  return guarded(err, [&] {
+    if (!pj || !scores_row_major) fail(GNM_ERR_INVALID, "NULL argument");
+    for (uint64_t i = 0; i < pj->acc.size(); ++i) scores_row_major[i] += pj->acc[i];
+  });
 }
 
 gnm_status gnm_score_run_ex(const gnm_prep_view* prep, const gnm_bed_view* bed,

@@ -329,6 +329,37 @@ gnm_status gnm_score_pgen(const gnm_prep_view* prep, const uint8_t* pgen, uint64
                           const gnm_run_options* opts, double* sums_out, uint32_t* missing_out,
                           gnm_error* err);
 
+/* ---- HWE-PCA projection blocks --------------------------------------------
+ * The GPU part of gnomon's projection onto a fitted HWE-PCA model
+ * (map/project.rs): per variant block, every sample's genotype codes are
+ * mapped through the block's per-variant coefficients (code 00 ->
+ * coeffs[3v], 10 -> coeffs[3v+1], 11 -> coeffs[3v+2], missing (01) -> 0;
+ * unpack_weighted_plink, map/project.rs:322-370) and multiplied by the
+ * block's loadings (compute_scores_block, :547-667); the blocks' sums are
+ * added into row-major f64 scores (:669-733).  The missing-data scan and the
+ * per-sample solves that follow stay with the caller, as in the reference.
+ * Sums accumulate in FP32 over 120 variants and in FP64 beyond (the
+ * reference: an FP32 SGEMM over the whole projection). */
+typedef struct gnm_projector gnm_projector;
+
+/* A projection of n_samples samples onto `components` axes; GNM_DECLINED
+ * without a device. */
+gnm_status gnm_project_create(uint64_t n_samples, uint64_t components, int device,
+                              gnm_projector** out, gnm_error* err);
+void gnm_project_destroy(gnm_projector* pj);
+
+/* One block of `filled` variants: packed .bed rows (host, ceil(n_samples/4)
+ * bytes each, back to back), coeffs [filled][3] and column-major loadings
+ * [components][filled] (f32, as the reference stages them).  Synchronous. */
+gnm_status gnm_project_block(gnm_projector* pj, const uint8_t* packed, uint64_t filled,
+                             const float* coeffs, const float* loadings_col_major,
+                             gnm_error* err);
+
+/* Add the projection's sums over every block so far into
+ * scores_row_major[n_samples][components] (+=, like the reference's
+ * copy-back). */
+gnm_status gnm_project_scores(const gnm_projector* pj, double* scores_row_major, gnm_error* err);
+
 /* ---- Allocation-free scoring ---------------------------------------------
  * No counterpart in the reference: an extra entry point of this library.
  *
