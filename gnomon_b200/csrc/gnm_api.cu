@@ -1005,10 +1005,34 @@ static gnm_plan* plan_create_projection(int device, uint64_t n, uint64_t K, uint
     p->V = V;
     p->engine = GNM_ENGINE_PLAIN;
     p->h_baseline.assign(K, 0.0);
-    for (uint64_t k = 0; k < K; ++k) {
-      double b = 0.0;
-      for (uint64_t v = 0; v < V; ++v) b += double(coeffs[3 * v]) * double(loadings_cm[k * V + v]);
-      p->h_baseline[k] = b;
+    p->rec_stride = V + kRecordPad;
+    std::vector<float4> rec(K * p->rec_stride);
+    // one axis per host thread: its records and its FP64 baseline
+    auto fill = [&](uint64_t k0, uint64_t k1) {
+      for (uint64_t k = k0; k < k1; ++k) {
+        float4* r = rec.data() + k * p->rec_stride;
+        const float* lk = loadings_cm + k * V;
+        double b = 0.0;
+        for (uint64_t v = 0; v < V; ++v) {
+          const double l = lk[v];
+          const double c0 = coeffs[3 * v], c1 = coeffs[3 * v + 1], c2 = coeffs[3 * v + 2];
+          b += c0 * l;
+          // member bits 0: the projection keeps no missing counts
+          r[v] = make_float4(float(-c0 * l), float((c1 - c0) * l), float((c2 - c0) * l), 0.f);
+        }
+        std::fill(r + V, r + p->rec_stride, make_float4(0.f, 0.f, 0.f, 0.f));
+        p->h_baseline[k] = b;
+      }
+    };
+    const uint64_t nt = std::min<uint64_t>(K, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    if (nt <= 1 || K * V < (uint64_t(1) << 16)) {
+      fill(0, K);
+    } else {
+      std::vector<std::thread> pool;
+      const uint64_t per = (K + nt - 1) / nt;
+      for (uint64_t i = 0; i < nt; ++i)
+        pool.emplace_back(fill, std::min(K, i * per), std::min(K, (i + 1) * per));
+      for (auto& th : pool) th.join();
     }
     p->d_baseline = dalloc<double>(p, K, "cudaMalloc(baseline)");
     check_cuda(cudaMemcpy(p->d_baseline, p->h_baseline.data(), K * sizeof(double),
@@ -1019,16 +1043,6 @@ static gnm_plan* plan_create_projection(int device, uint64_t n, uint64_t K, uint
     p->d_err = dalloc<uint32_t>(p, 1, "cudaMalloc(error word)");
     check_cuda(cudaMemset(p->d_err, 0, 4), "memset");
     plain_geometry(p);
-    p->rec_stride = V + kRecordPad;
-    std::vector<float4> rec(K * p->rec_stride, make_float4(0.f, 0.f, 0.f, 0.f));
-    for (uint64_t k = 0; k < K; ++k)
-      for (uint64_t v = 0; v < V; ++v) {
-        const double l = loadings_cm[k * V + v];
-        const double c0 = coeffs[3 * v], c1 = coeffs[3 * v + 1], c2 = coeffs[3 * v + 2];
-        // member bits 0: the projection keeps no missing counts
-        rec[k * p->rec_stride + v] =
-            make_float4(float(-c0 * l), float((c1 - c0) * l), float((c2 - c0) * l), 0.f);
-      }
     upload_plain_records(p, rec, trace);
     check_cuda(cudaStreamSynchronize(0), "plan upload");
   } catch (...) {
@@ -1043,35 +1057,62 @@ static void project_block_impl(gnm_projector* pj, const uint8_t* packed, uint64_
   if (!pj) fail(GNM_ERR_INVALID, "projector is NULL");
   if (filled == 0) return;
   if (!packed || !coeffs || !loadings_cm) fail(GNM_ERR_INVALID, "block buffers are NULL");
-  std::unique_ptr<gnm_plan, void (*)(gnm_plan*)> plan(
-      plan_create_projection(pj->device, pj->n, pj->K, filled, coeffs, loadings_cm),
-      gnm_plan_destroy);
+  PhaseTrace trace;
   DeviceGuard g(pj->device);
   const uint64_t bpv = (pj->n + 3) / 4, pitch = (bpv + 127) / 128 * 128;
   struct Bufs {
     std::vector<void*> p;
+    cudaStream_t s = nullptr;
     ~Bufs() {
+      if (s) cudaStreamDestroy(s);
       for (void* x : p) pool_free(x);
     }
   } b;
   b.p.push_back(pool_alloc(pj->device, filled * pitch, "projection rows"));
   auto* rows = static_cast<uint8_t*>(b.p.back());
+  b.p.push_back(pool_alloc(pj->device, filled * bpv, "projection staging"));
+  auto* staging = static_cast<uint8_t*>(b.p.back());
   b.p.push_back(pool_alloc(pj->device, pj->n * pj->K * 8, "projection sums"));
   auto* d_sums = static_cast<double*>(b.p.back());
   b.p.push_back(pool_alloc(pj->device, pj->n * pj->K * 4, "projection counts"));
   auto* d_counts = static_cast<uint32_t*>(b.p.back());
-  // rows back to back through the pinned ring, then to the kernel pitch on the device
-  b.p.push_back(pool_alloc(pj->device, filled * bpv, "projection staging"));
-  auto* staging = static_cast<uint8_t*>(b.p.back());
-  copy_to_device(staging, packed, filled * bpv, 0);
-  check_cuda(launch_repitch(staging, bpv, filled, rows, pitch, 0), "repitch launch");
-  plan_reset_impl(plan.get(), 0);
-  accumulate_impl(plan.get(), rows, pitch, 0, filled, 0);
-  finalize_impl(plan.get(), d_sums, d_counts, true, 0);
+  check_cuda(cudaStreamCreateWithFlags(&b.s, cudaStreamNonBlocking), "cudaStreamCreate");
+  // the plan (records, baseline, stage tables) is built on a helper thread
+  // while the rows go up through the pinned ring on their own stream
+  gnm_plan* built = nullptr;
+  std::exception_ptr plan_error;
+  std::thread planner([&] {
+    try {
+      built = plan_create_projection(pj->device, pj->n, pj->K, filled, coeffs, loadings_cm);
+    } catch (...) {
+      plan_error = std::current_exception();
+    }
+  });
+  struct Join {   // on an early exit: wait for the planner, free what it built
+    std::thread& t;
+    gnm_plan*& built;
+    ~Join() {
+      if (t.joinable()) t.join();
+      if (built) gnm_plan_destroy(built);
+    }
+  } join{planner, built};
+  copy_to_device(staging, packed, filled * bpv, b.s);
+  check_cuda(launch_repitch(staging, bpv, filled, rows, pitch, b.s), "repitch launch");
+  trace.mark("project: rows");
+  planner.join();
+  if (plan_error) std::rethrow_exception(plan_error);
+  std::unique_ptr<gnm_plan, void (*)(gnm_plan*)> plan(built, gnm_plan_destroy);
+  built = nullptr;
+  trace.mark("project: plan");
+  plan_reset_impl(plan.get(), b.s);
+  accumulate_impl(plan.get(), rows, pitch, 0, filled, b.s);
+  finalize_impl(plan.get(), d_sums, d_counts, true, b.s);
   std::vector<double> s(pj->n * pj->K);
-  check_cuda(cudaMemcpy(s.data(), d_sums, s.size() * 8, cudaMemcpyDeviceToHost), "sums");
-  sync_impl(plan.get(), 0);
+  check_cuda(cudaMemcpyAsync(s.data(), d_sums, s.size() * 8, cudaMemcpyDeviceToHost, b.s), "sums");
+  sync_impl(plan.get(), b.s);
+  trace.mark("project: accumulate");
   for (uint64_t i = 0; i < s.size(); ++i) pj->acc[i] += s[i];
+  trace.mark("project: add");
 }
 
 // The .pgen counterpart of the end-to-end run: the file is uploaded once, the
