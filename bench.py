@@ -610,15 +610,14 @@ def pgen_arm(args, rank, world, local_rank):
     distinct = 2048
     reps = max(1, args.pgen // distinct)
     cats = synth.pgen_ld_categories(w.seed, distinct, w.people)
-    data = np.frombuffer(synth.encode_pgen(cats, repeats=reps), np.uint8)
+    types, recs = synth._pgen_records(cats)      # record types and bodies, for the accounting
+    data = np.frombuffer(synth._pgen_file(w.people, types * reps, recs * reps), np.uint8)
     V, n = pgen_dims(data)
     bpv = (n + 3) // 4
     pitch = row_pitch(bpv)
     rows = torch.empty(V * pitch, dtype=torch.uint8, device=dev)
-    from oracle import pgen_oracle   # header counts for the byte accounting only
-    h = pgen_oracle.parse_header(data.tobytes())
-    kinds = np.bincount(h["types"] & 7, minlength=8)
-    record_bytes = int(h["lens"].astype(np.int64).sum())
+    kinds = np.bincount(np.asarray(types * reps) & 7, minlength=8)
+    record_bytes = reps * sum(len(r) for r in recs)
     n_ld = int(kinds[2] + kinds[3])
     algo_bytes = record_bytes + V * bpv                   # records read + rows written
     s = torch.cuda.Stream(dev)
@@ -676,6 +675,7 @@ def pgen_arm(args, rank, world, local_rank):
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary()}
     if rank == 0 and not args.no_cpu:
+        from oracle import pgen_oracle
         k = 64
         sub = synth.encode_pgen(cats[:k])
         t0 = time.perf_counter()
