@@ -18,6 +18,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <cmath>
 #include <exception>
 #include <mutex>
 #include <string>
@@ -991,6 +992,56 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
 // FP32 records), so the 3-variant stage tables give exactly
 // sum_v coeff(code) * L for any coefficients, accumulated in FP32 over 120
 // variants and in FP64 beyond.
+// Whether every variant's coefficients are linear in the dosage up to their
+// own FP32 rounding, |(c2 - c0) - 2 (c1 - c0)| <= 4 ulp of the largest: true
+// of the reference's HWE coefficients (g - 2p) * inv * weight, each rounded
+// to FP32 on its own.
+static bool projection_is_linear(const float* coeffs, uint64_t V) {
+  for (uint64_t v = 0; v < V; ++v) {
+    const double c0 = coeffs[3 * v], c1 = coeffs[3 * v + 1], c2 = coeffs[3 * v + 2];
+    const double m = std::max({std::fabs(c0), std::fabs(c1), std::fabs(c2)});
+    if (std::fabs((c2 - c0) - 2.0 * (c1 - c0)) > 4.0 * std::ldexp(m, -23)) return false;
+  }
+  return true;
+}
+
+// A block on the split-BF16 tensor engine, for 8 or more axes with linear
+// coefficients: one pass over the rows for every axis.  The cells are the
+// scoring engine's own: dosage weight (c1 - c0) * L, missing correction
+// c0 * L and baseline sum c0 * L, so code 11 gets 2 (c1 - c0) * L, within
+// the coefficients' FP32 rounding of (c2 - c0) * L.
+static gnm_plan* plan_create_projection_tensor(int device, uint64_t n, uint64_t K, uint64_t V,
+                                               const float* coeffs, const float* loadings_cm) {
+  std::vector<float> w(V * K), c(V * K);
+  std::vector<uint32_t> cols(V * K);
+  std::vector<uint64_t> offs(V + 1);
+  std::vector<double> base(K, 0.0);
+  for (uint64_t v = 0; v < V; ++v) {
+    offs[v] = v * K;
+    const double c0 = coeffs[3 * v], c1 = coeffs[3 * v + 1];
+    for (uint64_t k = 0; k < K; ++k) {
+      const double l = loadings_cm[k * V + v];
+      w[v * K + k] = float((c1 - c0) * l);
+      c[v * K + k] = float(c0 * l);
+      cols[v * K + k] = uint32_t(k);
+      base[k] += c0 * l;
+    }
+  }
+  offs[V] = V * K;
+  gnm_prep_view view{};
+  view.num_people = n;
+  view.total_people_in_fam = n;
+  view.bytes_per_variant = (n + 3) / 4;
+  view.num_scores = K;
+  view.num_variants = V;
+  view.sparse_weights = w.data();
+  view.sparse_missing_corrections = c.data();
+  view.sparse_score_columns = cols.data();
+  view.sparse_row_offsets = offs.data();
+  view.baseline = base.data();
+  return plan_create_impl(&view, GNM_ENGINE_TENSOR, device, true);
+}
+
 static gnm_plan* plan_create_projection(int device, uint64_t n, uint64_t K, uint64_t V,
                                         const float* coeffs, const float* loadings_cm) {
   PhaseTrace trace;
@@ -1081,9 +1132,13 @@ static void project_block_impl(gnm_projector* pj, const uint8_t* packed, uint64_
   // while the rows go up through the pinned ring on their own stream
   gnm_plan* built = nullptr;
   std::exception_ptr plan_error;
+  const bool tensor = pj->K >= kTensorMinScores && projection_is_linear(coeffs, filled);
   std::thread planner([&] {
     try {
-      built = plan_create_projection(pj->device, pj->n, pj->K, filled, coeffs, loadings_cm);
+      built = tensor ? plan_create_projection_tensor(pj->device, pj->n, pj->K, filled, coeffs,
+                                                     loadings_cm)
+                     : plan_create_projection(pj->device, pj->n, pj->K, filled, coeffs,
+                                              loadings_cm);
     } catch (...) {
       plan_error = std::current_exception();
     }

@@ -9,9 +9,13 @@ block (map/project.rs). Its GPU path does three things per block:
   :547-667);
 * adds the sums into row-major f64 scores (:669-733).
 
-``Projector`` does the same with the plain lookup-table engine: no dense
-matrix, FP32 sums over 120 variants, FP64 beyond. The missing-data scan and
-the per-sample solves that follow stay with the caller, as in the reference.
+``Projector`` does the same without a dense matrix or a GEMM:
+* with 8 or more axes and linear coefficients (the reference's HWE ones), on
+  the split-BF16 tensor engine in one pass;
+* otherwise on exact FP32 lookup tables, one pass per axis.
+
+The missing-data scan and the per-sample solves that follow stay with the
+caller, as in the reference.
 """
 from __future__ import annotations
 

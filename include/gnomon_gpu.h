@@ -338,8 +338,12 @@ gnm_status gnm_score_pgen(const gnm_prep_view* prep, const uint8_t* pgen, uint64
  * block's loadings (compute_scores_block, :547-667); the blocks' sums are
  * added into row-major f64 scores (:669-733).  The missing-data scan and the
  * per-sample solves that follow stay with the caller, as in the reference.
- * Sums accumulate in FP32 over 120 variants and in FP64 beyond (the
- * reference: an FP32 SGEMM over the whole projection). */
+ * Engine per block: with 8 or more axes and coefficients linear in the
+ * dosage up to their FP32 rounding (the reference's HWE coefficients), the
+ * split-BF16 tensor engine, one pass for all axes; otherwise exact 3-variant
+ * FP32 lookup tables, one pass per axis.  Both sum in FP32 within a block of
+ * variants and in FP64 across (the reference: an FP32 SGEMM over the whole
+ * projection). */
 typedef struct gnm_projector gnm_projector;
 
 /* A projection of n_samples samples onto `components` axes; GNM_DECLINED

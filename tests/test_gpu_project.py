@@ -70,3 +70,26 @@ def test_missing_calls_contribute_nothing(cuda):
     check(got, rows, n, coeffs, loadings)
     scale = np.abs(coeffs[:, [0]]).T @ np.abs(loadings)   # per component
     assert (np.abs(got[::2]) <= 1e-6 * scale + 1e-12).all()
+
+
+@pytest.mark.parametrize("k", [3, 10, 70])
+def test_nonlinear_coefficients(cuda, k):
+    """Coefficients that are not linear in the dosage take the exact lookup
+    tables at any axis count; linear ones with 8 or more axes take the
+    tensor engine (the other tests), within the same bar."""
+    n, filled = 1501, 700
+    rows, coeffs, loadings = block_case(5, n, filled, k)
+    coeffs = coeffs.copy()
+    coeffs[::3, 2] += 0.25                              # c2 off the line through c0, c1
+    with Projector(n, k) as pj:
+        pj.block(rows, coeffs, loadings)
+        check(pj.scores(), rows, n, coeffs, loadings)
+
+
+def test_wide_tensor_block(cuda):
+    """More than 64 linear axes: the wide tensor kernel."""
+    n, filled, k = 2049, 900, 72
+    rows, coeffs, loadings = block_case(6, n, filled, k)
+    with Projector(n, k) as pj:
+        pj.block(rows, coeffs, loadings)
+        check(pj.scores(), rows, n, coeffs, loadings)
