@@ -1114,8 +1114,11 @@ static void project_block_impl(gnm_projector* pj, const uint8_t* packed, uint64_
   struct Bufs {
     std::vector<void*> p;
     cudaStream_t s = nullptr;
-    ~Bufs() {
-      if (s) cudaStreamDestroy(s);
+    ~Bufs() {   // on an early exit, work on `s` may still use the buffers
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
       for (void* x : p) pool_free(x);
     }
   } b;
@@ -1200,18 +1203,6 @@ static void score_pgen_impl(const gnm_prep_view* prep, const uint8_t* pgen, uint
   std::unique_ptr<gnm_plan, void (*)(gnm_plan*)> plan(plan_create_impl(prep, engine, device, true),
                                                       gnm_plan_destroy);
   DeviceGuard g(device);
-  struct Stream {
-    cudaStream_t s = nullptr;
-    ~Stream() {
-      if (s) cudaStreamDestroy(s);
-    }
-  } st;
-  check_cuda(cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking), "cudaStreamCreate");
-  const uint64_t pitch = (prep->bytes_per_variant + 127) / 128 * 128;
-  // default block: every reconciled variant if its rows take at most 4 GiB
-  uint64_t B = opts && opts->block_variants ? opts->block_variants
-                                            : std::max<uint64_t>(1, (uint64_t(4) << 30) / pitch);
-  B = std::max<uint64_t>(1, std::min<uint64_t>(B, std::max<uint64_t>(V, 1)));
   struct Pool {
     std::vector<void*> p;
     ~Pool() {
@@ -1222,6 +1213,21 @@ static void score_pgen_impl(const gnm_prep_view* prep, const uint8_t* pgen, uint
       return p.back();
     }
   } pool;
+  struct Stream {   // destroyed before the pool: its work ends before buffers are freed
+    cudaStream_t s = nullptr;
+    ~Stream() {
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+    }
+  } st;
+  check_cuda(cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking), "cudaStreamCreate");
+  const uint64_t pitch = (prep->bytes_per_variant + 127) / 128 * 128;
+  // default block: every reconciled variant if its rows take at most 4 GiB
+  uint64_t B = opts && opts->block_variants ? opts->block_variants
+                                            : std::max<uint64_t>(1, (uint64_t(4) << 30) / pitch);
+  B = std::max<uint64_t>(1, std::min<uint64_t>(B, std::max<uint64_t>(V, 1)));
   auto* rows = static_cast<uint8_t*>(pool.get(device, B * pitch, ".pgen row block"));
   const uint64_t PK = prep->num_people * prep->num_scores;
   auto* d_sums = static_cast<double*>(pool.get(device, std::max<uint64_t>(PK, 1) * 8, "sums"));
