@@ -32,7 +32,11 @@ and ld_p.pgen, which hold the same genotypes.
 """
 from __future__ import annotations
 
+import ctypes as C
+import os
 import struct
+import subprocess
+from pathlib import Path
 
 import numpy as np
 
@@ -202,4 +206,45 @@ def decode_to_bed(data: bytes) -> np.ndarray:
         codes[:n] = CAT_TO_BED[cats]
         q = codes.reshape(bpv, 4)
         out[v] = q[:, 0] | (q[:, 1] << 2) | (q[:, 2] << 4) | (q[:, 3] << 6)
+    return out
+
+
+# ---- the C restatement (pgen_oracle.c), for timing a compiled CPU decoder ----
+
+_HERE = Path(__file__).resolve().parent
+_CLIB = _HERE / "_build" / "libpgen_oracle.so"
+_clib = None
+
+
+def _load_c():
+    global _clib
+    if _clib is None:
+        src = _HERE / "pgen_oracle.c"
+        if not _CLIB.exists() or _CLIB.stat().st_mtime < src.stat().st_mtime:
+            subprocess.run(["make", "-s", "-C", str(_HERE)], check=True)
+        lib = C.CDLL(str(_CLIB))
+        lib.pgen_oracle_dims.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_uint64)]
+        lib.pgen_oracle_dims.restype = C.c_int
+        lib.pgen_oracle_decode.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_int]
+        lib.pgen_oracle_decode.restype = C.c_int
+        _clib = lib
+    return _clib
+
+
+def decode_to_bed_c(data, threads: int = 0) -> np.ndarray:
+    """decode_to_bed through the C restatement on `threads` host threads
+    (0 = all); raises PgenError where decode_to_bed does."""
+    lib = _load_c()
+    buf = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else \
+        np.ascontiguousarray(data, np.uint8)
+    m, n = C.c_uint64(), C.c_uint64()
+    if lib.pgen_oracle_dims(buf.ctypes.data, buf.nbytes, C.byref(m), C.byref(n)):
+        raise PgenError("not a supported .pgen")
+    bpv = (n.value + 3) // 4
+    out = np.zeros((m.value, bpv), np.uint8)
+    rc = lib.pgen_oracle_decode(buf.ctypes.data, buf.nbytes, out.ctypes.data, bpv,
+                                threads or (os.cpu_count() or 1))
+    if rc:
+        raise PgenError("malformed or unsupported .pgen")
     return out

@@ -203,3 +203,30 @@ def test_ld_record_without_anchor_is_rejected_by_the_oracle():
     data = synth._pgen_file(100, types[first_ld:], recs[first_ld:])
     with pytest.raises(pgen_oracle.PgenError, match="anchor"):
         pgen_oracle.decode_to_bed(data)
+
+
+@pytest.mark.parametrize("n", [1, 5, 203, 300, 70001])
+def test_c_restatement_matches(n):
+    """oracle/pgen_oracle.c (the timed CPU decoder) against the Python oracle."""
+    cats = synth.pgen_ld_categories(n, 96 if n < 1000 else 24, n)
+    for j, fill in enumerate((0, 2, 3)):
+        cats[-3 + j] = fill
+        cats[-3 + j, ::37] = (fill + 1) % 4
+    data = synth.encode_pgen(cats)
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed_c(data, threads=3),
+                                  pgen_oracle.decode_to_bed(data))
+
+
+def test_c_restatement_fixture_and_errors():
+    z = np.load(GOLDEN / "ld_fixture.npz")
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed_c(ld_pgen(), threads=4), z["rows"])
+    cats = synth.pgen_ld_categories(7, 256, 9)
+    data = synth.encode_pgen(cats, repeats=300)      # two blocks
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed_c(data), expected_rows(cats, 300))
+    for bad in non_rising_pgens()[1:]:
+        with pytest.raises(pgen_oracle.PgenError):
+            pgen_oracle.decode_to_bed_c(bad)
+    types, recs = synth._pgen_records(synth.pgen_ld_categories(3, 8, 100))
+    first_ld = next(i for i, k in enumerate(types) if k in (2, 3))
+    with pytest.raises(pgen_oracle.PgenError):
+        pgen_oracle.decode_to_bed_c(synth._pgen_file(100, types[first_ld:], recs[first_ld:]))
