@@ -193,12 +193,48 @@ class CpuReferenceSample:
 
     @property
     def pairs(self):
-        return self.w.people * self.nv * self.w.scores
+        """Useful genotype*score pairs of one pass: people x the prefix's cells."""
+        return self.w.people * int(self.prep.sparse_row_offsets[-1])
 
     def describe(self, seconds):
         return (f"{self.w.people} people x {self.nv} variants (prefix of {self.w.variants}), "
                 f"K={self.w.scores}, restated reference CPU engine (decide.rs routing, person-major f32 "
                 f"mini-batches, variant-major f64) on {self.threads} threads, {seconds:.2f} s/pass")
+
+
+def sampled_parity(w, prep, person_begin, sums, counts, people_per_window=8):
+    """Checker for the bench's own output at full length: the extended-precision
+    oracle (oracle/) on four windows of people (first, a third in, two thirds
+    in, last) over every variant and score, against the GPU result rows of
+    those people.  Runs in the CPU-baseline leg only."""
+    from oracle import oracle
+    from gnomon_b200 import synth
+    from gnomon_b200.prepare import PreparationResult
+    P, K, V = prep.num_people_to_score, prep.num_scores, prep.num_reconciled_variants
+    n = min(people_per_window, P)
+    starts = sorted({0, P // 3, 2 * P // 3, P - n})
+    sums = np.asarray(sums).reshape(P, K)
+    counts = np.asarray(counts).reshape(P, K)
+    worst, exact = 0.0, True
+    t0 = time.perf_counter()
+    for a in starts:
+        rows = np.zeros((V, (n + 3) // 4), np.uint8)
+        for v0 in range(0, V, 100_000):
+            v1 = min(V, v0 + 100_000)
+            thr = synth.variant_thresholds(w.seed, v0, v1 - v0, w.p_lo, w.p_hi, w.missing_rate)
+            rows[v0:v1] = synth.synth_rows(w.seed, v0, v1 - v0, n, thr,
+                                           person_begin=person_begin + a)
+        sub = PreparationResult(prep.sparse_weights, prep.sparse_missing_corrections,
+                                prep.sparse_score_columns, prep.sparse_row_offsets,
+                                prep.score_names, n, baseline=prep.baseline)
+        es, ec = oracle.score_extended(rows, sub)
+        got_s, got_c = sums[a:a + n].reshape(-1), counts[a:a + n].reshape(-1)
+        exact &= bool(np.array_equal(got_c.astype(np.uint32), ec))
+        worst = max(worst, float(oracle.rel_err(got_s, es).max()))
+    return {"people": len(starts) * n, "windows": starts, "variants": V, "scores": K,
+            "counts_exact": exact, "max_rel_err_vs_extended_oracle": worst,
+            "seconds": round(time.perf_counter() - t0, 2),
+            "metric": "|a-b| / max(|a|, |b|, 1) (score/tests/gpu_tests.rs:135-147)"}
 
 
 def reference_arm(args, rank, world):
@@ -348,14 +384,18 @@ def gpu_arm(args, rank, world, local_rank):
         ms, kernel_ms = t.tolist()
         dist.barrier()
 
-    pairs = P * V * K
+    # useful genotype*score pairs: people x cells (a score's own variants only;
+    # P * V * K when every score covers every variant)
+    pairs = P * nnz
     value = world * pairs / (ms / 1e3)
     peak_hbm, peak_kind = peaks()
     if tensor and K <= NARROW_MAX_SCORES:
         # narrow engine: M = 128 people, N = 4 limb planes x 16 scores, two MMAs
         # (dosage, missing) per 16-variant slice; one launch per block
         ptiles, k16, vpad = -(-P // 128), -(-K // 16) * 16, -(-V // 64) * 64
-        flops = 2.0 * ptiles * 128 * vpad * (4 * k16) * 2
+        executed = 2.0 * ptiles * 128 * vpad * (4 * k16) * 2
+        # algorithmic: three BF16 weight limbs (hi/mid/lo) x the useful cells
+        flops = 2.0 * P * nnz * 3
         achieved = flops / (kernel_ms / 1e3) / 1e12
         pk = peaks_tc()[0]
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
@@ -363,6 +403,9 @@ def gpu_arm(args, rank, world, local_rank):
                 "peak_kind": peak_kind + " (bf16 sustained)",
                 "kernel": "gnm_tc_narrow (dosage + missing MMAs, one pass)",
                 "kernel_ms": kernel_ms, "algorithmic_flops_per_launch": flops,
+                "algorithmic": "2 x people x cells x 3 weight limbs",
+                "executed_flops_per_launch": executed,
+                "executed_tflops": executed / (kernel_ms / 1e3) / 1e12,
                 "row_bytes_gbs": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9,
                 "row_bytes_frac_of_hbm": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9
                 / peak_hbm}
@@ -370,14 +413,19 @@ def gpu_arm(args, rank, world, local_rank):
         # executed tensor-core work: 8 limb MMAs (4 dosage, 3 correction, 1 count)
         # over 256-person x 128-score tiles and 64-variant stages
         ptiles, kpad, vpad = -(-P // 256), -(-K // 128) * 128, -(-V // 64) * 64
-        flops = 2.0 * ptiles * 256 * vpad * kpad * 8
+        executed = 2.0 * ptiles * 256 * vpad * kpad * 8
+        flops = 2.0 * P * nnz * 3
         achieved = flops / (kernel_ms / 1e3) / 1e12
         pk = peaks_tc()[0]
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                 "frac": achieved / pk, "traffic": None,
                 "peak_kind": peak_kind + " (bf16 sustained)",
                 "kernel": "gnm_tc_accumulate (dosage + missing passes)", "kernel_ms": kernel_ms,
-                "algorithmic_flops_per_launch": flops}
+                "algorithmic_flops_per_launch": flops,
+                "algorithmic": "2 x people x cells x 3 weight limbs",
+                "executed_flops_per_launch": executed,
+                "executed_tflops": executed / (kernel_ms / 1e3) / 1e12,
+                "executed_frac": executed / (kernel_ms / 1e3) / 1e12 / pk}
     else:
         # one launch per score column; algorithmic bytes of a launch = packed rows
         # once + one weight record (4 B + flip bit) per cell of that score
@@ -450,6 +498,11 @@ def gpu_arm(args, rank, world, local_rank):
             t = statistics.median(smp.time_once() for _ in range(3))
             cpu = {"value": smp.pairs / t, "unit": "pairs/s", "cores": threads, "kind": "port",
                    "sample": smp.describe(t) + ", median of 3"}
+            # the oracle as the checker of this run's own output (full length)
+            parity = sampled_parity(w, prep, person_begin, s_host, counts.cpu().numpy())
+            cpu["parity_of_the_timed_output"] = parity
+            assert parity["counts_exact"], parity
+            assert parity["max_rel_err_vs_extended_oracle"] <= 1e-6, parity
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -457,6 +510,7 @@ def gpu_arm(args, rank, world, local_rank):
             "dtype": "f32" if not tensor else "bf16 limbs, f32 accumulate", "data": "synthetic",
             "config": {"workload": w.name, "samples": P, "variants": V, "scores": K,
                        "cells": nnz, "useful_pairs_per_step": P * nnz,
+                       "dense_pairs_per_step": P * V * K,
                        "packed_bytes": V * bpv,
                        "engine": ("split-BF16 tcgen05 (4+3 limbs), FP64 block reduce" if tensor
                                   else "plain (FP32 CUDA-core LUT, FP64 reduce)"),
@@ -564,13 +618,15 @@ def stream_arm(args, rank, world, local_rank):
     plan.sync(comp)
     ms = start.elapsed_time(stop) / args.steps
     h2d_bytes = V * pitch
-    line = {"metric": METRIC, "value": P * V * K / (ms / 1e3), "unit": "pairs/s",
+    cells = int(prep.sparse_row_offsets[-1])
+    line = {"metric": METRIC, "value": P * cells / (ms / 1e3), "unit": "pairs/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if engine == _lib.ENGINE_PLAIN else "bf16 limbs, f32 accumulate",
             "data": "synthetic (two pinned host blocks cycled through all variant blocks)",
             "config": {"workload": w.name, "samples": P, "variants": V, "scores": K,
-                       "cells": int(prep.sparse_row_offsets[-1]), "block_variants": B,
+                       "cells": cells, "useful_pairs_per_step": P * cells,
+                       "dense_pairs_per_step": P * V * K, "block_variants": B,
                        "blocks": nblk, "packed_bytes": V * bpv,
                        "engine": "tensor" if engine == _lib.ENGINE_TENSOR else "plain"},
             "stream": {"h2d_bytes_per_pass": h2d_bytes,

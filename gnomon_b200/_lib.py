@@ -15,6 +15,7 @@ GNM_OK, GNM_DECLINED, GNM_ERR_IO, GNM_ERR_COMPUTE, GNM_ERR_PRODUCER, GNM_ERR_TIM
 STATUS_NAMES = {0: "GNM_OK", 1: "GNM_DECLINED", 2: "GNM_ERR_IO", 3: "GNM_ERR_COMPUTE",
                 4: "GNM_ERR_PRODUCER", 5: "GNM_ERR_TIMEOUT", 6: "GNM_ERR_INVALID"}
 ENGINE_AUTO, ENGINE_PLAIN, ENGINE_TENSOR = 0, 1, 2
+DEVICE_CURRENT, DEVICE_BEST = -1, -2   # device arguments besides an ordinal
 
 u8p = C.POINTER(C.c_uint8)
 

@@ -70,6 +70,71 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+int resolve_device(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    fail(GNM_DECLINED, "no CUDA device available");
+  }
+  if (device >= 0) {
+    if (device >= n) fail(GNM_DECLINED, "no CUDA device with ordinal " + std::to_string(device));
+    return device;
+  }
+  if (device == -1) {
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    return device;
+  }
+  if (device != GNM_DEVICE_BEST) fail(GNM_ERR_INVALID, "device must be >= 0, -1 or GNM_DEVICE_BEST");
+  int prev = -1;
+  check_cuda(cudaGetDevice(&prev), "cudaGetDevice");
+  int best = -1;
+  size_t best_free = 0;
+  int best_sms = 0;
+  std::string rejected;
+  for (int d = 0; d < n; ++d) {
+    cudaDeviceProp pr{};
+    if (cudaGetDeviceProperties(&pr, d) != cudaSuccess) {
+      cudaGetLastError();
+      rejected += " " + std::to_string(d) + ": properties query failed;";
+      continue;
+    }
+    if (pr.major != 10 || pr.minor != 0) {   // the kernels are built for sm_100a only
+      rejected += " " + std::to_string(d) + ": compute capability " + std::to_string(pr.major) +
+                  "." + std::to_string(pr.minor) + ";";
+      continue;
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaSetDevice(d) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      rejected += " " + std::to_string(d) + ": memory query failed;";
+      continue;
+    }
+    if (best < 0 || free_b > best_free ||
+        (free_b == best_free && pr.multiProcessorCount > best_sms)) {
+      best = d;
+      best_free = free_b;
+      best_sms = pr.multiProcessorCount;
+    }
+  }
+  cudaSetDevice(prev);
+  if (best < 0) fail(GNM_DECLINED, "no visible device can run this library:" + rejected);
+  return best;
+}
+
+cudaError_t raise_smem_limit(const void* kernel, int bytes) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, int>> done;   // (kernel, device) pairs set
+  std::lock_guard<std::mutex> lock(mu);
+  for (const auto& d : done)
+    if (d.first == kernel && d.second == dev) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.emplace_back(kernel, dev);
+  return e;
+}
+
 CUtensorMap make_row_map(const uint8_t* d_rows, uint64_t bytes_per_row, uint64_t num_rows,
                          uint64_t pitch, uint32_t box_x, uint32_t box_y) {
   if (reinterpret_cast<uintptr_t>(d_rows) % 16 != 0)
@@ -235,27 +300,60 @@ static void validate_prep(const gnm_prep_view* p) {
 
 
 // ---- plan --------------------------------------------------------------------
+// Launch shape of the plain kernel: people tiles of tile_bytes (the last one
+// often partly populated), and variant-split counts weighted by each tile's
+// populated warps, so that every CTA carries about the same work and the grid
+// fills `mult` x the SMs' CTA slots (2 per SM with 1 KB tiles, 4 with 512 B).
+static void plain_shape(gnm_plan* p, uint32_t tile_bytes, double mult) {
+  const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
+  const uint64_t tiles = std::max<uint64_t>(1, (p->bpv + tile_bytes - 1) / tile_bytes);
+  const uint64_t warps = tile_bytes / 128;
+  const uint64_t last_bytes = p->bpv > (tiles - 1) * tile_bytes ? p->bpv - (tiles - 1) * tile_bytes : 1;
+  const double w_last = double(std::min<uint64_t>(warps, (last_bytes + 127) / 128)) / double(warps);
+  const double ctas = double(2048 / tile_bytes) * double(p->num_sms) * mult;
+  const double per_tile = ctas / (double(tiles - 1) + w_last);
+  uint64_t splits = std::max<uint64_t>(1, uint64_t(per_tile));
+  uint64_t last = tiles > 1 ? uint64_t(std::llround(double(splits) * w_last))
+                            : uint64_t(std::max(1.0, ctas));
+  splits = std::min(splits, stages);
+  last = std::min<uint64_t>(std::max<uint64_t>(1, last), stages);
+  p->tile_bytes = tile_bytes;
+  p->split_mult = mult;
+  p->tiles = uint32_t(tiles);
+  p->splits = uint32_t(splits);
+  p->last_splits = uint32_t(last);
+  p->slots = uint32_t(tiles > 1 ? std::max(splits, last) : last);
+}
+
 static void plain_geometry(gnm_plan* p) {
-  p->tiles = uint32_t(std::max<uint64_t>(1, (p->bpv + kPlainTileBytes - 1) / kPlainTileBytes));
-  p->part_stride = uint64_t(p->tiles) * kPlainTileBytes * 4;
-  int per_sm = 0;
+  // partial slots are padded to whole 1 KB tiles, so either tile width fits
+  p->part_stride = ((p->bpv + kPlainTileBytes - 1) / kPlainTileBytes) * kPlainTileBytes * 4;
+  if (p->part_stride == 0) p->part_stride = kPlainTileBytes * 4;
   check_cuda(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device),
              "cudaDeviceGetAttribute");
-  per_sm = 2;  // __launch_bounds__(256, 2) with ~108 KB of shared memory
-  const uint64_t slots = uint64_t(per_sm) * uint64_t(p->num_sms);
-  const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
-  uint64_t splits = std::max<uint64_t>(1, slots / p->tiles);
-  splits = std::min<uint64_t>(splits, stages);
+  plain_shape(p, kPlainTileBytes, 1.0);
   // keep partials of all scores within 8 GiB (many score columns still get a
-  // full-occupancy grid); allocate up to 4x the default split count so that
-  // gnm_plan_autotune can try finer splits
+  // full-occupancy grid); allocate room for the autotuner's largest candidate
+  // (twice the CTA slots, either tile width)
   const uint64_t per_split_bytes = p->K * p->part_stride * 12;
   const uint64_t cap = uint64_t(8) << 30;
-  while (splits > 1 && splits * per_split_bytes > cap) splits = (splits + 1) / 2;
-  uint64_t alloc = std::min<uint64_t>(4 * splits, stages);
-  while (alloc > splits && alloc * per_split_bytes > cap) --alloc;
-  p->splits = uint32_t(splits);
+  uint64_t alloc = p->slots;
+  for (uint32_t tb : {kPlainTileBytes, kPlainNarrowTileBytes}) {
+    gnm_plan probe = {};
+    probe.V = p->V;
+    probe.bpv = p->bpv;
+    probe.num_sms = p->num_sms;
+    plain_shape(&probe, tb, 2.0);
+    alloc = std::max<uint64_t>(alloc, probe.slots);
+  }
+  while (alloc > 1 && alloc * per_split_bytes > cap) --alloc;
   p->splits_alloc = uint32_t(alloc);
+  // shrink the default grid until its slots fit the allocation
+  double mult = 1.0;
+  while (p->slots > p->splits_alloc && mult > 1e-3) {
+    mult *= 0.5;
+    plain_shape(p, kPlainTileBytes, mult);
+  }
 }
 
 static void upload_plain_records(gnm_plan* p, const std::vector<float4>& rec, PhaseTrace& trace);
@@ -367,8 +465,7 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
   PhaseTrace trace;
   if (!validated) validate_prep(prep);
   trace.mark("  plan: validate");
-  if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  device = resolve_device(device);
   DeviceGuard g(device);
   auto* p = new gnm_plan();
   try {
@@ -427,9 +524,15 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
 static void plan_reset_impl(gnm_plan* p, cudaStream_t s) {
   DeviceGuard g(p->device);
   if (p->engine == GNM_ENGINE_PLAIN) {
-    const uint64_t part = p->K * uint64_t(p->splits_alloc) * p->part_stride;
-    check_cuda(cudaMemsetAsync(p->d_part_sum, 0, part * sizeof(double), s), "reset partials");
-    check_cuda(cudaMemsetAsync(p->d_part_cnt, 0, part * sizeof(uint32_t), s), "reset partials");
+    // the slots in use of every score: K rows of slots x part_stride entries
+    const uint64_t row = uint64_t(p->splits_alloc) * p->part_stride;
+    const uint64_t used = uint64_t(p->slots) * p->part_stride;
+    check_cuda(cudaMemset2DAsync(p->d_part_sum, row * sizeof(double), 0, used * sizeof(double),
+                                 p->K, s),
+               "reset partials");
+    check_cuda(cudaMemset2DAsync(p->d_part_cnt, row * sizeof(uint32_t), 0,
+                                 used * sizeof(uint32_t), p->K, s),
+               "reset partials");
   } else {
     tensor_reset(p, s);
   }
@@ -449,18 +552,21 @@ static void accumulate_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, 
   const CUtensorMap map = make_row_map(d_rows, p->bpv, nv, pitch, kPlainBoxBytes, kPlainRows);
   const uint64_t stages = (nv + kPlainRows - 1) / kPlainRows;
   const uint32_t sps = uint32_t((stages + p->splits - 1) / p->splits);
-  const uint32_t splits = uint32_t((stages + sps - 1) / sps);
+  const uint32_t lsps = uint32_t((stages + p->last_splits - 1) / p->last_splits);
   for (uint64_t k = 0; k < p->K; ++k) {
     PlainArgs a;
     a.tables = plain_tables_for(p, k, v0, nv, s);
     a.num_rows = nv;
     a.bytes_per_row = p->bpv;
+    a.tiles = p->tiles;
+    a.splits = uint32_t((stages + sps - 1) / sps);   // non-empty splits of a full tile
     a.stages_per_split = sps;
+    a.last_stages_per_split = lsps;
     a.part_sum = p->d_part_sum + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_stride = p->part_stride;
     a.err = p->d_err;
-    check_cuda(launch_plain_accumulate(map, a, p->tiles, splits, s), "plain accumulate launch");
+    check_cuda(launch_plain_accumulate(map, a, p->tile_bytes, s), "plain accumulate launch");
     ++p->launches;
   }
 }
@@ -477,7 +583,7 @@ static void finalize_impl(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool 
     a.part_sum = p->d_part_sum + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_stride = p->part_stride;
-    a.num_splits = p->splits;
+    a.num_splits = p->slots;
     a.baseline = add_baseline ? p->d_baseline : p->d_zero_base;
     a.out_to_fam = p->d_out_to_fam;
     a.num_people = p->P;
@@ -502,11 +608,14 @@ static void sync_impl(gnm_plan* p, cudaStream_t s) {
 
 // ---- autotuner -----------------------------------------------------------------
 // Times candidate launch shapes of the plan's accumulate on the caller's
-// resident rows and keeps the fastest: the plain engine's variant-split count
-// (1x, 2x, 4x the occupancy-derived default: more, shorter splits balance the
-// last wave at the cost of more FP64 partials), or the tensor engine's CTA
-// order (people tiles fastest: CTAs in flight share weight-limb tiles in L2;
-// score tiles fastest: they share genotype tiles).
+// resident rows and keeps the fastest.  Plain engine: the people-tile width
+// (1 KB tiles, 8 warps and 2 CTAs per SM; or 512-byte tiles, 4 warps and 4
+// CTAs per SM: a narrow cohort fills every warp of its one tile) times the
+// split count (half, one or two times the SMs' CTA slots: fewer splits write
+// fewer FP64 partials, more splits even out the last wave).  Tensor engine
+// with more than 64 scores: the CTA raster order (people tiles fastest: CTAs
+// in flight share weight-limb tiles in L2; score tiles fastest: they share
+// genotype tiles).
 static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t nv,
                           cudaStream_t s) {
   DeviceGuard g(p->device);
@@ -531,28 +640,42 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
     check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event time");
     return ms;
   };
-  const bool plain = p->engine == GNM_ENGINE_PLAIN;
-  std::vector<uint32_t> cand;
-  if (plain) {
-    for (uint32_t m : {1u, 2u, 4u})
-      if (p->splits * m <= p->splits_alloc && (cand.empty() || p->splits * m != cand.back()))
-        cand.push_back(p->splits * m);
-  } else {
-    cand = {0u, 1u};
-  }
-  const uint32_t base = plain ? p->splits : p->raster;
-  uint32_t best = base;
-  float best_ms = 1e30f;
-  for (uint32_t c : cand) {
-    (plain ? p->splits : p->raster) = c;
+  auto time_best = [&]() {
     time_once();  // warm-up
-    const float ms = std::min(time_once(), time_once());
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = c;
+    return std::min(time_once(), time_once());
+  };
+  float best_ms = 1e30f;
+  if (p->engine == GNM_ENGINE_PLAIN) {
+    uint32_t best_tile = p->tile_bytes;
+    double best_mult = p->split_mult;
+    p->tuning_log.clear();
+    for (uint32_t tb : {kPlainTileBytes, kPlainNarrowTileBytes}) {
+      for (double m : {0.5, 1.0, 2.0}) {
+        plain_shape(p, tb, m);
+        if (p->slots > p->splits_alloc) continue;
+        const float ms = time_best();
+        p->tuning_log.push_back({tb, m, p->splits, p->last_splits, ms});
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_tile = tb;
+          best_mult = m;
+        }
+      }
     }
+    plain_shape(p, best_tile, best_mult);
+  } else {
+    const uint32_t base = p->raster;
+    uint32_t best = base;
+    for (uint32_t c : {0u, 1u}) {
+      p->raster = c;
+      const float ms = time_best();
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+    p->raster = best;
   }
-  (plain ? p->splits : p->raster) = best;
   plan_reset_impl(p, s);
   sync_impl(p, s);
 }
@@ -758,8 +881,7 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   PhaseTrace trace;
   validate_prep(prep);
   int device = o.device;
-  if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  device = resolve_device(device);
   DeviceGuard g(device);
   const gnm_engine engine =
       o.engine == GNM_ENGINE_AUTO
@@ -1183,8 +1305,7 @@ static void score_pgen_impl(const gnm_prep_view* prep, const uint8_t* pgen, uint
   if (!sums_out || !missing_out) fail(GNM_ERR_INVALID, "output buffers are NULL");
   const gnm_engine engine = opts ? opts->engine : GNM_ENGINE_AUTO;
   int device = opts ? opts->device : -1;
-  if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  device = resolve_device(device);
   validate_prep(prep);
   std::unique_ptr<gnm_pgen, void (*)(gnm_pgen*)> pg(pgen_open_impl(pgen, pgen_len, device),
                                                      gnm_pgen_close);
@@ -1273,8 +1394,7 @@ gnm_status gnm_project_create(uint64_t n_samples, uint64_t components, int devic
     *out = nullptr;
     if (n_samples == 0 || components == 0)
       fail(GNM_ERR_INVALID, "a projection needs samples and components");
-    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-    if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    device = resolve_device(device);
     auto* pj = new gnm_projector;
     pj->device = device;
     pj->n = n_samples;
@@ -1384,7 +1504,8 @@ gnm_status gnm_plan_autotune(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch,
 
 uint32_t gnm_plan_tuned_shape(const gnm_plan* p) {
   if (!p) return 0;
-  return p->engine == GNM_ENGINE_PLAIN ? p->splits : p->raster;
+  return p->engine == GNM_ENGINE_PLAIN ? (p->tile_bytes << 16) | std::min<uint32_t>(p->splits, 0xFFFFu)
+                                       : p->raster;
 }
 
 gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv, uint64_t np,
@@ -1400,8 +1521,7 @@ gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv,
 
 gnm_status gnm_release_cached_memory(int device, gnm_error* err) {
   return guarded(err, [&] {
-    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-    if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    device = resolve_device(device);
     DeviceGuard g(device);
     check_cuda(cudaMemPoolTrimTo(run_pool(device), 0), "cudaMemPoolTrimTo");
     release_result_ring();
@@ -1411,8 +1531,7 @@ gnm_status gnm_release_cached_memory(int device, gnm_error* err) {
 gnm_status gnm_watchdog_selftest(int device, uint64_t wait_ns, uint64_t* waited_ns_out,
                                  gnm_error* err) {
   return guarded(err, [&] {
-    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-    if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    device = resolve_device(device);
     DeviceGuard g(device);
     void* d = nullptr;
     check_cuda(cudaMalloc(&d, 16), "cudaMalloc(watchdog words)");

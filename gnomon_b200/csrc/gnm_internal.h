@@ -16,8 +16,11 @@ enum : uint32_t {
 };
 
 // ---- plain engine shape ----------------------------------------------------
-constexpr uint32_t kPlainThreads = 256;      // one 32-bit word column (16 people) each
-constexpr uint32_t kPlainTileBytes = 1024;   // bytes of a row per CTA (4096 people)
+// A plain CTA scores a tile of 512 or 1024 bytes of every row (2048 or 4096
+// people) with one thread per 32-bit word column (16 people): 128 or 256
+// threads, 4 or 2 CTAs per SM.
+constexpr uint32_t kPlainTileBytes = 1024;   // the wide tile; also the partial-slot padding
+constexpr uint32_t kPlainNarrowTileBytes = 512;
 constexpr uint32_t kPlainBoxBytes = 256;     // TMA box inner extent (max 256 elements)
 constexpr uint32_t kPlainRows = 30;          // variant rows per pipeline stage (10 groups of 3)
 constexpr uint32_t kPlainGroups = kPlainRows / 3;
@@ -35,7 +38,7 @@ struct TableArgs {
   const float* corr;
   const uint8_t* member;   // null = every row is a member
   uint64_t row0;           // index of table row 0 in the source arrays
-  uint64_t num_rows;       // rows covered; tables for ceil(num_rows / 24) stages
+  uint64_t num_rows;       // rows covered; tables for ceil(num_rows / kPlainRows) stages
   uint8_t* tables;         // out: [stages][kPlainTableBytes]
 };
 
@@ -43,7 +46,10 @@ struct PlainArgs {
   const uint8_t* tables;   // [stages of this block][kPlainTableBytes], stage 0 = block row 0
   uint64_t num_rows;       // rows in this block
   uint64_t bytes_per_row;  // meaningful bytes of a row (ceil(people / 4))
-  uint32_t stages_per_split;
+  uint32_t tiles;          // people tiles (the last may be partly populated)
+  uint32_t splits;         // variant splits of each full tile (CTAs per full tile)
+  uint32_t stages_per_split;        // stages per split of a full tile
+  uint32_t last_stages_per_split;   // stages per split of the last tile
   double* part_sum;        // [splits][part_stride] partials of this score
   uint32_t* part_cnt;
   uint64_t part_stride;
@@ -63,10 +69,18 @@ struct FinalizeArgs {
   uint32_t* counts;
 };
 
+// Raises `kernel`'s dynamic shared-memory limit to `bytes` on the current
+// device, once per (kernel, device): the attribute belongs to one device's
+// context, so every GPU a process uses needs its own call (thread-safe).
+cudaError_t raise_smem_limit(const void* kernel, int bytes);
+
 cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s);
-cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tiles,
-                                    uint32_t splits, cudaStream_t s);
-uint32_t plain_smem_bytes();
+// Launches (tiles - 1) * splits + ceil(stages / last_stages_per_split) CTAs of
+// the tile_bytes-wide kernel (512 or 1024).
+cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tile_bytes,
+                                    cudaStream_t s);
+uint32_t plain_grid(const PlainArgs& a);
+uint32_t plain_smem_bytes(uint32_t tile_bytes);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
 cudaError_t launch_repitch(const uint8_t* src, uint64_t bpv, uint64_t nrows, uint8_t* dst,
                            uint64_t pitch, cudaStream_t s);

@@ -58,8 +58,7 @@ static unsigned char* scratch_on_current_device() {
   return static_cast<unsigned char*>(addr[dev]);
 }
 
-// Records {-corr, w', 2w', member mask} for rows [0, V + pad), baseline, and a
-// cleared watchdog word.
+// Writes the score's baseline into the scratch and clears the watchdog word.
 __global__ void gnm_noalloc_init(double baseline, double* base_out, uint32_t* err) {
   *base_out = baseline;
   *err = 0u;
@@ -78,6 +77,12 @@ static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uin
   if (!d_rows || !d_w || !d_corr || !d_sums || !d_counts)
     fail(GNM_ERR_INVALID, "gnm_score_noalloc: NULL buffer");
   const uint64_t bpv = (P + 3) / 4;
+  // the row-map rules, checked before anything is queued on the stream
+  if (reinterpret_cast<uintptr_t>(d_rows) % 16 != 0)
+    fail(GNM_ERR_INVALID, "gnm_score_noalloc: packed rows must start on a 16-byte boundary");
+  if (pitch % 16 != 0)
+    fail(GNM_ERR_INVALID, "gnm_score_noalloc: row pitch must be a multiple of 16 bytes");
+  if (pitch < bpv) fail(GNM_ERR_INVALID, "gnm_score_noalloc: row pitch is smaller than ceil(people / 4)");
   unsigned char* sc = scratch_on_current_device();
   uint8_t* tables = reinterpret_cast<uint8_t*>(sc + kNaTabOff);
   double* part_sum = reinterpret_cast<double*>(sc + kNaSumOff);
@@ -124,13 +129,15 @@ static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uin
     a.tables = tables;
     a.num_rows = nv;
     a.bytes_per_row = bpv;
+    a.tiles = tiles;
+    a.splits = uint32_t((cst + sps - 1) / sps);   // the same split count for every tile
     a.stages_per_split = sps;
+    a.last_stages_per_split = sps;
     a.part_sum = part_sum;
     a.part_cnt = part_cnt;
     a.part_stride = stride;
     a.err = err;
-    check_cuda(launch_plain_accumulate(map, a, tiles, uint32_t((cst + sps - 1) / sps), s),
-               "plain accumulate launch");
+    check_cuda(launch_plain_accumulate(map, a, kPlainTileBytes, s), "plain accumulate launch");
   }
   FinalizeArgs f;
   f.part_sum = part_sum;

@@ -806,9 +806,7 @@ gnm_status gnm_pgen_open(const uint8_t* pgen, uint64_t pgen_len, int device, gnm
   return guarded(err, [&] {
     if (!out) fail(GNM_ERR_INVALID, "out is NULL");
     *out = nullptr;
-    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-    int dev = device;
-    if (dev < 0) check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    const int dev = resolve_device(device);
     *out = pgen_open_impl(pgen, pgen_len, dev);
   });
 }
@@ -840,9 +838,7 @@ gnm_status gnm_pgen_decode_device(const uint8_t* pgen, uint64_t pgen_len, int de
                                   uint8_t* d_rows, uint64_t pitch, void* stream,
                                   gnm_error* err) {
   return guarded(err, [&] {
-    if (!device_available(device < 0 ? 0 : device)) fail(GNM_DECLINED, "no CUDA device available");
-    int dev = device;
-    if (dev < 0) check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    const int dev = resolve_device(device);
     std::unique_ptr<gnm_pgen> pg(pgen_open_impl(pgen, pgen_len, dev));
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     pgen_decode_impl(pg.get(), 0, pg->variants, d_rows, pitch, s);

@@ -9,8 +9,8 @@
 //     exactly rounded T_a[ca] + T_b[cb] + T_c[cc] with T = {0, -missing
 //     correction, dosage_weight, 2*dosage_weight} (prepare.rs:197-208 folding;
 //     code 00 contributes 0), so decode, effect-allele flip and the
-//     missing-call rule become ONE lookup per person per 3 variants; eight
-//     group tables and a membership word make one 2064-byte stage table;
+//     missing-call rule become ONE lookup per person per 3 variants; ten
+//     group tables and a membership word make one 2576-byte stage table;
 //   * packed .bed rows are TMA-staged (cp.async.bulk.tensor into this CTA only) in
 //     [30 rows x 1024 bytes] stages together with their stage table (a 1D bulk
 //     copy on the same mbarrier), three buffers deep (30 x 3 ran 4% faster
@@ -39,11 +39,15 @@
 
 namespace gnm {
 
-// Shared-memory layout of one plain CTA (dynamic smem, offsets in bytes).
+// Shared-memory layout of one plain CTA (dynamic smem, offsets in bytes) for
+// a people tile of TILE bytes of every row (TILE / 4 threads, 4 * TILE people).
+template <uint32_t TILE>
 struct PlainSmem {
   static constexpr uint32_t kStages = 3;
-  static constexpr uint32_t kWarps = kPlainThreads / 32;
-  static constexpr uint32_t kStageBytes = kPlainRows * kPlainTileBytes;      // 30720
+  static constexpr uint32_t kThreads = TILE / 4;
+  static constexpr uint32_t kWarps = kThreads / 32;
+  static constexpr uint32_t kBoxes = TILE / kPlainBoxBytes;                  // TMA boxes per stage
+  static constexpr uint32_t kStageBytes = kPlainRows * TILE;                 // 30720 at 1 KB
   static constexpr uint32_t kBoxBytes = kPlainRows * kPlainBoxBytes;         // 7680
   static constexpr uint32_t kTabStride = 3072;   // one stage table, padded to 1 KB in total
   static constexpr uint32_t kTabOff = 0;
@@ -52,6 +56,7 @@ struct PlainSmem {
   static constexpr uint32_t kRelOff = kBarOff + 8 * kStages;                // 3 release counters
   static constexpr uint32_t kLastOff = kRelOff + 4 * kStages;               // 3 last-issued stages
   static constexpr uint32_t kTotal = kLastOff + 4 * kStages;
+  static_assert(TILE % kPlainBoxBytes == 0 && TILE % 128 == 0, "whole boxes and warps");
   static_assert(kPlainRows % 3 == 0 && kPlainRows <= 32, "groups of 3 rows, one ballot");
   static_assert(kTabStride >= kPlainTableBytes && kTabStride % 256 == 0, "table stride");
   static_assert(kTileOff % 1024 == 0, "tile alignment");
@@ -130,30 +135,46 @@ __global__ void __launch_bounds__(kPlainGroups * 64) gnm_plain_tables(TableArgs 
 
 // ---- accumulate --------------------------------------------------------------
 
+template <uint32_t TILE>
 __device__ __forceinline__ void plain_issue_stage(const CUtensorMap* map, const uint8_t* tables,
                                                   uint32_t smem_base, uint32_t buf,
                                                   int32_t tile_x, int32_t row0, uint64_t stage) {
-  const uint32_t bar = smem_base + PlainSmem::kBarOff + 8 * buf;
-  mbar_arrive_expect_tx(bar, PlainSmem::kStageBytes + kPlainTableBytes);
-  const uint32_t tile = smem_base + PlainSmem::kTileOff + buf * PlainSmem::kStageBytes;
+  using L = PlainSmem<TILE>;
+  const uint32_t bar = smem_base + L::kBarOff + 8 * buf;
+  mbar_arrive_expect_tx(bar, L::kStageBytes + kPlainTableBytes);
+  const uint32_t tile = smem_base + L::kTileOff + buf * L::kStageBytes;
 #pragma unroll
-  for (uint32_t b = 0; b < kPlainTileBytes / kPlainBoxBytes; ++b)
-    tma_load_2d(tile + b * PlainSmem::kBoxBytes, map, tile_x + int32_t(b * kPlainBoxBytes), row0,
-                bar);
-  bulk_load(smem_base + PlainSmem::kTabOff + buf * PlainSmem::kTabStride,
-            tables + stage * kPlainTableBytes, kPlainTableBytes, bar);
+  for (uint32_t b = 0; b < L::kBoxes; ++b)
+    tma_load_2d(tile + b * L::kBoxBytes, map, tile_x + int32_t(b * kPlainBoxBytes), row0, bar);
+  bulk_load(smem_base + L::kTabOff + buf * L::kTabStride, tables + stage * kPlainTableBytes,
+            kPlainTableBytes, bar);
 }
 
-// grid = (people tiles, variant splits); block = kPlainThreads.
-__global__ void __launch_bounds__(kPlainThreads, 2)
+// One CTA per (people tile, variant split).  The grid is 1D: the first
+// (tiles - 1) * splits CTAs cover the full tiles, `splits` each, and the last
+// tile (often only partly populated by people) gets its own, smaller split
+// count, so every CTA carries about the same work and the grid fills the
+// SMs' CTA slots evenly.  block = TILE / 4 threads.
+template <uint32_t TILE>
+__global__ void __launch_bounds__(TILE / 4, 2048 / TILE)
     gnm_plain_accumulate(const __grid_constant__ CUtensorMap map, PlainArgs a) {
+  using L = PlainSmem<TILE>;
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t sbase = smem_u32(smem);
   const uint32_t tid = threadIdx.x, lane = tid & 31u;
-  const uint32_t tile = blockIdx.x;
-  const uint32_t split = blockIdx.y;
+  const uint32_t full_ctas = (a.tiles - 1) * a.splits;
+  uint32_t tile, split, sps;
+  if (blockIdx.x < full_ctas) {
+    tile = blockIdx.x / a.splits;
+    split = blockIdx.x % a.splits;
+    sps = a.stages_per_split;
+  } else {
+    tile = a.tiles - 1;
+    split = blockIdx.x - full_ctas;
+    sps = a.last_stages_per_split;
+  }
 
-  const uint64_t rows_per_split = uint64_t(a.stages_per_split) * kPlainRows;
+  const uint64_t rows_per_split = uint64_t(sps) * kPlainRows;
   const uint64_t r_begin = uint64_t(split) * rows_per_split;
   if (r_begin >= a.num_rows) return;
   // table addresses are formed by byte replacement: the window must be aligned
@@ -164,14 +185,14 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
   const uint64_t r_end = min(a.num_rows, r_begin + rows_per_split);
   const uint32_t nstages = uint32_t((r_end - r_begin + kPlainRows - 1) / kPlainRows);
   const uint64_t stage0 = r_begin / kPlainRows;   // block stage of this split's stage 0
-  const int32_t tile_x = int32_t(tile * kPlainTileBytes);
-  const uint32_t bar0 = sbase + PlainSmem::kBarOff;
-  const uint32_t rel0 = sbase + PlainSmem::kRelOff;
-  uint32_t* last_issued = reinterpret_cast<uint32_t*>(smem + PlainSmem::kLastOff);
+  const int32_t tile_x = int32_t(tile * TILE);
+  const uint32_t bar0 = sbase + L::kBarOff;
+  const uint32_t rel0 = sbase + L::kRelOff;
+  uint32_t* last_issued = reinterpret_cast<uint32_t*>(smem + L::kLastOff);
 
   if (tid == 0) {
     prefetch_tmap(&map);
-    for (uint32_t b = 0; b < PlainSmem::kStages; ++b) {
+    for (uint32_t b = 0; b < L::kStages; ++b) {
       mbar_init(bar0 + 8 * b, 1);
       sts_u32(rel0 + 4 * b, 0u);
       last_issued[b] = 0xFFFFFFFFu;
@@ -180,10 +201,10 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
   }
   __syncthreads();
   if (tid == 0) {
-    for (uint32_t s = 0; s < PlainSmem::kStages && s < nstages; ++s) {
+    for (uint32_t s = 0; s < L::kStages && s < nstages; ++s) {
       last_issued[s] = s;
-      plain_issue_stage(&map, a.tables, sbase, s, tile_x, int32_t(r_begin + s * kPlainRows),
-                        stage0 + s);
+      plain_issue_stage<TILE>(&map, a.tables, sbase, s, tile_x,
+                              int32_t(r_begin + s * kPlainRows), stage0 + s);
     }
   }
 
@@ -201,34 +222,34 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
 #pragma unroll
   for (int i = 0; i < 8; ++i) accp[i] = 0ull;
 
-  // Each thread reads word column `tid` of the 1024-byte stage row; the stage
-  // is stored as 4 TMA boxes of [kPlainRows rows][256 bytes].
-  const uint32_t word_off = (tid / (kPlainBoxBytes / 4)) * PlainSmem::kBoxBytes +
+  // Each thread reads word column `tid` of the TILE-byte stage row; the stage
+  // is stored as TILE / 256 TMA boxes of [kPlainRows rows][256 bytes].
+  const uint32_t word_off = (tid / (kPlainBoxBytes / 4)) * L::kBoxBytes +
                             (tid % (kPlainBoxBytes / 4)) * 4;
   // warps whose 128 bytes all lie past the row's last byte only hold padding
   const bool warp_active =
-      uint64_t(tile) * kPlainTileBytes + uint64_t(tid & ~31u) * 4 < a.bytes_per_row;
+      uint64_t(tile) * TILE + uint64_t(tid & ~31u) * 4 < a.bytes_per_row;
 
   bool failed = false;
   for (uint32_t st = 0; st < nstages; ++st) {
-    const uint32_t buf = st % PlainSmem::kStages;
-    const uint32_t parity = (st / PlainSmem::kStages) & 1u;
+    const uint32_t buf = st % L::kStages;
+    const uint32_t parity = (st / L::kStages) & 1u;
     if (!mbar_wait_bounded(bar0 + 8 * buf, parity)) {
       if (lane == 0) atomicOr(a.err, kErrTmaTimeout);
       failed = true;
       break;
     }
 
-    const uint8_t* tbase = smem + PlainSmem::kTileOff + buf * PlainSmem::kStageBytes + word_off;
-    const uint32_t lbase = sbase + PlainSmem::kTabOff + buf * PlainSmem::kTabStride;
-    const uint64_t members = *reinterpret_cast<const uint32_t*>(
-        smem + PlainSmem::kTabOff + buf * PlainSmem::kTabStride + kPlainGroups * 256);
+    // explicit shared-space loads (32-bit shared addresses) for rows and tables
+    const uint32_t tbase = sbase + L::kTileOff + buf * L::kStageBytes + word_off;
+    const uint32_t lbase = sbase + L::kTabOff + buf * L::kTabStride;
+    const uint64_t members = lds_u32(lbase + kPlainGroups * 256);
 
     uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
     auto group = [&](uint32_t g, uint32_t ma, uint32_t mb, uint32_t mc) {
-      const uint32_t xa = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 0) * kPlainBoxBytes);
-      const uint32_t xb = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 1) * kPlainBoxBytes);
-      const uint32_t xc = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 2) * kPlainBoxBytes);
+      const uint32_t xa = lds_u32(tbase + (3 * g + 0) * kPlainBoxBytes);
+      const uint32_t xb = lds_u32(tbase + (3 * g + 1) * kPlainBoxBytes);
+      const uint32_t xc = lds_u32(tbase + (3 * g + 2) * kPlainBoxBytes);
       // ---- per-person 6-bit indices (x4) ------------------------------
       // rows a and b get row c's lo bits XORed into their lo bits; row c
       // enters with its code bits swapped (see the table layout above)
@@ -288,26 +309,30 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
     __syncwarp();
     if (lane == 0) {
       const uint32_t old = atom_add_acq_rel(rel0 + 4 * buf, 1u);
-      if (old == PlainSmem::kWarps - 1) {
+      if (old == L::kWarps - 1) {
         sts_u32(rel0 + 4 * buf, 0u);
-        const uint32_t nxt = st + PlainSmem::kStages;
+        const uint32_t nxt = st + L::kStages;
         if (nxt < nstages) {
           last_issued[buf] = nxt;
           fence_proxy_async_smem();
-          plain_issue_stage(&map, a.tables, sbase, buf, tile_x,
-                            int32_t(r_begin + uint64_t(nxt) * kPlainRows), stage0 + nxt);
+          plain_issue_stage<TILE>(&map, a.tables, sbase, buf, tile_x,
+                                  int32_t(r_begin + uint64_t(nxt) * kPlainRows), stage0 + nxt);
         }
       }
     }
 
-    // FP32 sums and byte counters span four stages (120 variants, <= 120 calls
-    // per byte counter) before they are flushed to FP64 / 32-bit counts.
+    // FP32 sums span four stages (120 variants) before they are flushed to
+    // FP64; byte counters span eight (<= 240 calls per byte) before they are
+    // flushed to 32-bit counts.
     if ((st & 3u) == 3u || st + 1 == nstages) {
+      const bool counts_too = (st & 7u) == 7u || st + 1 == nstages;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (counts_too) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) cnt[4 * j + q] += (by[q] >> (8 * j)) & 0xFFu;
-        by[q] = 0u;
+          for (int j = 0; j < 4; ++j) cnt[4 * j + q] += (by[q] >> (8 * j)) & 0xFFu;
+          by[q] = 0u;
+        }
         float lo, hi;
         unpack_f32x2(accp[2 * q], lo, hi);
         acc64[q] += double(lo);
@@ -326,15 +351,17 @@ __global__ void __launch_bounds__(kPlainThreads, 2)
   // issued copy (bounded) so no TMA is in flight when the CTA exits.
   if (__syncthreads_or(failed)) {
     if (tid == 0) {
-      for (uint32_t b = 0; b < PlainSmem::kStages; ++b)
+      for (uint32_t b = 0; b < L::kStages; ++b)
         if (last_issued[b] != 0xFFFFFFFFu)
-          mbar_wait_bounded(bar0 + 8 * b, (last_issued[b] / PlainSmem::kStages) & 1u);
+          mbar_wait_bounded(bar0 + 8 * b, (last_issued[b] / L::kStages) & 1u);
     }
     return;
   }
 
-  // FP64 partials for this (split, person) accumulate across calls.
-  const uint64_t person0 = uint64_t(tile) * (kPlainTileBytes * 4) + uint64_t(tid) * 16;
+  // FP64 partials for this (split, person) accumulate across calls.  Warps
+  // that only held padding added nothing: their slots stay as they are.
+  if (!warp_active) return;
+  const uint64_t person0 = uint64_t(tile) * (TILE * 4) + uint64_t(tid) * 16;
   double* ps = a.part_sum + uint64_t(split) * a.part_stride + person0;
   uint32_t* pc = a.part_cnt + uint64_t(split) * a.part_stride + person0;
 #pragma unroll
@@ -460,21 +487,36 @@ cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tiles,
-                                    uint32_t splits, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(gnm_plain_accumulate,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(PlainSmem::kTotal));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  gnm_plain_accumulate<<<dim3(tiles, splits), kPlainThreads, PlainSmem::kTotal, s>>>(map, a);
+template <uint32_t TILE>
+static cudaError_t launch_plain_tile(const CUtensorMap& map, const PlainArgs& a, uint32_t grid,
+                                     cudaStream_t s) {
+  using L = PlainSmem<TILE>;
+  const cudaError_t e =
+      raise_smem_limit(reinterpret_cast<const void*>(gnm_plain_accumulate<TILE>), int(L::kTotal));
+  if (e != cudaSuccess) return e;
+  gnm_plain_accumulate<TILE><<<grid, L::kThreads, L::kTotal, s>>>(map, a);
   return cudaGetLastError();
 }
 
-uint32_t plain_smem_bytes() { return PlainSmem::kTotal; }
+uint32_t plain_grid(const PlainArgs& a) {
+  const uint64_t stages = (a.num_rows + kPlainRows - 1) / kPlainRows;
+  const uint64_t last = (stages + a.last_stages_per_split - 1) / a.last_stages_per_split;
+  return uint32_t(uint64_t(a.tiles - 1) * a.splits + last);
+}
+
+cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tile_bytes,
+                                    cudaStream_t s) {
+  if (a.tiles == 0 || a.splits == 0 || a.stages_per_split == 0 || a.last_stages_per_split == 0)
+    return cudaErrorInvalidValue;
+  const uint32_t grid = plain_grid(a);
+  if (tile_bytes == 1024) return launch_plain_tile<1024>(map, a, grid, s);
+  if (tile_bytes == 512) return launch_plain_tile<512>(map, a, grid, s);
+  return cudaErrorInvalidValue;
+}
+
+uint32_t plain_smem_bytes(uint32_t tile_bytes) {
+  return tile_bytes == 512 ? PlainSmem<512>::kTotal : PlainSmem<1024>::kTotal;
+}
 
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s) {
   const uint32_t blocks = uint32_t((a.num_people + 255) / 256);

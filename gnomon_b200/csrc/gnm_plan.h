@@ -67,6 +67,13 @@ inline bool device_available(int device) {
   return device < n;
 }
 
+// The device a call runs on: an ordinal (>= 0, must exist), -1 = the current
+// device, GNM_DEVICE_BEST = the visible sm_100 device with the most free
+// memory, ties broken by SM count (the reference's ranking of candidate
+// devices, score/cuda_backend.rs:894-991, whose tile sizes grow with free
+// memory).  Raises GNM_DECLINED when no such device exists.
+int resolve_device(int device);
+
 // Device buffers of plans come from the library's per-device memory pool.
 void* pool_alloc(int device, uint64_t bytes, const char* what);
 void pool_free(void* ptr);
@@ -116,11 +123,22 @@ struct gnm_plan {
   int num_sms = 0;
 
   // plain engine
-  uint32_t tiles = 0;          // people tiles of kPlainTileBytes
-  uint32_t splits = 0;         // variant splits in use (partial slots)
+  uint32_t tile_bytes = 1024;  // people tile width of the accumulate kernel (512 or 1024)
+  double split_mult = 1.0;     // CTA slots per SM multiplier the split counts are sized for
+  uint32_t tiles = 0;          // people tiles of tile_bytes
+  uint32_t splits = 0;         // variant splits of each full tile
+  uint32_t last_splits = 0;    // variant splits of the last (partly populated) tile
+  uint32_t slots = 0;          // partial slots in use: max(splits, last_splits)
   uint32_t splits_alloc = 0;   // partial slots allocated per score (autotune range)
   uint32_t raster = 0;         // tensor engine CTA order: 0 people-tile fastest, 1 score-tile
-  uint64_t part_stride = 0;    // people per partial slot (tiles * 4096)
+  uint64_t part_stride = 0;    // people per partial slot (bpv rounded up to 1024 bytes, x4)
+  struct Tuning {              // one autotuner candidate and its best accumulate time
+    uint32_t tile_bytes;
+    double mult;
+    uint32_t splits, last_splits;
+    float ms;
+  };
+  std::vector<Tuning> tuning_log;
   uint64_t rec_stride = 0;     // records per score (V + pad)
   float4* d_records = nullptr; // [K][rec_stride]
   uint8_t* d_tables = nullptr;  // stage tables of every score, [K][tab_stages][kPlainTableBytes]

@@ -1034,14 +1034,10 @@ template <int NP, int ST, bool MISSING, bool COUNT_LAST>
 static cudaError_t launch_tc(const CUtensorMap& amap, const CUtensorMap& pmap, const TcArgs& a,
                              uint32_t ptiles, uint32_t stiles, cudaStream_t s) {
   using L = TcSmem<NP, ST>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(gnm_tc_accumulate<NP, ST, MISSING, COUNT_LAST>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(L::kTotal));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  const cudaError_t e = raise_smem_limit(
+      reinterpret_cast<const void*>(gnm_tc_accumulate<NP, ST, MISSING, COUNT_LAST>),
+      int(L::kTotal));
+  if (e != cudaSuccess) return e;
   const dim3 grid = a.raster ? dim3(stiles, ptiles) : dim3(ptiles, stiles);
   gnm_tc_accumulate<NP, ST, MISSING, COUNT_LAST><<<grid, kTcThreads, L::kTotal, s>>>(amap, pmap,
                                                                                      a);
@@ -1229,13 +1225,8 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
     fail(GNM_ERR_INVALID, "tensor engine blocks must start at a multiple of 64 variants");
   if (t->narrow) {
     const CUtensorMap pmap = make_row_map(d_rows, p->bpv, nv, pitch, kNrM / 4, kTcK);
-    static bool attr = false;
-    if (!attr) {
-      check_cuda(cudaFuncSetAttribute(gnm_tc_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(NrSmem::kTotal)),
-                 "narrow shared memory");
-      attr = true;
-    }
+    check_cuda(raise_smem_limit(reinterpret_cast<const void*>(gnm_tc_narrow), int(NrSmem::kTotal)),
+               "narrow shared memory");
     NrArgs a;
     a.num_rows = nv;
     a.a_x0 = int32_t(v0);
@@ -1359,13 +1350,8 @@ void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float
                   CU_TENSOR_MAP_SWIZZLE_128B, "gradient limbs");
   const CUtensorMap dmap = make_2d_map(CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ds, K16, P_pad,
                                        kBwScores, kBwK, CU_TENSOR_MAP_SWIZZLE_NONE, "gradient");
-  static bool attr = false;
-  if (!attr) {
-    check_cuda(cudaFuncSetAttribute(gnm_tc_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(BwSmem::kTotal)),
-               "backward shared memory");
-    attr = true;
-  }
+  check_cuda(raise_smem_limit(reinterpret_cast<const void*>(gnm_tc_backward), int(BwSmem::kTotal)),
+             "backward shared memory");
   BwArgs a;
   a.V = p->V;
   a.K = p->K;

@@ -111,6 +111,65 @@ class BedSource:
         v.data_len = self.rows.size
         return v
 
+    def genotype_source(self, bytes_per_variant: int):
+        from .complex import GenotypeSource
+        return GenotypeSource.single(self.rows, bytes_per_variant)
+
+
+class ByteRangeSource:
+    """Row bytes behind a read callback, for sources that are not a local
+    file: ``ByteRangeSource::read_at`` (shared/files.rs:187-245) reads
+    ``length`` bytes at an offset of the row data (the bytes after the 3-byte
+    magic).
+
+    ``read_at(offset, length)`` returns exactly ``length`` bytes; a shorter
+    result or an exception makes the engine stop with
+    ``PipelineError("Producer")`` (GNM_ERR_PRODUCER), as a failing reader does
+    in the reference's producer thread.  The engine may call it from several
+    host threads at once."""
+
+    def __init__(self, read_at: Callable[[int, int], bytes]):
+        self._read_at = read_at
+        self.errors: list = []
+
+        def _cb(_ctx, offset, dst, length):
+            try:
+                b = read_at(int(offset), int(length))
+                if b is None or len(b) != length:
+                    return 1
+                C.memmove(dst, bytes(b), int(length))
+                return 0
+            except Exception as e:  # noqa: BLE001 - reported as a producer failure
+                self.errors.append(e)
+                return 1
+        self._cfn = _lib.READ_AT(_cb)   # kept alive as long as the source
+
+    def view(self) -> _lib.gnm_bed_view:
+        v = _lib.gnm_bed_view()
+        v.data = None
+        v.data_len = 0
+        v.read_at = self._cfn
+        v.user_ctx = None
+        return v
+
+    def genotype_source(self, bytes_per_variant: int):
+        from .complex import GenotypeSource
+
+        src = self
+
+        class _Rows(GenotypeSource):
+            def __init__(self):
+                super().__init__([np.zeros(0, np.uint8)], [0], bytes_per_variant)
+
+            def codes(self, bim_row, fam):
+                row = np.frombuffer(src._read_at(int(bim_row) * self.bpv, self.bpv), np.uint8)
+                if row.size != self.bpv:
+                    raise IOError(f"Genotype bytes of .bim row {bim_row} could not be read")
+                fam = np.asarray(fam)
+                return ((row[(fam // 4).astype(np.int64)] >> (2 * (fam % 4)).astype(np.uint8))
+                        & 3).astype(np.uint8)
+        return _Rows()
+
 
 def validate_plink_bed_header(head: bytes) -> None:
     if len(head) < 3 or head[:3] != PLINK_MAGIC:
@@ -124,7 +183,7 @@ def try_run_cuda(context: PipelineContext, bed, engine: int = _lib.ENGINE_AUTO,
     """``Some((sums, counts))`` -> tuple; ``Ok(None)`` (declined) -> ``None``; errors raise."""
     lib = _lib.load()
     prep = context.prep_result
-    src = bed if isinstance(bed, BedSource) else BedSource(bed)
+    src = bed if isinstance(bed, (BedSource, ByteRangeSource)) else BedSource(bed)
     P, K = prep.num_people_to_score, prep.num_scores
     sums = np.empty(P * K, dtype=np.float64)
     counts = np.empty(P * K, dtype=np.uint32)
@@ -175,13 +234,16 @@ def try_run_cuda(context: PipelineContext, bed, engine: int = _lib.ENGINE_AUTO,
         raise PipelineError("Io", f"Failed to write score checkpoint: {cb_errors[0]}",
                             _lib.GNM_ERR_IO) from cb_errors[0]
     if st != _lib.GNM_OK:
-        raise PipelineError(_KIND.get(st, "Compute"), err.message.decode(errors="replace"), st)
+        msg = err.message.decode(errors="replace")
+        if isinstance(src, ByteRangeSource) and src.errors:
+            msg += f" ({src.errors[0]!r})"
+        raise PipelineError(_KIND.get(st, "Compute"), msg, st)
     if prep.complex_rules:
         # multi-row loci, on the CPU after the engine (cuda_backend.rs:1465-1535)
-        from .complex import ComplexResolutionError, GenotypeSource, resolve_complex_variants
+        from .complex import ComplexResolutionError, resolve_complex_variants
         try:
             resolve_complex_variants(prep.complex_rules,
-                                     GenotypeSource.single(src.rows, prep.bytes_per_variant),
+                                     src.genotype_source(prep.bytes_per_variant),
                                      prep.output_idx_to_fam_idx, P, prep.score_names, sums,
                                      counts, prep.final_person_iids)
         except ComplexResolutionError as e:

@@ -59,6 +59,11 @@ typedef struct gnm_error {
 } gnm_error;
 
 /* Engine selection for gnm_score_run_ex. */
+/* Device argument: pick the visible sm_100 device with the most free memory,
+ * ties broken by SM count (the reference probes every visible device and
+ * ranks them the same way, score/cuda_backend.rs:894-991). */
+#define GNM_DEVICE_BEST (-2)
+
 typedef enum gnm_engine {
   GNM_ENGINE_AUTO = 0,     /* plain below 8 score columns, split-BF16 tensor cores from 8 */
   GNM_ENGINE_PLAIN = 1,    /* FP32 CUDA-core LUT kernel, FP64 cross-block reduce */
@@ -113,7 +118,9 @@ typedef int (*gnm_block_callback)(void* user_ctx, uint64_t completed_variants,
 
 typedef struct gnm_run_options {
   gnm_engine engine;
-  int device;                     /* CUDA ordinal; -1 = current device            */
+  int device;                     /* CUDA ordinal; -1 = current device;
+                                     GNM_DEVICE_BEST = the visible sm_100 device
+                                     with the most free memory (then SMs)        */
   uint64_t block_variants;        /* streaming block; 0 = default: the whole matrix
                                      if it fits (tensor engine: four blocks of at
                                      least 16,384 variants, each block's compute
@@ -373,8 +380,9 @@ gnm_status gnm_project_scores(const gnm_projector* pj, double* scores_row_major,
  * or a host that calls the scorer from a callback in which a device
  * allocation would implicitly synchronise the device and stall its other
  * streams.  gnm_score_noalloc scores one score column with the plain kernel
- * and allocates nothing: its scratch (per-variant weight records, FP64
- * partial sums and counts, the watchdog word) lives in one statically sized
+ * and allocates nothing: its scratch (the 3-variant stage tables of one chunk
+ * of up to 48,840 variants at a time, FP64 partial sums and counts, the
+ * baseline and the watchdog word) lives in one statically sized
  * device array of GNM_NOALLOC_SCRATCH_BYTES that every GPU loading this
  * library holds until process exit.  The caller passes inputs and outputs:
  *   d_rows                 packed rows (row v at d_rows + v*pitch, pitch a
@@ -393,7 +401,8 @@ gnm_status gnm_project_scores(const gnm_projector* pj, double* scores_row_major,
  * array's device address (once per device, that device current), so make
  * that first call before any stream capture.  Every call reuses the same
  * array and clears what must start at zero; calls that overlap on the GPU
- * (other streams, other host threads) race on it.  The call returns after
+ * (other streams, other host threads) race on it and corrupt each other's
+ * partial sums, so serialise the calls per device.  The call returns after
  * the work on `stream` has finished. */
 #define GNM_NOALLOC_MAX_VARIANTS 262144u
 #define GNM_NOALLOC_MAX_PEOPLE 65536u

@@ -403,29 +403,75 @@ int oracle_score_reference(const uint8_t* rows, uint64_t pitch, uint64_t bpv,
 /* Independent extended-precision scorer: per genotype, x87 long double
  * (64-bit significand), variant order.  sum = baseline + sum_v f(code),
  * f = {00: 0, 01: -corr, 10: w, 11: 2w}; counts = # of 01 over member cells. */
-int oracle_score_extended(const uint8_t* rows, uint64_t pitch, uint64_t num_people,
-                          const uint32_t* out_to_fam, uint64_t K, uint64_t V,
-                          const float* w, const float* corr, const uint32_t* cols,
-                          const uint64_t* offs, const double* baseline,
-                          double* sums, uint32_t* counts) {
+/* Extended-precision scorer: one thread per contiguous range of output
+ * people.  Every (person, score) cell is summed over the variants in row
+ * order whatever the thread count, so the result does not depend on it. */
+typedef struct {
+  const uint8_t* rows;
+  uint64_t pitch, o0, o1, K, V;
+  const uint32_t* out_to_fam;
+  const float *w, *corr;
+  const uint32_t* cols;
+  const uint64_t* offs;
+  long double* acc;     /* [o1 - o0][K] */
+  uint32_t* counts;     /* caller's [P][K] */
+} ExtArgs;
+
+static void* extended_worker(void* p) {
+  ExtArgs* a = (ExtArgs*)p;
+  const uint64_t K = a->K;
+  for (uint64_t v = 0; v < a->V; ++v) {
+    const uint8_t* row = a->rows + v * a->pitch;
+    const uint64_t e0 = a->offs[v], e1 = a->offs[v + 1];
+    if (e0 == e1) continue;
+    for (uint64_t o = a->o0; o < a->o1; ++o) {
+      uint32_t f = a->out_to_fam ? a->out_to_fam[o] : (uint32_t)o;
+      uint32_t g = (row[f >> 2] >> (2 * (f & 3))) & 3u;
+      if (g == 0) continue;
+      long double* acc = a->acc + (o - a->o0) * K;
+      uint32_t* cnt = a->counts + o * K;
+      for (uint64_t e = e0; e < e1; ++e) {
+        uint32_t k = a->cols[e];
+        if (g == 1) { acc[k] -= (long double)a->corr[e]; cnt[k] += 1; }
+        else if (g == 2) acc[k] += (long double)a->w[e];
+        else acc[k] += 2.0L * (long double)a->w[e];
+      }
+    }
+  }
+  return NULL;
+}
+
+int oracle_score_extended_mt(const uint8_t* rows, uint64_t pitch, uint64_t num_people,
+                             const uint32_t* out_to_fam, uint64_t K, uint64_t V,
+                             const float* w, const float* corr, const uint32_t* cols,
+                             const uint64_t* offs, const double* baseline,
+                             double* sums, uint32_t* counts, int n_threads) {
   uint64_t cells = num_people * K;
   long double* acc = (long double*)calloc(cells ? cells : 1, sizeof(long double));
   if (!acc) return -1;
   for (uint64_t x = 0; x < cells; ++x) counts[x] = 0;
-  for (uint64_t v = 0; v < V; ++v) {
-    const uint8_t* row = rows + v * pitch;
-    for (uint64_t o = 0; o < num_people; ++o) {
-      uint32_t f = out_to_fam ? out_to_fam[o] : (uint32_t)o;
-      uint32_t g = (row[f >> 2] >> (2 * (f & 3))) & 3u;
-      if (g == 0) continue;
-      for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
-        uint64_t x = o * K + cols[e];
-        if (g == 1) { acc[x] -= (long double)corr[e]; counts[x] += 1; }
-        else if (g == 2) acc[x] += (long double)w[e];
-        else acc[x] += 2.0L * (long double)w[e];
-      }
-    }
+  if (n_threads < 1) n_threads = 1;
+  if ((uint64_t)n_threads > num_people) n_threads = num_people ? (int)num_people : 1;
+  ExtArgs* args = (ExtArgs*)calloc((size_t)n_threads, sizeof(ExtArgs));
+  pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)n_threads);
+  if (!args || !th) { free(acc); free(args); free(th); return -1; }
+  const uint64_t per = (num_people + (uint64_t)n_threads - 1) / (uint64_t)n_threads;
+  for (int t = 0; t < n_threads; ++t) {
+    ExtArgs* a = &args[t];
+    a->rows = rows; a->pitch = pitch; a->K = K; a->V = V; a->out_to_fam = out_to_fam;
+    a->w = w; a->corr = corr; a->cols = cols; a->offs = offs; a->counts = counts;
+    a->o0 = (uint64_t)t * per < num_people ? (uint64_t)t * per : num_people;
+    a->o1 = a->o0 + per < num_people ? a->o0 + per : num_people;
+    a->acc = acc + a->o0 * K;
   }
+  int spawned = 0;
+  for (int t = 1; t < n_threads; ++t) {
+    if (pthread_create(&th[t], NULL, extended_worker, &args[t]) != 0) break;
+    spawned = t;
+  }
+  extended_worker(&args[0]);
+  for (int t = 1; t <= spawned; ++t) pthread_join(th[t], NULL);
+  for (int t = spawned + 1; t < n_threads; ++t) extended_worker(&args[t]);
   for (uint64_t x = 0; x < cells; ++x) {
     long double b = 0.0L;
     if (baseline) b = (long double)baseline[x % K];
@@ -437,8 +483,19 @@ int oracle_score_extended(const uint8_t* rows, uint64_t pitch, uint64_t num_peop
     for (uint64_t x = 0; x < cells; ++x) sums[x] = (double)(base[x % K] + acc[x]);
     free(base);
   }
+  free(args);
+  free(th);
   free(acc);
   return 0;
+}
+
+int oracle_score_extended(const uint8_t* rows, uint64_t pitch, uint64_t num_people,
+                          const uint32_t* out_to_fam, uint64_t K, uint64_t V,
+                          const float* w, const float* corr, const uint32_t* cols,
+                          const uint64_t* offs, const double* baseline,
+                          double* sums, uint32_t* counts) {
+  return oracle_score_extended_mt(rows, pitch, num_people, out_to_fam, K, V, w, corr, cols, offs,
+                                  baseline, sums, counts, 1);
 }
 
 /* Extended-precision gradient for the backward check (dense over all cells):

@@ -58,6 +58,9 @@ def load():
     lib.oracle_score_reference.restype = i32
     lib.oracle_score_extended.argtypes = [vp, u64, u64, vp, u64, u64, vp, vp, vp, vp, vp, vp, vp]
     lib.oracle_score_extended.restype = i32
+    lib.oracle_score_extended_mt.argtypes = [vp, u64, u64, vp, u64, u64, vp, vp, vp, vp, vp, vp,
+                                             vp, i32]
+    lib.oracle_score_extended_mt.restype = i32
     lib.oracle_backward_extended.argtypes = [vp, u64, u64, vp, u64, u64, vp, vp, vp, vp, vp]
     lib.oracle_backward_extended.restype = i32
     _lib = lib
@@ -79,10 +82,28 @@ def _prep_arrays(prep):
     return w, c, cols, offs, o2f, base
 
 
-def synth_rows(seed: int, v0: int, n: int, num_people: int, thr: np.ndarray, pitch: int):
+def synth_rows(seed: int, v0: int, n: int, num_people: int, thr: np.ndarray, pitch: int,
+               threads: int = 1):
+    """Synthetic rows [n, pitch] of variants v0..v0+n-1, people 0..num_people-1.
+
+    ``threads`` > 1 fills disjoint variant ranges from that many host threads
+    (ctypes releases the GIL during each call); the bytes do not depend on it."""
     rows = np.zeros((n, pitch), dtype=np.uint8)
     t = np.ascontiguousarray(thr, dtype=np.uint32)
-    load().oracle_synth_rows(rows.ctypes.data, pitch, v0, n, num_people, t.ctypes.data, seed)
+    lib = load()
+    if threads <= 1 or n < 2 * threads:
+        lib.oracle_synth_rows(rows.ctypes.data, pitch, v0, n, num_people, t.ctypes.data, seed)
+        return rows
+    from concurrent.futures import ThreadPoolExecutor
+    per = -(-n // threads)
+
+    def fill(j0):
+        j1 = min(n, j0 + per)
+        lib.oracle_synth_rows(rows.ctypes.data + j0 * pitch, pitch, v0 + j0, j1 - j0, num_people,
+                              t.ctypes.data + j0 * 12, seed)
+
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(fill, range(0, n, per)))
     return rows
 
 
@@ -116,16 +137,24 @@ def score_reference(rows: np.ndarray, prep, threads: int = 1, force_path: int = 
     return sums, counts
 
 
-def score_extended(rows: np.ndarray, prep):
+def score_extended(rows: np.ndarray, prep, threads: Optional[int] = None):
+    """Extended-precision (x87 long double) scorer: (sums f64 [P*K], counts u32 [P*K]).
+
+    People are split over ``threads`` host threads (default: all cores); each
+    cell is still summed in variant order, so the result is thread-count
+    independent."""
+    import os
+    threads = threads or os.cpu_count() or 1
     rows = np.ascontiguousarray(rows, dtype=np.uint8)
     V, pitch = rows.shape
     w, c, cols, offs, o2f, base = _prep_arrays(prep)
     P, K = prep.num_people_to_score, prep.num_scores
     sums = np.zeros(P * K, dtype=np.float64)
     counts = np.zeros(P * K, dtype=np.uint32)
-    r = load().oracle_score_extended(rows.ctypes.data, pitch, P, _p(o2f), K, V, w.ctypes.data,
-                                     c.ctypes.data, cols.ctypes.data, offs.ctypes.data,
-                                     base.ctypes.data, sums.ctypes.data, counts.ctypes.data)
+    r = load().oracle_score_extended_mt(rows.ctypes.data, pitch, P, _p(o2f), K, V, w.ctypes.data,
+                                        c.ctypes.data, cols.ctypes.data, offs.ctypes.data,
+                                        base.ctypes.data, sums.ctypes.data, counts.ctypes.data,
+                                        int(threads))
     if r != 0:
         raise MemoryError("oracle_score_extended failed")
     return sums, counts

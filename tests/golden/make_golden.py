@@ -25,7 +25,7 @@ Sources (SauersML/gnomon, read as text; the Rust code cannot run here):
   genotypes as a PLINK 2 variable-width .pgen (LD-compressed and 1-bit
   records), for PGEN decode parity against ld_fixture.npz.
 
-Run: python tests/golden/make_golden.py [--reference /root/reference]
+Run: python tests/golden/make_golden.py --reference <path of the reference checkout>
 """
 from __future__ import annotations
 
@@ -130,7 +130,8 @@ def gpu_tests_cohort(n_people=512, n_variants=256, n_scores=16):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="root of the reference source tree (read-only)")
     a = ap.parse_args()
     (HERE / "known_answers.json").write_text(json.dumps(
         {"engine_cases": known_answers(), "flip_cases": flip_cases()}, indent=1))

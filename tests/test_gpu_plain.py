@@ -350,3 +350,20 @@ def test_pinned_rows_staged_copy_and_repitch(cuda, engine):
     assert oracle.within_reference_tolerance(got[0], ref[0]).all()
     e = _lib.gnm_error()
     assert _lib.load().gnm_release_cached_memory(0, C.byref(e)) == _lib.GNM_OK, e.message
+
+
+def test_best_device_choice(cuda):
+    """device = GNM_DEVICE_BEST probes every visible device and runs on the
+    sm_100 device with the most free memory (score/cuda_backend.rs:894-991);
+    the result equals the run on an explicit ordinal.  An ordinal that does
+    not exist declines (the reference's Ok(None))."""
+    import torch
+    _, prep, rows, _ = synth_case(3000, 700, scores=2)
+    flat = np.ascontiguousarray(rows).reshape(-1)
+    best = run(PipelineContext(prep), flat, engine=PLAIN, device=_lib.DEVICE_BEST)
+    zero = run(PipelineContext(prep), flat, engine=PLAIN, device=0)
+    np.testing.assert_array_equal(best[1], zero[1])
+    np.testing.assert_array_equal(best[0], zero[0])
+    from gnomon_b200.pipeline import try_run_cuda
+    assert try_run_cuda(PipelineContext(prep), flat, engine=PLAIN,
+                        device=torch.cuda.device_count()) is None
