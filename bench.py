@@ -316,6 +316,13 @@ def gpu_arm(args, rank, world, local_rank):
     stream.synchronize()
 
     plan = DevicePlan(prep, engine=engine, device=local_rank)
+    tuned = None
+    if not args.no_autotune:
+        # the library's autotuner picks the launch shape on these resident rows
+        # (outside the timed region; the plan is left reset)
+        shape = plan.autotune(rows, pitch, stream=stream)
+        tuned = ({"kernel": shape >> 16, "splits_per_full_tile": shape & 0xFFFF}
+                 if not tensor else {"raster": shape})
     sums, counts = plan.outputs()
     grad_s = None
     if args.backward:
@@ -515,6 +522,7 @@ def gpu_arm(args, rank, world, local_rank):
                        "engine": ("split-BF16 tcgen05 (4+3 limbs), FP64 block reduce" if tensor
                                   else "plain (FP32 CUDA-core LUT, FP64 reduce)"),
                        "parallelism": f"person-shard x{world}" if world > 1 else "single GPU",
+                       "launch_shape": tuned if tuned is not None else "default (not autotuned)",
                        "l2": (f"inputs ({V * bpv / 1e9:.1f} GB) larger than L2 "
                               f"({l2_bytes >> 20} MB); no flush" if flush is None else
                               f"inputs ({V * bpv / 1e6:.1f} MB) fit in L2 ({l2_bytes >> 20} MB): "
@@ -834,6 +842,8 @@ def main():
     ap.add_argument("--backward", action="store_true", help="add dW = G^T dS to each step")
     ap.add_argument("--stream-block", type=int, default=0,
                     help="stream rows from pinned host memory in blocks of this many variants")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the plan's default launch shape instead of autotuning it")
     ap.add_argument("--variants", type=int, default=0,
                     help="override the variant count (small cases for profiler captures)")
     ap.add_argument("--pgen", type=int, default=0,

@@ -16,6 +16,8 @@ STATUS_NAMES = {0: "GNM_OK", 1: "GNM_DECLINED", 2: "GNM_ERR_IO", 3: "GNM_ERR_COM
                 4: "GNM_ERR_PRODUCER", 5: "GNM_ERR_TIMEOUT", 6: "GNM_ERR_INVALID"}
 ENGINE_AUTO, ENGINE_PLAIN, ENGINE_TENSOR = 0, 1, 2
 DEVICE_CURRENT, DEVICE_BEST = -1, -2   # device arguments besides an ordinal
+# plain accumulate kernels (gnm_plan_tuned_shape >> 16): tile bytes, +1 = producer warp
+PLAIN_KERNELS = (1024, 512, 1025, 2049)
 
 u8p = C.POINTER(C.c_uint8)
 
@@ -85,6 +87,7 @@ SIGNATURES = {
     "gnm_plan_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.POINTER(gnm_error)]),
     "gnm_plan_tuned_shape": (C.c_uint32, [C.c_void_p]),
+    "gnm_plan_set_shape": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(gnm_error)]),
     "gnm_decode_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_uint64, C.c_void_p, C.POINTER(gnm_error)]),
     "gnm_release_cached_memory": (C.c_int, [C.c_int, C.POINTER(gnm_error)]),

@@ -300,24 +300,25 @@ static void validate_prep(const gnm_prep_view* p) {
 
 
 // ---- plan --------------------------------------------------------------------
-// Launch shape of the plain kernel: people tiles of tile_bytes (the last one
-// often partly populated), and variant-split counts weighted by each tile's
-// populated warps, so that every CTA carries about the same work and the grid
-// fills `mult` x the SMs' CTA slots (2 per SM with 1 KB tiles, 4 with 512 B).
-static void plain_shape(gnm_plan* p, uint32_t tile_bytes, double mult) {
+// Launch shape of the plain kernel: people tiles of the kernel's width (the
+// last one often partly populated), and variant-split counts weighted by each
+// tile's populated warps, so that every CTA carries about the same work and
+// the grid fills `mult` x the SMs' CTA slots (1, 2 or 4 CTAs per SM).
+static void plain_shape(gnm_plan* p, uint32_t kernel, double mult) {
+  const uint32_t tile_bytes = plain_tile_bytes(kernel);
   const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
   const uint64_t tiles = std::max<uint64_t>(1, (p->bpv + tile_bytes - 1) / tile_bytes);
   const uint64_t warps = tile_bytes / 128;
   const uint64_t last_bytes = p->bpv > (tiles - 1) * tile_bytes ? p->bpv - (tiles - 1) * tile_bytes : 1;
   const double w_last = double(std::min<uint64_t>(warps, (last_bytes + 127) / 128)) / double(warps);
-  const double ctas = double(2048 / tile_bytes) * double(p->num_sms) * mult;
+  const double ctas = double(plain_ctas_per_sm(kernel)) * double(p->num_sms) * mult;
   const double per_tile = ctas / (double(tiles - 1) + w_last);
   uint64_t splits = std::max<uint64_t>(1, uint64_t(per_tile));
   uint64_t last = tiles > 1 ? uint64_t(std::llround(double(splits) * w_last))
                             : uint64_t(std::max(1.0, ctas));
   splits = std::min(splits, stages);
   last = std::min<uint64_t>(std::max<uint64_t>(1, last), stages);
-  p->tile_bytes = tile_bytes;
+  p->kernel = kernel;
   p->split_mult = mult;
   p->tiles = uint32_t(tiles);
   p->splits = uint32_t(splits);
@@ -325,25 +326,45 @@ static void plain_shape(gnm_plan* p, uint32_t tile_bytes, double mult) {
   p->slots = uint32_t(tiles > 1 ? std::max(splits, last) : last);
 }
 
+// A pinned shape: `splits` splits per full tile, the last tile's count scaled
+// by its populated warps (gnm_plan_set_shape).
+static void plain_shape_fixed(gnm_plan* p, uint32_t kernel, uint32_t splits) {
+  const uint32_t tile_bytes = plain_tile_bytes(kernel);
+  const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
+  const uint64_t tiles = std::max<uint64_t>(1, (p->bpv + tile_bytes - 1) / tile_bytes);
+  const uint64_t warps = tile_bytes / 128;
+  const uint64_t last_bytes = p->bpv > (tiles - 1) * tile_bytes ? p->bpv - (tiles - 1) * tile_bytes : 1;
+  const double w_last = double(std::min<uint64_t>(warps, (last_bytes + 127) / 128)) / double(warps);
+  const uint64_t sp = std::min<uint64_t>(std::max<uint32_t>(1, splits), stages);
+  uint64_t last = tiles > 1 ? uint64_t(std::llround(double(sp) * w_last)) : sp;
+  last = std::min<uint64_t>(std::max<uint64_t>(1, last), stages);
+  p->kernel = kernel;
+  p->tiles = uint32_t(tiles);
+  p->splits = uint32_t(sp);
+  p->last_splits = uint32_t(last);
+  p->slots = uint32_t(tiles > 1 ? std::max(sp, last) : last);
+}
+
 static void plain_geometry(gnm_plan* p) {
-  // partial slots are padded to whole 1 KB tiles, so either tile width fits
-  p->part_stride = ((p->bpv + kPlainTileBytes - 1) / kPlainTileBytes) * kPlainTileBytes * 4;
-  if (p->part_stride == 0) p->part_stride = kPlainTileBytes * 4;
+  // partial slots are padded to whole tiles of the widest kernel, so every
+  // kernel's people index stays inside a slot
+  p->part_stride = std::max<uint64_t>(1, (p->bpv + kPlainWideTileBytes - 1) / kPlainWideTileBytes) *
+                   kPlainWideTileBytes * 4;
   check_cuda(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device),
              "cudaDeviceGetAttribute");
-  plain_shape(p, kPlainTileBytes, 1.0);
+  plain_shape(p, kPlainDefaultKernel, 1.0);
   // keep partials of all scores within 8 GiB (many score columns still get a
   // full-occupancy grid); allocate room for the autotuner's largest candidate
-  // (twice the CTA slots, either tile width)
+  // (twice the CTA slots, any kernel)
   const uint64_t per_split_bytes = p->K * p->part_stride * 12;
   const uint64_t cap = uint64_t(8) << 30;
   uint64_t alloc = p->slots;
-  for (uint32_t tb : {kPlainTileBytes, kPlainNarrowTileBytes}) {
+  for (uint32_t kn : kPlainKernels) {
     gnm_plan probe = {};
     probe.V = p->V;
     probe.bpv = p->bpv;
     probe.num_sms = p->num_sms;
-    plain_shape(&probe, tb, 2.0);
+    plain_shape(&probe, kn, 2.0);
     alloc = std::max<uint64_t>(alloc, probe.slots);
   }
   while (alloc > 1 && alloc * per_split_bytes > cap) --alloc;
@@ -352,7 +373,7 @@ static void plain_geometry(gnm_plan* p) {
   double mult = 1.0;
   while (p->slots > p->splits_alloc && mult > 1e-3) {
     mult *= 0.5;
-    plain_shape(p, kPlainTileBytes, mult);
+    plain_shape(p, kPlainDefaultKernel, mult);
   }
 }
 
@@ -566,7 +587,7 @@ static void accumulate_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, 
     a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_stride = p->part_stride;
     a.err = p->d_err;
-    check_cuda(launch_plain_accumulate(map, a, p->tile_bytes, s), "plain accumulate launch");
+    check_cuda(launch_plain_accumulate(map, a, p->kernel, s), "plain accumulate launch");
     ++p->launches;
   }
 }
@@ -646,23 +667,29 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
   };
   float best_ms = 1e30f;
   if (p->engine == GNM_ENGINE_PLAIN) {
-    uint32_t best_tile = p->tile_bytes;
+    uint32_t best_kernel = p->kernel;
     double best_mult = p->split_mult;
     p->tuning_log.clear();
-    for (uint32_t tb : {kPlainTileBytes, kPlainNarrowTileBytes}) {
+    const char* tr = std::getenv("GNM_TRACE");
+    const bool trace = tr && std::strcmp(tr, "0") != 0;
+    for (uint32_t kn : kPlainKernels) {
       for (double m : {0.5, 1.0, 2.0}) {
-        plain_shape(p, tb, m);
+        plain_shape(p, kn, m);
         if (p->slots > p->splits_alloc) continue;
         const float ms = time_best();
-        p->tuning_log.push_back({tb, m, p->splits, p->last_splits, ms});
+        p->tuning_log.push_back({kn, m, p->splits, p->last_splits, ms});
+        if (trace)
+          std::fprintf(stderr, "[gnm autotune] tile %u B%s, %.1fx slots: %u splits (last tile "
+                               "%u), %.4f ms\n", plain_tile_bytes(kn),
+                       (kn & 1u) ? " + producer warp" : "", m, p->splits, p->last_splits, ms);
         if (ms < best_ms) {
           best_ms = ms;
-          best_tile = tb;
+          best_kernel = kn;
           best_mult = m;
         }
       }
     }
-    plain_shape(p, best_tile, best_mult);
+    plain_shape(p, best_kernel, best_mult);
   } else {
     const uint32_t base = p->raster;
     uint32_t best = base;
@@ -1502,9 +1529,37 @@ gnm_status gnm_plan_autotune(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch,
   });
 }
 
+gnm_status gnm_plan_set_shape(gnm_plan* p, uint32_t shape, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] {
+    if (p->engine != GNM_ENGINE_PLAIN) {
+      if (shape > 1) fail(GNM_ERR_INVALID, "tensor engine shape is a raster order (0 or 1)");
+      p->raster = shape;
+      return;
+    }
+    const uint32_t kernel = shape >> 16;
+    bool known = false;
+    for (uint32_t kn : kPlainKernels) known |= kn == kernel;
+    if (!known) fail(GNM_ERR_INVALID, "unknown plain kernel in shape " + std::to_string(shape));
+    const uint32_t k0 = p->kernel, t0 = p->tiles, s0 = p->splits, l0 = p->last_splits,
+                   n0 = p->slots;
+    plain_shape_fixed(p, kernel, shape & 0xFFFFu);
+    if (p->slots > p->splits_alloc) {
+      const uint32_t need = p->slots;
+      p->kernel = k0;
+      p->tiles = t0;
+      p->splits = s0;
+      p->last_splits = l0;
+      p->slots = n0;
+      fail(GNM_ERR_INVALID, "shape needs " + std::to_string(need) + " partial slots; the plan has " +
+                                std::to_string(p->splits_alloc));
+    }
+  });
+}
+
 uint32_t gnm_plan_tuned_shape(const gnm_plan* p) {
   if (!p) return 0;
-  return p->engine == GNM_ENGINE_PLAIN ? (p->tile_bytes << 16) | std::min<uint32_t>(p->splits, 0xFFFFu)
+  return p->engine == GNM_ENGINE_PLAIN ? (p->kernel << 16) | std::min<uint32_t>(p->splits, 0xFFFFu)
                                        : p->raster;
 }
 

@@ -16,11 +16,12 @@ enum : uint32_t {
 };
 
 // ---- plain engine shape ----------------------------------------------------
-// A plain CTA scores a tile of 512 or 1024 bytes of every row (2048 or 4096
-// people) with one thread per 32-bit word column (16 people): 128 or 256
-// threads, 4 or 2 CTAs per SM.
-constexpr uint32_t kPlainTileBytes = 1024;   // the wide tile; also the partial-slot padding
-constexpr uint32_t kPlainNarrowTileBytes = 512;
+// A plain CTA scores a tile of 512, 1024 or 2048 bytes of every row (2048,
+// 4096 or 8192 people) with one thread per 32-bit word column (16 people):
+// 128 or 256 threads and 4 or 2 CTAs per SM, or 512 threads plus a producer
+// warp and one CTA per SM.
+constexpr uint32_t kPlainTileBytes = 1024;
+constexpr uint32_t kPlainWideTileBytes = 2048;   // also the partial-slot padding
 constexpr uint32_t kPlainBoxBytes = 256;     // TMA box inner extent (max 256 elements)
 constexpr uint32_t kPlainRows = 30;          // variant rows per pipeline stage (10 groups of 3)
 constexpr uint32_t kPlainGroups = kPlainRows / 3;
@@ -75,12 +76,26 @@ struct FinalizeArgs {
 cudaError_t raise_smem_limit(const void* kernel, int bytes);
 
 cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s);
+// Plain accumulate kernels: the tile width in bytes, plus 1 for the variant
+// with a producer warp (its scoring warps only arrive on a release barrier).
+enum : uint32_t {
+  kPlain512 = 512,        // 4 warps, 4 CTAs per SM
+  kPlain1024 = 1024,      // 8 warps, 2 CTAs per SM
+  kPlain1024Ws = 1025,    // 8 warps + producer warp, 2 CTAs per SM
+  kPlain2048Ws = 2049     // 16 warps + producer warp, 1 CTA per SM
+};
+constexpr uint32_t kPlainKernels[] = {kPlain1024, kPlain512, kPlain1024Ws, kPlain2048Ws};
+constexpr uint32_t kPlainDefaultKernel = kPlain1024;
+inline uint32_t plain_tile_bytes(uint32_t kernel) { return kernel & ~1u; }
+inline uint32_t plain_ctas_per_sm(uint32_t kernel) {
+  return plain_tile_bytes(kernel) >= 2048 ? 1u : 2048u / plain_tile_bytes(kernel);
+}
+
 // Launches (tiles - 1) * splits + ceil(stages / last_stages_per_split) CTAs of
-// the tile_bytes-wide kernel (512 or 1024).
-cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tile_bytes,
+// the given plain kernel.
+cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t kernel,
                                     cudaStream_t s);
 uint32_t plain_grid(const PlainArgs& a);
-uint32_t plain_smem_bytes(uint32_t tile_bytes);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
 cudaError_t launch_repitch(const uint8_t* src, uint64_t bpv, uint64_t nrows, uint8_t* dst,
                            uint64_t pitch, cudaStream_t s);

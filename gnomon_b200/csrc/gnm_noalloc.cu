@@ -137,7 +137,7 @@ static void score_noalloc(const uint8_t* d_rows, uint64_t pitch, uint64_t V, uin
     a.part_cnt = part_cnt;
     a.part_stride = stride;
     a.err = err;
-    check_cuda(launch_plain_accumulate(map, a, kPlainTileBytes, s), "plain accumulate launch");
+    check_cuda(launch_plain_accumulate(map, a, kPlain1024, s), "plain accumulate launch");
   }
   FinalizeArgs f;
   f.part_sum = part_sum;

@@ -55,7 +55,9 @@ struct PlainSmem {
   static constexpr uint32_t kBarOff = kTileOff + kStages * kStageBytes;     // 3 mbarriers
   static constexpr uint32_t kRelOff = kBarOff + 8 * kStages;                // 3 release counters
   static constexpr uint32_t kLastOff = kRelOff + 4 * kStages;               // 3 last-issued stages
-  static constexpr uint32_t kTotal = kLastOff + 4 * kStages;
+  static constexpr uint32_t kEmptyOff = kLastOff + 4 * kStages;             // 3 "released" mbarriers
+  static constexpr uint32_t kTotal = kEmptyOff + 8 * kStages;
+  static_assert(kEmptyOff % 8 == 0, "mbarrier alignment");
   static_assert(TILE % kPlainBoxBytes == 0 && TILE % 128 == 0, "whole boxes and warps");
   static_assert(kPlainRows % 3 == 0 && kPlainRows <= 32, "groups of 3 rows, one ballot");
   static_assert(kTabStride >= kPlainTableBytes && kTabStride % 256 == 0, "table stride");
@@ -150,18 +152,29 @@ __device__ __forceinline__ void plain_issue_stage(const CUtensorMap* map, const 
             kPlainTableBytes, bar);
 }
 
+template <uint32_t TILE, bool WS>
+struct PlainShape {
+  static constexpr uint32_t kThreads = TILE / 4 + (WS ? 32u : 0u);
+  static constexpr uint32_t kMinBlocks = TILE >= 2048 ? 1u : 2048u / TILE;
+};
+
 // One CTA per (people tile, variant split).  The grid is 1D: the first
 // (tiles - 1) * splits CTAs cover the full tiles, `splits` each, and the last
 // tile (often only partly populated by people) gets its own, smaller split
 // count, so every CTA carries about the same work and the grid fills the
-// SMs' CTA slots evenly.  block = TILE / 4 threads.
-template <uint32_t TILE>
-__global__ void __launch_bounds__(TILE / 4, 2048 / TILE)
+// SMs' CTA slots evenly.  block = TILE / 4 scoring threads, plus (WS) one
+// producer warp that issues every stage's copies once the scoring warps have
+// released its buffer (they arrive on an mbarrier and never wait for one
+// another); without it the scoring warp that releases a buffer last issues
+// the refill.
+template <uint32_t TILE, bool WS>
+__global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TILE, WS>::kMinBlocks)
     gnm_plain_accumulate(const __grid_constant__ CUtensorMap map, PlainArgs a) {
   using L = PlainSmem<TILE>;
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t sbase = smem_u32(smem);
   const uint32_t tid = threadIdx.x, lane = tid & 31u;
+  const bool producer = WS && tid >= L::kThreads;
   const uint32_t full_ctas = (a.tiles - 1) * a.splits;
   uint32_t tile, split, sps;
   if (blockIdx.x < full_ctas) {
@@ -188,19 +201,50 @@ __global__ void __launch_bounds__(TILE / 4, 2048 / TILE)
   const int32_t tile_x = int32_t(tile * TILE);
   const uint32_t bar0 = sbase + L::kBarOff;
   const uint32_t rel0 = sbase + L::kRelOff;
+  const uint32_t empty0 = sbase + L::kEmptyOff;
   uint32_t* last_issued = reinterpret_cast<uint32_t*>(smem + L::kLastOff);
 
   if (tid == 0) {
     prefetch_tmap(&map);
     for (uint32_t b = 0; b < L::kStages; ++b) {
       mbar_init(bar0 + 8 * b, 1);
+      if (WS) mbar_init(empty0 + 8 * b, L::kWarps);
       sts_u32(rel0 + 4 * b, 0u);
       last_issued[b] = 0xFFFFFFFFu;
     }
     fence_mbar_init();
   }
   __syncthreads();
-  if (tid == 0) {
+  if (WS && producer) {
+    // ---- producer warp: every stage's copies, each once its buffer is free
+    bool ok = true;
+    if (lane == 0) {
+      for (uint32_t st = 0; st < nstages; ++st) {
+        const uint32_t buf = st % L::kStages;
+        if (st >= L::kStages) {
+          // the scoring warps released stage st - 3 of this buffer
+          if (!mbar_wait_bounded(empty0 + 8 * buf, ((st / L::kStages) - 1) & 1u)) {
+            atomicOr(a.err, kErrTmaTimeout);
+            ok = false;
+            break;
+          }
+          fence_proxy_async_smem();
+        }
+        last_issued[buf] = st;
+        plain_issue_stage<TILE>(&map, a.tables, sbase, buf, tile_x,
+                                int32_t(r_begin + uint64_t(st) * kPlainRows), stage0 + st);
+      }
+    }
+    // every warp of the CTA meets here (the scoring warps at the end of their loop)
+    if (__syncthreads_or(!__shfl_sync(0xFFFFFFFFu, ok ? 1 : 0, 0))) {
+      if (lane == 0)   // drain each buffer's last issued copy (bounded)
+        for (uint32_t b = 0; b < L::kStages; ++b)
+          if (last_issued[b] != 0xFFFFFFFFu)
+            mbar_wait_bounded(bar0 + 8 * b, (last_issued[b] / L::kStages) & 1u);
+    }
+    return;
+  }
+  if (!WS && tid == 0) {
     for (uint32_t s = 0; s < L::kStages && s < nstages; ++s) {
       last_issued[s] = s;
       plain_issue_stage<TILE>(&map, a.tables, sbase, s, tile_x,
@@ -307,7 +351,9 @@ __global__ void __launch_bounds__(TILE / 4, 2048 / TILE)
     // warp's release, so all reads of the buffer are done before it hands the
     // buffer to the async proxy for the stage three ahead.
     __syncwarp();
-    if (lane == 0) {
+    if (WS) {
+      if (lane == 0) mbar_arrive(empty0 + 8 * buf);
+    } else if (lane == 0) {
       const uint32_t old = atom_add_acq_rel(rel0 + 4 * buf, 1u);
       if (old == L::kWarps - 1) {
         sts_u32(rel0 + 4 * buf, 0u);
@@ -350,7 +396,7 @@ __global__ void __launch_bounds__(TILE / 4, 2048 / TILE)
   // wait for (bounded).  Once every warp is here, drain each buffer's last
   // issued copy (bounded) so no TMA is in flight when the CTA exits.
   if (__syncthreads_or(failed)) {
-    if (tid == 0) {
+    if (!WS && tid == 0) {   // (WS: the producer warp drains)
       for (uint32_t b = 0; b < L::kStages; ++b)
         if (last_issued[b] != 0xFFFFFFFFu)
           mbar_wait_bounded(bar0 + 8 * b, (last_issued[b] / L::kStages) & 1u);
@@ -487,14 +533,14 @@ cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <uint32_t TILE>
+template <uint32_t TILE, bool WS>
 static cudaError_t launch_plain_tile(const CUtensorMap& map, const PlainArgs& a, uint32_t grid,
                                      cudaStream_t s) {
   using L = PlainSmem<TILE>;
-  const cudaError_t e =
-      raise_smem_limit(reinterpret_cast<const void*>(gnm_plain_accumulate<TILE>), int(L::kTotal));
+  const cudaError_t e = raise_smem_limit(
+      reinterpret_cast<const void*>(gnm_plain_accumulate<TILE, WS>), int(L::kTotal));
   if (e != cudaSuccess) return e;
-  gnm_plain_accumulate<TILE><<<grid, L::kThreads, L::kTotal, s>>>(map, a);
+  gnm_plain_accumulate<TILE, WS><<<grid, PlainShape<TILE, WS>::kThreads, L::kTotal, s>>>(map, a);
   return cudaGetLastError();
 }
 
@@ -504,18 +550,18 @@ uint32_t plain_grid(const PlainArgs& a) {
   return uint32_t(uint64_t(a.tiles - 1) * a.splits + last);
 }
 
-cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t tile_bytes,
+cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, uint32_t kernel,
                                     cudaStream_t s) {
   if (a.tiles == 0 || a.splits == 0 || a.stages_per_split == 0 || a.last_stages_per_split == 0)
     return cudaErrorInvalidValue;
   const uint32_t grid = plain_grid(a);
-  if (tile_bytes == 1024) return launch_plain_tile<1024>(map, a, grid, s);
-  if (tile_bytes == 512) return launch_plain_tile<512>(map, a, grid, s);
-  return cudaErrorInvalidValue;
-}
-
-uint32_t plain_smem_bytes(uint32_t tile_bytes) {
-  return tile_bytes == 512 ? PlainSmem<512>::kTotal : PlainSmem<1024>::kTotal;
+  switch (kernel) {
+    case kPlain512: return launch_plain_tile<512, false>(map, a, grid, s);
+    case kPlain1024: return launch_plain_tile<1024, false>(map, a, grid, s);
+    case kPlain1024Ws: return launch_plain_tile<1024, true>(map, a, grid, s);
+    case kPlain2048Ws: return launch_plain_tile<2048, true>(map, a, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s) {

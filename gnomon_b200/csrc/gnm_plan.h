@@ -123,17 +123,17 @@ struct gnm_plan {
   int num_sms = 0;
 
   // plain engine
-  uint32_t tile_bytes = 1024;  // people tile width of the accumulate kernel (512 or 1024)
+  uint32_t kernel = 1024;      // plain accumulate kernel (gnm_internal.h kPlain*)
   double split_mult = 1.0;     // CTA slots per SM multiplier the split counts are sized for
-  uint32_t tiles = 0;          // people tiles of tile_bytes
+  uint32_t tiles = 0;          // people tiles of the kernel's width
   uint32_t splits = 0;         // variant splits of each full tile
   uint32_t last_splits = 0;    // variant splits of the last (partly populated) tile
   uint32_t slots = 0;          // partial slots in use: max(splits, last_splits)
   uint32_t splits_alloc = 0;   // partial slots allocated per score (autotune range)
   uint32_t raster = 0;         // tensor engine CTA order: 0 people-tile fastest, 1 score-tile
-  uint64_t part_stride = 0;    // people per partial slot (bpv rounded up to 1024 bytes, x4)
+  uint64_t part_stride = 0;    // people per partial slot (bpv rounded up to 2048 bytes, x4)
   struct Tuning {              // one autotuner candidate and its best accumulate time
-    uint32_t tile_bytes;
+    uint32_t kernel;
     double mult;
     uint32_t splits, last_splits;
     float ms;

@@ -115,6 +115,15 @@ class DevicePlan:
                                               _stream_ptr(stream), C.byref(e)), e)
         return int(self.lib.gnm_plan_tuned_shape(self.handle))
 
+    def set_shape(self, shape: int) -> None:
+        """Pin a launch shape (a value ``autotune`` returned)."""
+        e = self._err()
+        _lib.check(self.lib.gnm_plan_set_shape(self.handle, int(shape), C.byref(e)), e)
+
+    @property
+    def shape(self) -> int:
+        return int(self.lib.gnm_plan_tuned_shape(self.handle))
+
     def capture(self, rows: torch.Tensor, pitch: int, sums=None, counts=None):
         """Record one full scoring pass (reset + accumulate + finalize) into a CUDA
         graph; ``graph.replay()`` reruns it with no per-launch host work.  Returns

@@ -217,15 +217,26 @@ uint64_t gnm_plan_launch_count(const gnm_plan* plan);
 /* Autotuner (no reference counterpart; the reference sizes its tiles from free
  * memory only, score/cuda_backend.rs:803-975): times the plan's accumulate on
  * the first `variant_count` resident rows for each candidate launch shape —
- * plain engine: variant-split count (1x/2x/4x of the default); tensor engine
- * with more than 64 scores: CTA raster order (the narrow kernel used up to 64
- * scores has a single order) — keeps the fastest, and leaves the plan reset.
- * Blocks until done. */
+ * plain engine: the kernel (people tiles of 512 bytes with 4 warps, 1024 bytes
+ * with 8 warps, 1024 bytes with 8 warps and a producer warp, 2048 bytes with
+ * 16 warps and a producer warp) times the variant-split count (0.5x, 1x, 2x
+ * the SMs' CTA slots, split between people tiles by their populated warps);
+ * tensor engine with more than 64 scores: CTA raster order (the narrow kernel
+ * used up to 64 scores has a single order) — keeps the fastest, and leaves the
+ * plan reset.  Blocks until done.  With the environment variable GNM_TRACE
+ * set, every candidate's time is printed on stderr. */
 gnm_status gnm_plan_autotune(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
                              uint64_t variant_count, void* stream, gnm_error* err);
 
-/* The tuned shape: split count (plain) or raster order (tensor). */
+/* The tuned shape.  Plain engine: (kernel << 16) | splits per full people
+ * tile, kernel = tile bytes (512, 1024, 2048) + 1 with a producer warp;
+ * tensor engine: the raster order. */
 uint32_t gnm_plan_tuned_shape(const gnm_plan* plan);
+
+/* Pin a shape (a value gnm_plan_tuned_shape returned, e.g. saved from an
+ * earlier autotune of the same workload).  GNM_ERR_INVALID for an unknown
+ * kernel or more splits than the plan's partial slots hold. */
+gnm_status gnm_plan_set_shape(gnm_plan* plan, uint32_t shape, gnm_error* err);
 
 /* ---- Packed-row utilities ------------------------------------------------ */
 

@@ -367,3 +367,93 @@ def test_best_device_choice(cuda):
     from gnomon_b200.pipeline import try_run_cuda
     assert try_run_cuda(PipelineContext(prep), flat, engine=PLAIN,
                         device=torch.cuda.device_count()) is None
+
+
+def _c_rows_case(people, variants, scores, config="plain_2k_x_50k"):
+    """Workload weights with rows from the threaded C generator (large cases)."""
+    import os
+    from gnomon_b200.prepare import from_workload
+    w = synth.scaled(synth.WORKLOADS[config], people, variants, scores)
+    thr = synth.variant_thresholds(w.seed, 0, variants, w.p_lo, w.p_hi, w.missing_rate)
+    rows = oracle.synth_rows(w.seed, 0, variants, people, thr, w.bytes_per_variant,
+                             threads=os.cpu_count() or 1)
+    return from_workload(w), rows
+
+
+@pytest.mark.parametrize("kernel", _lib.PLAIN_KERNELS)
+@pytest.mark.parametrize("people,variants", [(20_001, 2_001), (2_000, 4_000), (9_000, 70),
+                                             (130, 301)])
+def test_every_plain_kernel_and_split(cuda, kernel, people, variants):
+    """Each plain accumulate kernel (512 / 1024-byte tiles; 1024 / 2048-byte
+    tiles with a producer warp), pinned with gnm_plan_set_shape at several
+    split counts (one split, uneven splits, more splits than a full tile has
+    CTA slots), against the restated reference engine: counts bit-exact, sums
+    within the reference's 1e-6 metric.  Ragged last tiles and last stages
+    included."""
+    import torch
+    from gnomon_b200.device import DevicePlan, row_pitch
+    prep, rows = _c_rows_case(people, variants, 2)
+    pitch = row_pitch(prep.bytes_per_variant)
+    dev = np.zeros((variants, pitch), np.uint8)
+    dev[:, :rows.shape[1]] = rows
+    d_rows = torch.from_numpy(dev).cuda()
+    rs, rc = oracle.score_reference(rows, prep, threads=8)
+    plan = DevicePlan(prep, engine=PLAIN)
+    try:
+        for splits in (1, 7, 64):
+            plan.set_shape((kernel << 16) | splits)
+            assert plan.shape >> 16 == kernel
+            s, c = plan.score(d_rows, pitch)
+            plan.sync()
+            np.testing.assert_array_equal(c.cpu().numpy().astype(np.uint32), rc)
+            assert oracle.within_reference_tolerance(s.cpu().numpy(), rs).all(), splits
+    finally:
+        plan.close()
+
+
+def test_set_shape_rejects_unknown_kernels(cuda):
+    from gnomon_b200.device import DevicePlan
+    _, prep, _, _ = synth_case(500, 100, scores=1)
+    plan = DevicePlan(prep, engine=PLAIN)
+    try:
+        with pytest.raises(_lib.GnomonGpuError):
+            plan.set_shape((768 << 16) | 4)
+        with pytest.raises(_lib.GnomonGpuError):   # more partial slots than allocated
+            plan.set_shape((1024 << 16) | 0xFFFF)
+        assert plan.shape >> 16 in _lib.PLAIN_KERNELS
+    finally:
+        plan.close()
+
+
+@pytest.mark.parametrize("people,variants", [(2_000, 50_000), (50_000, 60_000)])
+def test_autotuned_shapes_keep_results(cuda, people, variants):
+    """The autotuner times every plain kernel at three split counts on the
+    resident rows and keeps the fastest; the tuned plan's result equals the
+    default plan's (counts exact, sums within 1e-9 relative: only the FP64
+    grouping of split partials changes).  The chosen shape is printed
+    (TUNED_SHAPE line, pytest -s) for the small- and large-cohort shapes."""
+    import json
+    import torch
+    from gnomon_b200.device import DevicePlan, row_pitch
+    prep, rows = _c_rows_case(people, variants, 1)
+    pitch = row_pitch(prep.bytes_per_variant)
+    dev = np.zeros((variants, pitch), np.uint8)
+    dev[:, :rows.shape[1]] = rows
+    d_rows = torch.from_numpy(dev).cuda()
+    del dev
+    plan = DevicePlan(prep, engine=PLAIN)
+    try:
+        s0, c0 = plan.score(d_rows, pitch)
+        plan.sync()
+        s0, c0 = s0.cpu().numpy(), c0.cpu().numpy()
+        default = plan.shape
+        shape = plan.autotune(d_rows, pitch)
+        s1, c1 = plan.score(d_rows, pitch)
+        plan.sync()
+        np.testing.assert_array_equal(c1.cpu().numpy(), c0)
+        assert oracle.rel_err(s1.cpu().numpy(), s0).max() < 1e-9
+        print("TUNED_SHAPE " + json.dumps({"people": people, "variants": variants,
+                                           "default": [default >> 16, default & 0xFFFF],
+                                           "tuned": [shape >> 16, shape & 0xFFFF]}))
+    finally:
+        plan.close()
