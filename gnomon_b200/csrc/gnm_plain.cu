@@ -25,8 +25,8 @@
 //     issues the TMA of the stage three ahead — no CTA-wide barrier per stage;
 //   * missing calls (code 01) are counted with SWAR bit tricks on the raw row
 //     words (x & ~(x>>1) & member_mask, three rows summed with one add);
-//   * FP32 partial sums (packed pairs, add.rn.f32x2) cover 120 variants and are
-//     flushed to FP64 registers; variant splits write FP64 partials that
+//   * FP32 partial sums (packed pairs, add.rn.f32x2) cover one 30-variant
+//     stage and are flushed to FP64 registers; variant splits write FP64 partials that
 //     gnm_finalize reduces in a fixed order (deterministic) and gathers
 //     through output_idx_to_fam_idx, adding the FP64 baseline
 //     (pipeline.rs:1739-1775).
@@ -284,16 +284,20 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       break;
     }
 
-    // explicit shared-space loads (32-bit shared addresses) for rows and tables
-    const uint32_t tbase = sbase + L::kTileOff + buf * L::kStageBytes + word_off;
+    // Row words are ordinary loads from the shared array (the compiler may
+    // hoist the next group's rows above this group's lookups; the mbarrier
+    // wait above clobbers memory, so none moves above it); table lookups go
+    // through 32-bit shared addresses.
+    const uint8_t* tbase = smem + L::kTileOff + buf * L::kStageBytes + word_off;
     const uint32_t lbase = sbase + L::kTabOff + buf * L::kTabStride;
-    const uint64_t members = lds_u32(lbase + kPlainGroups * 256);
+    const uint64_t members = *reinterpret_cast<const uint32_t*>(
+        smem + L::kTabOff + buf * L::kTabStride + kPlainGroups * 256);
 
     uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
     auto group = [&](uint32_t g, uint32_t ma, uint32_t mb, uint32_t mc) {
-      const uint32_t xa = lds_u32(tbase + (3 * g + 0) * kPlainBoxBytes);
-      const uint32_t xb = lds_u32(tbase + (3 * g + 1) * kPlainBoxBytes);
-      const uint32_t xc = lds_u32(tbase + (3 * g + 2) * kPlainBoxBytes);
+      const uint32_t xa = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 0) * kPlainBoxBytes);
+      const uint32_t xb = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 1) * kPlainBoxBytes);
+      const uint32_t xc = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 2) * kPlainBoxBytes);
       // ---- per-person 6-bit indices (x4) ------------------------------
       // rows a and b get row c's lo bits XORed into their lo bits; row c
       // enters with its code bits swapped (see the table layout above)
@@ -367,10 +371,13 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       }
     }
 
-    // FP32 sums span four stages (120 variants) before they are flushed to
-    // FP64; byte counters span eight (<= 240 calls per byte) before they are
-    // flushed to 32-bit counts.
-    if ((st & 3u) == 3u || st + 1 == nstages) {
+    // FP32 sums span one stage (10 lookups, 30 variants) before they are
+    // flushed to FP64: the FP32 rounding error of a sum grows with the square
+    // root of that span, and over 10^6 variants 120-variant spans left sums
+    // within a few 1e-7 of the reference's 1e-6 tolerance.  Byte counters
+    // span eight stages (<= 240 calls per byte) before they are flushed to
+    // 32-bit counts.
+    {
       const bool counts_too = (st & 7u) == 7u || st + 1 == nstages;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {

@@ -70,6 +70,7 @@ struct TensorPlan {
   uint64_t nslot = 0;                     // narrow: elements per split slot (K16 * P_pad)
   CUtensorMap map_dos, map_mis;
   bool narrow = false;                    // few scores: gnm_tc_narrow (people as M)
+  bool can_narrow = false;                // K <= 64: either kernel can run the plan
   CUtensorMap nmap_dos, nmap_mis;         // narrow boxes: 16 scores x 4 planes
 };
 
@@ -1123,7 +1124,8 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   t->ptiles = uint32_t(std::max<uint64_t>(1, (p->fam + kTcN - 1) / kTcN));
   t->stiles = uint32_t(t->K_pad / kTcM);
   t->P_pad = uint64_t(t->ptiles) * kTcN;
-  t->narrow = p->K <= kNarrowMaxScores;
+  t->can_narrow = p->K <= kNarrowMaxScores;
+  t->narrow = t->can_narrow;
   if (t->V_pad > (uint64_t(1) << 31)) fail(GNM_ERR_INVALID, "too many variants for the tensor engine");
 
   const uint64_t plane = t->K_pad * t->V_pad;
@@ -1133,7 +1135,10 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   };
   alloc(reinterpret_cast<void**>(&t->d_planes_dos), 4 * plane * 2, "cudaMalloc(limb planes)");
   alloc(reinterpret_cast<void**>(&t->d_planes_mis), 4 * plane * 2, "cudaMalloc(limb planes)");
-  if (t->narrow) {
+  // partials hold either kernel's layout when both can run the plan (the
+  // autotuner chooses between them)
+  t->part_elems = t->K_pad * t->P_pad;
+  if (t->can_narrow) {
     const uint64_t k16 = (p->K + kNrScores - 1) / kNrScores * kNrScores;
     const uint64_t base = ((p->fam + kNrM - 1) / kNrM) * (k16 / kNrScores);
     int sms = 0;
@@ -1141,9 +1146,7 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
                "cudaDeviceGetAttribute");
     t->nsplits = narrow_splits(base, t->V_pad / kTcK, std::max(1, sms));
     t->nslot = k16 * t->P_pad;
-    t->part_elems = uint64_t(t->nsplits) * t->nslot;
-  } else {
-    t->part_elems = t->K_pad * t->P_pad;
+    t->part_elems = std::max(t->part_elems, uint64_t(t->nsplits) * t->nslot);
   }
   alloc(reinterpret_cast<void**>(&t->d_part_sum), t->part_elems * 8, "cudaMalloc(partials)");
   alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->part_elems * 4, "cudaMalloc(partials)");
@@ -1195,7 +1198,7 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   mark("  tensor: plane build");
   t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcM, kTcPlanes);
   t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcM, kTcPlanes);
-  if (t->narrow) {
+  if (t->can_narrow) {
     t->nmap_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kNrScores, 4);
     t->nmap_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kNrScores, 4);
   }
@@ -1210,6 +1213,14 @@ void tensor_plan_destroy(gnm_plan* p) {
   pool_free(t->d_part_cnt);
   delete t;
   p->tensor = nullptr;
+}
+
+bool tensor_can_narrow(const gnm_plan* p) { return p->tensor && p->tensor->can_narrow; }
+bool tensor_is_narrow(const gnm_plan* p) { return p->tensor && p->tensor->narrow; }
+void tensor_set_narrow(gnm_plan* p, bool narrow) {
+  if (narrow && !tensor_can_narrow(p))
+    fail(GNM_ERR_INVALID, "the narrow tensor kernel serves at most 64 scores");
+  p->tensor->narrow = narrow;
 }
 
 void tensor_reset(gnm_plan* p, cudaStream_t s) {

@@ -22,6 +22,11 @@ struct PhaseTrace;
 void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trace);
 void tensor_plan_destroy(gnm_plan* p);
 void tensor_reset(gnm_plan* p, cudaStream_t s);
+// Up to 64 scores either tensor kernel can run a plan: the narrow one (people
+// as the MMA's M, the default) or the wide one (scores as M).
+bool tensor_can_narrow(const gnm_plan* p);
+bool tensor_is_narrow(const gnm_plan* p);
+void tensor_set_narrow(gnm_plan* p, bool narrow);
 void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,
                        uint64_t nv, cudaStream_t s);
 void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_baseline,

@@ -221,16 +221,16 @@ uint64_t gnm_plan_launch_count(const gnm_plan* plan);
  * with 8 warps, 1024 bytes with 8 warps and a producer warp, 2048 bytes with
  * 16 warps and a producer warp) times the variant-split count (0.5x, 1x, 2x
  * the SMs' CTA slots, split between people tiles by their populated warps);
- * tensor engine with more than 64 scores: CTA raster order (the narrow kernel
- * used up to 64 scores has a single order) — keeps the fastest, and leaves the
- * plan reset.  Blocks until done.  With the environment variable GNM_TRACE
+ * tensor engine: up to 64 scores the narrow kernel (people as the MMA's M)
+ * against the wide kernel (scores as M), and the wide kernel's CTA raster
+ * order — keeps the fastest, and leaves the plan reset.  Blocks until done.  With the environment variable GNM_TRACE
  * set, every candidate's time is printed on stderr. */
 gnm_status gnm_plan_autotune(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
                              uint64_t variant_count, void* stream, gnm_error* err);
 
 /* The tuned shape.  Plain engine: (kernel << 16) | splits per full people
  * tile, kernel = tile bytes (512, 1024, 2048) + 1 with a producer warp;
- * tensor engine: the raster order. */
+ * tensor engine: raster order | (2 if the narrow kernel runs the plan). */
 uint32_t gnm_plan_tuned_shape(const gnm_plan* plan);
 
 /* Pin a shape (a value gnm_plan_tuned_shape returned, e.g. saved from an
