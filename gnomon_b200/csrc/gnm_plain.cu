@@ -66,17 +66,10 @@ struct PlainSmem {
   // address is the table address with its low byte replaced by the index.
 };
 
-// Two FP32 additions in one instruction (sm_100 packed f32x2): acc += {lo, hi}.
-__device__ __forceinline__ uint64_t add_f32x2(uint64_t acc, float lo, float hi) {
-  uint64_t r;
-  asm("{\n\t.reg .b64 t;\n\tmov.b64 t, {%2, %3};\n\tadd.rn.f32x2 %0, %1, t;\n\t}"
-      : "=l"(r)
-      : "l"(acc), "f"(lo), "f"(hi));
-  return r;
-}
-
-__device__ __forceinline__ void unpack_f32x2(uint64_t v, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+__device__ __forceinline__ int32_t lds_s32(uint32_t addr) {
+  int32_t v;
+  asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(addr));
+  return v;
 }
 
 // Shared-memory atomic add with acquire-release ordering at CTA scope.
@@ -98,8 +91,16 @@ __device__ __forceinline__ void sts_u32(uint32_t addr, uint32_t v) {
 // c (bit 4).  The two entries that share a bank therefore differ in the lo bit
 // of all three codes (code 01 missing / 11 hom-alt), so one of them needs two
 // such calls in one person and lanes rarely meet on a bank with different
-// addresses.  The sum of the three FP32 terms is exact in FP64 and rounded to
-// FP32 once.
+// addresses.
+//
+// Entries are int32 fixed-point values on a per-stage grid: q = (largest
+// |entry| of the stage) / 2^27, entry = round(exact FP64 sum of the three
+// FP32 terms / q), so |entry| <= 2^27 + 1 and the ten lookups of a stage add
+// up EXACTLY in int32 (|sum| < 2^31).  The kernel converts each stage's
+// integer sums to FP64 once (sum * q).  The only rounding before FP64 is the
+// grid itself, <= q/2 per lookup; FP32 running sums lose up to half an ulp of
+// the running partial at every add, which over 10^6 variants came near the
+// reference's 1e-6 tolerance.  q sits in the stage table's tail (word 1).
 
 __device__ __forceinline__ float table_term(const TableArgs& a, uint64_t row, uint32_t j) {
   if (a.records) return reinterpret_cast<const float*>(a.records + a.row0 + row)[j];
@@ -114,8 +115,9 @@ __device__ __forceinline__ bool table_member(const TableArgs& a, uint64_t row) {
   return a.member == nullptr || a.member[a.row0 + row] != 0;
 }
 
-// grid.x = stages, block = 8 groups x 64 entries.
+// grid.x = stages, block = kPlainGroups groups x 64 entries.
 __global__ void __launch_bounds__(kPlainGroups * 64) gnm_plain_tables(TableArgs a) {
+  __shared__ float s_max[kPlainGroups * 2];
   const uint64_t stage = blockIdx.x;
   const uint32_t e = threadIdx.x, g = e >> 6, idx = e & 63u;
   const uint32_t lc = (idx >> 5) & 1u;
@@ -125,28 +127,42 @@ __global__ void __launch_bounds__(kPlainGroups * 64) gnm_plain_tables(TableArgs 
 #pragma unroll
   for (int r = 0; r < 3; ++r)
     if (code[r] != 0 && row0 + r < a.num_rows) v += double(table_term(a, row0 + r, code[r] - 1));
+  // largest |entry| of the stage (exact FP64 sums rounded up to FP32)
+  float m = __double2float_ru(fabs(v));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  if ((e & 31u) == 0) s_max[e >> 5] = m;
+  __syncthreads();
+  float mx = 0.0f;
+#pragma unroll
+  for (uint32_t w = 0; w < kPlainGroups * 2; ++w) mx = fmaxf(mx, s_max[w]);
+  const float q = mx > 0.0f ? ldexpf(mx, -27) : 1.0f;   // exact power-of-two scaling
   uint8_t* tab = a.tables + stage * kPlainTableBytes;
-  reinterpret_cast<float*>(tab)[e] = float(v);
+  reinterpret_cast<int32_t*>(tab)[e] = int32_t(__double2ll_rn(v / double(q)));
   if (e < 32) {
     const uint64_t row = stage * kPlainRows + e;
-    const bool m = e < kPlainRows && row < a.num_rows && table_member(a, row);
-    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, m);
-    if (e < 4) reinterpret_cast<uint32_t*>(tab + kPlainGroups * 256)[e] = e == 0 ? bits : 0u;
+    const bool mem = e < kPlainRows && row < a.num_rows && table_member(a, row);
+    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, mem);
+    if (e < 4)
+      reinterpret_cast<uint32_t*>(tab + kPlainGroups * 256)[e] =
+          e == 0 ? bits : (e == 1 ? __float_as_uint(q) : 0u);
   }
 }
 
 // ---- accumulate --------------------------------------------------------------
 
+// Copies of one stage: the tile's first `boxes` row boxes (the ones that hold
+// row bytes) and the stage table, on the buffer's mbarrier.
 template <uint32_t TILE>
 __device__ __forceinline__ void plain_issue_stage(const CUtensorMap* map, const uint8_t* tables,
                                                   uint32_t smem_base, uint32_t buf,
-                                                  int32_t tile_x, int32_t row0, uint64_t stage) {
+                                                  int32_t tile_x, int32_t row0, uint64_t stage,
+                                                  uint32_t boxes) {
   using L = PlainSmem<TILE>;
   const uint32_t bar = smem_base + L::kBarOff + 8 * buf;
-  mbar_arrive_expect_tx(bar, L::kStageBytes + kPlainTableBytes);
+  mbar_arrive_expect_tx(bar, boxes * L::kBoxBytes + kPlainTableBytes);
   const uint32_t tile = smem_base + L::kTileOff + buf * L::kStageBytes;
-#pragma unroll
-  for (uint32_t b = 0; b < L::kBoxes; ++b)
+  for (uint32_t b = 0; b < boxes; ++b)
     tma_load_2d(tile + b * L::kBoxBytes, map, tile_x + int32_t(b * kPlainBoxBytes), row0, bar);
   bulk_load(smem_base + L::kTabOff + buf * L::kTabStride, tables + stage * kPlainTableBytes,
             kPlainTableBytes, bar);
@@ -199,6 +215,13 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
   const uint32_t nstages = uint32_t((r_end - r_begin + kPlainRows - 1) / kPlainRows);
   const uint64_t stage0 = r_begin / kPlainRows;   // block stage of this split's stage 0
   const int32_t tile_x = int32_t(tile * TILE);
+  // The last tile may hold fewer row bytes than TILE: only its populated
+  // warps score (the others skip the stage loop and release nothing) and
+  // only its populated boxes are copied, so a partly filled tile costs in
+  // proportion to its bytes.
+  const uint64_t used = min(uint64_t(TILE), a.bytes_per_row - uint64_t(tile) * TILE);
+  const uint32_t active_warps = uint32_t((used + 127) / 128);
+  const uint32_t boxes = uint32_t((used + kPlainBoxBytes - 1) / kPlainBoxBytes);
   const uint32_t bar0 = sbase + L::kBarOff;
   const uint32_t rel0 = sbase + L::kRelOff;
   const uint32_t empty0 = sbase + L::kEmptyOff;
@@ -208,7 +231,7 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     prefetch_tmap(&map);
     for (uint32_t b = 0; b < L::kStages; ++b) {
       mbar_init(bar0 + 8 * b, 1);
-      if (WS) mbar_init(empty0 + 8 * b, L::kWarps);
+      if (WS) mbar_init(empty0 + 8 * b, active_warps);
       sts_u32(rel0 + 4 * b, 0u);
       last_issued[b] = 0xFFFFFFFFu;
     }
@@ -232,7 +255,7 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
         }
         last_issued[buf] = st;
         plain_issue_stage<TILE>(&map, a.tables, sbase, buf, tile_x,
-                                int32_t(r_begin + uint64_t(st) * kPlainRows), stage0 + st);
+                                int32_t(r_begin + uint64_t(st) * kPlainRows), stage0 + st, boxes);
       }
     }
     // every warp of the CTA meets here (the scoring warps at the end of their loop)
@@ -248,13 +271,13 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     for (uint32_t s = 0; s < L::kStages && s < nstages; ++s) {
       last_issued[s] = s;
       plain_issue_stage<TILE>(&map, a.tables, sbase, s, tile_x,
-                              int32_t(r_begin + s * kPlainRows), stage0 + s);
+                              int32_t(r_begin + s * kPlainRows), stage0 + s, boxes);
     }
   }
 
-  // FP32 sums as packed pairs for add.rn.f32x2: accp[2q] holds people
-  // (q, 4+q), accp[2q+1] people (8+q, 12+q) of this thread's 16.
-  uint64_t accp[8];
+  // int32 fixed-point sums of the current stage: iacc[4j + q] is person
+  // 4j + q of this thread's 16 (exact: <= 10 lookups of |entry| <= 2^27 + 1).
+  int32_t iacc[16];
   double acc64[16];
   uint32_t cnt[16];
   uint32_t by[4] = {0u, 0u, 0u, 0u};   // byte counters: byte j = person 4j+q
@@ -264,18 +287,17 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     cnt[i] = 0u;
   }
 #pragma unroll
-  for (int i = 0; i < 8; ++i) accp[i] = 0ull;
+  for (int i = 0; i < 16; ++i) iacc[i] = 0;
 
   // Each thread reads word column `tid` of the TILE-byte stage row; the stage
   // is stored as TILE / 256 TMA boxes of [kPlainRows rows][256 bytes].
   const uint32_t word_off = (tid / (kPlainBoxBytes / 4)) * L::kBoxBytes +
                             (tid % (kPlainBoxBytes / 4)) * 4;
   // warps whose 128 bytes all lie past the row's last byte only hold padding
-  const bool warp_active =
-      uint64_t(tile) * TILE + uint64_t(tid & ~31u) * 4 < a.bytes_per_row;
+  const bool warp_active = (tid >> 5) < active_warps;
 
   bool failed = false;
-  for (uint32_t st = 0; st < nstages; ++st) {
+  for (uint32_t st = 0; st < (warp_active ? nstages : 0u); ++st) {
     const uint32_t buf = st % L::kStages;
     const uint32_t parity = (st / L::kStages) & 1u;
     if (!mbar_wait_bounded(bar0 + 8 * buf, parity)) {
@@ -292,6 +314,9 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     const uint32_t lbase = sbase + L::kTabOff + buf * L::kTabStride;
     const uint64_t members = *reinterpret_cast<const uint32_t*>(
         smem + L::kTabOff + buf * L::kTabStride + kPlainGroups * 256);
+    // the stage's grid step, read before the buffer is released
+    const float stage_q = *reinterpret_cast<const float*>(
+        smem + L::kTabOff + buf * L::kTabStride + kPlainGroups * 256 + 4);
 
     uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
     auto group = [&](uint32_t g, uint32_t ma, uint32_t mb, uint32_t mc) {
@@ -314,12 +339,10 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       const uint32_t lg = lbase + g * 256;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        float v[4];
         // address = table address with its low byte replaced by index byte j
+        // (byte j of ix[q] is person 4j + q)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) v[j] = lds_f32(__byte_perm(ix[q], lg, 0x7650u + j));
-        accp[2 * q] = add_f32x2(accp[2 * q], v[0], v[1]);
-        accp[2 * q + 1] = add_f32x2(accp[2 * q + 1], v[2], v[3]);
+        for (int j = 0; j < 4; ++j) iacc[4 * j + q] += lds_s32(__byte_perm(ix[q], lg, 0x7650u + j));
       }
       // ---- missing counts (code 01 of member rows) ---------------------
       const uint32_t c3 = (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
@@ -359,42 +382,36 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       if (lane == 0) mbar_arrive(empty0 + 8 * buf);
     } else if (lane == 0) {
       const uint32_t old = atom_add_acq_rel(rel0 + 4 * buf, 1u);
-      if (old == L::kWarps - 1) {
+      if (old == active_warps - 1) {
         sts_u32(rel0 + 4 * buf, 0u);
         const uint32_t nxt = st + L::kStages;
         if (nxt < nstages) {
           last_issued[buf] = nxt;
           fence_proxy_async_smem();
           plain_issue_stage<TILE>(&map, a.tables, sbase, buf, tile_x,
-                                  int32_t(r_begin + uint64_t(nxt) * kPlainRows), stage0 + nxt);
+                                  int32_t(r_begin + uint64_t(nxt) * kPlainRows), stage0 + nxt,
+                                  boxes);
         }
       }
     }
 
-    // FP32 sums span one stage (10 lookups, 30 variants) before they are
-    // flushed to FP64: the FP32 rounding error of a sum grows with the square
-    // root of that span, and over 10^6 variants 120-variant spans left sums
-    // within a few 1e-7 of the reference's 1e-6 tolerance.  Byte counters
-    // span eight stages (<= 240 calls per byte) before they are flushed to
-    // 32-bit counts.
+    // The stage's exact integer sums go to FP64 with the stage's grid step;
+    // byte counters span eight stages (<= 240 calls per byte) before they
+    // are flushed to 32-bit counts.
     {
-      const bool counts_too = (st & 7u) == 7u || st + 1 == nstages;
+      const double q = double(stage_q);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (counts_too) {
+      for (int i = 0; i < 16; ++i) {
+        acc64[i] = fma(double(iacc[i]), q, acc64[i]);
+        iacc[i] = 0;
+      }
+      if ((st & 7u) == 7u || st + 1 == nstages) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) cnt[4 * j + q] += (by[q] >> (8 * j)) & 0xFFu;
-          by[q] = 0u;
+        for (int q4 = 0; q4 < 4; ++q4) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) cnt[4 * j + q4] += (by[q4] >> (8 * j)) & 0xFFu;
+          by[q4] = 0u;
         }
-        float lo, hi;
-        unpack_f32x2(accp[2 * q], lo, hi);
-        acc64[q] += double(lo);
-        acc64[4 + q] += double(hi);
-        unpack_f32x2(accp[2 * q + 1], lo, hi);
-        acc64[8 + q] += double(lo);
-        acc64[12 + q] += double(hi);
-        accp[2 * q] = 0ull;
-        accp[2 * q + 1] = 0ull;
       }
     }
   }
