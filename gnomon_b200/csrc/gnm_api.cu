@@ -300,49 +300,32 @@ static void validate_prep(const gnm_prep_view* p) {
 
 
 // ---- plan --------------------------------------------------------------------
-// Launch shape of the plain kernel: people tiles of the kernel's width (the
-// last one often partly populated), and variant-split counts weighted by each
-// tile's populated warps, so that every CTA carries about the same work and
-// the grid fills `mult` x the SMs' CTA slots (1, 2 or 4 CTAs per SM).
-static void plain_shape(gnm_plan* p, uint32_t kernel, double mult) {
-  const uint32_t tile_bytes = plain_tile_bytes(kernel);
-  const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
-  const uint64_t tiles = std::max<uint64_t>(1, (p->bpv + tile_bytes - 1) / tile_bytes);
-  const uint64_t warps = tile_bytes / 128;
-  const uint64_t last_bytes = p->bpv > (tiles - 1) * tile_bytes ? p->bpv - (tiles - 1) * tile_bytes : 1;
-  const double w_last = double(std::min<uint64_t>(warps, (last_bytes + 127) / 128)) / double(warps);
-  const double ctas = double(plain_ctas_per_sm(kernel)) * double(p->num_sms) * mult;
-  const double per_tile = ctas / (double(tiles - 1) + w_last);
-  uint64_t splits = std::max<uint64_t>(1, uint64_t(per_tile));
-  uint64_t last = tiles > 1 ? uint64_t(std::llround(double(splits) * w_last))
-                            : uint64_t(std::max(1.0, ctas));
-  splits = std::min(splits, stages);
-  last = std::min<uint64_t>(std::max<uint64_t>(1, last), stages);
-  p->kernel = kernel;
-  p->split_mult = mult;
-  p->tiles = uint32_t(tiles);
-  p->splits = uint32_t(splits);
-  p->last_splits = uint32_t(last);
-  p->slots = uint32_t(tiles > 1 ? std::max(splits, last) : last);
-}
-
-// A pinned shape: `splits` splits per full tile, the last tile's count scaled
-// by its populated warps (gnm_plan_set_shape).
+// Launch shape of the plain kernel: people tiles of the kernel's width and
+// `splits` variant splits per tile, with tiles x splits about `mult` x the SMs'
+// CTA slots (1, 2 or 4 CTAs per SM).  Every tile, the partly filled last one
+// included, gets the same split count: a CTA's time per stage is set by the
+// dependency chains of each warp's own column, not by how many of its warps
+// hold people, so a last-tile CTA with more stages would finish last (giving
+// it a quarter as many splits for a quarter-filled tile doubled the kernel
+// time on the bandwidth workload).
 static void plain_shape_fixed(gnm_plan* p, uint32_t kernel, uint32_t splits) {
   const uint32_t tile_bytes = plain_tile_bytes(kernel);
   const uint64_t stages = std::max<uint64_t>(1, (p->V + kPlainRows - 1) / kPlainRows);
   const uint64_t tiles = std::max<uint64_t>(1, (p->bpv + tile_bytes - 1) / tile_bytes);
-  const uint64_t warps = tile_bytes / 128;
-  const uint64_t last_bytes = p->bpv > (tiles - 1) * tile_bytes ? p->bpv - (tiles - 1) * tile_bytes : 1;
-  const double w_last = double(std::min<uint64_t>(warps, (last_bytes + 127) / 128)) / double(warps);
   const uint64_t sp = std::min<uint64_t>(std::max<uint32_t>(1, splits), stages);
-  uint64_t last = tiles > 1 ? uint64_t(std::llround(double(sp) * w_last)) : sp;
-  last = std::min<uint64_t>(std::max<uint64_t>(1, last), stages);
   p->kernel = kernel;
   p->tiles = uint32_t(tiles);
   p->splits = uint32_t(sp);
-  p->last_splits = uint32_t(last);
-  p->slots = uint32_t(tiles > 1 ? std::max(sp, last) : last);
+  p->last_splits = uint32_t(sp);
+  p->slots = uint32_t(sp);
+}
+
+static void plain_shape(gnm_plan* p, uint32_t kernel, double mult) {
+  const uint32_t tile_bytes = plain_tile_bytes(kernel);
+  const uint64_t tiles = std::max<uint64_t>(1, (p->bpv + tile_bytes - 1) / tile_bytes);
+  const double ctas = double(plain_ctas_per_sm(kernel)) * double(p->num_sms) * mult;
+  plain_shape_fixed(p, kernel, uint32_t(std::max(1.0, std::floor(ctas / double(tiles)))));
+  p->split_mult = mult;
 }
 
 static void plain_geometry(gnm_plan* p) {

@@ -93,10 +93,10 @@ __device__ __forceinline__ void sts_u32(uint32_t addr, uint32_t v) {
 // such calls in one person and lanes rarely meet on a bank with different
 // addresses.
 //
-// Entries are int32 fixed-point values on a per-stage grid: q = (largest
-// |entry| of the stage) / 2^27, entry = round(exact FP64 sum of the three
-// FP32 terms / q), so |entry| <= 2^27 + 1 and the ten lookups of a stage add
-// up EXACTLY in int32 (|sum| < 2^31).  The kernel converts each stage's
+// Entries are int32 fixed-point values on a per-stage grid: q = 2^(E - 27)
+// with 2^E the smallest power of two >= the stage's largest |entry|, entry =
+// round(exact FP64 sum of the three FP32 terms / q), so |entry| <= 2^27 and
+// the ten lookups of a stage add up EXACTLY in int32 (|sum| < 2^31).  The kernel converts each stage's
 // integer sums to FP64 once (sum * q).  The only rounding before FP64 is the
 // grid itself, <= q/2 per lookup; FP32 running sums lose up to half an ulp of
 // the running partial at every add, which over 10^6 variants came near the
@@ -136,7 +136,11 @@ __global__ void __launch_bounds__(kPlainGroups * 64) gnm_plain_tables(TableArgs 
   float mx = 0.0f;
 #pragma unroll
   for (uint32_t w = 0; w < kPlainGroups * 2; ++w) mx = fmaxf(mx, s_max[w]);
-  const float q = mx > 0.0f ? ldexpf(mx, -27) : 1.0f;   // exact power-of-two scaling
+  // grid step: the power of two 2^(E - 27) with 2^E >= max |entry|, so
+  // |entry / q| <= 2^27 and values with few significant bits stay exact
+  int ex = 0;
+  frexpf(mx, &ex);
+  const float q = mx > 0.0f ? ldexpf(1.0f, ex - 27) : 1.0f;
   uint8_t* tab = a.tables + stage * kPlainTableBytes;
   reinterpret_cast<int32_t*>(tab)[e] = int32_t(__double2ll_rn(v / double(q)));
   if (e < 32) {
