@@ -85,7 +85,7 @@ enum : uint32_t {
   kPlain2048Ws = 2049     // 16 warps + producer warp, 1 CTA per SM
 };
 constexpr uint32_t kPlainKernels[] = {kPlain1024, kPlain512, kPlain1024Ws, kPlain2048Ws};
-constexpr uint32_t kPlainDefaultKernel = kPlain1024;
+constexpr uint32_t kPlainDefaultKernel = kPlain2048Ws;   // fastest on the bandwidth workload
 inline uint32_t plain_tile_bytes(uint32_t kernel) { return kernel & ~1u; }
 inline uint32_t plain_ctas_per_sm(uint32_t kernel) {
   return plain_tile_bytes(kernel) >= 2048 ? 1u : 2048u / plain_tile_bytes(kernel);

@@ -1,33 +1,36 @@
-// gnm_plain.cu — plain (FP32 CUDA-core) scoring path for sm_100a.
+// gnm_plain.cu — plain (FP32 weights, CUDA-core) scoring path for sm_100a.
 //
 // Replaces the reference GPU engine's unpack_plink -> zero -> scatter ->
 // 3x SGEMM -> combine chain (score/cuda_backend.rs:62-218, 2067-2333) for small
 // score counts with one fused accumulate kernel per score column:
 //
 //   * the weights of every 3 consecutive variant rows are folded once per plan
-//     (gnm_plain_tables) into a 64-entry FP32 table: entry (ca, cb, cc) is the
-//     exactly rounded T_a[ca] + T_b[cb] + T_c[cc] with T = {0, -missing
-//     correction, dosage_weight, 2*dosage_weight} (prepare.rs:197-208 folding;
-//     code 00 contributes 0), so decode, effect-allele flip and the
-//     missing-call rule become ONE lookup per person per 3 variants; ten
-//     group tables and a membership word make one 2576-byte stage table;
-//   * packed .bed rows are TMA-staged (cp.async.bulk.tensor into this CTA only) in
-//     [30 rows x 1024 bytes] stages together with their stage table (a 1D bulk
-//     copy on the same mbarrier), three buffers deep (30 x 3 ran 4% faster
-//     than 24 x 4, 18 x 5 and 12 x 8 slower: the per-stage wait, release and
-//     flush are amortised over more rows);
+//     (gnm_plain_tables) into a 64-entry table: entry (ca, cb, cc) is the exact
+//     sum T_a[ca] + T_b[cb] + T_c[cc] with T = {0, -missing correction,
+//     dosage_weight, 2*dosage_weight} (prepare.rs:197-208 folding; code 00
+//     contributes 0), put on the stage's int32 fixed-point grid, so decode,
+//     effect-allele flip and the missing-call rule become ONE lookup per
+//     person per 3 variants; ten group tables, the membership word and the
+//     grid step make one 2576-byte stage table;
+//   * packed .bed rows are TMA-staged (cp.async.bulk.tensor into this CTA
+//     only) in [30 rows x TILE bytes] stages with their stage table (a 1D bulk
+//     copy on the same mbarrier), three buffers deep; TILE is 512, 1024 or
+//     2048 bytes of every row (2048, 4096 or 8192 people), the autotuner's
+//     choice;
 //   * each thread owns one 32-bit word column = 16 people; per 3 rows it
 //     transposes the 2-bit codes into per-person 6-bit indices (one byte each,
 //     pre-scaled by 4) with shift/mask ops and turns each byte into a
 //     shared-memory address with one byte permute;
 //   * warps run the stages independently: a warp waits only for the stage's
-//     TMA, and releases the buffer through a shared counter whose last arriver
-//     issues the TMA of the stage three ahead — no CTA-wide barrier per stage;
+//     TMA; it releases the buffer either through a shared counter whose last
+//     arriver issues the TMA of the stage three ahead, or (producer-warp
+//     kernels) by arriving on a release mbarrier that a producer warp waits on
+//     before it issues that TMA — no CTA-wide barrier per stage;
 //   * missing calls (code 01) are counted with SWAR bit tricks on the raw row
 //     words (x & ~(x>>1) & member_mask, three rows summed with one add);
-//   * FP32 partial sums (packed pairs, add.rn.f32x2) cover one 30-variant
-//     stage and are flushed to FP64 registers; variant splits write FP64 partials that
-//     gnm_finalize reduces in a fixed order (deterministic) and gathers
+//   * a stage's ten lookups per person add up exactly in int32 and reach FP64
+//     once per stage (sum x grid step); variant splits write FP64 partials
+//     that gnm_finalize reduces in a fixed order (deterministic) and gathers
 //     through output_idx_to_fam_idx, adding the FP64 baseline
 //     (pipeline.rs:1739-1775).
 #include <cstdint>
@@ -65,6 +68,13 @@ struct PlainSmem {
   // Each 64-entry group table starts on a 256-byte boundary, so a lookup
   // address is the table address with its low byte replaced by the index.
 };
+
+// Multipliers for left shifts and adds written as integer multiply-adds: held
+// in constant memory, unknown at compile time, they make the compiler issue
+// IMAD on the FMA pipe instead of shift / add on the integer ALU pipe, which
+// the index transposes, byte permutes and masks already keep busy (the kernel
+// is bound by that pipe).
+__constant__ uint32_t c_mul[5] = {2u, 4u, 16u, 64u, 1u};
 
 __device__ __forceinline__ int32_t lds_s32(uint32_t addr) {
   int32_t v;
@@ -332,13 +342,13 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       // enters with its code bits swapped (see the table layout above)
       const uint32_t ya = xa ^ (xc & 0x55555555u);
       const uint32_t yb = xb ^ (xc & 0x55555555u);
-      const uint32_t xs = ((xc >> 1) & 0x55555555u) | ((xc << 1) & 0xAAAAAAAAu);
-      const uint32_t E = (ya & 0x33333333u) | ((yb << 2) & 0xCCCCCCCCu);
+      const uint32_t xs = ((xc >> 1) & 0x55555555u) | ((xc * c_mul[0]) & 0xAAAAAAAAu);
+      const uint32_t E = (ya & 0x33333333u) | ((yb * c_mul[1]) & 0xCCCCCCCCu);
       const uint32_t O = ((ya >> 2) & 0x33333333u) | (yb & 0xCCCCCCCCu);
       uint32_t ix[4];
-      ix[0] = ((E << 2) & 0x3C3C3C3Cu) | ((xs << 6) & 0xC0C0C0C0u);
-      ix[1] = ((O << 2) & 0x3C3C3C3Cu) | ((xs << 4) & 0xC0C0C0C0u);
-      ix[2] = ((E >> 2) & 0x3C3C3C3Cu) | ((xs << 2) & 0xC0C0C0C0u);
+      ix[0] = ((E * c_mul[1]) & 0x3C3C3C3Cu) | ((xs * c_mul[3]) & 0xC0C0C0C0u);
+      ix[1] = ((O * c_mul[1]) & 0x3C3C3C3Cu) | ((xs * c_mul[2]) & 0xC0C0C0C0u);
+      ix[2] = ((E >> 2) & 0x3C3C3C3Cu) | ((xs * c_mul[1]) & 0xC0C0C0C0u);
       ix[3] = ((O >> 2) & 0x3C3C3C3Cu) | (xs & 0xC0C0C0C0u);
       const uint32_t lg = lbase + g * 256;
 #pragma unroll
@@ -346,12 +356,14 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
         // address = table address with its low byte replaced by index byte j
         // (byte j of ix[q] is person 4j + q)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) iacc[4 * j + q] += lds_s32(__byte_perm(ix[q], lg, 0x7650u + j));
+        for (int j = 0; j < 4; ++j)
+          iacc[4 * j + q] = int32_t(uint32_t(lds_s32(__byte_perm(ix[q], lg, 0x7650u + j))) *
+                                        c_mul[4] + uint32_t(iacc[4 * j + q]));
       }
       // ---- missing counts (code 01 of member rows) ---------------------
       const uint32_t c3 = (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
-      ev += c3 & 0x33333333u;
-      od += (c3 >> 2) & 0x33333333u;
+      ev = (c3 & 0x33333333u) * c_mul[4] + ev;
+      od = ((c3 >> 2) & 0x33333333u) * c_mul[4] + od;
       if ((g % 5) == 4 || g == kPlainGroups - 1) {
         by[0] += ev & 0x0F0F0F0Fu;
         by[2] += (ev >> 4) & 0x0F0F0F0Fu;
