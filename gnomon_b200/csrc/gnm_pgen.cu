@@ -9,14 +9,16 @@
 // the GPU, straight into the engines' row layout.
 //
 // Supported: storage modes 0x02 (fixed-width hard calls) and 0x10 / 0x11
-// (variable-width) with biallelic records whose main track is type 0 (2-bit),
+// (variable-width) with biallelic records, with or without phase and dosage
+// tracks (dosages fill missing hard calls, see gnm_pgen_dosage), whose main
+// track is type 0 (2-bit),
 // 1 (two categories as a bit array + difflist), 2 / 3 (LD-compressed against
 // the most recent non-LD record of the same 2^16-variant block; 3 swaps REF and
 // ALT homozygotes after the patch) or 4 / 6 / 7 (all hom REF / hom ALT /
 // missing + difflist) — shared/adapt_plink2.rs:2237-2257, 2574-2666.  Phase
 // tracks follow the main track and do not change hard calls.  Records with
-// multiallelic or dosage tracks are rejected (the reference projects or
-// coerces them; this decoder does not).
+// multiallelic tracks are rejected (the reference projects them onto each
+// ALT; this decoder does not).
 //
 // Layout of the work: the bijection category -> .bed code lets every step
 // run on .bed codes directly.  A decode is two launches over the same
@@ -71,6 +73,7 @@ struct PgArgs {
   const uint32_t* vids;
   const uint32_t* arow;
   uint32_t* err;               // [0] error bits, [1] first bad variant (atomicMin)
+  uint32_t any_dosage;         // some record carries a dosage track
 };
 
 // Row i of a decode: an output row, or a scratch row past the output's end.
@@ -485,6 +488,289 @@ __global__ void __launch_bounds__(kPgThreads, 8) gnm_pgen_ld(PgArgs a) {
 }
 
 
+// ---- dosage tracks ---------------------------------------------------------------
+// A biallelic record may carry, after its main track (and its phase track,
+// vrtype bit 4), a dosage track (bits 5-6, shared/adapt_plink2.rs:2416-2520):
+// u16 ALT dosages (16384 per allele copy, 65535 = none) for a sample list
+// (bit 5: an id-only difflist), for every sample (bit 6), or for the samples
+// of a presence bit array (bits 5 + 6); bit 7 adds a phased-dosage track
+// after it, which does not change hard calls.  Where the hard call is missing,
+// the dosage becomes the nearest whole allele count if it lies within 0.10 of
+// it (f32 arithmetic, :3211-3255), else the call stays missing.  Hard calls are
+// never overridden; samples are diploid (the .pvar/.psam that give the
+// reference its ploidy are not read here).  The overlay runs after both decode
+// kernels, on whole rows, so LD records still read their anchors' raw calls.
+
+// .bed code of a u16 diploid ALT dosage, or 01 (missing) when none applies.
+__device__ __forceinline__ uint32_t dosage_code(uint32_t v) {
+  if (v == 65535u) return 1u;
+  const float ds = float(v) * (1.0f / 32768.0f) * 2.0f;
+  // nearest of 0, 1, 2 (first wins a tie, as the reference scans them in order)
+  const float d0 = fabsf(ds), d1 = fabsf(ds - 1.0f), d2 = fabsf(ds - 2.0f);
+  uint32_t best = 0;
+  float bd = d0;
+  if (d1 < bd) { best = 1; bd = d1; }
+  if (d2 < bd) { best = 2; bd = d2; }
+  if (!(bd <= 0.10f)) return 1u;
+  return best == 2 ? 0u : (best == 1 ? 2u : 3u);   // ALT count 2 -> 00, 1 -> 10, 0 -> 11
+}
+
+// Sum over the 256 threads of the CTA (every thread calls it).
+__device__ __forceinline__ uint32_t cta_sum(uint32_t x, uint32_t* sh) {
+#pragma unroll
+  for (uint32_t d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, d);
+  __syncthreads();
+  if ((threadIdx.x & 31u) == 0) sh[threadIdx.x >> 5] = x;
+  __syncthreads();
+  uint32_t t = 0;
+#pragma unroll
+  for (uint32_t w = 0; w < kPgWarps; ++w) t += sh[w];
+  return t;
+}
+
+// Exclusive prefix over the 256 threads of the CTA; `total` gets the sum.
+__device__ __forceinline__ uint32_t cta_exclusive(uint32_t x, uint32_t* sh, uint32_t& total) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t incl = x;
+#pragma unroll
+  for (uint32_t d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= d) incl += y;
+  }
+  __syncthreads();
+  if (lane == 31) sh[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0;
+  total = 0;
+#pragma unroll
+  for (uint32_t w = 0; w < kPgWarps; ++w) {
+    if (w < warp) before += sh[w];
+    total += sh[w];
+  }
+  return before + incl - x;
+}
+
+// Byte just past a difflist at `cur` (ids_only: no 2-bit values, the dosage
+// track's sample list).  Every thread returns it; false = the list overruns
+// the record.  Group byte lengths are summed by the CTA, the last group's
+// deltas walked by thread 0.
+__device__ bool cta_difflist_end(const Rec& r, uint32_t cur, uint64_t n, bool ids_only,
+                                 uint32_t* sh, uint32_t& end) {
+  uint64_t l = 0;
+  bool ok = r.varint(cur, l) && l <= n;
+  if (!ok) return false;
+  if (l == 0) {
+    end = cur;
+    return true;
+  }
+  const uint32_t len = uint32_t(l);
+  const uint32_t groups = (len + 63) / 64;
+  const uint32_t wid = n <= (1u << 8) ? 1 : n <= (1u << 16) ? 2 : n <= (1u << 24) ? 3 : 4;
+  const uint64_t glen_at = uint64_t(cur) + uint64_t(groups) * wid;
+  const uint64_t deltas = glen_at + groups - 1 + (ids_only ? 0 : (len + 3) / 4);
+  if (deltas > r.len) return false;
+  uint32_t part = 0;
+  for (uint32_t g = threadIdx.x; g + 1 < groups; g += blockDim.x)
+    part += uint32_t(r.p[glen_at + g]) + 63u;
+  const uint32_t before_last = cta_sum(part, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t at = uint32_t(min(deltas + before_last, uint64_t(0xFFFFFFFFu)));
+    const uint32_t count = len - 64u * (groups - 1);
+    bool good = deltas + before_last <= r.len;
+    for (uint32_t e = 1; good && e < count; ++e) {
+      uint64_t d;
+      good = r.varint(at, d);
+    }
+    sh[kPgWarps] = good ? at : 0xFFFFFFFFu;
+  }
+  __syncthreads();
+  end = sh[kPgWarps];
+  __syncthreads();
+  return end != 0xFFFFFFFFu;
+}
+
+// One CTA per output row; rows whose record has no dosage track return at
+// once.  Runs after gnm_pgen_direct and gnm_pgen_ld have written the rows.
+__global__ void __launch_bounds__(kPgThreads) gnm_pgen_dosage(PgArgs a) {
+  __shared__ uint32_t sh[kPgWarps + 2];
+  const uint32_t i = blockIdx.x;
+  if (i >= a.count) return;
+  const uint32_t v = variant_at(a, i);
+  const uint32_t t = a.types[v];
+  if (!(t & 0x60u)) return;
+  const Rec r{a.pgen + a.offsets[v], a.lens[v]};
+  const uint64_t n = a.n;
+  const uint64_t bpv = (n + 3) / 4;
+  uint8_t* row = a.rows + uint64_t(i) * a.pitch;
+  uint32_t* row32 = reinterpret_cast<uint32_t*>(row);
+  const uint64_t words = (bpv + 3) / 4;
+  auto bad = [&]() {
+    if (threadIdx.x == 0) flag(a, kPgErrBounds, v);
+  };
+
+  // ---- the main track's end ----
+  const uint32_t kind = t & 7u;
+  uint32_t cur = 0;
+  if (kind == 0) {
+    cur = uint32_t(bpv);
+  } else {
+    const uint32_t start = kind == 1 ? uint32_t(1 + (n + 7) / 8) : 0u;
+    if (!cta_difflist_end(r, start, n, false, sh, cur)) return bad();
+  }
+  if (cur > r.len) return bad();
+
+  // ---- the phase track: one flag bit, per-het presence bits padded to a
+  // byte when the flag is set, one bit per phased het ----
+  if (t & 0x10u) {
+    if (cur >= r.len) return bad();
+    uint32_t hets = 0;   // het calls of the main track (.bed code 10)
+    for (uint64_t w = threadIdx.x; w < words; w += blockDim.x) {
+      uint32_t x = row32[w];
+      const uint64_t b0 = 4 * w;
+      if (b0 + 4 > bpv) x &= (1u << (8 * (bpv - b0))) - 1u;   // bytes past the row
+      hets += __popc((x >> 1) & ~x & 0x55555555u);
+    }
+    const uint32_t h = cta_sum(hets, sh);
+    uint64_t bits = 1 + uint64_t(h);
+    if (r.p[cur] & 1u) {
+      // presence bits 1 .. h, then one phase bit per present het
+      uint32_t present = 0;
+      const uint64_t nbytes = (1 + uint64_t(h) + 7) / 8;
+      if (cur + nbytes > r.len) return bad();
+      for (uint64_t b = threadIdx.x; b < nbytes; b += blockDim.x) {
+        uint32_t byte = r.p[cur + b];
+        if (b == 0) byte &= ~1u;
+        const uint64_t hi = 1 + uint64_t(h) - 8 * b;   // bits of this byte in range
+        if (hi < 8) byte &= (1u << hi) - 1u;
+        present += __popc(byte);
+      }
+      const uint32_t phased = cta_sum(present, sh);
+      bits = (bits + 7) / 8 * 8 + phased;
+    }
+    const uint64_t next = cur + (bits + 7) / 8;
+    if (next > r.len) return bad();
+    cur = uint32_t(next);
+  }
+
+  // ---- the dosage track ----
+  const bool b5 = t & 0x20u, b6 = t & 0x40u;
+  if (b6 && !b5) {
+    // dense: every sample's value
+    if (uint64_t(cur) + 2 * n > r.len) return bad();
+    const uint8_t* vals = r.p + cur;
+    for (uint64_t w = threadIdx.x; w < words; w += blockDim.x) {
+      const uint32_t x = row32[w];
+      uint32_t y = x;
+#pragma unroll 4
+      for (uint32_t k = 0; k < 16; ++k) {
+        const uint64_t smp = 16 * w + k;
+        if (smp >= n) break;
+        if (((x >> (2 * k)) & 3u) != 1u) continue;
+        const uint32_t dv = uint32_t(vals[2 * smp]) | (uint32_t(vals[2 * smp + 1]) << 8);
+        y = (y & ~(3u << (2 * k))) | (dosage_code(dv) << (2 * k));
+      }
+      if (y != x) row32[w] = y;
+    }
+    return;
+  }
+  if (b5 && b6) {
+    // presence bit array, then the values of the present samples in order
+    const uint64_t pbytes = (n + 7) / 8;
+    if (uint64_t(cur) + pbytes > r.len) return bad();
+    const uint8_t* pres = r.p + cur;
+    const uint64_t vals_at = uint64_t(cur) + pbytes;
+    uint32_t base = 0;   // present samples before this chunk of words
+    for (uint64_t w0 = 0; w0 < words; w0 += blockDim.x) {
+      const uint64_t w = w0 + threadIdx.x;
+      uint32_t mask = 0;   // presence bits of the word's 16 samples
+      if (w < words) {
+        for (uint32_t k = 0; k < 16; ++k) {
+          const uint64_t smp = 16 * w + k;
+          if (smp < n && ((pres[smp >> 3] >> (smp & 7)) & 1u)) mask |= 1u << k;
+        }
+      }
+      uint32_t total = 0;
+      const uint32_t before = base + cta_exclusive(__popc(mask), sh, total);
+      if (w < words && mask) {
+        const uint32_t x = row32[w];
+        uint32_t y = x, rank = 0;
+        for (uint32_t k = 0; k < 16; ++k) {
+          if (!((mask >> k) & 1u)) continue;
+          const uint64_t at = vals_at + 2 * uint64_t(before + rank);
+          ++rank;
+          if (((x >> (2 * k)) & 3u) != 1u) continue;
+          if (at + 2 > r.len) {
+            flag(a, kPgErrBounds, v);
+            break;
+          }
+          const uint32_t dv = uint32_t(r.p[at]) | (uint32_t(r.p[at + 1]) << 8);
+          y = (y & ~(3u << (2 * k))) | (dosage_code(dv) << (2 * k));
+        }
+        if (y != x) row32[w] = y;
+      }
+      base += total;
+    }
+    if (threadIdx.x == 0 && vals_at + 2 * uint64_t(base) > r.len) flag(a, kPgErrBounds, v);
+    return;
+  }
+  // b5 alone: an id-only difflist, then one value per listed sample
+  uint32_t list_end = 0;
+  if (!cta_difflist_end(r, cur, n, true, sh, list_end)) return bad();
+  uint64_t l = 0;
+  uint32_t c2 = cur;
+  r.varint(c2, l);
+  if (l == 0) return;
+  const uint32_t len = uint32_t(l);
+  if (uint64_t(list_end) + 2 * uint64_t(len) > r.len) return bad();
+  const uint32_t groups = (len + 63) / 64;
+  const uint32_t wid = n <= (1u << 8) ? 1 : n <= (1u << 16) ? 2 : n <= (1u << 24) ? 3 : 4;
+  const uint32_t first_at = c2;
+  const uint32_t glen_at = first_at + groups * wid;
+  const uint32_t deltas0 = glen_at + groups - 1;
+  auto first_id = [&](uint32_t g) {
+    uint64_t id = 0;
+    for (uint32_t k = 0; k < wid; ++k) id |= uint64_t(r.p[first_at + g * wid + k]) << (8 * k);
+    return id;
+  };
+  uint32_t base = deltas0;   // first delta byte of this chunk's first group
+  bool broken = false;
+  for (uint32_t g0 = 0; g0 < groups; g0 += blockDim.x) {
+    const uint32_t g = g0 + threadIdx.x;
+    const uint32_t mine = g + 1 < groups ? uint32_t(r.p[glen_at + g]) + 63u : 0u;
+    uint32_t total = 0;
+    uint32_t at = base + cta_exclusive(g < groups ? mine : 0u, sh, total);
+    if (g < groups) {
+      const uint32_t count = g + 1 < groups ? 64u : len - 64u * (groups - 1);
+      const uint32_t start = at;
+      uint64_t id = first_id(g);
+      for (uint32_t e = 0; e < count; ++e) {
+        if (e > 0) {
+          uint64_t d = 0;
+          if (!r.varint(at, d) || d == 0) {
+            broken = true;
+            break;
+          }
+          id += d;
+        }
+        if (id >= n) continue;
+        const uint32_t w = uint32_t(id >> 4), sh2 = 2 * uint32_t(id & 15u);
+        if (((row32[w] >> sh2) & 3u) != 1u) continue;
+        const uint64_t vat = uint64_t(list_end) + 2 * (64 * uint64_t(g) + e);
+        const uint32_t dv = uint32_t(r.p[vat]) | (uint32_t(r.p[vat + 1]) << 8);
+        const uint32_t code = dosage_code(dv);
+        // field is 01: xor it to the new code (ids rise, so no other lane
+        // writes this field; fields of one word commute)
+        if (code != 1u) atomicXor(row32 + w, (1u ^ code) << sh2);
+      }
+      if (!broken && g + 1 < groups && (at != start + mine || id >= first_id(g + 1)))
+        broken = true;   // group length mismatch, or ids not rising into the next group
+    }
+    base += total;
+  }
+  if (broken) flag(a, kPgErrBounds, v);
+}
+
 // ---- host ----------------------------------------------------------------------
 
 struct PgenIndex {
@@ -558,9 +844,12 @@ PgenIndex parse_pgen(const uint8_t* d, uint64_t len) {
   for (uint64_t v = 0; v < m; ++v) {
     if (ix.offsets[v] + ix.lens[v] > len || ix.offsets[v] > len)
       fail(GNM_ERR_IO, "truncated .pgen: record " + std::to_string(v) + " lies past the end");
-    if (ix.types[v] & 0xE8u)
+    if (ix.types[v] & 0x08u)
       fail(GNM_ERR_INVALID, "variant " + std::to_string(v) +
-                                ": multiallelic or dosage tracks are not supported");
+                                ": multiallelic records are not supported");
+    if ((ix.types[v] & 0x80u) && !(ix.types[v] & 0x60u))
+      fail(GNM_ERR_IO, "variant " + std::to_string(v) +
+                           ": phased dosage track without a dosage track");
     const uint32_t kind = ix.types[v] & 7u;
     if (kind == 5) fail(GNM_ERR_INVALID, "variant " + std::to_string(v) + ": main-track type 5");
   }
@@ -638,6 +927,8 @@ gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device) {
   a.lens = static_cast<const uint32_t*>(up(ix.lens.data(), m * 4, ".pgen index"));
   a.types = static_cast<const uint8_t*>(up(ix.types.data(), m, ".pgen index"));
   a.anchor_of = static_cast<const uint32_t*>(up(anchor_of.data(), m * 4, ".pgen index"));
+  a.any_dosage = 0u;
+  for (uint64_t v = 0; v < m && !a.any_dosage; ++v) a.any_dosage = (ix.types[v] & 0x60u) ? 1u : 0u;
   const uint32_t init_err[2] = {0u, 0xFFFFFFFFu};
   a.err = static_cast<uint32_t*>(up(init_err, 8, ".pgen error word"));
   a.spitch = ((ix.samples + 3) / 4 + 15) / 16 * 16;
@@ -679,6 +970,10 @@ static void launch_decode(const PgArgs& a, cudaStream_t s) {
   check_cuda(cudaGetLastError(), "pgen decode launch");
   gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen LD decode launch");
+  if (a.any_dosage) {   // missing hard calls take their dosages, on the finished rows
+    gnm_pgen_dosage<<<a.count, kPgThreads, 0, s>>>(a);
+    check_cuda(cudaGetLastError(), "pgen dosage launch");
+  }
 }
 
 // Decode the listed variants (any order) into consecutive rows.  An LD

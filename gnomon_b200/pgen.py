@@ -7,10 +7,12 @@ A1 = ALT dosage.  Here that decode runs on the device
 (``gnm_pgen_decode_device``), writing rows straight into HBM where
 ``DevicePlan`` reads them; the file's bytes cross PCIe once, compressed.
 
-Supported: storage modes 0x02 and 0x10 / 0x11 with biallelic hard-call
-records (main-track types 0-4, 6, 7; phase tracks are skipped).  Records
-with multiallelic or dosage tracks are rejected with ``GNM_ERR_INVALID``,
-truncated or malformed files with ``GNM_ERR_IO``.
+Supported: storage modes 0x02 and 0x10 / 0x11 with biallelic records
+(main-track types 0-4, 6, 7; phase tracks are skipped; a dosage track fills
+missing hard calls with the nearest allele count within 0.10, as the
+reference's virtual .bed does, samples taken as diploid).  Records with
+multiallelic tracks are rejected with ``GNM_ERR_INVALID``, truncated or
+malformed files with ``GNM_ERR_IO``.
 """
 from __future__ import annotations
 

@@ -317,6 +317,102 @@ def _pgen_file(n: int, types, recs) -> bytes:
     return bytes(head) + b"".join(recs)
 
 
+def _difflist_id_bytes(ids: np.ndarray, n: int) -> bytes:
+    """An id-only difflist (a dosage track's sample list): varint length,
+    first ids, group byte lengths minus 63, base-128 deltas."""
+    ids = np.asarray(ids, np.int64)
+    length = len(ids)
+    out = bytearray(_varint_bytes(length))
+    if length == 0:
+        return bytes(out)
+    wid = 1 if n <= 1 << 8 else 2 if n <= 1 << 16 else 3 if n <= 1 << 24 else 4
+    groups = (length + 63) // 64
+    out += b"".join(int(f).to_bytes(wid, "little") for f in ids[::64])
+    in_group = np.arange(length) % 64 != 0
+    deltas = np.diff(ids, prepend=0)[in_group]
+    vbytes, nb = _varints(deltas)
+    group_of = (np.arange(length) // 64)[in_group]
+    gbytes = np.bincount(group_of, weights=nb, minlength=groups).astype(np.int64)
+    out += (gbytes[:groups - 1] - 63).astype(np.uint8).tobytes()
+    out += vbytes.tobytes()
+    return bytes(out)
+
+
+def _phase_track(cats_v: np.ndarray, rng, partial: bool) -> bytes:
+    """A phase track for the hets of one variant: all hets phased (flag 0),
+    or (partial) a presence bit per het, padded to a byte, then one phase bit
+    per present het."""
+    h = int(np.count_nonzero(cats_v == 1))
+    if not partial:
+        bits = np.concatenate([[0], rng.integers(0, 2, h)]).astype(np.uint8)
+    else:
+        pres = rng.integers(0, 2, h).astype(np.uint8)
+        head = np.concatenate([[1], pres]).astype(np.uint8)
+        head = np.concatenate([head, np.zeros((-len(head)) % 8, np.uint8)])
+        bits = np.concatenate([head, rng.integers(0, 2, int(pres.sum()))]).astype(np.uint8)
+    return np.packbits(bits, bitorder="little").tobytes()
+
+
+def _dosage_track(dos_v: np.ndarray, kind: str, phased: bool, rng) -> tuple[int, bytes]:
+    """(type bits, track bytes) of one variant's u16 ALT dosages; 65535 marks
+    samples without a value.  kind: "list" (id difflist, bit 5), "dense"
+    (every sample, bit 6) or "bits" (presence bit array, bits 5+6); phased
+    adds a phased-dosage track (bit 7)."""
+    n = len(dos_v)
+    present = np.nonzero(dos_v != 65535)[0]
+    if kind == "dense":
+        bits, body, d = 0b0100_0000, dos_v.astype("<u2").tobytes(), n
+    elif kind == "list":
+        bits = 0b0010_0000
+        body = _difflist_id_bytes(present, n) + dos_v[present].astype("<u2").tobytes()
+        d = len(present)
+    elif kind == "bits":
+        bits = 0b0110_0000
+        mask = np.zeros(n, np.uint8)
+        mask[present] = 1
+        body = np.packbits(mask, bitorder="little").tobytes() + dos_v[present].astype("<u2").tobytes()
+        d = len(present)
+    else:
+        raise ValueError(kind)
+    if phased:
+        bits |= 0b1000_0000
+        if kind == "dense":
+            body += rng.integers(0, 65535, n).astype("<u2").tobytes()
+        else:
+            pres = rng.integers(0, 2, d).astype(np.uint8)
+            body += np.packbits(pres, bitorder="little").tobytes()
+            body += rng.integers(0, 65535, int(pres.sum())).astype("<u2").tobytes()
+    return bits, body
+
+
+def encode_pgen_tracks(cats: np.ndarray, dosage: np.ndarray | None = None,
+                       dosage_kind: str | list = "list", phase: str | None = None,
+                       phased_dosage: bool = False, seed: int = 0) -> bytes:
+    """encode_pgen plus the tracks that follow a record's main track: a phase
+    track (phase = "all" or "partial") and a dosage track holding
+    ``dosage[v]`` (u16 ALT dosages, 16384 per allele copy, 65535 = no value)
+    of each variant that has a value, as a sample list, dense array or
+    presence bit array (``dosage_kind``, one for all variants or one per
+    variant)."""
+    cats = np.asarray(cats, np.uint8)
+    V, n = cats.shape
+    rng = np.random.default_rng(seed)
+    types, recs = _pgen_records(cats)
+    types, recs = list(types), list(recs)
+    for v in range(V):
+        body = recs[v]
+        if phase is not None:
+            body = body + _phase_track(cats[v], rng, phase == "partial")
+            types[v] |= 0b0001_0000
+        if dosage is not None and np.any(dosage[v] != 65535):
+            kind = dosage_kind if isinstance(dosage_kind, str) else dosage_kind[v]
+            bits, track = _dosage_track(np.asarray(dosage[v], np.uint16), kind, phased_dosage, rng)
+            body = body + track
+            types[v] |= bits
+        recs[v] = body
+    return _pgen_file(n, types, recs)
+
+
 def encode_pgen(cats: np.ndarray, repeats: int = 1) -> bytes:
     """Genotype categories [V][N] (0 hom REF, 1 het, 2 hom ALT, 3 missing) ->
     a variable-width (mode 0x10) .pgen, 8-bit record types, 4-byte lengths.

@@ -21,8 +21,14 @@ of shared/adapt_plink2.rs). The restated steps are:
 * packing into .bed codes, with padding fields set to the missing code
   (:1136-1158).
 
-Records with multiallelic (vrtype bit 3) or dosage (bits 5-6) tracks are
-rejected. The reference also reads those tracks; this decoder does not.
+* the dosage tracks of biallelic records (bits 5-7, :2416-2520): where the
+  hard call is missing, the record's ALT dosage (u16, 16384 per allele copy)
+  becomes the nearest whole allele count when it lies within 0.10 of it
+  (f32 arithmetic, :3211-3255), else the call stays missing; hard calls are
+  never overridden.  Samples are treated as diploid (the reference takes
+  ploidy from the .pvar/.psam, which this decoder does not read).
+
+Records with multiallelic tracks (vrtype bit 3) are rejected.
 Difflists whose sample ids do not rise strictly are rejected as malformed
 (PLINK 2 writes strictly rising ids; the reference would apply such a list in
 order, later entries winning).
@@ -101,6 +107,102 @@ def _difflist(buf, cur, n):
     return ids, vals, cur
 
 
+def _difflist_ids(buf, cur, n):
+    """An id-only difflist (the dosage track's sample list, :1824-1918):
+    -> (ids, cursor after the list)."""
+    length, cur = _varint(buf, cur)
+    if length == 0:
+        return [], cur
+    groups = (length + 63) // 64
+    w = _sid_bytes(n)
+    first = []
+    for _ in range(groups):
+        if cur + w > len(buf):
+            raise PgenError("EOF in difflist first ids")
+        first.append(int.from_bytes(buf[cur:cur + w], "little"))
+        cur += w
+    glen = [b + 63 for b in buf[cur:cur + groups - 1]]
+    cur += groups - 1
+    ids = []
+    for g in range(groups):
+        count = 64 if g < groups - 1 else length - 64 * (groups - 1)
+        start = cur
+        ids.append(first[g])
+        for _ in range(count - 1):
+            d, cur = _varint(buf, cur)
+            ids.append(ids[-1] + d)
+        if g < groups - 1 and cur - start != glen[g]:
+            raise PgenError("difflist group byte-length mismatch")
+    return ids, cur
+
+
+DOSAGE_TOLERANCE = np.float32(0.10)
+
+
+def dosage_to_hardcall(v: int) -> int:
+    """u16 ALT dosage of a diploid sample -> allele count 0/1/2, or 255 when
+    missing (65535) or farther than 0.10 from every whole count
+    (shared/adapt_plink2.rs:3211-3255, f32 arithmetic)."""
+    if v == 65535:
+        return 255
+    ds = np.float32(v) * np.float32(1.0 / 32768.0) * np.float32(2.0)
+    best, best_d = 255, np.float32(np.inf)
+    for c in range(3):
+        d = np.float32(abs(ds - np.float32(c)))
+        if d < best_d:
+            best, best_d = c, d
+    return best if best_d <= DOSAGE_TOLERANCE else 255
+
+
+def _skip_phase(rec, cur, cats):
+    """Cursor after a phase track (:2362-2413): one flag bit, then (flag set)
+    one presence bit per het padded to a byte, then one bit per phased het."""
+    if cur >= len(rec):
+        raise PgenError("EOF in phase header")
+    h = int(np.count_nonzero(cats == 1))
+    bit = 1
+    phased = h
+    if rec[cur] & 1:
+        pres = np.unpackbits(np.frombuffer(rec, np.uint8, (1 + h + 7) // 8, cur),
+                             bitorder="little")[1:1 + h] if h else np.zeros(0, np.uint8)
+        if len(pres) < h:
+            raise PgenError("EOF in phase presence")
+        phased = int(pres.sum())
+        bit = 1 + h
+        bit += (-bit) % 8
+    bit += phased
+    nbytes = (bit + 7) // 8
+    if cur + nbytes > len(rec):
+        raise PgenError("EOF in phase track")
+    return cur + nbytes
+
+
+def _dosage_overlay(rec, cur, t, n, cats):
+    """Missing hard calls take their dosage's nearest allele count (:2416-2520)."""
+    b5, b6 = bool(t & 0b0010_0000), bool(t & 0b0100_0000)
+    if b5 and not b6:
+        ids, cur = _difflist_ids(rec, cur, n)
+    elif b6 and not b5:
+        ids = list(range(n))
+    else:
+        if cur + (n + 7) // 8 > len(rec):
+            raise PgenError("EOF in dosage presence bits")
+        bits = np.unpackbits(np.frombuffer(rec, np.uint8, (n + 7) // 8, cur),
+                             bitorder="little")[:n]
+        ids = list(np.nonzero(bits)[0])
+        cur += (n + 7) // 8
+    if cur + 2 * len(ids) > len(rec):
+        raise PgenError("EOF in dosage values")
+    vals = np.frombuffer(rec, "<u2", len(ids), cur)
+    out = cats.copy()
+    for sid, v in zip(ids, vals):
+        if sid < n and out[sid] == 3:
+            hc = dosage_to_hardcall(int(v))
+            if hc != 255:
+                out[sid] = hc
+    return out
+
+
 def parse_header(data: bytes):
     """-> dict(mode, variants, samples, offsets[V], types[V], lens[V])."""
     if len(data) < 12 or data[0] != 0x6C or data[1] != 0x1B:
@@ -152,12 +254,15 @@ def parse_header(data: bytes):
 
 
 def _main_track(rec, kind, n, anchor):
+    """-> (categories [n], cursor after the main track)."""
     cats = np.full(n, 3, np.uint8)
     cur = 0
     if kind == 0:
+        if len(rec) < (n + 3) // 4:
+            raise PgenError("EOF in 2-bit array")
         raw = np.frombuffer(rec, np.uint8, (n + 3) // 4)
         c = np.stack([(raw >> (2 * s)) & 3 for s in range(4)], 1).reshape(-1)[:n]
-        return c.astype(np.uint8)
+        return c.astype(np.uint8), (n + 3) // 4
     if kind == 1:
         pairs = {1: (0, 1), 2: (0, 2), 3: (0, 3), 5: (1, 2), 6: (1, 3), 9: (2, 3)}
         if rec[0] not in pairs:
@@ -173,13 +278,13 @@ def _main_track(rec, kind, n, anchor):
         cats[:] = {4: 0, 6: 2, 7: 3}[kind]
     else:
         raise PgenError(f"unsupported main-track type {kind}")
-    ids, vals, _ = _difflist(rec, cur, n)
+    ids, vals, cur = _difflist(rec, cur, n)
     for i, v in zip(ids, vals):
         if i < n:
             cats[i] = v
     if kind == 3:
         cats = np.where(cats == 0, 2, np.where(cats == 2, 0, cats)).astype(np.uint8)
-    return cats
+    return cats, cur
 
 
 def decode_to_bed(data: bytes) -> np.ndarray:
@@ -191,17 +296,23 @@ def decode_to_bed(data: bytes) -> np.ndarray:
     anchor, anchor_idx = None, -1
     for v in range(m):
         t = int(h["types"][v])
-        if t & 0b1110_1000:
-            raise PgenError(f"variant {v}: multiallelic or dosage tracks are not supported")
+        if t & 0b0000_1000:
+            raise PgenError(f"variant {v}: multiallelic tracks are not supported")
+        if (t & 0b1000_0000) and not (t & 0b0110_0000):
+            raise PgenError(f"variant {v}: phased dosage track without a dosage track")
         kind = t & 7
         rec = data[int(h["offsets"][v]):int(h["offsets"][v]) + int(h["lens"][v])]
         if kind in (2, 3):
             if anchor is None or (anchor_idx >> 16) != (v >> 16):
                 raise PgenError(f"variant {v}: LD-compressed record without an anchor in its block")
-            cats = _main_track(rec, kind, n, anchor)
+            cats, cur = _main_track(rec, kind, n, anchor)
         else:
-            cats = _main_track(rec, kind, n, None)
-            anchor, anchor_idx = cats, v
+            cats, cur = _main_track(rec, kind, n, None)
+            anchor, anchor_idx = cats, v   # anchors are the raw main-track categories
+        if t & 0b0001_0000:
+            cur = _skip_phase(rec, cur, cats)
+        if t & 0b0110_0000:
+            cats = _dosage_overlay(rec, cur, t, n, cats)
         codes = np.full(bpv * 4, 0b01, np.uint8)
         codes[:n] = CAT_TO_BED[cats]
         q = codes.reshape(bpv, 4)

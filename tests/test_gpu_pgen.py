@@ -233,3 +233,79 @@ def test_zero_variants_and_missing_anchor(cuda):
     with pytest.raises(_lib.GnomonGpuError) as ei:
         PgenFile(bad)
     assert ei.value.status == _lib.GNM_ERR_IO and "anchor" in str(ei.value)
+
+
+def _dosage_case(n, V, seed, near_frac=0.6):
+    """LD-linked categories and u16 ALT dosages: every missing call gets a
+    value, most of them near a whole allele count; some calls get none."""
+    rng = np.random.default_rng(seed)
+    cats = synth.pgen_ld_categories(seed, V, n)
+    dos = rng.integers(0, 32769, cats.shape).astype(np.uint16)
+    near = rng.random(cats.shape) < near_frac
+    dos[near] = (rng.integers(0, 3, near.sum()) * 16384 +
+                 rng.integers(-1700, 1700, near.sum())).clip(0, 32768).astype(np.uint16)
+    dos[rng.random(cats.shape) < 0.2] = 65535
+    return cats, dos
+
+
+@pytest.mark.parametrize("kind", ["list", "dense", "bits"])
+@pytest.mark.parametrize("phase", [None, "all", "partial"])
+@pytest.mark.parametrize("n", [5, 203, 4097, 70001])
+def test_dosage_tracks_fill_missing_calls(cuda, kind, phase, n):
+    """Dosage tracks of every layout (sample list, dense, presence bits),
+    after either phase-track layout and followed by a phased-dosage track, on
+    2-bit, 1-bit, fill and LD records: the device rows equal the oracle's
+    (missing calls take the dosage's allele count within 0.10, hard calls
+    stand), byte for byte, and the bytes past each row are untouched."""
+    V = 60 if n < 10_000 else 12
+    cats, dos = _dosage_case(n, V, seed=n)
+    data = synth.encode_pgen_tracks(cats, dos, kind, phase, phased_dosage=kind != "list",
+                                    seed=n + 1)
+    want = pgen_oracle.decode_to_bed(data)
+    assert not np.array_equal(want, expected_rows(cats))   # some calls were filled
+    np.testing.assert_array_equal(device_rows(data, n), want)
+
+
+def test_reference_dense_dosage_record_on_the_device(cuda):
+    """shared/adapt_plink2.rs:3516-3570: categories {0, 1, 3, 3} with dense
+    dosages {0, 18022, 18022, 18023} decode to ALT counts {0, 1, 1, missing}."""
+    from test_pgen import _one_record_pgen
+    cats = np.array([0, 1, 3, 3], np.uint8)
+    body = bytes([int(cats[0] | (cats[1] << 2) | (cats[2] << 4) | (cats[3] << 6))])
+    body += np.array([0, 18022, 18022, 18023], "<u2").tobytes()
+    got = device_rows(_one_record_pgen(4, 0b0100_0000, body), 4)
+    np.testing.assert_array_equal(got, expected_rows(np.array([[0, 1, 1, 3]], np.uint8)))
+
+
+def test_truncated_dosage_track_is_an_io_error(cuda):
+    """A dosage track cut short is reported (GNM_ERR_IO) and the context
+    decodes the next file correctly."""
+    from test_pgen import _one_record_pgen
+    cats = np.array([3, 3, 3, 3, 0, 1], np.uint8)
+    packed = synth.pack_codes(cats[None, :])[0]
+    body = packed.tobytes() + np.array([16384, 0, 32768, 100, 0], "<u2").tobytes()  # one short
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        device_rows(_one_record_pgen(6, 0b0100_0000, body), 6)
+    assert ei.value.status == _lib.GNM_ERR_IO
+    test_reference_dense_dosage_record_on_the_device(cuda)
+
+
+def test_score_from_dosage_pgen_equals_bed_of_the_filled_calls(cuda):
+    """Scoring a .pgen whose missing calls carry dosages equals scoring the
+    .bed rows the oracle fills them into (engine plain and tensor)."""
+    people, V = 1501, 400
+    w, prep, rows, _ = synth_case(people, V, 3)
+    cats = _as_pgen(rows, people)
+    rng = np.random.default_rng(4)
+    dos = np.full(cats.shape, 65535, np.uint16)
+    miss = cats == 3
+    dos[miss] = (rng.integers(0, 3, miss.sum()) * 16384 +
+                 rng.integers(-2000, 2000, miss.sum())).clip(0, 32768).astype(np.uint16)
+    data = synth.encode_pgen_tracks(cats, dos, "list", "all", seed=2)
+    filled = pgen_oracle.decode_to_bed(data)
+    for engine in (_lib.ENGINE_PLAIN, _lib.ENGINE_TENSOR):
+        s, c = score_pgen(prep, data, engine=engine)
+        bs, bc = run(PipelineContext(prep), np.ascontiguousarray(filled).reshape(-1),
+                     engine=engine)
+        np.testing.assert_array_equal(c, bc)
+        np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)

@@ -99,7 +99,7 @@ def test_abi_rejects_bad_files():
     assert _status(corrupt(data, 2, 0x03)) == _lib.GNM_ERR_INVALID     # unsupported mode
     kind = data[types_at]
     assert _status(corrupt(data, types_at, kind | 0x08)) == _lib.GNM_ERR_INVALID  # multiallelic
-    assert _status(corrupt(data, types_at, kind | 0x20)) == _lib.GNM_ERR_INVALID  # dosage
+    assert _status(corrupt(data, types_at, kind | 0x80)) == _lib.GNM_ERR_IO  # phased dosage alone
     assert _status(corrupt(data, types_at, 5)) == _lib.GNM_ERR_INVALID           # type 5
     # the oracle rejects the same files
     with pytest.raises(pgen_oracle.PgenError):
@@ -230,3 +230,64 @@ def test_c_restatement_fixture_and_errors():
     first_ld = next(i for i, k in enumerate(types) if k in (2, 3))
     with pytest.raises(pgen_oracle.PgenError):
         pgen_oracle.decode_to_bed_c(synth._pgen_file(100, types[first_ld:], recs[first_ld:]))
+
+
+def test_abi_dosage_bits_are_accepted():
+    cats = synth.pgen_ld_categories(2, 40, 300)
+    dos = np.full(cats.shape, 65535, np.uint16)
+    dos[cats == 3] = 16384
+    for kind in ("list", "dense", "bits"):
+        assert pgen_dims(synth.encode_pgen_tracks(cats, dos, kind)) == (40, 300)
+
+
+def test_dosage_hardcall_rule_matches_the_reference_boundaries():
+    """shared/adapt_plink2.rs:3413-3470 (diploid): one allele copy is 16384;
+    1638/16384 lies inside the 0.10 tolerance, 1639/16384 outside; 1.5 has
+    no hard call; 65535 is missing."""
+    f = pgen_oracle.dosage_to_hardcall
+    for v, want in [(int(0.05 / 2.0 * 32768.0), 0), (int(1.00 / 2.0 * 32768.0), 1),
+                    (int(1.09 / 2.0 * 32768.0), 1), (int(2.00 / 2.0 * 32768.0), 2),
+                    (0, 0), (16384, 1), (32768, 2), (16384 + 1638, 1), (16384 + 1639, 255),
+                    (16384 - 1638, 1), (16384 - 1639, 255), (24576, 255), (65535, 255)]:
+        assert f(v) == want, v
+
+
+def _one_record_pgen(n, rtype, body):
+    return synth._pgen_file(n, [rtype], [bytes(body)])
+
+
+def test_reference_dense_dosage_record():
+    """shared/adapt_plink2.rs:3516-3570: a 2-bit main track of categories
+    {0, 1, 3, 3} and a dense dosage track {0, 18022, 18022, 18023} (type bit
+    6): the hard calls stand, sample 2's dosage 1.09997 becomes a het, sample
+    3's 1.10004 stays missing -> ALT counts {0, 1, 1, missing}."""
+    cats = np.array([0, 1, 3, 3], np.uint8)
+    body = bytes([int(cats[0] | (cats[1] << 2) | (cats[2] << 4) | (cats[3] << 6))])
+    body += np.array([0, 18022, 18022, 18023], "<u2").tobytes()
+    rows = pgen_oracle.decode_to_bed(_one_record_pgen(4, 0b0100_0000, body))
+    assert rows.shape == (1, 1)
+    assert rows[0, 0] == expected_rows(np.array([[0, 1, 1, 3]], np.uint8))[0, 0]
+
+
+@pytest.mark.parametrize("kind", ["list", "dense", "bits"])
+@pytest.mark.parametrize("phase", [None, "all", "partial"])
+def test_oracle_dosage_tracks_fill_missing_calls(kind, phase):
+    """Every dosage-track layout, behind either phase-track layout, on LD
+    records too: missing calls take the dosage's allele count when it is
+    within 0.10, hard calls never change, phased dosages change nothing."""
+    rng = np.random.default_rng(5)
+    cats = synth.pgen_ld_categories(9, 90, 517)
+    dos = rng.integers(0, 32769, cats.shape).astype(np.uint16)
+    dos[rng.random(cats.shape) < 0.3] = 65535
+    near = rng.random(cats.shape) < 0.5       # half of them snapped near a whole count
+    dos[near] = (rng.integers(0, 3, near.sum()) * 16384 +
+                 rng.integers(-1700, 1700, near.sum())).clip(0, 32768).astype(np.uint16)
+    data = synth.encode_pgen_tracks(cats, dos, kind, phase, phased_dosage=kind != "list",
+                                    seed=11)
+    want = cats.copy()
+    for v, i in zip(*np.nonzero(cats == 3)):
+        hc = pgen_oracle.dosage_to_hardcall(int(dos[v, i]))
+        if hc != 255:
+            want[v, i] = hc
+    assert (want != cats).any()
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(want))
