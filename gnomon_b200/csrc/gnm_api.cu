@@ -338,7 +338,7 @@ static void plain_geometry(gnm_plan* p) {
   plain_shape(p, kPlainDefaultKernel, 1.0);
   // keep partials of all scores within 8 GiB (many score columns still get a
   // full-occupancy grid); allocate room for the autotuner's largest candidate
-  // (twice the CTA slots, any kernel)
+  // (four times the CTA slots, any kernel)
   const uint64_t per_split_bytes = p->K * p->part_stride * 12;
   const uint64_t cap = uint64_t(8) << 30;
   uint64_t alloc = p->slots;
@@ -347,7 +347,7 @@ static void plain_geometry(gnm_plan* p) {
     probe.V = p->V;
     probe.bpv = p->bpv;
     probe.num_sms = p->num_sms;
-    plain_shape(&probe, kn, 2.0);
+    plain_shape(&probe, kn, 4.0);
     alloc = std::max<uint64_t>(alloc, probe.slots);
   }
   while (alloc > 1 && alloc * per_split_bytes > cap) --alloc;
@@ -615,7 +615,7 @@ static void sync_impl(gnm_plan* p, cudaStream_t s) {
 // resident rows and keeps the fastest.  Plain engine: the people-tile width
 // (1 KB tiles, 8 warps and 2 CTAs per SM; or 512-byte tiles, 4 warps and 4
 // CTAs per SM: a narrow cohort fills every warp of its one tile) times the
-// split count (half, one or two times the SMs' CTA slots: fewer splits write
+// split count (0.5x to 4x the SMs' CTA slots: fewer splits write
 // fewer FP64 partials, more splits even out the last wave).  Tensor engine
 // with more than 64 scores: the CTA raster order (people tiles fastest: CTAs
 // in flight share weight-limb tiles in L2; score tiles fastest: they share
@@ -656,7 +656,7 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
     const char* tr = std::getenv("GNM_TRACE");
     const bool trace = tr && std::strcmp(tr, "0") != 0;
     for (uint32_t kn : kPlainKernels) {
-      for (double m : {0.5, 1.0, 2.0}) {
+      for (double m : {0.5, 1.0, 2.0, 3.0, 4.0}) {
         plain_shape(p, kn, m);
         if (p->slots > p->splits_alloc) continue;
         const float ms = time_best();

@@ -219,8 +219,8 @@ uint64_t gnm_plan_launch_count(const gnm_plan* plan);
  * the first `variant_count` resident rows for each candidate launch shape —
  * plain engine: the kernel (people tiles of 512 bytes with 4 warps, 1024 bytes
  * with 8 warps, 1024 bytes with 8 warps and a producer warp, 2048 bytes with
- * 16 warps and a producer warp) times the variant-split count (0.5x, 1x, 2x
- * the SMs' CTA slots, split between people tiles by their populated warps);
+ * 16 warps and a producer warp) times the variant-split count (0.5x to 4x
+ * the SMs' CTA slots, the same count for every people tile);
  * tensor engine: up to 64 scores the narrow kernel (people as the MMA's M)
  * against the wide kernel (scores as M), and the wide kernel's CTA raster
  * order — keeps the fastest, and leaves the plan reset.  Blocks until done.  With the environment variable GNM_TRACE

@@ -240,6 +240,7 @@ def _dosage_case(n, V, seed, near_frac=0.6):
     value, most of them near a whole allele count; some calls get none."""
     rng = np.random.default_rng(seed)
     cats = synth.pgen_ld_categories(seed, V, n)
+    cats[rng.random(cats.shape) < 0.05] = 3      # enough missing calls at any n
     dos = rng.integers(0, 32769, cats.shape).astype(np.uint16)
     near = rng.random(cats.shape) < near_frac
     dos[near] = (rng.integers(0, 3, near.sum()) * 16384 +
