@@ -317,7 +317,12 @@ def gpu_arm(args, rank, world, local_rank):
 
     plan = DevicePlan(prep, engine=engine, device=local_rank)
     tuned = None
-    if not args.no_autotune:
+    if args.shape:
+        # a pinned launch shape (kernel:splits, e.g. 512:94), as profiling runs use
+        kern, splits = (int(x) for x in args.shape.split(":"))
+        plan.set_shape((kern << 16) | splits)
+        tuned = {"kernel": kern, "splits_per_full_tile": splits, "pinned": True}
+    elif not args.no_autotune:
         # the library's autotuner picks the launch shape on these resident rows
         # (outside the timed region; the plan is left reset)
         shape = plan.autotune(rows, pitch, stream=stream)
@@ -844,6 +849,8 @@ def main():
                     help="stream rows from pinned host memory in blocks of this many variants")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the plan's default launch shape instead of autotuning it")
+    ap.add_argument("--shape", default="",
+                    help="pin the plain engine's launch shape, kernel:splits (e.g. 512:94)")
     ap.add_argument("--variants", type=int, default=0,
                     help="override the variant count (small cases for profiler captures)")
     ap.add_argument("--pgen", type=int, default=0,

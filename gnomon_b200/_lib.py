@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "GNM_OK", 1: "GNM_DECLINED", 2: "GNM_ERR_IO", 3: "GNM_ERR_COM
 ENGINE_AUTO, ENGINE_PLAIN, ENGINE_TENSOR = 0, 1, 2
 DEVICE_CURRENT, DEVICE_BEST = -1, -2   # device arguments besides an ordinal
 # plain accumulate kernels (gnm_plan_tuned_shape >> 16): tile bytes, +1 = producer warp
-PLAIN_KERNELS = (1024, 512, 1025, 2049)
+PLAIN_KERNELS = (1024, 512, 513, 1025, 2049)
 
 u8p = C.POINTER(C.c_uint8)
 

@@ -80,11 +80,13 @@ cudaError_t launch_plain_tables(const TableArgs& a, cudaStream_t s);
 // with a producer warp (its scoring warps only arrive on a release barrier).
 enum : uint32_t {
   kPlain512 = 512,        // 4 warps, 4 CTAs per SM
+  kPlain512Ws = 513,      // 4 warps + producer warp, 4 CTAs per SM
   kPlain1024 = 1024,      // 8 warps, 2 CTAs per SM
   kPlain1024Ws = 1025,    // 8 warps + producer warp, 2 CTAs per SM
   kPlain2048Ws = 2049     // 16 warps + producer warp, 1 CTA per SM
 };
-constexpr uint32_t kPlainKernels[] = {kPlain1024, kPlain512, kPlain1024Ws, kPlain2048Ws};
+constexpr uint32_t kPlainKernels[] = {kPlain1024, kPlain512, kPlain512Ws, kPlain1024Ws,
+                                      kPlain2048Ws};
 constexpr uint32_t kPlainDefaultKernel = kPlain2048Ws;   // fastest on the bandwidth workload
 inline uint32_t plain_tile_bytes(uint32_t kernel) { return kernel & ~1u; }
 inline uint32_t plain_ctas_per_sm(uint32_t kernel) {

@@ -597,6 +597,7 @@ cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, 
   const uint32_t grid = plain_grid(a);
   switch (kernel) {
     case kPlain512: return launch_plain_tile<512, false>(map, a, grid, s);
+    case kPlain512Ws: return launch_plain_tile<512, true>(map, a, grid, s);
     case kPlain1024: return launch_plain_tile<1024, false>(map, a, grid, s);
     case kPlain1024Ws: return launch_plain_tile<1024, true>(map, a, grid, s);
     case kPlain2048Ws: return launch_plain_tile<2048, true>(map, a, grid, s);
