@@ -20,7 +20,8 @@
 //   * each thread owns one 32-bit word column = 16 people; per 3 rows it
 //     transposes the 2-bit codes into per-person 6-bit indices (one byte each,
 //     pre-scaled by 4) with shift/mask ops and turns each byte into a
-//     shared-memory address with one byte permute;
+//     shared-memory address with one integer dot product (__dp4a); two
+//     groups' lookups go into a person's sum with one three-input add;
 //   * warps run the stages independently: a warp waits only for the stage's
 //     TMA; it releases the buffer either through a shared counter whose last
 //     arriver issues the TMA of the stage three ahead, or (producer-warp
@@ -63,18 +64,25 @@ struct PlainSmem {
   static_assert(kEmptyOff % 8 == 0, "mbarrier alignment");
   static_assert(TILE % kPlainBoxBytes == 0 && TILE % 128 == 0, "whole boxes and warps");
   static_assert(kPlainRows % 3 == 0 && kPlainRows <= 32, "groups of 3 rows, one ballot");
+  static_assert(kPlainGroups % 2 == 0, "groups are scored in pairs");
   static_assert(kTabStride >= kPlainTableBytes && kTabStride % 256 == 0, "table stride");
   static_assert(kTileOff % 1024 == 0, "tile alignment");
   // Each 64-entry group table starts on a 256-byte boundary, so a lookup
-  // address is the table address with its low byte replaced by the index.
+  // address is the table address plus the index byte (no carry).
 };
 
 // Multipliers for left shifts and adds written as integer multiply-adds: held
 // in constant memory, unknown at compile time, they make the compiler issue
 // IMAD on the FMA pipe instead of shift / add on the integer ALU pipe, which
-// the index transposes, byte permutes and masks already keep busy (the kernel
-// is bound by that pipe).
+// the index transposes, masks and three-input adds already keep busy.
 __constant__ uint32_t c_mul[5] = {2u, 4u, 16u, 64u, 1u};
+
+// Byte selectors for the lookup addresses: __dp4a(ix, c_sel[j], table) is
+// byte j of ix plus the table address (the other three byte products are
+// zero), one integer dot-product instruction on the FMA pipe where a byte
+// permute would take the integer ALU pipe.  Held in constant memory so that
+// the compiler keeps the dot product.
+__constant__ uint32_t c_sel[4] = {0x1u, 0x100u, 0x10000u, 0x1000000u};
 
 __device__ __forceinline__ int32_t lds_s32(uint32_t addr) {
   int32_t v;
@@ -190,9 +198,10 @@ struct PlainShape {
 
 // One CTA per (people tile, variant split).  The grid is 1D: the first
 // (tiles - 1) * splits CTAs cover the full tiles, `splits` each, and the last
-// tile (often only partly populated by people) gets its own, smaller split
-// count, so every CTA carries about the same work and the grid fills the
-// SMs' CTA slots evenly.  block = TILE / 4 scoring threads, plus (WS) one
+// tile (often only partly populated by people) has its own stages-per-split
+// field; the host gives it the same split count as the others, because a
+// CTA's time per stage is set by each warp's dependency chains, not by how
+// many of its warps hold people.  block = TILE / 4 scoring threads, plus (WS) one
 // producer warp that issues every stage's copies once the scoring warps have
 // released its buffer (they arrive on an mbarrier and never wait for one
 // another); without it the scoring warp that releases a buffer last issues
@@ -333,11 +342,13 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
         smem + L::kTabOff + buf * L::kTabStride + kPlainGroups * 256 + 4);
 
     uint32_t ev = 0, od = 0;             // nibble counters (people 2j / 2j+1)
-    auto group = [&](uint32_t g, uint32_t ma, uint32_t mb, uint32_t mc) {
+    // Row words of group g -> four index words; returns the group's missing
+    // calls (code 01 of member rows) summed into 2-bit fields.
+    auto index = [&](uint32_t g, uint32_t (&ix)[4], uint32_t ma, uint32_t mb,
+                     uint32_t mc) -> uint32_t {
       const uint32_t xa = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 0) * kPlainBoxBytes);
       const uint32_t xb = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 1) * kPlainBoxBytes);
       const uint32_t xc = *reinterpret_cast<const uint32_t*>(tbase + (3 * g + 2) * kPlainBoxBytes);
-      // ---- per-person 6-bit indices (x4) ------------------------------
       // rows a and b get row c's lo bits XORed into their lo bits; row c
       // enters with its code bits swapped (see the table layout above)
       const uint32_t ya = xa ^ (xc & 0x55555555u);
@@ -345,26 +356,33 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       const uint32_t xs = ((xc >> 1) & 0x55555555u) | ((xc * c_mul[0]) & 0xAAAAAAAAu);
       const uint32_t E = (ya & 0x33333333u) | ((yb * c_mul[1]) & 0xCCCCCCCCu);
       const uint32_t O = ((ya >> 2) & 0x33333333u) | (yb & 0xCCCCCCCCu);
-      uint32_t ix[4];
+      // byte j of ix[q] is person 4j + q's 6-bit index, pre-scaled by 4
       ix[0] = ((E * c_mul[1]) & 0x3C3C3C3Cu) | ((xs * c_mul[3]) & 0xC0C0C0C0u);
       ix[1] = ((O * c_mul[1]) & 0x3C3C3C3Cu) | ((xs * c_mul[2]) & 0xC0C0C0C0u);
       ix[2] = ((E >> 2) & 0x3C3C3C3Cu) | ((xs * c_mul[1]) & 0xC0C0C0C0u);
       ix[3] = ((O >> 2) & 0x3C3C3C3Cu) | (xs & 0xC0C0C0C0u);
-      const uint32_t lg = lbase + g * 256;
+      return (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
+    };
+    // Groups g and g + 1 together: each person's two lookups go into its
+    // stage sum with one three-input add.  Nibble counters take four groups
+    // (<= 12 calls) before they are flushed to the byte counters.
+    auto pair = [&](uint32_t g, uint32_t m0, uint32_t m1, uint32_t m2, uint32_t m3,
+                    uint32_t m4, uint32_t m5) {
+      uint32_t i0[4], i1[4];
+      const uint32_t c0 = index(g, i0, m0, m1, m2);
+      const uint32_t c1 = index(g + 1, i1, m3, m4, m5);
+      const uint32_t l0 = lbase + g * 256, l1 = l0 + 256;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        // address = table address with its low byte replaced by index byte j
-        // (byte j of ix[q] is person 4j + q)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          iacc[4 * j + q] = int32_t(uint32_t(lds_s32(__byte_perm(ix[q], lg, 0x7650u + j))) *
-                                        c_mul[4] + uint32_t(iacc[4 * j + q]));
+          iacc[4 * j + q] = int32_t(uint32_t(iacc[4 * j + q]) +
+                                    uint32_t(lds_s32(__dp4a(i0[q], c_sel[j], l0))) +
+                                    uint32_t(lds_s32(__dp4a(i1[q], c_sel[j], l1))));
       }
-      // ---- missing counts (code 01 of member rows) ---------------------
-      const uint32_t c3 = (xa & ~(xa >> 1) & ma) + (xb & ~(xb >> 1) & mb) + (xc & ~(xc >> 1) & mc);
-      ev = (c3 & 0x33333333u) * c_mul[4] + ev;
-      od = ((c3 >> 2) & 0x33333333u) * c_mul[4] + od;
-      if ((g % 5) == 4 || g == kPlainGroups - 1) {
+      ev = (c0 & 0x33333333u) + (c1 & 0x33333333u) + ev;
+      od = ((c0 >> 2) & 0x33333333u) + ((c1 >> 2) & 0x33333333u) + od;
+      if ((g / 2) % 2 == 1 || g + 2 == kPlainGroups) {
         by[0] += ev & 0x0F0F0F0Fu;
         by[2] += (ev >> 4) & 0x0F0F0F0Fu;
         by[1] += od & 0x0F0F0F0Fu;
@@ -378,14 +396,16 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     } else if (members == (uint64_t(1) << kPlainRows) - 1) {
       // every row of the stage is a member of this score (the common case)
 #pragma unroll
-      for (uint32_t g = 0; g < kPlainGroups; ++g) group(g, 0x55555555u, 0x55555555u, 0x55555555u);
+      for (uint32_t g = 0; g < kPlainGroups; g += 2)
+        pair(g, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
     } else {
 #pragma unroll
-      for (uint32_t g = 0; g < kPlainGroups; ++g) {
-        const uint32_t ma = (0u - uint32_t((members >> (3 * g + 0)) & 1u)) & 0x55555555u;
-        const uint32_t mb = (0u - uint32_t((members >> (3 * g + 1)) & 1u)) & 0x55555555u;
-        const uint32_t mc = (0u - uint32_t((members >> (3 * g + 2)) & 1u)) & 0x55555555u;
-        group(g, ma, mb, mc);
+      for (uint32_t g = 0; g < kPlainGroups; g += 2) {
+        uint32_t m[6];
+#pragma unroll
+        for (uint32_t r = 0; r < 6; ++r)
+          m[r] = (0u - uint32_t((members >> (3 * g + r)) & 1u)) & 0x55555555u;
+        pair(g, m[0], m[1], m[2], m[3], m[4], m[5]);
       }
     }
 
