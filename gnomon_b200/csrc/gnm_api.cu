@@ -612,11 +612,12 @@ static void sync_impl(gnm_plan* p, cudaStream_t s) {
 
 // ---- autotuner -----------------------------------------------------------------
 // Times candidate launch shapes of the plan's accumulate on the caller's
-// resident rows and keeps the fastest.  Plain engine: the people-tile width
-// (1 KB tiles, 8 warps and 2 CTAs per SM; or 512-byte tiles, 4 warps and 4
-// CTAs per SM: a narrow cohort fills every warp of its one tile) times the
-// split count (0.5x to 4x the SMs' CTA slots: fewer splits write
-// fewer FP64 partials, more splits even out the last wave).  Tensor engine
+// resident rows and keeps the fastest.  Plain engine: the five accumulate
+// kernels (512-byte, 1 KB and 2 KB people tiles with 4, 8 and 16 scoring warps
+// and 4, 2 and 1 CTAs per SM, with or without a producer warp; a narrow
+// cohort fills every warp of a narrow tile) times the split count (0.5x to 4x
+// the SMs' CTA slots: fewer splits write fewer FP64 partials, more splits
+// even out the last wave).  Tensor engine
 // with more than 64 scores: the CTA raster order (people tiles fastest: CTAs
 // in flight share weight-limb tiles in L2; score tiles fastest: they share
 // genotype tiles).

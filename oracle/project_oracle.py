@@ -14,7 +14,10 @@ It restates the reference's GPU projection of a variant block
 Parity is pinned by the reference's own known-answer test of the last step
 (map/project.rs:3927-3944) and by the kernel's formula. The reference holds
 no golden vectors for the first two steps, so their parity is unpinned beyond
-that formula.
+that formula. ``tests/golden/ld_projection_fixture.npz`` freezes this
+module's scores for one block over the reference's real ``ld.bed`` rows
+(data/testdata), so the restatement and the kernel are held to the same
+numbers on real genotypes.
 """
 from __future__ import annotations
 

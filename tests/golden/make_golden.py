@@ -24,6 +24,13 @@ Sources (SauersML/gnomon, read as text; the Rust code cannot run here):
 * ld_pgen_fixture.npz — the bytes of data/testdata/ld_p.pgen, the same
   genotypes as a PLINK 2 variable-width .pgen (LD-compressed and 1-bit
   records), for PGEN decode parity against ld_fixture.npz.
+* ld_projection_fixture.npz — one HWE-PCA projection block over the real
+  ld.bed rows (all 1,500 variants, 200 samples, 6 axes): coefficients from
+  the rows' own allele frequencies ((g - 2p) / sqrt(2p(1-p)), map/project.rs
+  :2960-2975; every 7th variant allele-swapped), seeded loadings, and the
+  expected scores from the float64 restatement of the reference's block
+  projection (map/project.rs:322-370, 547-667), frozen here so that the
+  kernel and the restatement are both held to the same numbers.
 
 Run: python tests/golden/make_golden.py --reference <path of the reference checkout>
 """
@@ -128,6 +135,26 @@ def gpu_tests_cohort(n_people=512, n_variants=256, n_scores=16):
     return packed, w, flipped
 
 
+def ld_projection(rows: np.ndarray, n_people: int, axes: int = 6, seed: int = 2027):
+    import sys
+    sys.path.insert(0, str(HERE.parents[1]))
+    from oracle import project_oracle
+    bpv = (n_people + 3) // 4
+    codes = np.stack([(rows >> (2 * s)) & 3 for s in range(4)], axis=-1).reshape(rows.shape[0], -1)
+    codes = codes[:, :n_people]
+    g = np.choose(codes, [0.0, np.nan, 1.0, 2.0])           # A2 copies; code 01 missing
+    p = np.nanmean(g, axis=1) / 2.0
+    scale = np.sqrt(2.0 * p * (1.0 - p))
+    inv = np.where(scale > 0, 1.0 / np.where(scale > 0, scale, 1.0), 0.0)
+    c = (np.arange(3.0)[None, :] - 2.0 * p[:, None]) * inv[:, None]
+    c[::7] = c[::7, ::-1]
+    coeffs = c.astype(np.float32)
+    rng = np.random.default_rng(seed)
+    loadings = (rng.standard_normal((rows.shape[0], axes)) / np.sqrt(rows.shape[0])).astype(np.float32)
+    scores = project_oracle.project_block(rows.reshape(-1, bpv), n_people, coeffs, loadings)
+    return coeffs, loadings, scores
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True,
@@ -145,6 +172,11 @@ def main():
         bpv = (n_people + 3) // 4
         rows = raw[3:].reshape(n_var, bpv)
         np.savez_compressed(HERE / "ld_fixture.npz", rows=rows, num_people=n_people)
+    if (HERE / "ld_fixture.npz").exists():
+        f = np.load(HERE / "ld_fixture.npz")
+        coeffs, loadings, scores = ld_projection(f["rows"], int(f["num_people"]))
+        np.savez_compressed(HERE / "ld_projection_fixture.npz", coeffs=coeffs, loadings=loadings,
+                            scores=scores)
     pg = Path(a.reference) / "data" / "testdata" / "ld_p.pgen"
     if pg.exists():
         np.savez_compressed(HERE / "ld_pgen_fixture.npz",

@@ -93,3 +93,21 @@ def test_wide_tensor_block(cuda):
     with Projector(n, k) as pj:
         pj.block(rows, coeffs, loadings)
         check(pj.scores(), rows, n, coeffs, loadings)
+
+
+def test_real_ld_block_against_fixture(cuda):
+    """All 1,500 variants of the reference's ld.bed (200 samples) as one block,
+    coefficients from the rows' own allele frequencies, against the frozen
+    float64 scores of the same block."""
+    from pathlib import Path
+    g = Path(__file__).resolve().parent / "golden"
+    f, d = np.load(g / "ld_fixture.npz"), np.load(g / "ld_projection_fixture.npz")
+    rows, n = f["rows"], int(f["num_people"])
+    coeffs, loadings = d["coeffs"], d["loadings"]
+    with Projector(n, loadings.shape[1]) as pj:
+        pj.block(rows, coeffs, loadings)
+        got = pj.scores()
+    scale = project_oracle.abs_terms(rows, n, coeffs, loadings) + \
+        (np.abs(coeffs[:, 0].astype(np.float64)) @ np.abs(loadings.astype(np.float64)))[None, :]
+    err = np.abs(got - d["scores"])
+    assert (err <= TOL * scale + 1e-30).all(), f"max err / scale {np.max(err / (scale + 1e-30)):.2e}"

@@ -47,3 +47,12 @@ def test_create_declines_without_a_device():
     with pytest.raises(_lib.GnomonGpuError) as ei:
         Projector(10, 2)
     assert ei.value.status == _lib.GNM_DECLINED
+
+
+def test_ld_projection_fixture_reproduces():
+    """The restatement still gives the frozen scores of the real ld.bed block."""
+    from pathlib import Path
+    g = Path(__file__).resolve().parent / "golden"
+    f, d = np.load(g / "ld_fixture.npz"), np.load(g / "ld_projection_fixture.npz")
+    got = project_oracle.project_block(f["rows"], int(f["num_people"]), d["coeffs"], d["loadings"])
+    np.testing.assert_allclose(got, d["scores"], rtol=1e-12, atol=1e-12)
