@@ -801,9 +801,14 @@ PgenIndex parse_pgen(const uint8_t* d, uint64_t len) {
   ix.lens.resize(m);
   ix.types.assign(m, 0);
   if (mode == 0x02) {
+    // records start after the 12 header bytes, one more byte and (reference
+    // flag mode 3) one reference flag bit per variant, where the reference's
+    // reader puts them (shared/adapt_plink2.rs:2048-2057, asserted by its
+    // test at :3826-3866)
     const uint64_t rec = (ix.samples + 3) / 4;
+    const uint64_t base = 13 + (((d[11] >> 6) & 3) == 3 ? (m + 7) / 8 : 0);
     for (uint64_t v = 0; v < m; ++v) {
-      ix.offsets[v] = 12 + v * rec;
+      ix.offsets[v] = base + v * rec;
       ix.lens[v] = uint32_t(rec);
     }
   } else if (mode == 0x10 || mode == 0x11) {

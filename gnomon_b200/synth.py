@@ -413,6 +413,120 @@ def encode_pgen_tracks(cats: np.ndarray, dosage: np.ndarray | None = None,
     return _pgen_file(n, types, recs)
 
 
+def _bitarray_bytes(bits) -> bytes:
+    bits = np.asarray(bits, np.uint8)
+    return np.packbits(bits, bitorder="little").tobytes() if len(bits) else b""
+
+
+def _packed_bytes(vals, width: int) -> bytes:
+    if width == 0 or len(vals) == 0:
+        return b""
+    vals = np.asarray(vals, np.uint64)
+    bits = ((vals[:, None] >> np.arange(width, dtype=np.uint64)) & 1).astype(np.uint8).ravel()
+    return np.packbits(bits, bitorder="little").tobytes()
+
+
+def _het_alt_width(ac: int) -> int:
+    return 0 if ac == 2 else 1 if ac == 3 else 2 if ac <= 5 else 4 if ac <= 17 else \
+        8 if ac <= 257 else 16
+
+
+def _homalt_pair_width(ac: int) -> int:
+    return 2 if ac <= 4 else 4 if ac <= 16 else 8 if ac <= 256 else 16
+
+
+def multiallelic_categories(alleles: np.ndarray) -> np.ndarray:
+    """Per-sample allele pairs [V][N][2] (0 REF, 1.. ALT ordinal, -1 missing)
+    -> PGEN categories [V][N]: 3 missing, else the number of non-REF alleles."""
+    a = np.asarray(alleles)
+    miss = (a < 0).any(axis=2)
+    c = (a > 0).sum(axis=2).astype(np.uint8)
+    c[miss] = 3
+    return c
+
+
+def _multiallelic_patch(cats_v, alleles_v, ac: int, het_fmt: int, hom_fmt: int,
+                        swap_pairs: bool) -> bytes:
+    """The multiallelic patch of one record: hets whose ALT is not ALT 1, and
+    hom-ALT-category samples whose allele pair is not (1, 1).  het_fmt /
+    hom_fmt: 0 = bit array over the category's samples, 1 = id difflist; a
+    category with nothing to patch is written as 15 (absent)."""
+    n = len(cats_v)
+    het = np.nonzero(cats_v == 1)[0]
+    hom = np.nonzero(cats_v == 2)[0]
+    het_alt = alleles_v[het].max(axis=1)
+    het_mask = het_alt != 1
+    pairs = np.sort(alleles_v[hom], axis=1)
+    hom_mask = ~((pairs[:, 0] == 1) & (pairs[:, 1] == 1))
+    f1 = het_fmt if het_mask.any() else 15
+    f2 = hom_fmt if hom_mask.any() else 15
+    out = bytearray([f1 | (f2 << 4)])
+    if f1 != 15:
+        out += _bitarray_bytes(het_mask) if f1 == 0 else _difflist_id_bytes(het[het_mask], n)
+        out += _packed_bytes(het_alt[het_mask] - 2, _het_alt_width(ac))
+    if f2 != 15:
+        out += _bitarray_bytes(hom_mask) if f2 == 0 else _difflist_id_bytes(hom[hom_mask], n)
+        sel = pairs[hom_mask]
+        if ac == 2:
+            out += _bitarray_bytes((sel[:, 0] == 2) & (sel[:, 1] == 2))
+        else:
+            if swap_pairs:                   # the reader sorts each pair
+                sel = sel[:, ::-1]
+            out += _packed_bytes((sel - 1).ravel(), _homalt_pair_width(ac))
+    return bytes(out)
+
+
+def encode_pgen_multiallelic(alleles: np.ndarray, alt_counts, het_fmt: int = 0,
+                             hom_fmt: int = 0, patch: np.ndarray | None = None,
+                             phase: str | None = None, dosage: np.ndarray | None = None,
+                             dosage_kind: str = "list", seed: int = 0) -> bytes:
+    """A .pgen of variants with ``alt_counts[v]`` ALT alleles from per-sample
+    allele pairs [V][N][2] (0 REF, j = ALT j, -1 missing).  Every variant with
+    two or more ALTs and ``patch[v]`` (default: all of them) carries a
+    multiallelic patch (vrtype bit 3) after its main track; phase and dosage
+    tracks follow as in ``encode_pgen_tracks``."""
+    alleles = np.asarray(alleles, np.int64)
+    V, n, _ = alleles.shape
+    cats = multiallelic_categories(alleles)
+    rng = np.random.default_rng(seed)
+    types, recs = _pgen_records(cats)
+    types, recs = list(types), list(recs)
+    for v in range(V):
+        body = recs[v]
+        if int(alt_counts[v]) >= 2 and (patch is None or patch[v]):
+            body = body + _multiallelic_patch(cats[v], alleles[v], int(alt_counts[v]), het_fmt,
+                                              hom_fmt, bool(v % 2))
+            types[v] |= 0b0000_1000
+        if phase is not None:
+            body = body + _phase_track(cats[v], rng, phase == "partial")
+            types[v] |= 0b0001_0000
+        if dosage is not None and np.any(dosage[v] != 65535):
+            bits, track = _dosage_track(np.asarray(dosage[v], np.uint16), dosage_kind, False, rng)
+            body = body + track
+            types[v] |= bits
+        recs[v] = body
+    return _pgen_file(n, types, recs)
+
+
+def multiallelic_alleles(seed: int, alt_counts, num_people: int, missing_rate: float = 0.02,
+                         het_rate: float = 0.3, hom_rate: float = 0.15) -> np.ndarray:
+    """Seeded allele pairs [V][N][2] for variants with ``alt_counts[v]`` ALTs:
+    REF/REF, het REF/ALT j, ALT pairs (hom or two different ALTs) and missing."""
+    rng = np.random.default_rng(seed)
+    V = len(alt_counts)
+    out = np.zeros((V, num_people, 2), np.int64)
+    for v in range(V):
+        ac = int(alt_counts[v])
+        u = rng.random(num_people)
+        alt = rng.integers(1, ac + 1, size=(num_people, 2))
+        het = (u >= missing_rate) & (u < missing_rate + het_rate)
+        hom = (u >= missing_rate + het_rate) & (u < missing_rate + het_rate + hom_rate)
+        out[v, het, 1] = alt[het, 0]
+        out[v, hom] = alt[hom]
+        out[v, u < missing_rate] = -1
+    return out
+
+
 def encode_pgen(cats: np.ndarray, repeats: int = 1) -> bytes:
     """Genotype categories [V][N] (0 hom REF, 1 het, 2 hom ALT, 3 missing) ->
     a variable-width (mode 0x10) .pgen, 8-bit record types, 4-byte lengths.

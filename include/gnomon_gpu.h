@@ -277,13 +277,16 @@ gnm_status gnm_backward_dw_device(gnm_plan* plan, const uint8_t* d_rows, uint64_
  * GPU, straight into device rows the scoring plans read (gnm_plan_accumulate /
  * gnm_score_device), one row per .pgen variant in file order.
  *
- * Supported: storage modes 0x02 and 0x10 / 0x11, biallelic hard-call records
- * (main-track types 0-4, 6, 7, optionally followed by a phase track).
- * Records with multiallelic or dosage tracks, external-index modes, and more
- * than 2^31 samples are rejected with GNM_ERR_INVALID; truncated or
- * malformed files give GNM_ERR_IO.  The reference additionally projects
- * multiallelic records, coerces dosages to hard calls and applies
- * sex-chromosome ploidy from the .pvar / .psam; callers handle those. */
+ * Supported: storage modes 0x02 and 0x10 / 0x11, biallelic records
+ * (main-track types 0-4, 6, 7), optionally followed by a phase track (skipped)
+ * and a dosage track: a hard call that is missing takes the nearest whole
+ * allele count of its dosage when that lies within 0.10, as the reference's
+ * reader coerces dosages (shared/adapt_plink2.rs:14-18); phased-dosage
+ * tracks are skipped.  Records with multiallelic tracks, external-index
+ * modes, and more than 2^31 samples are rejected with GNM_ERR_INVALID;
+ * truncated or malformed files give GNM_ERR_IO.  The reference additionally
+ * projects multiallelic records onto each ALT and applies sex-chromosome
+ * ploidy from the .pvar / .psam; callers handle those. */
 
 /* Variant and sample counts from a .pgen header (host bytes). */
 gnm_status gnm_pgen_dims(const uint8_t* pgen, uint64_t pgen_len, uint64_t* num_variants,

@@ -57,9 +57,11 @@ static int parse(const uint8_t* d, uint64_t len, pg_index* ix) {
   ix->anchor = calloc(m ? m : 1, 4);
   if (!ix->offs || !ix->lens || !ix->types || !ix->anchor) return -2;
   if (mode == 0x02) {
+    /* body after 13 bytes (+ reference flags), adapt_plink2.rs:2048-2057 */
     const uint64_t rec = (n + 3) / 4;
+    const uint64_t base = 13 + (((d[11] >> 6) & 3) == 3 ? (m + 7) / 8 : 0);
     for (uint64_t v = 0; v < m; ++v) {
-      ix->offs[v] = 12 + v * rec;
+      ix->offs[v] = base + v * rec;
       ix->lens[v] = (uint32_t)rec;
     }
   } else if (mode == 0x10 || mode == 0x11) {

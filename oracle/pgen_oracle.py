@@ -28,7 +28,17 @@ of shared/adapt_plink2.rs). The restated steps are:
   never overridden.  Samples are treated as diploid (the reference takes
   ploidy from the .pvar/.psam, which this decoder does not read).
 
-Records with multiallelic tracks (vrtype bit 3) are rejected.
+* multiallelic records (vrtype bit 3, :2704-2881) when the input variants'
+  ALT counts are given (the reference reads them from the .pvar): an output
+  row is one (variant, ALT ordinal j) pair of the virtual .bim, and holds the
+  number of copies of ALT j. Hets default to ALT 1 and hom-ALTs to ALT 1 / ALT
+  1; the record's patch (one format nibble per category: 0 = bit array over
+  the category's samples, 1 = id-only difflist, 15 = none; then fixed-width
+  ALT values, or for two ALTs a hom-ALT2 flag array) overrides them. The
+  reference's own edges are kept: a record without bit 3 gives every ALT row
+  the plain categories, a bit-3 record of a variant with one ALT is read as
+  biallelic without consuming its patch, and only the rows of ALT 1 read the
+  dosage track (:2420). Without ALT counts, bit-3 records are rejected.
 Difflists whose sample ids do not rise strictly are rejected as malformed
 (PLINK 2 writes strictly rising ids; the reference would apply such a list in
 order, later entries winning).
@@ -203,6 +213,91 @@ def _dosage_overlay(rec, cur, t, n, cats):
     return out
 
 
+def _bitarray_indices(rec, cur, nbits):
+    """Set bits of an nbits-long bit array (:1753-1777) -> (indices, cursor)."""
+    nbytes = (nbits + 7) // 8
+    if cur + nbytes > len(rec):
+        raise PgenError("EOF in bitarray")
+    if nbits == 0:
+        return [], cur
+    bits = np.unpackbits(np.frombuffer(rec, np.uint8, nbytes, cur), bitorder="little")[:nbits]
+    return [int(x) for x in np.nonzero(bits)[0]], cur + nbytes
+
+
+def _packed(rec, cur, width, count):
+    """``count`` fixed-width little-endian bit fields (:1779-1810) -> (values, cursor)."""
+    if width == 0:
+        return [0] * count, cur
+    nbytes = (width * count + 7) // 8
+    if cur + nbytes > len(rec):
+        raise PgenError("EOF in packed values")
+    bits = np.unpackbits(np.frombuffer(rec, np.uint8, nbytes, cur), bitorder="little")
+    vals = [int(sum(int(bits[i * width + k]) << k for k in range(width))) for i in range(count)]
+    return vals, cur + nbytes
+
+
+def _het_width(ac):
+    """Bits of one het's ALT value (value + 2 = its ALT) for ``ac`` ALTs."""
+    return 0 if ac == 2 else 1 if ac == 3 else 2 if ac <= 5 else 4 if ac <= 17 else \
+        8 if ac <= 257 else 16
+
+
+def _homalt_width(ac):
+    """Bits of one allele of a non-(1,1) hom-ALT-category pair (ac >= 3)."""
+    return 2 if ac <= 4 else 4 if ac <= 16 else 8 if ac <= 256 else 16
+
+
+def _patch_ids(rec, cur, n, fmt, members, what):
+    if fmt == 0:
+        idx, cur = _bitarray_indices(rec, cur, len(members))
+        return [int(members[i]) for i in idx], cur
+    if fmt == 1:
+        ids, cur = _difflist_ids(rec, cur, n)
+        if any(b <= a for a, b in zip(ids, ids[1:])):
+            raise PgenError("multiallelic patch sample ids do not rise")
+        return ids, cur
+    raise PgenError(f"unsupported multiallelic {what} patch format")
+
+
+def _project_multiallelic(rec, cur, n, cats, alt_count, alt_ord):
+    """Copies of ALT ``alt_ord`` per sample (as categories 0/1/2, 3 missing)
+    and the cursor after the patch (:2704-2881)."""
+    if alt_count <= 1:
+        return cats.copy(), cur            # read as biallelic; the patch is not consumed
+    if cur >= len(rec):
+        raise PgenError("EOF before multiallelic patch header")
+    fmt = rec[cur]
+    cur += 1
+    f1, f2 = fmt & 15, fmt >> 4
+    het_alt, pair = {}, {}
+    if f1 != 15:
+        sids, cur = _patch_ids(rec, cur, n, f1, np.nonzero(cats == 1)[0], "het")
+        w = _het_width(alt_count)
+        vals, cur = _packed(rec, cur, w, len(sids))
+        for sid, v in zip(sids, vals):
+            het_alt[sid] = 2 if w == 0 else v + 2
+    if f2 != 15:
+        sids, cur = _patch_ids(rec, cur, n, f2, np.nonzero(cats == 2)[0], "hom-ALT")
+        k = len(sids)
+        if alt_count == 2:
+            flags, cur = _bitarray_indices(rec, cur, k)
+            two = set(flags)
+            for i, sid in enumerate(sids):
+                pair[sid] = (2, 2) if i in two else (1, 2)
+        else:
+            vals, cur = _packed(rec, cur, _homalt_width(alt_count), 2 * k)
+            for i, sid in enumerate(sids):
+                lo, hi = vals[2 * i] + 1, vals[2 * i + 1] + 1
+                pair[sid] = (min(lo, hi), max(lo, hi))
+    out = cats.copy()
+    for i in np.nonzero(cats == 1)[0]:
+        out[i] = 1 if het_alt.get(int(i), 1) == alt_ord else 0
+    for i in np.nonzero(cats == 2)[0]:
+        p = pair.get(int(i), (1, 1))
+        out[i] = int(p[0] == alt_ord) + int(p[1] == alt_ord)
+    return out, cur
+
+
 def parse_header(data: bytes):
     """-> dict(mode, variants, samples, offsets[V], types[V], lens[V])."""
     if len(data) < 12 or data[0] != 0x6C or data[1] != 0x1B:
@@ -210,8 +305,12 @@ def parse_header(data: bytes):
     mode = data[2]
     m, n = struct.unpack_from("<II", data, 3)
     if mode == 0x02:
+        # the reference's reader puts the body after 13 bytes, plus the
+        # reference-flag bit array in flag mode 3 (:2048-2057; its test at
+        # :3826-3866 asserts 12 + 1)
         rec = (n + 3) // 4
-        offs = 12 + rec * np.arange(m, dtype=np.uint64)
+        base = 13 + ((m + 7) // 8 if ((data[11] >> 6) & 3) == 3 else 0)
+        offs = base + rec * np.arange(m, dtype=np.uint64)
         return dict(mode=mode, variants=m, samples=n, offsets=offs,
                     types=np.zeros(m, np.uint8), lens=np.full(m, rec, np.uint32))
     if mode not in (0x10, 0x11):
@@ -287,17 +386,24 @@ def _main_track(rec, kind, n, anchor):
     return cats, cur
 
 
-def decode_to_bed(data: bytes) -> np.ndarray:
-    """Decode every variant -> [V][ceil(N/4)] .bed rows (padding fields = 01)."""
+def decode_to_bed(data: bytes, alt_counts=None, rows=None) -> np.ndarray:
+    """Decode -> [R][ceil(N/4)] .bed rows (padding fields = 01).
+
+    Without ``rows``: one row per variant (ALT 1). ``rows`` = [(variant, ALT
+    ordinal)] pairs of a virtual .bim; ``alt_counts`` = each input variant's
+    ALT count, needed when a record carries a multiallelic patch."""
     h = parse_header(data)
     m, n = h["variants"], h["samples"]
     bpv = (n + 3) // 4
-    out = np.zeros((m, bpv), np.uint8)
-    anchor, anchor_idx = None, -1
+    ac = None if alt_counts is None else [int(x) for x in alt_counts]
+    if ac is not None and len(ac) != m:
+        raise PgenError("one ALT count per variant")
+    # every record's main track, in file order (LD records read their anchors')
+    main, anchor, anchor_idx = [], None, -1
     for v in range(m):
         t = int(h["types"][v])
-        if t & 0b0000_1000:
-            raise PgenError(f"variant {v}: multiallelic tracks are not supported")
+        if (t & 0b0000_1000) and ac is None:
+            raise PgenError(f"variant {v}: multiallelic tracks need the ALT counts")
         if (t & 0b1000_0000) and not (t & 0b0110_0000):
             raise PgenError(f"variant {v}: phased dosage track without a dosage track")
         kind = t & 7
@@ -309,14 +415,27 @@ def decode_to_bed(data: bytes) -> np.ndarray:
         else:
             cats, cur = _main_track(rec, kind, n, None)
             anchor, anchor_idx = cats, v   # anchors are the raw main-track categories
+        main.append((rec, t, cats, cur))
+    plan = [(v, 1) for v in range(m)] if rows is None else list(rows)
+    out = np.zeros((len(plan), bpv), np.uint8)
+    for r, (v, j) in enumerate(plan):
+        rec, t, cats, cur = main[v]
+        a = 1 if ac is None else ac[v]
+        if ac is not None and not 1 <= j <= max(a, 1):
+            raise PgenError(f"row {r}: ALT ordinal {j} of a variant with {a} ALT alleles")
+        got = cats
+        if t & 0b0000_1000:
+            got, cur = _project_multiallelic(rec, cur, n, cats, a, j)
         if t & 0b0001_0000:
-            cur = _skip_phase(rec, cur, cats)
+            cur = _skip_phase(rec, cur, cats)       # het count of the main track
         if t & 0b0110_0000:
-            cats = _dosage_overlay(rec, cur, t, n, cats)
+            filled = _dosage_overlay(rec, cur, t, n, got)
+            if a <= 1 or j == 1:
+                got = filled
         codes = np.full(bpv * 4, 0b01, np.uint8)
-        codes[:n] = CAT_TO_BED[cats]
+        codes[:n] = CAT_TO_BED[got]
         q = codes.reshape(bpv, 4)
-        out[v] = q[:, 0] | (q[:, 1] << 2) | (q[:, 2] << 4) | (q[:, 3] << 6)
+        out[r] = q[:, 0] | (q[:, 1] << 2) | (q[:, 2] << 4) | (q[:, 3] << 6)
     return out
 
 

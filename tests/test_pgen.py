@@ -125,20 +125,28 @@ def test_decode_declines_without_a_device():
     assert st == _lib.GNM_DECLINED
 
 
-def encode_fixed_width(cats):
-    """A storage-mode 0x02 .pgen: 2-bit category arrays, no index."""
+def encode_fixed_width(cats, ref_flags: bool = False):
+    """A storage-mode 0x02 .pgen: 2-bit category arrays, no index, laid out
+    where the reference's reader looks for them: the body after 12 header
+    bytes and one more (shared/adapt_plink2.rs:2048-2057), and after one
+    reference-flag bit per variant when the format byte's bits 6-7 are 3."""
     V, n = cats.shape
     q = np.zeros((V, (n + 3) // 4 * 4), np.uint8)
     q[:, :n] = cats
     q = q.reshape(V, -1, 4)
     body = (q[..., 0] | (q[..., 1] << 2) | (q[..., 2] << 4) | (q[..., 3] << 6)).astype(np.uint8)
-    return b"\x6c\x1b\x02" + np.array([V, n], "<u4").tobytes() + b"\x00" + body.tobytes()
+    fmt = b"\xc0" if ref_flags else b"\x00"
+    flags = bytes((V + 7) // 8) if ref_flags else b""
+    return (b"\x6c\x1b\x02" + np.array([V, n], "<u4").tobytes() + fmt + b"\x00" + flags +
+            body.tobytes())
 
 
 def test_fixed_width_mode_oracle_and_dims():
     cats = synth.pgen_categories(4, 50, 301)
     data = encode_fixed_width(cats)
     np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(cats))
+    np.testing.assert_array_equal(pgen_oracle.decode_to_bed(encode_fixed_width(cats, True)),
+                                  expected_rows(cats))
     assert pgen_dims(data) == (50, 301)
     assert _status(data[:-1]) == _lib.GNM_ERR_IO
 
