@@ -112,6 +112,15 @@ SIGNATURES = {
     "gnm_pgen_check": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(gnm_error)]),
     "gnm_pgen_decode_list": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                        C.c_uint64, C.c_void_p, C.POINTER(gnm_error)]),
+    "gnm_pgen_open_alleles": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_int,
+                                        C.POINTER(C.c_void_p), C.POINTER(gnm_error)]),
+    "gnm_pgen_decode_alleles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                          C.c_void_p, C.c_uint64, C.c_void_p,
+                                          C.POINTER(gnm_error)]),
+    "gnm_score_pgen_alleles": (C.c_int, [C.POINTER(gnm_prep_view), C.c_void_p, C.c_uint64,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                         C.POINTER(gnm_run_options), C.c_void_p, C.c_void_p,
+                                         C.POINTER(gnm_error)]),
     "gnm_project_create": (C.c_int, [C.c_uint64, C.c_uint64, C.c_int, C.POINTER(C.c_void_p),
                                      C.POINTER(gnm_error)]),
     "gnm_project_destroy": (None, [C.c_void_p]),

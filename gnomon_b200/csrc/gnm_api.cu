@@ -1320,25 +1320,40 @@ static void project_block_impl(gnm_projector* pj, const uint8_t* packed, uint64_
 // The .pgen counterpart of the end-to-end run: the file is uploaded once, the
 // reconciled variants (required_bim_indices) are decoded on the device block
 // by block into one row buffer, and each block is accumulated as it lands.
+// With ALT counts, the .bim rows are a virtual .bim (the reference's split of
+// multiallelic variants, shared/adapt_plink2.rs:1295-1330): row r holds ALT
+// bim_alt[r] of .pgen variant bim_variant[r].
 static void score_pgen_impl(const gnm_prep_view* prep, const uint8_t* pgen, uint64_t pgen_len,
                             const gnm_run_options* opts, double* sums_out,
-                            uint32_t* missing_out) {
+                            uint32_t* missing_out, const uint32_t* alt_counts = nullptr,
+                            const uint64_t* bim_variant = nullptr,
+                            const uint32_t* bim_alt = nullptr, uint64_t bim_rows = 0) {
   if (!prep) fail(GNM_ERR_INVALID, "prep is NULL");
   if (!sums_out || !missing_out) fail(GNM_ERR_INVALID, "output buffers are NULL");
   const gnm_engine engine = opts ? opts->engine : GNM_ENGINE_AUTO;
   int device = opts ? opts->device : -1;
   device = resolve_device(device);
   validate_prep(prep);
-  std::unique_ptr<gnm_pgen, void (*)(gnm_pgen*)> pg(pgen_open_impl(pgen, pgen_len, device),
-                                                     gnm_pgen_close);
+  if (alt_counts && (!bim_variant || !bim_alt))
+    fail(GNM_ERR_INVALID, "bim_variant and bim_alt are needed with alt_counts");
+  std::unique_ptr<gnm_pgen, void (*)(gnm_pgen*)> pg(
+      pgen_open_impl(pgen, pgen_len, device, alt_counts), gnm_pgen_close);
   const uint64_t n = pgen_samples(pg.get()), m = pgen_variants(pg.get());
   if (n != prep->total_people_in_fam || (n + 3) / 4 != prep->bytes_per_variant)
     fail(GNM_ERR_INVALID, "the .pgen has " + std::to_string(n) + " samples, the preparation " +
                               std::to_string(prep->total_people_in_fam));
   const uint64_t V = prep->num_variants;
   std::vector<uint64_t> req(V);
+  std::vector<uint32_t> alts(alt_counts ? V : 0);
   for (uint64_t v = 0; v < V; ++v) {
     req[v] = prep->required_bim_indices ? prep->required_bim_indices[v] : v;
+    if (alt_counts) {
+      if (req[v] >= bim_rows)
+        fail(GNM_ERR_INVALID, "required .bim row " + std::to_string(req[v]) + " is past the " +
+                                  std::to_string(bim_rows) + " rows");
+      alts[v] = bim_alt[req[v]];
+      req[v] = bim_variant[req[v]];
+    }
     if (req[v] >= m)
       fail(GNM_ERR_INVALID, "required variant " + std::to_string(req[v]) +
                                 " is past the .pgen's " + std::to_string(m) + " variants");
@@ -1378,7 +1393,8 @@ static void score_pgen_impl(const gnm_prep_view* prep, const uint8_t* pgen, uint
   plan_reset_impl(plan.get(), st.s);
   for (uint64_t b0 = 0; b0 < V; b0 += B) {
     const uint64_t nb = std::min(B, V - b0);
-    pgen_decode_list_impl(pg.get(), req.data() + b0, nb, rows, pitch, st.s);
+    pgen_decode_list_impl(pg.get(), req.data() + b0, nb, rows, pitch, st.s,
+                          alt_counts ? alts.data() + b0 : nullptr);
     accumulate_impl(plan.get(), rows, pitch, b0, nb, st.s);
   }
   finalize_impl(plan.get(), d_sums, d_counts, true, st.s);
@@ -1407,6 +1423,18 @@ gnm_status gnm_score_pgen(const gnm_prep_view* prep, const uint8_t* pgen, uint64
                           const gnm_run_options* opts, double* sums_out, uint32_t* missing_out,
                           gnm_error* err) {
   return guarded(err, [&] { score_pgen_impl(prep, pgen, pgen_len, opts, sums_out, missing_out); });
+}
+
+gnm_status gnm_score_pgen_alleles(const gnm_prep_view* prep, const uint8_t* pgen,
+                                  uint64_t pgen_len, const uint32_t* alt_counts,
+                                  const uint64_t* bim_variant, const uint32_t* bim_alt,
+                                  uint64_t bim_rows, const gnm_run_options* opts,
+                                  double* sums_out, uint32_t* missing_out, gnm_error* err) {
+  return guarded(err, [&] {
+    if (!alt_counts) fail(GNM_ERR_INVALID, "alt_counts is NULL");
+    score_pgen_impl(prep, pgen, pgen_len, opts, sums_out, missing_out, alt_counts, bim_variant,
+                    bim_alt, bim_rows);
+  });
 }
 
 gnm_status gnm_project_create(uint64_t n_samples, uint64_t components, int device,

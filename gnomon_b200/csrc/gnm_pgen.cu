@@ -9,22 +9,23 @@
 // the GPU, straight into the engines' row layout.
 //
 // Supported: storage modes 0x02 (fixed-width hard calls) and 0x10 / 0x11
-// (variable-width) with biallelic records, with or without phase and dosage
-// tracks (dosages fill missing hard calls, see gnm_pgen_dosage), whose main
-// track is type 0 (2-bit),
+// (variable-width) with or without phase and dosage tracks (dosages fill
+// missing hard calls) and, given the variants' ALT counts, multiallelic
+// patches (each output row one ALT of a variant; see gnm_pgen_tracks), whose
+// main track is type 0 (2-bit),
 // 1 (two categories as a bit array + difflist), 2 / 3 (LD-compressed against
 // the most recent non-LD record of the same 2^16-variant block; 3 swaps REF and
 // ALT homozygotes after the patch) or 4 / 6 / 7 (all hom REF / hom ALT /
 // missing + difflist) — shared/adapt_plink2.rs:2237-2257, 2574-2666.  Phase
 // tracks follow the main track and do not change hard calls.  Records with
-// multiallelic tracks are rejected (the reference projects them onto each
-// ALT; this decoder does not).
+// multiallelic patches are rejected when no ALT counts are given.
 //
 // Layout of the work: the bijection category -> .bed code lets every step
 // run on .bed codes directly.  A decode is two launches over the same
-// records.  Kernel 1 decodes the non-LD records, one CTA each: they are few
-// and long (a table pass over a whole 2-bit or 1-bit array, or a fill), so
-// eight warps share one.  Kernel 2 decodes the LD-compressed records from
+// records, and a third (gnm_pgen_tracks, one CTA per output row) when some
+// record carries a multiallelic patch or a dosage track.  Kernel 1 decodes
+// the non-LD records, one CTA each: they are few and long (a table pass over
+// a whole 2-bit or 1-bit array, or a fill), so eight warps share one.  Kernel 2 decodes the LD-compressed records from
 // their anchors' rows, one warp each: they are many, and their work is a
 // chain of dependent byte reads, so 64 records per SM stay in flight.  A
 // difflist's groups of 64 entries go one per lane: a shuffle scan over the
@@ -50,7 +51,7 @@ constexpr uint32_t kPgThreads = 256;
 constexpr uint32_t kPgWarps = kPgThreads / 32;     // one record per warp
 constexpr uint64_t kPgMaxSamples = uint64_t(1) << 31;
 
-enum : uint32_t { kPgErrBounds = 1u, kPgErrPair = 2u };
+enum : uint32_t { kPgErrBounds = 1u, kPgErrPair = 2u, kPgErrPatch = 4u };
 
 constexpr uint32_t kNoAnchor = 0xFFFFFFFFu;
 
@@ -74,6 +75,10 @@ struct PgArgs {
   const uint32_t* arow;
   uint32_t* err;               // [0] error bits, [1] first bad variant (atomicMin)
   uint32_t any_dosage;         // some record carries a dosage track
+  const uint32_t* alt_counts;  // [V] ALT alleles per variant (null: every variant biallelic)
+  const uint32_t* alt_ords;    // [count] ALT (1-based) of each output row (null: ALT 1)
+  uint32_t any_multi;          // some record carries a multiallelic patch to read
+  uint32_t ma_smem;            // dynamic shared bytes of the tracks kernel (multiallelic rows)
 };
 
 // Row i of a decode: an output row, or a scratch row past the output's end.
@@ -590,15 +595,288 @@ __device__ bool cta_difflist_end(const Rec& r, uint32_t cur, uint64_t n, bool id
   return end != 0xFFFFFFFFu;
 }
 
-// One CTA per output row; rows whose record has no dosage track return at
-// once.  Runs after gnm_pgen_direct and gnm_pgen_ld have written the rows.
-__global__ void __launch_bounds__(kPgThreads) gnm_pgen_dosage(PgArgs a) {
+// Walk an id-only difflist that starts at `cur` (already checked whole by
+// cta_difflist_end): fn(e, id) for every entry e whose sample id is below n,
+// called by the thread that owns the entry's group of 64.  Returns false on
+// ids that do not rise or a group byte length that does not match (the same
+// on every thread).
+template <class F>
+__device__ bool cta_walk_ids(const Rec& r, uint32_t cur, uint64_t n, uint32_t* sh, F fn) {
+  uint64_t l = 0;
+  uint32_t c2 = cur;
+  r.varint(c2, l);
+  if (l == 0) return true;
+  const uint32_t len = uint32_t(l);
+  const uint32_t groups = (len + 63) / 64;
+  const uint32_t wid = n <= (1u << 8) ? 1 : n <= (1u << 16) ? 2 : n <= (1u << 24) ? 3 : 4;
+  const uint32_t first_at = c2;
+  const uint32_t glen_at = first_at + groups * wid;
+  const uint32_t deltas0 = glen_at + groups - 1;
+  auto first_id = [&](uint32_t g) {
+    uint64_t id = 0;
+    for (uint32_t k = 0; k < wid; ++k) id |= uint64_t(r.p[first_at + g * wid + k]) << (8 * k);
+    return id;
+  };
+  uint32_t base = deltas0;   // first delta byte of this chunk's first group
+  bool broken = false;
+  for (uint32_t g0 = 0; g0 < groups; g0 += blockDim.x) {
+    const uint32_t g = g0 + threadIdx.x;
+    const uint32_t mine = g + 1 < groups ? uint32_t(r.p[glen_at + g]) + 63u : 0u;
+    uint32_t total = 0;
+    uint32_t at = base + cta_exclusive(g < groups ? mine : 0u, sh, total);
+    if (g < groups && !broken) {
+      const uint32_t count = g + 1 < groups ? 64u : len - 64u * (groups - 1);
+      const uint32_t start = at;
+      uint64_t id = first_id(g);
+      for (uint32_t e = 0; e < count; ++e) {
+        if (e > 0) {
+          uint64_t d = 0;
+          if (!r.varint(at, d) || d == 0) {
+            broken = true;
+            break;
+          }
+          id += d;
+        }
+        if (id < n) fn(64u * g + e, id);
+      }
+      if (!broken && g + 1 < groups && (at != start + mine || id >= first_id(g + 1)))
+        broken = true;   // group length mismatch, or ids not rising into the next group
+    }
+    base += total;
+  }
+  return !__syncthreads_or(broken);
+}
+
+// ---- multiallelic patches --------------------------------------------------------
+// A record of a variant with two or more ALT alleles may carry, right after
+// its main track, a patch (vrtype bit 3, shared/adapt_plink2.rs:2704-2881):
+// one format byte (low nibble: hets, high nibble: hom-ALT category; 0 = a bit
+// array over that category's samples in order, 1 = an id-only difflist, 15 =
+// no patch), then per category the patched samples and their values: a het's
+// ALT minus 2 in a fixed width set by the ALT count, or a hom-ALT-category
+// pair's two ALTs minus 1 (two ALTs: one flag bit per sample, set = ALT 2 /
+// ALT 2, clear = ALT 1 / ALT 2).  Unpatched hets are REF / ALT 1 and unpatched
+// hom-ALTs ALT 1 / ALT 1.  A decoded row holds the copies of one ALT j as .bed
+// codes, the reference's virtual .bed splitting the variant into one row per
+// ALT.
+
+__device__ __forceinline__ uint32_t het_alt_width(uint32_t ac) {
+  return ac == 2 ? 0u : ac == 3 ? 1u : ac <= 5 ? 2u : ac <= 17 ? 4u : ac <= 257 ? 8u : 16u;
+}
+__device__ __forceinline__ uint32_t homalt_width(uint32_t ac) {
+  return ac <= 4 ? 2u : ac <= 16 ? 4u : ac <= 256 ? 8u : 16u;
+}
+// .bed code of `c` copies of the row's ALT
+__device__ __forceinline__ uint32_t copies_code(uint32_t c) {
+  return c == 2 ? 0u : (c == 1 ? 2u : 3u);
+}
+// Field e of a run of w-bit little-endian fields (1 <= w <= 16) at byte `at`;
+// the caller checked that the run lies inside the record.
+__device__ __forceinline__ uint32_t packed_field(const uint8_t* p, uint64_t at, uint32_t w,
+                                                 uint64_t e) {
+  const uint64_t bit = e * w;
+  const uint8_t* b = p + at + (bit >> 3);
+  const uint32_t s = uint32_t(bit & 7u);
+  uint32_t x = b[0];
+  if (s + w > 8) x |= uint32_t(b[1]) << 8;
+  if (s + w > 16) x |= uint32_t(b[2]) << 16;
+  return (x >> s) & ((1u << w) - 1u);
+}
+// Bits [b0, b0 + cnt) (cnt <= 16) of a bit array of `nbytes` bytes at `at`.
+__device__ __forceinline__ uint32_t bits_at(const uint8_t* p, uint64_t at, uint64_t nbytes,
+                                            uint64_t b0, uint32_t cnt) {
+  if (cnt == 0) return 0u;
+  const uint64_t byte0 = b0 >> 3;
+  const uint32_t s = uint32_t(b0 & 7u);
+  uint32_t x = 0;
+  for (uint32_t k = 0; k < 3 && 8 * k < s + cnt; ++k)
+    if (byte0 + k < nbytes) x |= uint32_t(p[at + byte0 + k]) << (8 * k);
+  return (x >> s) & ((1u << cnt) - 1u);
+}
+
+struct MaSection {
+  uint32_t fmt;       // 0 bit array, 1 id difflist, 15 none
+  uint32_t sel_at;    // the bit array or difflist
+  uint64_t sel_bytes; // bit array bytes
+  uint32_t k;         // patched samples
+  uint32_t vals_at;   // their values
+};
+
+// Parse one category's section at `cur` (every thread, same result); false =
+// it overruns the record.  `members`: the category's sample count.
+__device__ bool ma_section(const Rec& r, uint32_t& cur, uint32_t fmt, uint64_t n,
+                           uint32_t members, bool het, uint32_t ac, uint32_t* sh, MaSection& s) {
+  s.fmt = fmt;
+  s.k = 0;
+  s.sel_at = s.vals_at = cur;
+  s.sel_bytes = 0;
+  if (fmt == 15) return true;
+  if (fmt == 0) {
+    s.sel_bytes = (uint64_t(members) + 7) / 8;
+    if (uint64_t(cur) + s.sel_bytes > r.len) return false;
+    uint32_t part = 0;
+    for (uint64_t b = threadIdx.x; b < s.sel_bytes; b += blockDim.x) {
+      uint32_t byte = r.p[cur + b];
+      const uint64_t left = uint64_t(members) - 8 * b;
+      if (left < 8) byte &= (1u << left) - 1u;
+      part += __popc(byte);
+    }
+    s.k = cta_sum(part, sh);
+    cur += uint32_t(s.sel_bytes);
+  } else {
+    uint32_t end = 0;
+    if (!cta_difflist_end(r, cur, n, true, sh, end)) return false;
+    uint64_t l = 0;
+    uint32_t c2 = cur;
+    r.varint(c2, l);
+    s.k = uint32_t(l);
+    cur = end;
+  }
+  s.vals_at = cur;
+  const uint64_t vb = het ? (uint64_t(s.k) * het_alt_width(ac) + 7) / 8
+                          : ac == 2 ? (uint64_t(s.k) + 7) / 8
+                                    : (2 * uint64_t(s.k) * homalt_width(ac) + 7) / 8;
+  if (uint64_t(cur) + vb > r.len) return false;
+  cur += uint32_t(vb);
+  return true;
+}
+
+// ALT of the het in patch entry e.
+__device__ __forceinline__ uint32_t ma_het_alt(const Rec& r, const MaSection& s, uint32_t ac,
+                                               uint64_t e) {
+  const uint32_t w = het_alt_width(ac);
+  return w == 0 ? 2u : packed_field(r.p, s.vals_at, w, e) + 2u;
+}
+// Copies of ALT j in the hom-ALT-category pair of patch entry e.
+__device__ __forceinline__ uint32_t ma_hom_copies(const Rec& r, const MaSection& s, uint32_t ac,
+                                                  uint64_t e, uint32_t j) {
+  if (ac == 2) {
+    const bool two = (r.p[s.vals_at + (e >> 3)] >> (e & 7u)) & 1u;   // ALT 2 / ALT 2
+    return two ? (j == 2 ? 2u : 0u) : (j <= 2 ? 1u : 0u);
+  }
+  const uint32_t w = homalt_width(ac);
+  const uint32_t lo = packed_field(r.p, s.vals_at, w, 2 * e) + 1u;
+  const uint32_t hi = packed_field(r.p, s.vals_at, w, 2 * e + 1) + 1u;
+  return uint32_t(lo == j) + uint32_t(hi == j);
+}
+
+// Project a multiallelic record's row onto ALT j.  The row holds the main
+// track's codes; `orig` (shared, one word per 16 samples) gets a copy of
+// them, which the patch entries are checked against.  `cur` is at the patch
+// and ends past it.  Returns 0, or the error bit to set.
+__device__ uint32_t ma_project(const Rec& r, uint32_t& cur, uint64_t n, uint32_t ac, uint32_t j,
+                               uint32_t* row32, uint64_t words, uint32_t* orig, uint32_t* sh) {
+  auto valid = [&](uint64_t w) {   // 2-bit fields of real samples in word w
+    const uint64_t s0 = 16 * w;
+    return s0 + 16 <= n ? 0xFFFFFFFFu : (n > s0 ? (1u << (2 * (n - s0))) - 1u : 0u);
+  };
+  uint32_t hets = 0, homs = 0;
+  for (uint64_t w = threadIdx.x; w < words; w += blockDim.x) {
+    const uint32_t x = row32[w];
+    orig[w] = x;
+    hets += __popc((x >> 1) & ~x & 0x55555555u & valid(w));    // code 10
+    homs += __popc(~x & ~(x >> 1) & 0x55555555u & valid(w));   // code 00
+  }
+  hets = cta_sum(hets, sh);
+  homs = cta_sum(homs, sh);
+  if (cur >= r.len) return kPgErrBounds;
+  const uint32_t fmt = r.p[cur++];
+  const uint32_t f1 = fmt & 15u, f2 = fmt >> 4;
+  MaSection s1, s2;
+  if (f1 != 0 && f1 != 1 && f1 != 15) return kPgErrPatch;
+  if (!ma_section(r, cur, f1, n, hets, true, ac, sh, s1)) return kPgErrBounds;
+  if (f2 != 0 && f2 != 1 && f2 != 15) return kPgErrPatch;
+  if (!ma_section(r, cur, f2, n, homs, false, ac, sh, s2)) return kPgErrBounds;
+  const uint32_t het_dflt = j == 1 ? 2u : 3u;                // REF / ALT 1
+  const uint32_t hom_dflt = copies_code(j == 1 ? 2u : 0u);   // ALT 1 / ALT 1
+
+  // Pass 1, a word of 16 samples per thread: unpatched calls and the patches
+  // given as bit arrays (ranks within the category by CTA scans).
+  uint32_t base_h = 0, base_a = 0, base_hv = 0, base_av = 0;
+  for (uint64_t w0 = 0; w0 < words; w0 += blockDim.x) {
+    const uint64_t w = w0 + threadIdx.x;
+    uint32_t x = 0, hm = 0, am = 0;
+    if (w < words) {
+      x = orig[w];
+      hm = (x >> 1) & ~x & 0x55555555u & valid(w);
+      am = ~x & ~(x >> 1) & 0x55555555u & valid(w);
+    }
+    uint32_t tot = 0;
+    const uint32_t hr = base_h + cta_exclusive(__popc(hm), sh, tot);   // rank of the word's first het
+    base_h += tot;
+    const uint32_t ar = base_a + cta_exclusive(__popc(am), sh, tot);
+    base_a += tot;
+    const uint32_t hb = s1.fmt == 0 && w < words
+                            ? bits_at(r.p, s1.sel_at, s1.sel_bytes, hr, __popc(hm)) : 0u;
+    const uint32_t ab = s2.fmt == 0 && w < words
+                            ? bits_at(r.p, s2.sel_at, s2.sel_bytes, ar, __popc(am)) : 0u;
+    const uint32_t hv = base_hv + cta_exclusive(__popc(hb), sh, tot);   // value index of its first patch
+    base_hv += tot;
+    const uint32_t av = base_av + cta_exclusive(__popc(ab), sh, tot);
+    base_av += tot;
+    if (w < words) {
+      uint32_t y = x, hi = 0, ai = 0, hs = 0, as = 0;
+      for (uint32_t k = 0; k < 16; ++k) {
+        const uint32_t f = 2 * k;
+        uint32_t code;
+        if ((hm >> f) & 1u) {
+          code = het_dflt;
+          if ((hb >> hi) & 1u) code = ma_het_alt(r, s1, ac, hv + hs++) == j ? 2u : 3u;
+          ++hi;
+        } else if ((am >> f) & 1u) {
+          code = hom_dflt;
+          if ((ab >> ai) & 1u) code = copies_code(ma_hom_copies(r, s2, ac, av + as++, j));
+          ++ai;
+        } else {
+          continue;
+        }
+        y = (y & ~(3u << f)) | (code << f);
+      }
+      if (y != x) row32[w] = y;
+    }
+  }
+  __syncthreads();
+  // Pass 2: patches given as sample lists; a listed sample of the right
+  // category flips its field from the pass-1 code to the patched one.
+  bool ok = true;
+  if (s1.fmt == 1)
+    ok = cta_walk_ids(r, s1.sel_at, n, sh, [&](uint32_t e, uint64_t id) {
+      const uint32_t wd = uint32_t(id >> 4), f = 2 * uint32_t(id & 15u);
+      if (((orig[wd] >> f) & 3u) != 2u) return;
+      const uint32_t code = ma_het_alt(r, s1, ac, e) == j ? 2u : 3u;
+      if (code != het_dflt) atomicXor(row32 + wd, (code ^ het_dflt) << f);
+    });
+  if (ok && s2.fmt == 1)
+    ok = cta_walk_ids(r, s2.sel_at, n, sh, [&](uint32_t e, uint64_t id) {
+      const uint32_t wd = uint32_t(id >> 4), f = 2 * uint32_t(id & 15u);
+      if (((orig[wd] >> f) & 3u) != 0u) return;
+      const uint32_t code = copies_code(ma_hom_copies(r, s2, ac, e, j));
+      if (code != hom_dflt) atomicXor(row32 + wd, (code ^ hom_dflt) << f);
+    });
+  __syncthreads();
+  return ok ? 0u : kPgErrBounds;
+}
+
+// One CTA per output row; rows whose record has neither a multiallelic patch
+// (for a variant with two or more ALTs) nor a dosage track return at once.
+// Runs after gnm_pgen_direct and gnm_pgen_ld have written the rows, so LD
+// records read their anchors' raw calls.  Dynamic shared memory: one word per
+// 16 samples when the decode holds multiallelic rows.
+__global__ void __launch_bounds__(kPgThreads) gnm_pgen_tracks(PgArgs a) {
+  extern __shared__ uint32_t s_orig[];
   __shared__ uint32_t sh[kPgWarps + 2];
   const uint32_t i = blockIdx.x;
   if (i >= a.count) return;
   const uint32_t v = variant_at(a, i);
   const uint32_t t = a.types[v];
-  if (!(t & 0x60u)) return;
+  const uint32_t ac = a.alt_counts ? a.alt_counts[v] : 1u;
+  const uint32_t j = a.alt_ords ? a.alt_ords[i] : 1u;
+  // shared/adapt_plink2.rs:2348-2362: the patch is read only for a variant
+  // with two or more ALTs (otherwise the record reads as biallelic and the
+  // patch bytes are not skipped); only ALT 1 rows take dosages (:2420)
+  const bool multi = (t & 0x08u) && ac >= 2;
+  if (!multi && !(t & 0x60u)) return;
+  const bool apply_dosage = ac <= 1 || j == 1;
   const Rec r{a.pgen + a.offsets[v], a.lens[v]};
   const uint64_t n = a.n;
   const uint64_t bpv = (n + 3) / 4;
@@ -620,18 +898,32 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_dosage(PgArgs a) {
   }
   if (cur > r.len) return bad();
 
-  // ---- the phase track: one flag bit, per-het presence bits padded to a
-  // byte when the flag is set, one bit per phased het ----
+  // het calls of the main track (.bed code 10), which size the phase track
+  uint32_t h = 0;
   if (t & 0x10u) {
-    if (cur >= r.len) return bad();
-    uint32_t hets = 0;   // het calls of the main track (.bed code 10)
+    uint32_t hets = 0;
     for (uint64_t w = threadIdx.x; w < words; w += blockDim.x) {
       uint32_t x = row32[w];
       const uint64_t b0 = 4 * w;
       if (b0 + 4 > bpv) x &= (1u << (8 * (bpv - b0))) - 1u;   // bytes past the row
       hets += __popc((x >> 1) & ~x & 0x55555555u);
     }
-    const uint32_t h = cta_sum(hets, sh);
+    h = cta_sum(hets, sh);
+  }
+
+  // ---- the multiallelic patch ----
+  if (multi) {
+    const uint32_t e = ma_project(r, cur, n, ac, j, row32, words, s_orig, sh);
+    if (e) {
+      if (threadIdx.x == 0) flag(a, e, v);
+      return;
+    }
+  }
+
+  // ---- the phase track: one flag bit, per-het presence bits padded to a
+  // byte when the flag is set, one bit per phased het ----
+  if (t & 0x10u) {
+    if (cur >= r.len) return bad();
     uint64_t bits = 1 + uint64_t(h);
     if (r.p[cur] & 1u) {
       // presence bits 1 .. h, then one phase bit per present het
@@ -653,14 +945,18 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_dosage(PgArgs a) {
     cur = uint32_t(next);
   }
 
-  // ---- the dosage track ----
+  // ---- the dosage track (read for its bounds on every row, applied on rows
+  // of ALT 1); row words are read through L2 (a multiallelic patch may have
+  // just updated them with atomics) ----
+  if (!(t & 0x60u)) return;
   const bool b5 = t & 0x20u, b6 = t & 0x40u;
   if (b6 && !b5) {
     // dense: every sample's value
     if (uint64_t(cur) + 2 * n > r.len) return bad();
+    if (!apply_dosage) return;
     const uint8_t* vals = r.p + cur;
     for (uint64_t w = threadIdx.x; w < words; w += blockDim.x) {
-      const uint32_t x = row32[w];
+      const uint32_t x = __ldcg(row32 + w);
       uint32_t y = x;
 #pragma unroll 4
       for (uint32_t k = 0; k < 16; ++k) {
@@ -692,8 +988,8 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_dosage(PgArgs a) {
       }
       uint32_t total = 0;
       const uint32_t before = base + cta_exclusive(__popc(mask), sh, total);
-      if (w < words && mask) {
-        const uint32_t x = row32[w];
+      if (apply_dosage && w < words && mask) {
+        const uint32_t x = __ldcg(row32 + w);
         uint32_t y = x, rank = 0;
         for (uint32_t k = 0; k < 16; ++k) {
           if (!((mask >> k) & 1u)) continue;
@@ -720,55 +1016,19 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_dosage(PgArgs a) {
   uint64_t l = 0;
   uint32_t c2 = cur;
   r.varint(c2, l);
-  if (l == 0) return;
-  const uint32_t len = uint32_t(l);
-  if (uint64_t(list_end) + 2 * uint64_t(len) > r.len) return bad();
-  const uint32_t groups = (len + 63) / 64;
-  const uint32_t wid = n <= (1u << 8) ? 1 : n <= (1u << 16) ? 2 : n <= (1u << 24) ? 3 : 4;
-  const uint32_t first_at = c2;
-  const uint32_t glen_at = first_at + groups * wid;
-  const uint32_t deltas0 = glen_at + groups - 1;
-  auto first_id = [&](uint32_t g) {
-    uint64_t id = 0;
-    for (uint32_t k = 0; k < wid; ++k) id |= uint64_t(r.p[first_at + g * wid + k]) << (8 * k);
-    return id;
-  };
-  uint32_t base = deltas0;   // first delta byte of this chunk's first group
-  bool broken = false;
-  for (uint32_t g0 = 0; g0 < groups; g0 += blockDim.x) {
-    const uint32_t g = g0 + threadIdx.x;
-    const uint32_t mine = g + 1 < groups ? uint32_t(r.p[glen_at + g]) + 63u : 0u;
-    uint32_t total = 0;
-    uint32_t at = base + cta_exclusive(g < groups ? mine : 0u, sh, total);
-    if (g < groups) {
-      const uint32_t count = g + 1 < groups ? 64u : len - 64u * (groups - 1);
-      const uint32_t start = at;
-      uint64_t id = first_id(g);
-      for (uint32_t e = 0; e < count; ++e) {
-        if (e > 0) {
-          uint64_t d = 0;
-          if (!r.varint(at, d) || d == 0) {
-            broken = true;
-            break;
-          }
-          id += d;
-        }
-        if (id >= n) continue;
-        const uint32_t w = uint32_t(id >> 4), sh2 = 2 * uint32_t(id & 15u);
-        if (((row32[w] >> sh2) & 3u) != 1u) continue;
-        const uint64_t vat = uint64_t(list_end) + 2 * (64 * uint64_t(g) + e);
-        const uint32_t dv = uint32_t(r.p[vat]) | (uint32_t(r.p[vat + 1]) << 8);
-        const uint32_t code = dosage_code(dv);
-        // field is 01: xor it to the new code (ids rise, so no other lane
-        // writes this field; fields of one word commute)
-        if (code != 1u) atomicXor(row32 + w, (1u ^ code) << sh2);
-      }
-      if (!broken && g + 1 < groups && (at != start + mine || id >= first_id(g + 1)))
-        broken = true;   // group length mismatch, or ids not rising into the next group
-    }
-    base += total;
-  }
-  if (broken) flag(a, kPgErrBounds, v);
+  if (uint64_t(list_end) + 2 * l > r.len) return bad();
+  const bool ok = cta_walk_ids(r, cur, n, sh, [&](uint32_t e, uint64_t id) {
+    if (!apply_dosage) return;
+    const uint32_t w = uint32_t(id >> 4), sh2 = 2 * uint32_t(id & 15u);
+    if (((__ldcg(row32 + w) >> sh2) & 3u) != 1u) return;
+    const uint64_t vat = uint64_t(list_end) + 2 * uint64_t(e);
+    const uint32_t dv = uint32_t(r.p[vat]) | (uint32_t(r.p[vat + 1]) << 8);
+    const uint32_t code = dosage_code(dv);
+    // the field is 01: xor it to the new code (ids rise, so no other thread
+    // writes this field; fields of one word commute)
+    if (code != 1u) atomicXor(row32 + w, (1u ^ code) << sh2);
+  });
+  if (!ok) bad();
 }
 
 // ---- host ----------------------------------------------------------------------
@@ -788,7 +1048,7 @@ uint64_t le(const uint8_t* p, int bytes) {
 
 // Header of a .pgen (shared/adapt_plink2.rs:1512-1716): per-variant record
 // offsets, lengths and types.  Validates everything the kernels rely on.
-PgenIndex parse_pgen(const uint8_t* d, uint64_t len) {
+PgenIndex parse_pgen(const uint8_t* d, uint64_t len, bool have_alts = false) {
   if (!d || len < 12 || d[0] != 0x6C || d[1] != 0x1B) fail(GNM_ERR_IO, "not a .pgen (bad magic)");
   PgenIndex ix;
   const uint8_t mode = d[2];
@@ -849,9 +1109,9 @@ PgenIndex parse_pgen(const uint8_t* d, uint64_t len) {
   for (uint64_t v = 0; v < m; ++v) {
     if (ix.offsets[v] + ix.lens[v] > len || ix.offsets[v] > len)
       fail(GNM_ERR_IO, "truncated .pgen: record " + std::to_string(v) + " lies past the end");
-    if (ix.types[v] & 0x08u)
+    if ((ix.types[v] & 0x08u) && !have_alts)
       fail(GNM_ERR_INVALID, "variant " + std::to_string(v) +
-                                ": multiallelic records are not supported");
+                                ": a multiallelic record needs the variants' ALT counts");
     if ((ix.types[v] & 0x80u) && !(ix.types[v] & 0x60u))
       fail(GNM_ERR_IO, "variant " + std::to_string(v) +
                            ": phased dosage track without a dosage track");
@@ -871,6 +1131,7 @@ struct gnm_pgen {
   int device = 0;
   uint64_t variants = 0, samples = 0, file_bytes = 0, device_bytes = 0;
   std::vector<uint32_t> anchor_of;   // host copy: which anchors a decode needs
+  std::vector<uint32_t> alt_counts;  // host copy (empty: every variant biallelic)
   std::vector<void*> bufs;
   gnm::PgArgs base{};
   // list-mode buffers, grown on demand (device and host copies)
@@ -891,9 +1152,27 @@ struct gnm_pgen {
 
 namespace gnm {
 
-gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device) {
-  PgenIndex ix = parse_pgen(pgen, pgen_len);
+// Largest dynamic shared memory of a tracks CTA (one word per 16 samples of
+// a multiallelic row), under the 227 KB per-block limit.
+constexpr uint64_t kPgMaSmemMax = 220 * 1024;
+
+gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device,
+                         const uint32_t* alt_counts) {
+  PgenIndex ix = parse_pgen(pgen, pgen_len, alt_counts != nullptr);
   const uint64_t m = ix.variants;
+  bool any_multi = false;
+  if (alt_counts) {
+    for (uint64_t v = 0; v < m; ++v) {
+      if (alt_counts[v] < 1 || alt_counts[v] > 65535)
+        fail(GNM_ERR_INVALID, "variant " + std::to_string(v) + ": ALT count " +
+                                  std::to_string(alt_counts[v]) + " is outside 1..65535");
+      any_multi = any_multi || ((ix.types[v] & 0x08u) && alt_counts[v] >= 2);
+    }
+  }
+  const uint64_t ma_smem = any_multi ? ((ix.samples + 3) / 4 + 3) / 4 * 4 : 0;
+  if (ma_smem > kPgMaSmemMax)
+    fail(GNM_ERR_INVALID, "multiallelic records of more than " +
+                              std::to_string(kPgMaSmemMax / 4 * 16) + " samples");
   // one CTA per variant: the grid's x extent bounds the variant count
   if (m > 0x7FFFFFFEull) fail(GNM_ERR_INVALID, "more than 2^31 - 2 .pgen variants");
   // LD-compressed records diff against the most recent non-LD record of their
@@ -934,6 +1213,12 @@ gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device) {
   a.anchor_of = static_cast<const uint32_t*>(up(anchor_of.data(), m * 4, ".pgen index"));
   a.any_dosage = 0u;
   for (uint64_t v = 0; v < m && !a.any_dosage; ++v) a.any_dosage = (ix.types[v] & 0x60u) ? 1u : 0u;
+  a.alt_counts = alt_counts ? static_cast<const uint32_t*>(up(alt_counts, m * 4, ".pgen ALT counts"))
+                            : nullptr;
+  a.alt_ords = nullptr;
+  a.any_multi = any_multi ? 1u : 0u;
+  a.ma_smem = uint32_t(ma_smem);
+  pg->alt_counts.assign(alt_counts ? alt_counts : nullptr, alt_counts ? alt_counts + m : nullptr);
   const uint32_t init_err[2] = {0u, 0xFFFFFFFFu};
   a.err = static_cast<uint32_t*>(up(init_err, 8, ".pgen error word"));
   a.spitch = ((ix.samples + 3) / 4 + 15) / 16 * 16;
@@ -975,9 +1260,12 @@ static void launch_decode(const PgArgs& a, cudaStream_t s) {
   check_cuda(cudaGetLastError(), "pgen decode launch");
   gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen LD decode launch");
-  if (a.any_dosage) {   // missing hard calls take their dosages, on the finished rows
-    gnm_pgen_dosage<<<a.count, kPgThreads, 0, s>>>(a);
-    check_cuda(cudaGetLastError(), "pgen dosage launch");
+  if (a.any_dosage || a.any_multi) {   // patches and dosages, on the finished rows
+    if (a.ma_smem > 48 * 1024)
+      check_cuda(raise_smem_limit(reinterpret_cast<const void*>(gnm_pgen_tracks), int(a.ma_smem)),
+                 "pgen tracks shared memory");
+    gnm_pgen_tracks<<<a.count, kPgThreads, a.any_multi ? a.ma_smem : 0u, s>>>(a);
+    check_cuda(cudaGetLastError(), "pgen tracks launch");
   }
 }
 
@@ -985,10 +1273,21 @@ static void launch_decode(const PgArgs& a, cudaStream_t s) {
 // record whose anchor is not listed reads it from a scratch row the same
 // launch decodes; every such anchor is decoded once.
 void pgen_decode_list_impl(gnm_pgen* pg, const uint64_t* list, uint64_t count,
-                                  uint8_t* d_rows, uint64_t pitch, cudaStream_t s) {
+                                  uint8_t* d_rows, uint64_t pitch, cudaStream_t s,
+                                  const uint32_t* alt_ords) {
   if (!pg) fail(GNM_ERR_INVALID, "pgen handle is NULL");
   if (count == 0) return;
   if (!list) fail(GNM_ERR_INVALID, "variant list is NULL");
+  if (alt_ords) {
+    for (uint64_t i = 0; i < count; ++i) {
+      if (list[i] >= pg->variants) break;   // reported below
+      const uint32_t ac = pg->alt_counts.empty() ? 1u : pg->alt_counts[list[i]];
+      if (alt_ords[i] < 1 || alt_ords[i] > ac)
+        fail(GNM_ERR_INVALID, "row " + std::to_string(i) + ": ALT " + std::to_string(alt_ords[i]) +
+                                  " of variant " + std::to_string(list[i]) + ", which has " +
+                                  std::to_string(ac) + " ALT allele(s)");
+    }
+  }
   check_rows(pg, d_rows, pitch);
   if (count > 0x3FFFFFFFull) fail(GNM_ERR_INVALID, "more than 2^30 - 1 listed variants");
   std::vector<std::pair<uint32_t, uint32_t>> sorted(count);   // (variant, row)
@@ -1019,11 +1318,12 @@ void pgen_decode_list_impl(gnm_pgen* pg, const uint64_t* list, uint64_t count,
       h[count + i] = uint32_t(count) + sl->second;
     }
   }
-  // layout on the device: vids [count + extra], arow [count]
-  std::vector<uint32_t> dev(2 * count + extra.size());
+  // layout on the device: vids [count + extra], arow [count], ALTs [count]
+  std::vector<uint32_t> dev(2 * count + extra.size() + (alt_ords ? count : 0));
   std::copy(h.begin(), h.begin() + count, dev.begin());
   std::copy(extra.begin(), extra.end(), dev.begin() + count);
   std::copy(h.begin() + count, h.end(), dev.begin() + count + extra.size());
+  if (alt_ords) std::copy(alt_ords, alt_ords + count, dev.begin() + 2 * count + extra.size());
   pg->h_list.swap(dev);   // kept alive by the handle until the next call
   DeviceGuard g(pg->device);
   grow(pg, pg->d_list, pg->list_cap, pg->h_list.size(), sizeof(uint32_t), ".pgen variant list");
@@ -1040,6 +1340,7 @@ void pgen_decode_list_impl(gnm_pgen* pg, const uint64_t* list, uint64_t count,
   a.extra_rows = uint32_t(extra.size());
   a.vids = pg->d_list;
   a.arow = pg->d_list + count + extra.size();
+  a.alt_ords = alt_ords ? pg->d_list + 2 * count + extra.size() : nullptr;
   launch_decode(a, s);
 }
 
@@ -1081,8 +1382,9 @@ void pgen_check_impl(gnm_pgen* pg, cudaStream_t s) {
   check_cuda(cudaStreamSynchronize(s), "pgen decode");
   if (err[0])
     fail(GNM_ERR_IO, "malformed .pgen record (variant " + std::to_string(err[1]) +
-                         (err[0] & kPgErrPair ? ": bad 1-bit pair code or main-track type"
-                                              : ": overruns its length") +
+                         (err[0] & kPgErrPair    ? ": bad 1-bit pair code or main-track type"
+                          : err[0] & kPgErrPatch ? ": unsupported multiallelic patch format"
+                                                 : ": overruns its length") +
                          ")");
 }
 
@@ -1127,6 +1429,28 @@ gnm_status gnm_pgen_decode_list(gnm_pgen* pg, const uint64_t* variants, uint64_t
                                 uint8_t* d_rows, uint64_t pitch, void* stream, gnm_error* err) {
   return guarded(err, [&] {
     pgen_decode_list_impl(pg, variants, count, d_rows, pitch, static_cast<cudaStream_t>(stream));
+  });
+}
+
+gnm_status gnm_pgen_open_alleles(const uint8_t* pgen, uint64_t pgen_len,
+                                 const uint32_t* alt_counts, int device, gnm_pgen** out,
+                                 gnm_error* err) {
+  return guarded(err, [&] {
+    if (!out) fail(GNM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!alt_counts) fail(GNM_ERR_INVALID, "alt_counts is NULL");
+    const int dev = resolve_device(device);
+    *out = pgen_open_impl(pgen, pgen_len, dev, alt_counts);
+  });
+}
+
+gnm_status gnm_pgen_decode_alleles(gnm_pgen* pg, const uint64_t* variants,
+                                   const uint32_t* alt_ords, uint64_t count, uint8_t* d_rows,
+                                   uint64_t pitch, void* stream, gnm_error* err) {
+  return guarded(err, [&] {
+    if (count && !alt_ords) fail(GNM_ERR_INVALID, "alt_ords is NULL");
+    pgen_decode_list_impl(pg, variants, count, d_rows, pitch, static_cast<cudaStream_t>(stream),
+                          alt_ords);
   });
 }
 

@@ -104,9 +104,12 @@ struct PhaseTrace {
 void copy_to_device(void* dst, const void* src, uint64_t bytes, cudaStream_t s);
 
 // PLINK 2 .pgen decoding (gnm_pgen.cu), for the end-to-end .pgen run.
-gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device);
+// alt_counts: ALT alleles per variant (null: every variant read as biallelic);
+// alt_ords: the ALT (1-based) each listed row holds (null: ALT 1).
+gnm_pgen* pgen_open_impl(const uint8_t* pgen, uint64_t pgen_len, int device,
+                         const uint32_t* alt_counts = nullptr);
 void pgen_decode_list_impl(gnm_pgen* pg, const uint64_t* list, uint64_t count, uint8_t* d_rows,
-                           uint64_t pitch, cudaStream_t s);
+                           uint64_t pitch, cudaStream_t s, const uint32_t* alt_ords = nullptr);
 void pgen_check_impl(gnm_pgen* pg, cudaStream_t s);
 uint64_t pgen_samples(const gnm_pgen* pg);
 uint64_t pgen_variants(const gnm_pgen* pg);

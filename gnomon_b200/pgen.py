@@ -7,12 +7,14 @@ A1 = ALT dosage.  Here that decode runs on the device
 (``gnm_pgen_decode_device``), writing rows straight into HBM where
 ``DevicePlan`` reads them; the file's bytes cross PCIe once, compressed.
 
-Supported: storage modes 0x02 and 0x10 / 0x11 with biallelic records
-(main-track types 0-4, 6, 7; phase tracks are skipped; a dosage track fills
-missing hard calls with the nearest allele count within 0.10, as the
-reference's virtual .bed does, samples taken as diploid).  Records with
-multiallelic tracks are rejected with ``GNM_ERR_INVALID``, truncated or
-malformed files with ``GNM_ERR_IO``.
+Supported: storage modes 0x02 and 0x10 / 0x11 (main-track types 0-4, 6, 7;
+phase tracks are skipped; a dosage track fills missing hard calls with the
+nearest allele count within 0.10, as the reference's virtual .bed does,
+samples taken as diploid).  Given each variant's ALT count (the ``.pvar``'s
+ALT column), multiallelic records decode one row per (variant, ALT): the
+copies of that ALT, as the reference splits them (:2704-2881).  Without ALT
+counts they are rejected with ``GNM_ERR_INVALID``; truncated or malformed
+files give ``GNM_ERR_IO``.
 """
 from __future__ import annotations
 
@@ -78,9 +80,10 @@ def decode_to_device(data: PgenSource, device: Optional[int] = None,
 class PgenFile:
     """A ``.pgen`` resident on one device (``gnm_pgen_open``): decode any
     variant range on demand, asynchronously, e.g. block by block into a
-    streaming buffer.  Use from one stream at a time."""
+    streaming buffer.  Use from one stream at a time.  ``alt_counts`` (one
+    per variant) enables multiallelic records (``gnm_pgen_open_alleles``)."""
 
-    def __init__(self, data: PgenSource, device: Optional[int] = None):
+    def __init__(self, data: PgenSource, device: Optional[int] = None, alt_counts=None):
         self.lib = _lib.load()
         buf = _bytes(data)
         self.variants, self.samples = pgen_dims(buf)
@@ -88,8 +91,15 @@ class PgenFile:
         self.device = torch.cuda.current_device() if device is None else device
         handle = C.c_void_p()
         e = _lib.gnm_error()
-        _lib.check(self.lib.gnm_pgen_open(buf.ctypes.data, buf.nbytes, self.device,
-                                          C.byref(handle), C.byref(e)), e)
+        if alt_counts is None:
+            _lib.check(self.lib.gnm_pgen_open(buf.ctypes.data, buf.nbytes, self.device,
+                                              C.byref(handle), C.byref(e)), e)
+        else:
+            ac = np.ascontiguousarray(alt_counts, dtype=np.uint32).reshape(-1)
+            if len(ac) != self.variants:
+                raise ValueError("one ALT count per variant")
+            _lib.check(self.lib.gnm_pgen_open_alleles(buf.ctypes.data, buf.nbytes, ac.ctypes.data,
+                                                      self.device, C.byref(handle), C.byref(e)), e)
         self.handle = handle
 
     def close(self):
@@ -133,6 +143,20 @@ class PgenFile:
                                                  rows.data_ptr(), pitch, _stream_ptr(stream),
                                                  C.byref(e)), e)
 
+    def decode_alleles(self, rows: torch.Tensor, pitch: int, variants, alt_ords, stream=None):
+        """Enqueue the decode of (variant, ALT) pairs: row i = the copies of ALT
+        ``alt_ords[i]`` (1-based) of variant ``variants[i]``."""
+        lst = np.ascontiguousarray(variants, dtype=np.uint64).reshape(-1)
+        ords = np.ascontiguousarray(alt_ords, dtype=np.uint32).reshape(-1)
+        if len(ords) != len(lst):
+            raise ValueError("one ALT ordinal per listed variant")
+        if not (rows.is_cuda and rows.dtype == torch.uint8 and rows.numel() >= len(lst) * pitch):
+            raise ValueError("rows must be a CUDA uint8 tensor of at least count x pitch bytes")
+        e = _lib.gnm_error()
+        _lib.check(self.lib.gnm_pgen_decode_alleles(self.handle, lst.ctypes.data, ords.ctypes.data,
+                                                    len(lst), rows.data_ptr(), pitch,
+                                                    _stream_ptr(stream), C.byref(e)), e)
+
     def check(self, stream=None):
         """Wait for ``stream``; raise if any record decoded so far was malformed."""
         e = _lib.gnm_error()
@@ -140,15 +164,17 @@ class PgenFile:
 
 
 def score_pgen(prep: PreparationResult, data: PgenSource, engine: int = _lib.ENGINE_AUTO,
-               device: Optional[int] = None,
-               block_variants: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+               device: Optional[int] = None, block_variants: int = 0, alt_counts=None,
+               bim_variant=None, bim_alt=None) -> Tuple[np.ndarray, np.ndarray]:
     """Score a ``.pgen`` whose variants are the ``.bim``-order rows ``prep`` indexes
     (``gnm_score_pgen``): the reconciled variants (``required_bim_indices``)
     are decoded on the device block by block and scored as they land.
     Returns host (sums f64, missing counts u32), person-major like
     ``gnm_score_run``.  Multi-row loci (``prep.complex_rules``) are resolved on
     the CPU afterwards from the decoded rows, as ``try_run_cuda`` does for a
-    ``.bed``."""
+    ``.bed``.  With ``alt_counts`` the ``.bim`` is virtual
+    (``gnm_score_pgen_alleles``): row r holds ALT ``bim_alt[r]`` of variant
+    ``bim_variant[r]``."""
     from .pipeline import prep_view
     buf = _bytes(data)
     lib = _lib.load()
@@ -161,13 +187,33 @@ def score_pgen(prep: PreparationResult, data: PgenSource, engine: int = _lib.ENG
     opts.device = -1 if device is None else device
     opts.block_variants = block_variants
     e = _lib.gnm_error()
-    _lib.check(lib.gnm_score_pgen(C.byref(pv), buf.ctypes.data, buf.nbytes, C.byref(opts),
-                                  sums.ctypes.data, counts.ctypes.data, C.byref(e)), e)
+    if alt_counts is None:
+        _lib.check(lib.gnm_score_pgen(C.byref(pv), buf.ctypes.data, buf.nbytes, C.byref(opts),
+                                      sums.ctypes.data, counts.ctypes.data, C.byref(e)), e)
+    else:
+        ac = np.ascontiguousarray(alt_counts, dtype=np.uint32).reshape(-1)
+        bv = np.ascontiguousarray(bim_variant, dtype=np.uint64).reshape(-1)
+        ba = np.ascontiguousarray(bim_alt, dtype=np.uint32).reshape(-1)
+        if len(bv) != len(ba):
+            raise ValueError("bim_variant and bim_alt differ in length")
+        _lib.check(lib.gnm_score_pgen_alleles(C.byref(pv), buf.ctypes.data, buf.nbytes,
+                                              ac.ctypes.data, bv.ctypes.data, ba.ctypes.data,
+                                              len(bv), C.byref(opts), sums.ctypes.data,
+                                              counts.ctypes.data, C.byref(e)), e)
     if prep.complex_rules:
         from .complex import GenotypeSource, resolve_complex_variants
         m, n = pgen_dims(buf)
-        rows, pitch = decode_to_device(buf, device=device)
         bpv = (n + 3) // 4
+        if alt_counts is None:
+            rows, pitch = decode_to_device(buf, device=device)
+        else:                               # every row of the virtual .bim
+            m, pitch = len(bv), row_pitch(bpv)
+            dev = torch.cuda.current_device() if device is None else device
+            rows = torch.zeros(max(m, 1) * pitch, dtype=torch.uint8,
+                               device=torch.device("cuda", dev))
+            with PgenFile(buf, device=dev, alt_counts=ac) as pg:
+                pg.decode_alleles(rows, pitch, bv, ba)
+                pg.check()
         host = rows[:m * pitch].view(m, pitch)[:, :bpv].cpu().numpy().reshape(-1)
         resolve_complex_variants(prep.complex_rules, GenotypeSource.single(host, bpv),
                                  prep.output_idx_to_fam_idx, P, prep.score_names, sums,

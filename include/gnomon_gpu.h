@@ -282,11 +282,14 @@ gnm_status gnm_backward_dw_device(gnm_plan* plan, const uint8_t* d_rows, uint64_
  * and a dosage track: a hard call that is missing takes the nearest whole
  * allele count of its dosage when that lies within 0.10, as the reference's
  * reader coerces dosages (shared/adapt_plink2.rs:14-18); phased-dosage
- * tracks are skipped.  Records with multiallelic tracks, external-index
- * modes, and more than 2^31 samples are rejected with GNM_ERR_INVALID;
- * truncated or malformed files give GNM_ERR_IO.  The reference additionally
- * projects multiallelic records onto each ALT and applies sex-chromosome
- * ploidy from the .pvar / .psam; callers handle those. */
+ * tracks are skipped.  Multiallelic records (vrtype bit 3) need the
+ * variants' ALT counts (gnm_pgen_open_alleles): each decoded row then holds
+ * the copies of one ALT, as the reference's virtual .bim splits a
+ * multiallelic variant into one row per ALT (shared/adapt_plink2.rs:2704-
+ * 2881).  Without ALT counts such records, external-index modes and more
+ * than 2^31 samples are rejected with GNM_ERR_INVALID; truncated or
+ * malformed files give GNM_ERR_IO.  The reference additionally applies
+ * sex-chromosome ploidy from the .pvar / .psam; callers handle that. */
 
 /* Variant and sample counts from a .pgen header (host bytes). */
 gnm_status gnm_pgen_dims(const uint8_t* pgen, uint64_t pgen_len, uint64_t* num_variants,
@@ -338,6 +341,25 @@ gnm_status gnm_pgen_decode_list(gnm_pgen* pg, const uint64_t* variants, uint64_t
  * malformed (the message names the first such variant). */
 gnm_status gnm_pgen_check(gnm_pgen* pg, void* stream, gnm_error* err);
 
+/* gnm_pgen_open with each variant's ALT allele count (the .pvar's ALT column,
+ * 1..65535; the reference's VariantPlan alts_per_in, shared/adapt_plink2.rs:
+ * 740-768): multiallelic records are accepted and decode per ALT.  As in the
+ * reference, a record without a patch gives every ALT row the plain
+ * categories, a patched record of a variant with one ALT reads as
+ * biallelic, and only ALT 1 rows take dosages.  GNM_ERR_INVALID above
+ * 928,000 samples when the file holds patched multiallelic records. */
+gnm_status gnm_pgen_open_alleles(const uint8_t* pgen, uint64_t pgen_len,
+                                 const uint32_t* alt_counts, int device, gnm_pgen** out,
+                                 gnm_error* err);
+
+/* gnm_pgen_decode_list where row i holds the copies of ALT alt_ords[i]
+ * (1-based, at most the variant's ALT count) of variant variants[i]: the
+ * reference's (in_idx, alt_ord) mapping of a virtual .bim row
+ * (shared/adapt_plink2.rs:1295-1330). */
+gnm_status gnm_pgen_decode_alleles(gnm_pgen* pg, const uint64_t* variants,
+                                   const uint32_t* alt_ords, uint64_t count, uint8_t* d_rows,
+                                   uint64_t pitch, void* stream, gnm_error* err);
+
 /* gnm_score_run_ex with a .pgen (host bytes) as the genotype source: the
  * reference's virtual-.bed route (shared/adapt_plink2.rs:1093-1158), with the
  * decode on the device.  The .pgen's variants are the .bim rows
@@ -349,6 +371,16 @@ gnm_status gnm_pgen_check(gnm_pgen* pg, void* stream, gnm_error* err);
 gnm_status gnm_score_pgen(const gnm_prep_view* prep, const uint8_t* pgen, uint64_t pgen_len,
                           const gnm_run_options* opts, double* sums_out, uint32_t* missing_out,
                           gnm_error* err);
+
+/* gnm_score_pgen over a virtual .bim that splits multiallelic variants:
+ * .bim row r (what required_bim_indices index, bim_rows of them) holds ALT
+ * bim_alt[r] of .pgen variant bim_variant[r]; alt_counts as for
+ * gnm_pgen_open_alleles. */
+gnm_status gnm_score_pgen_alleles(const gnm_prep_view* prep, const uint8_t* pgen,
+                                  uint64_t pgen_len, const uint32_t* alt_counts,
+                                  const uint64_t* bim_variant, const uint32_t* bim_alt,
+                                  uint64_t bim_rows, const gnm_run_options* opts,
+                                  double* sums_out, uint32_t* missing_out, gnm_error* err);
 
 /* ---- HWE-PCA projection blocks --------------------------------------------
  * The GPU part of gnomon's projection onto a fitted HWE-PCA model

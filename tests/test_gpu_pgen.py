@@ -310,3 +310,108 @@ def test_score_from_dosage_pgen_equals_bed_of_the_filled_calls(cuda):
                      engine=engine)
         np.testing.assert_array_equal(c, bc)
         np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)
+
+
+# ---- multiallelic records ---------------------------------------------------------
+
+from gnomon_b200.pgen import PgenFile                       # noqa: E402
+from test_pgen import MA_COUNTS, alt_copy_rows, ma_case     # noqa: E402
+
+
+def allele_rows(data, n, alt_counts, rows):
+    """Decode (variant, ALT) rows into sentinel-filled device rows."""
+    bpv = (n + 3) // 4
+    pitch = (bpv + 127) // 128 * 128
+    out = torch.full((max(len(rows), 1) * pitch,), SENTINEL, dtype=torch.uint8, device="cuda")
+    with PgenFile(data, alt_counts=alt_counts) as pg:
+        pg.decode_alleles(out, pitch, [v for v, _ in rows], [j for _, j in rows])
+        pg.check()
+    host = out[:len(rows) * pitch].view(len(rows), pitch).cpu().numpy()
+    assert (host[:, bpv:] == SENTINEL).all(), "bytes past the row were changed"
+    return host[:, :bpv]
+
+
+@pytest.mark.parametrize("n", [3, 300, 4097, 70001])
+@pytest.mark.parametrize("het_fmt,hom_fmt", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_multiallelic_rows(cuda, n, het_fmt, hom_fmt):
+    """Every (variant, ALT) row of variants with 1-300 ALTs, patches as bit
+    arrays or sample lists, with a phase track behind them."""
+    alleles, rows = ma_case(n, seed=n + het_fmt * 2 + hom_fmt)
+    rows = rows if n < 10_000 else [r for r in rows if r[1] <= 6]
+    data = synth.encode_pgen_multiallelic(alleles, MA_COUNTS, het_fmt, hom_fmt, phase="partial")
+    got = allele_rows(data, n, MA_COUNTS, rows)
+    np.testing.assert_array_equal(got, pgen_oracle.decode_to_bed(data, MA_COUNTS, rows))
+    np.testing.assert_array_equal(got, alt_copy_rows(alleles, rows))
+
+
+def test_multiallelic_edges_and_dosages(cuda):
+    """The reference's edges: an unpatched record gives every ALT row the plain
+    categories, a patched record of a one-ALT variant reads as biallelic, and
+    only ALT 1 rows take dosages; rows listed in any order, ALTs repeated."""
+    n = 515
+    alleles, rows = ma_case(n, seed=11)
+    cats = synth.multiallelic_categories(alleles)
+    dos = np.full(cats.shape, 65535, np.uint16)
+    dos[cats == 3] = 32768
+    patch = np.arange(len(MA_COUNTS)) % 3 != 2
+    data = synth.encode_pgen_multiallelic(alleles, MA_COUNTS, 1, 0, patch=patch, dosage=dos,
+                                          dosage_kind="bits", phase="all")
+    rng = np.random.default_rng(2)
+    rows = [rows[i] for i in rng.permutation(len(rows))] + rows[:5]
+    np.testing.assert_array_equal(allele_rows(data, n, MA_COUNTS, rows),
+                                  pgen_oracle.decode_to_bed(data, MA_COUNTS, rows))
+    ones = [1] * len(MA_COUNTS)
+    plain_rows = [(v, 1) for v in range(len(MA_COUNTS))]
+    np.testing.assert_array_equal(allele_rows(data, n, ones, plain_rows),
+                                  pgen_oracle.decode_to_bed(data, ones, plain_rows))
+
+
+def test_multiallelic_argument_and_record_errors(cuda):
+    n = 200
+    alleles, rows = ma_case(n, seed=4)
+    data = synth.encode_pgen_multiallelic(alleles, MA_COUNTS, 0, 0)
+    pitch = 128
+    out = torch.zeros(4 * pitch, dtype=torch.uint8, device="cuda")
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        PgenFile(data)                                     # ALT counts needed
+    assert ei.value.status == _lib.GNM_ERR_INVALID
+    with pytest.raises(_lib.GnomonGpuError) as ei:
+        PgenFile(data, alt_counts=[0] + MA_COUNTS[1:])     # a variant with no ALT
+    assert ei.value.status == _lib.GNM_ERR_INVALID
+    with PgenFile(data, alt_counts=MA_COUNTS) as pg:
+        for bad in ([1], [0], [3]):                        # variant 1 has two ALTs
+            with pytest.raises(_lib.GnomonGpuError) as ei:
+                pg.decode_alleles(out, pitch, [1], bad if bad != [1] else [9])
+            assert ei.value.status == _lib.GNM_ERR_INVALID
+    # one 3-ALT record (2-bit main track) whose patch is cut short or has an
+    # unknown format: malformed, as the oracle finds too
+    types, recs = synth._pgen_records(np.tile(np.arange(4, dtype=np.uint8), n // 4)[None, :n])
+    main = recs[0]
+    assert types[0] & 7 == 0
+    for patch in (b"\x00", b"\x02", b"\xf1\x05"):       # no bit array; format 2; list cut
+        bad = synth._pgen_file(n, [types[0] | 0x08], [main + patch])
+        with pytest.raises(pgen_oracle.PgenError):
+            pgen_oracle.decode_to_bed(bad, [3], [(0, 2)])
+        with PgenFile(bad, alt_counts=[3]) as pg:
+            pg.decode_alleles(out, pitch, [0], [2])
+            with pytest.raises(_lib.GnomonGpuError) as ei:
+                pg.check()
+            assert ei.value.status == _lib.GNM_ERR_IO
+
+
+def test_score_pgen_over_a_split_bim(cuda):
+    """Scoring through a virtual .bim of (variant, ALT) rows equals scoring the
+    oracle's decoded rows as a .bed."""
+    n = 777
+    alleles, rows = ma_case(n, seed=21)
+    rows = [r for r in rows if r[1] <= 40]             # 75 virtual .bim rows
+    data = synth.encode_pgen_multiallelic(alleles, MA_COUNTS, 1, 1)
+    bed_rows = pgen_oracle.decode_to_bed(data, MA_COUNTS, rows)
+    w, prep, _, _ = synth_case(n, len(rows), 4)
+    for engine in (_lib.ENGINE_PLAIN, _lib.ENGINE_TENSOR):
+        s, c = score_pgen(prep, data, engine=engine, alt_counts=MA_COUNTS,
+                          bim_variant=[v for v, _ in rows], bim_alt=[j for _, j in rows])
+        bs, bc = run(PipelineContext(prep), np.ascontiguousarray(bed_rows).reshape(-1),
+                     engine=engine)
+        np.testing.assert_array_equal(c, bc)
+        np.testing.assert_allclose(s, bs, rtol=1e-12, atol=1e-12)

@@ -299,3 +299,81 @@ def test_oracle_dosage_tracks_fill_missing_calls(kind, phase):
             want[v, i] = hc
     assert (want != cats).any()
     np.testing.assert_array_equal(pgen_oracle.decode_to_bed(data), expected_rows(want))
+
+
+# ---- multiallelic records (vrtype bit 3) ---------------------------------------
+
+def alt_copy_rows(alleles, rows):
+    """.bed rows holding the copies of ALT j per (variant, j), padding 01."""
+    out = []
+    n = alleles.shape[1]
+    for v, j in rows:
+        cnt = (alleles[v] == j).sum(axis=1)
+        cat = np.where((alleles[v] < 0).any(axis=1), 3, cnt).astype(np.uint8)
+        codes = np.full((n + 3) // 4 * 4, 0b01, np.uint8)
+        codes[:n] = pgen_oracle.CAT_TO_BED[cat]
+        q = codes.reshape(-1, 4)
+        out.append(q[:, 0] | (q[:, 1] << 2) | (q[:, 2] << 4) | (q[:, 3] << 6))
+    return np.array(out, np.uint8)
+
+
+MA_COUNTS = [1, 2, 3, 5, 2, 18, 4, 300]
+
+
+def ma_case(n, seed=7):
+    alleles = synth.multiallelic_alleles(seed, MA_COUNTS, n)
+    alleles[0] = np.minimum(alleles[0], 1)          # a biallelic variant among them
+    rows = [(v, j) for v, a in enumerate(MA_COUNTS) for j in range(1, a + 1)]
+    return alleles, rows
+
+
+def test_reference_multiallelic_known_answer():
+    """shared/adapt_plink2.rs:3806-3815: a het patched to ALT 3 and a hom-ALT
+    pair patched to ALT 3 / ALT 3, projected onto ALT 1 of a 3-ALT variant."""
+    rec = bytes([0x00, 0x01, 0x01, 0x01, 0x0A])
+    out, cur = pgen_oracle._project_multiallelic(rec, 0, 3, np.array([1, 2, 2], np.uint8), 3, 1)
+    assert list(out) == [0, 0, 2] and cur == len(rec)
+
+
+@pytest.mark.parametrize("het_fmt,hom_fmt", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_oracle_projects_multiallelic_records(het_fmt, hom_fmt):
+    alleles, rows = ma_case(301)
+    data = synth.encode_pgen_multiallelic(alleles, MA_COUNTS, het_fmt, hom_fmt, phase="partial")
+    got = pgen_oracle.decode_to_bed(data, alt_counts=MA_COUNTS, rows=rows)
+    np.testing.assert_array_equal(got, alt_copy_rows(alleles, rows))
+
+
+def test_oracle_keeps_the_references_multiallelic_edges():
+    alleles, rows = ma_case(200, seed=3)
+    cats = synth.multiallelic_categories(alleles)
+    # no patch: every ALT row reads the plain categories (ALT 1's copies where
+    # the record is right, as :2348-2362 reads it)
+    plain = synth.encode_pgen_multiallelic(alleles, MA_COUNTS, patch=np.zeros(len(MA_COUNTS), bool))
+    got = pgen_oracle.decode_to_bed(plain, alt_counts=MA_COUNTS, rows=rows)
+    want = expected_rows(cats)[[v for v, _ in rows]]
+    np.testing.assert_array_equal(got, want)
+    # a patched record of a variant given one ALT reads as biallelic
+    data = synth.encode_pgen_multiallelic(alleles, MA_COUNTS)
+    ones = [1] * len(MA_COUNTS)
+    got = pgen_oracle.decode_to_bed(data, alt_counts=ones)
+    np.testing.assert_array_equal(got, expected_rows(cats))
+    with pytest.raises(pgen_oracle.PgenError):
+        pgen_oracle.decode_to_bed(data)               # ALT counts needed
+    with pytest.raises(pgen_oracle.PgenError):
+        pgen_oracle.decode_to_bed(data, alt_counts=MA_COUNTS, rows=[(1, 3)])   # only 2 ALTs
+
+
+def test_oracle_multiallelic_dosage_only_on_alt1():
+    alleles, rows = ma_case(150, seed=5)
+    cats = synth.multiallelic_categories(alleles)
+    dos = np.full(cats.shape, 65535, np.uint16)
+    dos[cats == 3] = 16384                             # one copy for every missing call
+    data = synth.encode_pgen_multiallelic(alleles, MA_COUNTS, dosage=dos)
+    got = pgen_oracle.decode_to_bed(data, alt_counts=MA_COUNTS, rows=rows)
+    want = alt_copy_rows(alleles, rows)
+    for r, (v, j) in enumerate(rows):
+        if j == 1 or MA_COUNTS[v] <= 1:
+            filled = alleles.copy()
+            filled[v][(alleles[v] < 0).any(axis=1)] = [0, j]
+            want[r] = alt_copy_rows(filled, [(v, j)])[0]
+    np.testing.assert_array_equal(got, want)
