@@ -528,15 +528,9 @@ static gnm_plan* plan_create_impl(const gnm_prep_view* prep, gnm_engine engine, 
 static void plan_reset_impl(gnm_plan* p, cudaStream_t s) {
   DeviceGuard g(p->device);
   if (p->engine == GNM_ENGINE_PLAIN) {
-    // the slots in use of every score: K rows of slots x part_stride entries
-    const uint64_t row = uint64_t(p->splits_alloc) * p->part_stride;
-    const uint64_t used = uint64_t(p->slots) * p->part_stride;
-    check_cuda(cudaMemset2DAsync(p->d_part_sum, row * sizeof(double), 0, used * sizeof(double),
-                                 p->K, s),
-               "reset partials");
-    check_cuda(cudaMemset2DAsync(p->d_part_cnt, row * sizeof(uint32_t), 0,
-                                 used * sizeof(uint32_t), p->K, s),
-               "reset partials");
+    // nothing to clear: the next accumulate writes the slots it covers, and
+    // finalize sums only slots written since this reset
+    p->valid_slots = 0;
   } else {
     tensor_reset(p, s);
   }
@@ -557,6 +551,23 @@ static void accumulate_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, 
   const uint64_t stages = (nv + kPlainRows - 1) / kPlainRows;
   const uint32_t sps = uint32_t((stages + p->splits - 1) / p->splits);
   const uint32_t lsps = uint32_t((stages + p->last_splits - 1) / p->last_splits);
+  // Slots this launch covers (every tile gets the same count).  The first
+  // launch after a reset writes them; a later one adds, after clearing any
+  // slots past those written so far.
+  const uint32_t covered = uint32_t((stages + sps - 1) / sps);
+  const bool store = p->valid_slots == 0;
+  if (!store && covered > p->valid_slots) {
+    const uint64_t row = uint64_t(p->splits_alloc) * p->part_stride;
+    const uint64_t off = uint64_t(p->valid_slots) * p->part_stride;
+    const uint64_t add = uint64_t(covered - p->valid_slots) * p->part_stride;
+    check_cuda(cudaMemset2DAsync(p->d_part_sum + off, row * sizeof(double), 0,
+                                 add * sizeof(double), p->K, s),
+               "clear partials");
+    check_cuda(cudaMemset2DAsync(p->d_part_cnt + off, row * sizeof(uint32_t), 0,
+                                 add * sizeof(uint32_t), p->K, s),
+               "clear partials");
+  }
+  p->valid_slots = std::max(p->valid_slots, covered);
   for (uint64_t k = 0; k < p->K; ++k) {
     PlainArgs a;
     a.tables = plain_tables_for(p, k, v0, nv, s);
@@ -570,6 +581,7 @@ static void accumulate_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, 
     a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_stride = p->part_stride;
     a.err = p->d_err;
+    a.store = store ? 1u : 0u;
     check_cuda(launch_plain_accumulate(map, a, p->kernel, s), "plain accumulate launch");
     ++p->launches;
   }
@@ -587,7 +599,7 @@ static void finalize_impl(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool 
     a.part_sum = p->d_part_sum + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_cnt = p->d_part_cnt + k * uint64_t(p->splits_alloc) * p->part_stride;
     a.part_stride = p->part_stride;
-    a.num_splits = p->slots;
+    a.num_splits = p->valid_slots;
     a.baseline = add_baseline ? p->d_baseline : p->d_zero_base;
     a.out_to_fam = p->d_out_to_fam;
     a.num_people = p->P;

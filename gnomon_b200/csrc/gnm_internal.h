@@ -55,6 +55,7 @@ struct PlainArgs {
   uint32_t* part_cnt;
   uint64_t part_stride;
   uint32_t* err;
+  uint32_t store = 0;      // 1: write the partials (first launch since a reset); 0: add to them
 };
 
 struct FinalizeArgs {

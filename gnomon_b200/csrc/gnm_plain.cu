@@ -464,33 +464,62 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     return;
   }
 
-  // FP64 partials for this (split, person) accumulate across calls.  Warps
-  // that only held padding added nothing: their slots stay as they are.
+  // FP64 partials for this (split, person) accumulate across calls; the first
+  // launch after a reset writes them (every split of every tile has a CTA, so
+  // every slot it covers is written).  Warps that only held padding added
+  // nothing: their slots (people past the row) stay as they are.
   if (!warp_active) return;
   const uint64_t person0 = uint64_t(tile) * (TILE * 4) + uint64_t(tid) * 16;
   double* ps = a.part_sum + uint64_t(split) * a.part_stride + person0;
   uint32_t* pc = a.part_cnt + uint64_t(split) * a.part_stride + person0;
+  if (a.store) {
 #pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    ps[i] += acc64[i];
-    pc[i] += cnt[i];
+    for (int i = 0; i < 16; ++i) {
+      ps[i] = acc64[i];
+      pc[i] = cnt[i];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      ps[i] += acc64[i];
+      pc[i] += cnt[i];
+    }
   }
 }
 
-// out[o*K + k] = init + sum_s part[s][fam(o)] in split order.  One launch per
-// score column k (partials of column k).  init = baseline[k] (fresh run).
-__global__ void gnm_finalize(FinalizeArgs a) {
-  const uint64_t o = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (o >= a.num_people) return;
-  const uint64_t f = a.out_to_fam ? a.out_to_fam[o] : o;
-  double s = a.baseline[a.k];
+// out[o*K + k] = init + sum over splits of part[s][fam(o)], init = baseline[k]
+// (fresh run).  One launch per score column k.  A CTA takes 32 people; warp g
+// sums splits g, g + 8, g + 16, ... of each (a lane per person, so every
+// load is 32 consecutive people of one split), and lane o of warp 0 adds the
+// eight sums in order g = 0..7: a fixed order, so results are deterministic.
+constexpr uint32_t kFinWarps = 8;
+__global__ void __launch_bounds__(32 * kFinWarps) gnm_finalize(FinalizeArgs a) {
+  __shared__ double s_sum[kFinWarps][32];
+  __shared__ uint32_t s_cnt[kFinWarps][32];
+  const uint32_t lane = threadIdx.x & 31u, g = threadIdx.x >> 5;
+  const uint64_t o = uint64_t(blockIdx.x) * 32 + lane;
+  double s = 0.0;
   uint32_t c = 0;
-  for (uint32_t sp = 0; sp < a.num_splits; ++sp) {
-    s += a.part_sum[uint64_t(sp) * a.part_stride + f];
-    c += a.part_cnt[uint64_t(sp) * a.part_stride + f];
+  if (o < a.num_people) {
+    const uint64_t f = a.out_to_fam ? a.out_to_fam[o] : o;
+    for (uint32_t sp = g; sp < a.num_splits; sp += kFinWarps) {
+      s += a.part_sum[uint64_t(sp) * a.part_stride + f];
+      c += a.part_cnt[uint64_t(sp) * a.part_stride + f];
+    }
   }
-  a.sums[o * a.K + a.k] = s;
-  a.counts[o * a.K + a.k] = c;
+  s_sum[g][lane] = s;
+  s_cnt[g][lane] = c;
+  __syncthreads();
+  if (g != 0 || o >= a.num_people) return;
+  double t = a.baseline[a.k];
+  uint32_t n = 0;
+#pragma unroll
+  for (uint32_t w = 0; w < kFinWarps; ++w) {
+    t += s_sum[w][lane];
+    n += s_cnt[w][lane];
+  }
+  a.sums[o * a.K + a.k] = t;
+  a.counts[o * a.K + a.k] = n;
 }
 
 __global__ void gnm_decode(const uint8_t* rows, uint64_t pitch, uint64_t nv, uint64_t np,
@@ -626,8 +655,8 @@ cudaError_t launch_plain_accumulate(const CUtensorMap& map, const PlainArgs& a, 
 }
 
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s) {
-  const uint32_t blocks = uint32_t((a.num_people + 255) / 256);
-  gnm_finalize<<<blocks ? blocks : 1, 256, 0, s>>>(a);
+  const uint32_t blocks = uint32_t((a.num_people + 31) / 32);
+  gnm_finalize<<<blocks ? blocks : 1, 32 * kFinWarps, 0, s>>>(a);
   return cudaGetLastError();
 }
 

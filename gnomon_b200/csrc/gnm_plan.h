@@ -132,6 +132,7 @@ struct gnm_plan {
   uint32_t splits = 0;         // variant splits of each full tile
   uint32_t last_splits = 0;    // variant splits of the last (partly populated) tile
   uint32_t slots = 0;          // partial slots in use: max(splits, last_splits)
+  uint32_t valid_slots = 0;    // slots written since the last reset (finalize sums these)
   uint32_t splits_alloc = 0;   // partial slots allocated per score (autotune range)
   uint32_t raster = 0;         // tensor engine CTA order: 0 people-tile fastest, 1 score-tile
   uint64_t part_stride = 0;    // people per partial slot (bpv rounded up to 2048 bytes, x4)
