@@ -320,6 +320,10 @@ static void plain_shape_fixed(gnm_plan* p, uint32_t kernel, uint32_t splits) {
   p->slots = uint32_t(sp);
 }
 
+// The autotuner's split multipliers (of the SMs' CTA slots).
+constexpr double kPlainSplitMults[] = {0.5, 1.0, 2.0, 3.0, 4.0, 6.0, 8.0};
+constexpr double kPlainMaxSplitMult = 8.0;
+
 static void plain_shape(gnm_plan* p, uint32_t kernel, double mult) {
   const uint32_t tile_bytes = plain_tile_bytes(kernel);
   const uint64_t tiles = std::max<uint64_t>(1, (p->bpv + tile_bytes - 1) / tile_bytes);
@@ -338,7 +342,7 @@ static void plain_geometry(gnm_plan* p) {
   plain_shape(p, kPlainDefaultKernel, 1.0);
   // keep partials of all scores within 8 GiB (many score columns still get a
   // full-occupancy grid); allocate room for the autotuner's largest candidate
-  // (four times the CTA slots, any kernel)
+  // (eight times the CTA slots, any kernel)
   const uint64_t per_split_bytes = p->K * p->part_stride * 12;
   const uint64_t cap = uint64_t(8) << 30;
   uint64_t alloc = p->slots;
@@ -347,7 +351,7 @@ static void plain_geometry(gnm_plan* p) {
     probe.V = p->V;
     probe.bpv = p->bpv;
     probe.num_sms = p->num_sms;
-    plain_shape(&probe, kn, 4.0);
+    plain_shape(&probe, kn, kPlainMaxSplitMult);
     alloc = std::max<uint64_t>(alloc, probe.slots);
   }
   while (alloc > 1 && alloc * per_split_bytes > cap) --alloc;
@@ -629,7 +633,8 @@ static void sync_impl(gnm_plan* p, cudaStream_t s) {
 // and 4, 2 and 1 CTAs per SM, with or without a producer warp; a narrow
 // cohort fills every warp of a narrow tile) times the split count (0.5x to 4x
 // the SMs' CTA slots: fewer splits write fewer FP64 partials, more splits
-// even out the last wave).  Tensor engine
+// even out the last wave).  A candidate is timed over accumulate + finalize,
+// since the finalize reads every split's partials.  Tensor engine
 // with more than 64 scores: the CTA raster order (people tiles fastest: CTAs
 // in flight share weight-limb tiles in L2; score tiles fastest: they share
 // genotype tiles).
@@ -647,10 +652,20 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
       cudaEventDestroy(b);
     }
   } ev{e0, e1};
+  // scratch outputs for the plain engine's finalize
+  struct Scratch {
+    void* p = nullptr;
+    ~Scratch() { pool_free(p); }
+  } out;
+  const uint64_t PK = std::max<uint64_t>(1, p->P * p->K);
+  if (p->engine == GNM_ENGINE_PLAIN) out.p = pool_alloc(p->device, PK * 12, "autotune outputs");
   auto time_once = [&]() {
     plan_reset_impl(p, s);
     check_cuda(cudaEventRecord(e0, s), "event");
     accumulate_impl(p, d_rows, pitch, 0, nv, s);
+    if (out.p)
+      finalize_impl(p, static_cast<double*>(out.p),
+                    reinterpret_cast<uint32_t*>(static_cast<double*>(out.p) + PK), true, s);
     check_cuda(cudaEventRecord(e1, s), "event");
     sync_impl(p, s);
     float ms = 0.f;
@@ -669,7 +684,7 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
     const char* tr = std::getenv("GNM_TRACE");
     const bool trace = tr && std::strcmp(tr, "0") != 0;
     for (uint32_t kn : kPlainKernels) {
-      for (double m : {0.5, 1.0, 2.0, 3.0, 4.0}) {
+      for (double m : kPlainSplitMults) {
         plain_shape(p, kn, m);
         if (p->slots > p->splits_alloc) continue;
         const float ms = time_best();

@@ -217,10 +217,11 @@ uint64_t gnm_plan_launch_count(const gnm_plan* plan);
 /* Autotuner (no reference counterpart; the reference sizes its tiles from free
  * memory only, score/cuda_backend.rs:803-975): times the plan's accumulate on
  * the first `variant_count` resident rows for each candidate launch shape —
- * plain engine: the kernel (people tiles of 512 bytes with 4 warps, with or
- * without a producer warp; 1024 bytes with 8 warps, with or without one;
- * 2048 bytes with 16 warps and a producer warp) times the variant-split count (0.5x to 4x
- * the SMs' CTA slots, the same count for every people tile);
+ * plain engine (accumulate + finalize, which reads every split's partials):
+ * the kernel (people tiles of 512 bytes with 4 warps, with or without a
+ * producer warp; 1024 bytes with 8 warps, with or without one; 2048 bytes
+ * with 16 warps and a producer warp) times the variant-split count (0.5x to
+ * 8x the SMs' CTA slots, the same count for every people tile);
  * tensor engine: up to 64 scores the narrow kernel (people as the MMA's M)
  * against the wide kernel (scores as M), and the wide kernel's CTA raster
  * order — keeps the fastest, and leaves the plan reset.  Blocks until done.  With the environment variable GNM_TRACE
