@@ -35,7 +35,6 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "bandwidth_50k_x_1m"
 METRIC = "genotype*score pairs/s"
-NARROW_MAX_SCORES = 64   # the tensor engine's people-as-M kernel serves up to 64 scores
 PROFILE = ROOT / "profiles" / "plain_accumulate_bandwidth_50k_x_1m.md"
 
 
@@ -317,17 +316,26 @@ def gpu_arm(args, rank, world, local_rank):
 
     plan = DevicePlan(prep, engine=engine, device=local_rank)
     tuned = None
+    def tensor_shape(shape):
+        return {"shape": shape, "raster": shape & 1, "narrow": bool(shape & 2),
+                "int8_limbs": bool(shape & 4)}
     if args.shape:
-        # a pinned launch shape (kernel:splits, e.g. 512:94), as profiling runs use
-        kern, splits = (int(x) for x in args.shape.split(":"))
-        plan.set_shape((kern << 16) | splits)
-        tuned = {"kernel": kern, "splits_per_full_tile": splits, "pinned": True}
+        # a pinned launch shape, as profiling runs use: kernel:splits (plain,
+        # e.g. 512:94) or the tensor engine's shape bits (e.g. 4)
+        if ":" in args.shape:
+            kern, splits = (int(x) for x in args.shape.split(":"))
+            plan.set_shape((kern << 16) | splits)
+            tuned = {"kernel": kern, "splits_per_full_tile": splits, "pinned": True}
+        else:
+            plan.set_shape(int(args.shape))
+            tuned = dict(tensor_shape(int(args.shape)), pinned=True)
     elif not args.no_autotune:
         # the library's autotuner picks the launch shape on these resident rows
         # (outside the timed region; the plan is left reset)
         shape = plan.autotune(rows, pitch, stream=stream)
         tuned = ({"kernel": shape >> 16, "splits_per_full_tile": shape & 0xFFFF}
-                 if not tensor else {"raster": shape})
+                 if not tensor else tensor_shape(shape))
+    tshape = plan.shape if tensor else 0
     sums, counts = plan.outputs()
     grad_s = None
     if args.backward:
@@ -401,7 +409,7 @@ def gpu_arm(args, rank, world, local_rank):
     pairs = P * nnz
     value = world * pairs / (ms / 1e3)
     peak_hbm, peak_kind = peaks()
-    if tensor and K <= NARROW_MAX_SCORES:
+    if tensor and tshape & 2:
         # narrow engine: M = 128 people, N = 4 limb planes x 16 scores, two MMAs
         # (dosage, missing) per 16-variant slice; one launch per block
         ptiles, k16, vpad = -(-P // 128), -(-K // 16) * 16, -(-V // 64) * 64
@@ -421,6 +429,25 @@ def gpu_arm(args, rank, world, local_rank):
                 "row_bytes_gbs": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9,
                 "row_bytes_frac_of_hbm": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9
                 / peak_hbm}
+    elif tensor and tshape & 4:
+        # 8-bit limbs: 9 integer MMA planes (4 dosage, 4 correction, 1 count)
+        # over 256-person x 128-score tiles and 128-variant stages; the integer
+        # peak is taken as twice the BF16 one (the nominal dense ratio, 4.5 / 2.25)
+        ptiles, kpad, vpad = -(-P // 256), -(-K // 128) * 128, -(-V // 128) * 128
+        executed = 2.0 * ptiles * 256 * vpad * kpad * 9
+        flops = 2.0 * P * nnz * 3
+        achieved = flops / (kernel_ms / 1e3) / 1e12
+        pk = peaks_tc()[0]
+        roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
+                "frac": achieved / pk, "traffic": None,
+                "peak_kind": peak_kind + " (bf16 sustained)",
+                "kernel": "gnm_t8_accumulate (8-bit limbs, dosage + missing + count passes)",
+                "kernel_ms": kernel_ms, "algorithmic_flops_per_launch": flops,
+                "algorithmic": "2 x people x cells x 3 weight limbs",
+                "executed_int_ops_per_launch": executed,
+                "executed_tops": executed / (kernel_ms / 1e3) / 1e12,
+                "executed_frac_of_int8_peak": executed / (kernel_ms / 1e3) / 1e12 / (2 * pk),
+                "int8_peak": "2 x the bf16 figure (nominal dense ratio)"}
     elif tensor:
         # executed tensor-core work: 8 limb MMAs (4 dosage, 3 correction, 1 count)
         # over 256-person x 128-score tiles and 64-variant stages

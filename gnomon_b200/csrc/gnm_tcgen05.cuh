@@ -38,6 +38,17 @@ __device__ __forceinline__ void tc_mma_f16(uint32_t d_tmem, uint64_t adesc, uint
       : "memory");
 }
 
+// D (S32, TMEM) (+)= A x B with 8-bit integer operands from shared memory.
+__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Arrive once on `bar` when every tcgen05 op this thread issued so far is done.
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
   asm volatile(
@@ -99,6 +110,13 @@ __device__ __forceinline__ uint64_t desc_kmajor_sw128(uint32_t saddr) {
 // K-major, shape M x N (M in {64,128}, N a multiple of 16 up to 256).
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(uint32_t M, uint32_t N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// Instruction descriptor for kind::i8: S32 accumulator, signed 8-bit A,
+// unsigned 8-bit B, both K-major, shape M x N (bits 4-5 accumulator format,
+// 7-9 A format, 10-12 B format, 17-22 N / 8, 24-28 M / 16).
+__host__ __device__ constexpr uint32_t idesc_s8u8_s32(uint32_t M, uint32_t N) {
+  return (2u << 4) | (1u << 7) | (0u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }
 
 // 3D tiled TMA load (x innermost; x * element size must be a multiple of 16).

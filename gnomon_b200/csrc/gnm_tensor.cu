@@ -69,6 +69,11 @@ struct TensorPlan {
   uint32_t nsplits = 1;                   // narrow: variant splits (grid z)
   uint64_t nslot = 0;                     // narrow: elements per split slot (K16 * P_pad)
   CUtensorMap map_dos, map_mis;
+  int8_t* d_planes8 = nullptr;            // [9][K_pad][V_pad8] 8-bit limbs (dosage, -corr, member)
+  double* d_quanta8 = nullptr;            // [9][K_pad] quantum of each 8-bit plane
+  uint64_t V_pad8 = 0;
+  CUtensorMap map8_2, map8_1;             // boxes of two planes / one plane
+  bool i8 = false;                        // wide GEMM on 8-bit limbs (gnm_t8_accumulate)
   bool narrow = false;                    // few scores: gnm_tc_narrow (people as M)
   bool can_narrow = false;                // K <= 64: either kernel can run the plan
   CUtensorMap nmap_dos, nmap_mis;         // narrow boxes: 16 scores x 4 planes
@@ -310,6 +315,297 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
+  }
+}
+
+// ---- 8-bit integer wide engine ---------------------------------------------------
+// The wide GEMM of gnm_tc_accumulate with tcgen05.mma kind::i8: twice the MMA
+// rate of BF16 per instruction, signed 8-bit weight limbs against unsigned
+// 8-bit genotype operands (dosage 0/1/2 or the missing indicator), S32
+// accumulators in tensor memory.  Every value x of score k is split as
+// l0 q0 + l1 q1 + l2 q2 + l3 q3 with q0 = max |x| of the score / 127,
+// q(i+1) = q(i) / 128 and integers |l0| <= 127, |l1..l3| <= 64, so the residual
+// is below q0 / 2^22 (2^-29 of the score's largest weight).  Products and
+// their sums are exact integers (below 2^23 per 16384-variant block); each
+// plane's block sum reaches FP64 as int x its quantum at the flush.  Nine
+// planes: dosage limbs 0-3, -correction limbs 0-3 and the member plane, in
+// five passes (two planes per pass, the member plane alone), each re-expanding
+// the genotypes.  K = 128 variants per stage (a 128-byte K-major row), so a
+// stage holds twice the variants of the BF16 kernel in the same bytes.
+constexpr uint32_t kT8K = 128;       // variants per stage
+constexpr uint32_t kT8Flush = 128;   // stages per exact block (16384 variants)
+constexpr int kT8Planes = 9;
+
+template <int NP, int ST>
+struct T8Smem {
+  static constexpr uint32_t kPlane = kTcM * kT8K;       // 16 KB
+  static constexpr uint32_t kAStage = NP * kPlane;
+  static constexpr uint32_t kB = kTcN * kT8K;           // 32 KB
+  static constexpr uint32_t kPk = kT8K * (kTcN / 4);    // 8 KB
+  static constexpr uint32_t kAOff = 0;
+  static constexpr uint32_t kBOff = kAOff + ST * kAStage;
+  static constexpr uint32_t kPkOff = kBOff + ST * kB;
+  static constexpr uint32_t kBarOff = kPkOff + ST * kPk;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (3 * ST + 2);
+  static constexpr uint32_t kTotal = kHolder + 16 + 1024;  // + alignment slack
+  static_assert(kTotal <= 227 * 1024, "shared memory");
+};
+
+struct T8Args {
+  uint64_t num_rows;       // rows of this block
+  int32_t a_x0;            // absolute variant index of block row 0 (multiple of 128)
+  double* part_sum;
+  uint32_t* part_cnt;
+  uint64_t P_pad;
+  uint64_t K_pad;
+  const double* quanta;    // [kT8Planes][K_pad] quantum of every plane of every score
+  uint32_t* err;
+  uint32_t raster;         // 0: blockIdx.x = people tile, 1: blockIdx.x = score tile
+  int32_t z0;              // first plane of this pass (TMA z coordinate)
+};
+
+// Per byte of y (genotype codes 0..3): the allele-2 dosage (00 -> 0, 01 -> 0,
+// 10 -> 1, 11 -> 2), or the missing indicator (01 -> 1).
+template <bool MISSING>
+__device__ __forceinline__ uint32_t code_bytes(uint32_t y) {
+  const uint32_t hi = (y >> 1) & 0x01010101u, lo = y & 0x01010101u;
+  return MISSING ? (lo & ~hi) : hi + (hi & lo);
+}
+
+template <int NP, int ST, bool MISSING, bool COUNT_LAST>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    gnm_t8_accumulate(const __grid_constant__ CUtensorMap amap,
+                      const __grid_constant__ CUtensorMap pmap, T8Args a) {
+  using L = T8Smem<NP, ST>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sb = smem_u32(smem);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ptile = a.raster ? blockIdx.y : blockIdx.x;
+  const uint32_t stile = a.raster ? blockIdx.x : blockIdx.y;
+  const uint32_t nit = uint32_t((a.num_rows + kT8K - 1) / kT8K);
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
+  auto bready = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
+  auto empty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (2 * ST + s); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  const uint32_t abort_addr = sb + L::kHolder + 8;
+
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < ST; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(bready(s), 128);
+      mbar_init(empty(s), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, 128);
+    *abort_flag = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&amap);
+    prefetch_tmap(&pmap);
+  }
+  if (warp == 1) {
+    tmem_alloc(sb + L::kHolder, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + L::kHolder);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        if (!mbar_wait_bounded(empty(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
+        tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kT8K),
+                    int32_t(stile * kTcM), a.z0, full(s));
+        tma_load_2d(sb + L::kPkOff + s * L::kPk, &pmap, int32_t(ptile * (kTcN / 4)),
+                    int32_t(it * kT8K), full(s));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_s8u8_s32(kTcM, kTcN);
+      uint32_t blk = 0;
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        const bool first = (it % kT8Flush) == 0;
+        if (first && it > 0) {
+          if (!mbar_wait_bounded(accempty, (blk - 1) & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            break;
+          }
+        }
+        if (!mbar_wait_bounded(bready(s), ph)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        tc_fence_after();
+        const uint32_t a0 = sb + L::kAOff + s * L::kAStage;
+        const uint32_t b0 = sb + L::kBOff + s * L::kB;
+#pragma unroll
+        for (uint32_t kk = 0; kk < kT8K / 32; ++kk) {   // K = 32 bytes per MMA
+          const uint64_t bdesc = desc_kmajor_sw128(b0 + kk * 32);
+#pragma unroll
+          for (uint32_t j = 0; j < NP; ++j) {
+            const uint64_t adesc = desc_kmajor_sw128(a0 + j * L::kPlane + kk * 32);
+            tc_mma_i8(tmem + j * kTcN, adesc, bdesc, idesc, (first && kk == 0) ? 0u : 1u);
+          }
+        }
+        tc_commit(empty(s));
+        if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+          tc_commit(accfull);
+          ++blk;
+        }
+      }
+    }
+  } else {
+    // ---------------- genotype expansion + epilogue (warps 2-5) ----------------
+    const uint32_t pt = threadIdx.x - 64;      // 0..127
+    const uint32_t col = pt & 31;              // byte column: people 4col..4col+3
+    const uint32_t vg = pt >> 5;               // 16-variant chunks 2vg, 2vg+1
+    const uint32_t quad = warp & 3;            // TMEM lane quadrant of this warp
+    uint32_t blk = 0;
+    for (uint32_t it = 0; it < nit; ++it) {
+      const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      if (!mbar_wait_bounded(full(s), ph)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrTmaTimeout);
+        break;
+      }
+      if (lds_volatile_u32(abort_addr)) break;
+      const uint32_t pk = sb + L::kPkOff + s * L::kPk;
+      const uint32_t bt = sb + L::kBOff + s * L::kB;
+#pragma unroll
+      for (uint32_t h = 0; h < kTcN / 128; ++h) {
+        const uint32_t bc = 32 * h + col;   // byte column: people 4bc..4bc+3
+#pragma unroll
+        for (uint32_t cc = 0; cc < 2; ++cc) {
+          const uint32_t c = 2 * vg + cc;   // 16-byte chunk (16 variants) of the operand row
+          uint32_t x[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+          for (uint32_t i = 0; i < 16; ++i)
+            x[i >> 2] |= lds_u8(pk + (16 * c + i) * (kTcN / 4) + bc) << (8 * (i & 3));
+#pragma unroll
+          for (uint32_t q = 0; q < 4; ++q) {
+            uint4 v;
+            v.x = code_bytes<MISSING>((x[0] >> (2 * q)) & 0x03030303u);
+            v.y = code_bytes<MISSING>((x[1] >> (2 * q)) & 0x03030303u);
+            v.z = code_bytes<MISSING>((x[2] >> (2 * q)) & 0x03030303u);
+            v.w = code_bytes<MISSING>((x[3] >> (2 * q)) & 0x03030303u);
+            // operand row of person 128h + 4col + q (conflict-free 16-byte stores)
+            const uint32_t n = 128 * h + 32 * q + col;
+            sts_u128(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4), v);
+          }
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(bready(s));
+
+      if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        tc_fence_after();
+        const uint64_t k = uint64_t(stile) * kTcM + 32 * quad + lane;
+        double* ps = a.part_sum + k * a.P_pad + uint64_t(ptile) * kTcN;
+        uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(ptile) * kTcN;
+        const uint32_t lane_base = tmem + ((32 * quad) << 16);
+        constexpr uint32_t kSum = COUNT_LAST ? uint32_t(NP) - 1u : uint32_t(NP);
+        double qv[NP];
+#pragma unroll
+        for (uint32_t j = 0; j < uint32_t(NP); ++j) qv[j] = a.quanta[(a.z0 + j) * a.K_pad + k];
+#pragma unroll 1
+        for (uint32_t cb = 0; cb < kTcN / 32; ++cb) {
+          if constexpr (kSum > 0) {
+            double acc[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+#pragma unroll
+            for (uint32_t j = 0; j < kSum; ++j) {
+              uint32_t r[32];
+              tmem_ld32(lane_base + j * kTcN + 32 * cb, r);
+              tmem_ld_wait();
+#pragma unroll
+              for (int i = 0; i < 32; ++i) acc[i] = fma(double(int32_t(r[i])), qv[j], acc[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < 32; ++i) ps[32 * cb + i] += acc[i];
+          }
+          if (COUNT_LAST) {
+            uint32_t r[32];
+            tmem_ld32(lane_base + (NP - 1) * kTcN + 32 * cb, r);
+            tmem_ld_wait();
+#pragma unroll
+            for (int i = 0; i < 32; ++i) pc[32 * cb + i] += r[i];
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(accempty);
+        ++blk;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// 8-bit limb planes [kT8Planes][K_pad][V_pad] and their quanta [kT8Planes][K_pad]
+// from the CSR: one thread per variant; the quanta by one thread per score.
+__global__ void gnm_t8_quanta(const uint32_t* amax_bits, uint64_t K_pad, double* quanta) {
+  const uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= K_pad) return;
+  const float am = __uint_as_float(amax_bits[k]);
+  double q = am > 0.0f ? double(am) / 127.0 : 1.0;
+  for (int l = 0; l < 4; ++l, q /= 128.0) {
+    quanta[l * K_pad + k] = q;          // dosage limb l
+    quanta[(4 + l) * K_pad + k] = q;    // correction limb l
+  }
+  quanta[8 * K_pad + k] = 1.0;          // member plane: counts
+}
+
+__global__ void gnm_t8_build_planes(const float* w, const float* corr, const uint32_t* cols,
+                                    const uint64_t* offs, uint64_t V, const double* quanta,
+                                    int8_t* planes, uint64_t K_pad, uint64_t V_pad) {
+  const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const uint64_t plane = K_pad * V_pad;
+  for (uint64_t e = offs[v]; e < offs[v + 1]; ++e) {
+    const uint32_t k = cols[e];
+    const uint64_t at = uint64_t(k) * V_pad + v;
+    const double xs[2] = {double(w[e]), -double(corr[e])};
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      double r = xs[t];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const double q = quanta[l * K_pad + k];
+        const double li = fmin(fmax(rint(r / q), -127.0), 127.0);
+        r -= li * q;
+        planes[(4 * t + l) * plane + at] = int8_t(li);
+      }
+    }
+    planes[8 * plane + at] = 1;
   }
 }
 
@@ -1045,6 +1341,20 @@ static cudaError_t launch_tc(const CUtensorMap& amap, const CUtensorMap& pmap, c
   return cudaGetLastError();
 }
 
+template <int NP, int ST, bool MISSING, bool COUNT_LAST>
+static cudaError_t launch_t8(const CUtensorMap& amap, const CUtensorMap& pmap, const T8Args& a,
+                             uint32_t ptiles, uint32_t stiles, cudaStream_t s) {
+  using L = T8Smem<NP, ST>;
+  const cudaError_t e = raise_smem_limit(
+      reinterpret_cast<const void*>(gnm_t8_accumulate<NP, ST, MISSING, COUNT_LAST>),
+      int(L::kTotal));
+  if (e != cudaSuccess) return e;
+  const dim3 grid = a.raster ? dim3(stiles, ptiles) : dim3(ptiles, stiles);
+  gnm_t8_accumulate<NP, ST, MISSING, COUNT_LAST><<<grid, kTcThreads, L::kTotal, s>>>(amap, pmap,
+                                                                                     a);
+  return cudaGetLastError();
+}
+
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -1072,6 +1382,22 @@ static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, u
       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled failed for limb planes");
+  return map;
+}
+
+// 8-bit limb planes [kT8Planes][K_pad][V_pad]; a box holds `np` consecutive planes.
+static CUtensorMap make_plane_map8(const int8_t* planes, uint64_t V_pad, uint64_t K_pad,
+                                   uint32_t np) {
+  CUtensorMap map;
+  cuuint64_t dims[3] = {V_pad, K_pad, uint64_t(kT8Planes)};
+  cuuint64_t strides[2] = {V_pad, K_pad * V_pad};
+  cuuint32_t box[3] = {kT8K, kTcM, np};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = tensor_map_encoder()(
+      &map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(planes), dims, strides, box,
+      estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(GNM_ERR_COMPUTE, "cuTensorMapEncodeTiled failed for 8-bit planes");
   return map;
 }
 
@@ -1152,6 +1478,11 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->part_elems * 4, "cudaMalloc(partials)");
   check_cuda(cudaMemset(t->d_planes_dos, 0, 4 * plane * 2), "memset planes");
   check_cuda(cudaMemset(t->d_planes_mis, 0, 4 * plane * 2), "memset planes");
+  t->V_pad8 = std::max<uint64_t>(kT8K, (p->V + kT8K - 1) / kT8K * kT8K);
+  const uint64_t plane8 = t->K_pad * t->V_pad8;
+  alloc(reinterpret_cast<void**>(&t->d_planes8), kT8Planes * plane8, "cudaMalloc(8-bit planes)");
+  alloc(reinterpret_cast<void**>(&t->d_quanta8), kT8Planes * t->K_pad * 8, "cudaMalloc(quanta)");
+  check_cuda(cudaMemset(t->d_planes8, 0, kT8Planes * plane8), "memset planes");
   mark("  tensor: planes alloc");
 
   const uint64_t nnz = p->V ? prep->sparse_row_offsets[p->V] : 0;
@@ -1194,8 +1525,17 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
         dw, dc, dcol, doff, p->V, dq, t->d_planes_dos, t->d_planes_mis, t->K_pad, t->V_pad);
     check_cuda(cudaGetLastError(), "plane build launch");
   }
+  gnm_t8_quanta<<<uint32_t((t->K_pad + 255) / 256), 256>>>(dq, t->K_pad, t->d_quanta8);
+  check_cuda(cudaGetLastError(), "quanta launch");
+  if (p->V) {
+    gnm_t8_build_planes<<<uint32_t((p->V + 255) / 256), 256>>>(
+        dw, dc, dcol, doff, p->V, t->d_quanta8, t->d_planes8, t->K_pad, t->V_pad8);
+    check_cuda(cudaGetLastError(), "8-bit plane build launch");
+  }
   check_cuda(cudaStreamSynchronize(0), "plane build");
   mark("  tensor: plane build");
+  t->map8_2 = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, 2);
+  t->map8_1 = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, 1);
   t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcM, kTcPlanes);
   t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcM, kTcPlanes);
   if (t->can_narrow) {
@@ -1209,6 +1549,8 @@ void tensor_plan_destroy(gnm_plan* p) {
   if (!t) return;
   pool_free(t->d_planes_dos);
   pool_free(t->d_planes_mis);
+  pool_free(t->d_planes8);
+  pool_free(t->d_quanta8);
   pool_free(t->d_part_sum);
   pool_free(t->d_part_cnt);
   delete t;
@@ -1217,6 +1559,8 @@ void tensor_plan_destroy(gnm_plan* p) {
 
 bool tensor_can_narrow(const gnm_plan* p) { return p->tensor && p->tensor->can_narrow; }
 bool tensor_is_narrow(const gnm_plan* p) { return p->tensor && p->tensor->narrow; }
+bool tensor_is_i8(const gnm_plan* p) { return p->tensor && p->tensor->i8; }
+void tensor_set_i8(gnm_plan* p, bool i8) { p->tensor->i8 = i8; }
 void tensor_set_narrow(gnm_plan* p, bool narrow) {
   if (narrow && !tensor_can_narrow(p))
     fail(GNM_ERR_INVALID, "the narrow tensor kernel serves at most 64 scores");
@@ -1253,6 +1597,39 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
     gnm_tc_narrow<<<grid, kNrThreads, NrSmem::kTotal, s>>>(t->nmap_dos, t->nmap_mis, pmap, a);
     check_cuda(cudaGetLastError(), "narrow tensor launch");
     p->launches += 1;
+    return;
+  }
+  if (t->i8 && v0 % kT8K == 0) {
+    // dosage limbs 0-1 and 2-3, correction limbs 0-1 and 2-3, then the counts
+    const CUtensorMap pmap8 = make_row_map(d_rows, p->bpv, nv, pitch, kTcN / 4, kT8K);
+    T8Args b;
+    b.num_rows = nv;
+    b.a_x0 = int32_t(v0);
+    b.part_sum = t->d_part_sum;
+    b.part_cnt = t->d_part_cnt;
+    b.P_pad = t->P_pad;
+    b.K_pad = t->K_pad;
+    b.quanta = t->d_quanta8;
+    b.err = p->d_err;
+    b.raster = p->raster;
+    if (b.raster && t->ptiles > 65535u) b.raster = 0;  // grid.y limit
+    for (int32_t z : {0, 2}) {
+      b.z0 = z;
+      check_cuda((launch_t8<2, kTcStages, false, false>(t->map8_2, pmap8, b, t->ptiles,
+                                                        t->stiles, s)),
+                 "8-bit tensor dosage launch");
+    }
+    for (int32_t z : {4, 6}) {
+      b.z0 = z;
+      check_cuda((launch_t8<2, kTcStages, true, false>(t->map8_2, pmap8, b, t->ptiles,
+                                                       t->stiles, s)),
+                 "8-bit tensor missing launch");
+    }
+    b.z0 = 8;
+    check_cuda((launch_t8<1, kTcStages, true, true>(t->map8_1, pmap8, b, t->ptiles, t->stiles,
+                                                    s)),
+               "8-bit tensor count launch");
+    p->launches += 5;
     return;
   }
   const CUtensorMap pmap = make_row_map(d_rows, p->bpv, nv, pitch, kTcN / 4, kTcK);
