@@ -2,10 +2,11 @@
 on a subset of its people, through the drop-in host call (``gnm_score_run``)
 with both engines, against the CPU oracle.
 
-Both engines sum in FP32 inside blocks (120 variants for the plain kernel,
-16,384 for the split-BF16 engine) and in FP64 across them, so the error of a
-sum depends on how many blocks it crosses: only full-length runs give the
-per-workload error figures.  People are the first ``people`` of each cohort
+The engines round inside blocks (the plain kernel's int32 stage grid, the
+split-BF16 and 8-bit limb residuals) and sum in FP64 across them, so the
+error of a sum depends on how many blocks it crosses: only full-length runs
+give the per-workload error figures.  ``tensor_i8`` is the wide tensor
+engine on 8-bit integer limbs, pinned through a device plan.  People are the first ``people`` of each cohort
 (the generator keys every call by (variant, person), so these are exactly the
 full workload's genotypes for those people); weights and score subsets are
 the full workload's.
@@ -85,12 +86,32 @@ def sum_abs_terms(prep, rows, people):
     return out.reshape(-1)
 
 
-@pytest.mark.parametrize("engine", ["plain", "tensor"])
+def score_i8(prep, rows):
+    """The wide tensor engine on 8-bit limbs (shape bit 2), through a device plan."""
+    import torch
+    from gnomon_b200.device import DevicePlan, row_pitch
+    bpv = prep.bytes_per_variant
+    pitch = row_pitch(bpv)
+    d = torch.zeros((rows.shape[0], pitch), dtype=torch.uint8, device="cuda")
+    d[:, :bpv] = torch.from_numpy(np.ascontiguousarray(rows[:, :bpv])).cuda()
+    plan = DevicePlan(prep, engine=_lib.ENGINE_TENSOR)
+    plan.set_shape(4)
+    s, c = plan.score(d, pitch)
+    plan.sync()
+    out = s.cpu().numpy(), c.cpu().numpy().astype(np.uint32)
+    plan.close()
+    return out
+
+
+@pytest.mark.parametrize("engine", ["plain", "tensor", "tensor_i8"])
 @pytest.mark.parametrize("name", list(FULL_LENGTH))
 def test_full_length_parity(cuda, name, engine):
     w, prep, rows, (es, ec) = full_length_case(name)
-    eng = _lib.ENGINE_PLAIN if engine == "plain" else _lib.ENGINE_TENSOR
-    s, c = run(PipelineContext(prep), np.ascontiguousarray(rows).reshape(-1), engine=eng)
+    if engine == "tensor_i8":
+        s, c = score_i8(prep, rows)
+    else:
+        eng = _lib.ENGINE_PLAIN if engine == "plain" else _lib.ENGINE_TENSOR
+        s, c = run(PipelineContext(prep), np.ascontiguousarray(rows).reshape(-1), engine=eng)
     np.testing.assert_array_equal(c, ec)
     rel = oracle.rel_err(s, es)
     report = {"workload": name, "engine": engine, "people": w.people, "variants": w.variants,
