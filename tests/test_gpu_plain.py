@@ -414,8 +414,9 @@ def test_every_plain_kernel_and_split(cuda, kernel, people, variants):
 def test_set_shape_rejects_unknown_kernels(cuda):
     from gnomon_b200.device import DevicePlan
     from gnomon_b200.prepare import from_workload
-    # 3,334 stages, so split counts are not capped by the stage count
-    prep = from_workload(synth.scaled(synth.WORKLOADS["plain_2k_x_50k"], 500, 100_000, 1))
+    # 6,667 stages: more than the 4,736 splits the autotuner's largest
+    # candidate (8x the CTA slots of the 512-byte kernel) allocates for
+    prep = from_workload(synth.scaled(synth.WORKLOADS["plain_2k_x_50k"], 500, 200_000, 1))
     plan = DevicePlan(prep, engine=PLAIN)
     try:
         with pytest.raises(_lib.GnomonGpuError):
