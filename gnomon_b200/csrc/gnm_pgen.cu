@@ -1397,7 +1397,9 @@ extern "C" {
 gnm_status gnm_pgen_dims(const uint8_t* pgen, uint64_t pgen_len, uint64_t* num_variants,
                          uint64_t* num_samples, gnm_error* err) {
   return guarded(err, [&] {
-    const PgenIndex ix = parse_pgen(pgen, pgen_len);
+    // the counts only: multiallelic records are checked when the file is
+    // opened, with or without ALT counts
+    const PgenIndex ix = parse_pgen(pgen, pgen_len, true);
     if (num_variants) *num_variants = ix.variants;
     if (num_samples) *num_samples = ix.samples;
   });
