@@ -546,13 +546,18 @@ def gpu_arm(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if not tensor else "bf16 limbs, f32 accumulate", "data": "synthetic",
+            "dtype": ("f32" if not tensor else
+                      "s8 limbs x u8 genotypes, s32 accumulate" if tshape & 4 else
+                      "bf16 limbs, f32 accumulate"), "data": "synthetic",
             "config": {"workload": w.name, "samples": P, "variants": V, "scores": K,
                        "cells": nnz, "useful_pairs_per_step": P * nnz,
                        "dense_pairs_per_step": P * V * K,
                        "packed_bytes": V * bpv,
-                       "engine": ("split-BF16 tcgen05 (4+3 limbs), FP64 block reduce" if tensor
-                                  else "plain (FP32 CUDA-core LUT, FP64 reduce)"),
+                       "engine": ("plain (int32 stage-table LUT on CUDA cores, FP64 reduce)"
+                                  if not tensor else
+                                  "tcgen05 kind::i8, 8-bit limbs (4 dosage + 4 correction + "
+                                  "count), FP64 block reduce" if tshape & 4 else
+                                  "split-BF16 tcgen05 (4+3 limbs), FP64 block reduce"),
                        "parallelism": f"person-shard x{world}" if world > 1 else "single GPU",
                        "launch_shape": tuned if tuned is not None else "default (not autotuned)",
                        "l2": (f"inputs ({V * bpv / 1e9:.1f} GB) larger than L2 "

@@ -5,8 +5,10 @@ with both engines, against the CPU oracle.
 The engines round inside blocks (the plain kernel's int32 stage grid, the
 split-BF16 and 8-bit limb residuals) and sum in FP64 across them, so the
 error of a sum depends on how many blocks it crosses: only full-length runs
-give the per-workload error figures.  ``tensor_i8`` is the wide tensor
-engine on 8-bit integer limbs, pinned through a device plan.  People are the first ``people`` of each cohort
+give the per-workload error figures.  ``tensor`` is the engine's default
+(the narrow kernel up to 64 scores, else the wide kernel on 8-bit limbs);
+``tensor_i8`` and ``tensor_bf16`` pin the wide kernel on 8-bit and on BF16
+limbs through a device plan.  People are the first ``people`` of each cohort
 (the generator keys every call by (variant, person), so these are exactly the
 full workload's genotypes for those people); weights and score subsets are
 the full workload's.
@@ -86,8 +88,9 @@ def sum_abs_terms(prep, rows, people):
     return out.reshape(-1)
 
 
-def score_i8(prep, rows):
-    """The wide tensor engine on 8-bit limbs (shape bit 2), through a device plan."""
+def score_shape(prep, rows, shape):
+    """The tensor engine pinned to a shape (4: wide on 8-bit limbs, 0: wide
+    on BF16 limbs), through a device plan."""
     import torch
     from gnomon_b200.device import DevicePlan, row_pitch
     bpv = prep.bytes_per_variant
@@ -95,7 +98,7 @@ def score_i8(prep, rows):
     d = torch.zeros((rows.shape[0], pitch), dtype=torch.uint8, device="cuda")
     d[:, :bpv] = torch.from_numpy(np.ascontiguousarray(rows[:, :bpv])).cuda()
     plan = DevicePlan(prep, engine=_lib.ENGINE_TENSOR)
-    plan.set_shape(4)
+    plan.set_shape(shape)
     s, c = plan.score(d, pitch)
     plan.sync()
     out = s.cpu().numpy(), c.cpu().numpy().astype(np.uint32)
@@ -103,12 +106,12 @@ def score_i8(prep, rows):
     return out
 
 
-@pytest.mark.parametrize("engine", ["plain", "tensor", "tensor_i8"])
+@pytest.mark.parametrize("engine", ["plain", "tensor", "tensor_i8", "tensor_bf16"])
 @pytest.mark.parametrize("name", list(FULL_LENGTH))
 def test_full_length_parity(cuda, name, engine):
     w, prep, rows, (es, ec) = full_length_case(name)
-    if engine == "tensor_i8":
-        s, c = score_i8(prep, rows)
+    if engine in ("tensor_i8", "tensor_bf16"):
+        s, c = score_shape(prep, rows, 4 if engine == "tensor_i8" else 0)
     else:
         eng = _lib.ENGINE_PLAIN if engine == "plain" else _lib.ENGINE_TENSOR
         s, c = run(PipelineContext(prep), np.ascontiguousarray(rows).reshape(-1), engine=eng)
