@@ -490,9 +490,12 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
 // out[o*K + k] = init + sum over splits of part[s][fam(o)], init = baseline[k]
 // (fresh run).  One launch per score column k.  A CTA takes 32 people; warp g
 // sums splits g, g + 8, g + 16, ... of each (a lane per person, so every
-// load is 32 consecutive people of one split), and lane o of warp 0 adds the
-// eight sums in order g = 0..7: a fixed order, so results are deterministic.
+// load is 32 consecutive people of one split) into eight independent
+// accumulators, so eight loads are in flight per thread; the accumulators,
+// then the eight warps' sums (lane o of warp 0, g = 0..7), are added in a
+// fixed order, so results are deterministic.
 constexpr uint32_t kFinWarps = 8;
+constexpr uint32_t kFinLanes = 8;   // independent accumulators per thread
 __global__ void __launch_bounds__(32 * kFinWarps) gnm_finalize(FinalizeArgs a) {
   __shared__ double s_sum[kFinWarps][32];
   __shared__ uint32_t s_cnt[kFinWarps][32];
@@ -502,10 +505,30 @@ __global__ void __launch_bounds__(32 * kFinWarps) gnm_finalize(FinalizeArgs a) {
   uint32_t c = 0;
   if (o < a.num_people) {
     const uint64_t f = a.out_to_fam ? a.out_to_fam[o] : o;
-    for (uint32_t sp = g; sp < a.num_splits; sp += kFinWarps) {
-      s += a.part_sum[uint64_t(sp) * a.part_stride + f];
-      c += a.part_cnt[uint64_t(sp) * a.part_stride + f];
+    double acc[kFinLanes];
+#pragma unroll
+    for (uint32_t u = 0; u < kFinLanes; ++u) acc[u] = 0.0;
+    constexpr uint32_t kStep = kFinWarps * kFinLanes;
+    uint32_t sp0 = g;
+    for (; sp0 + (kFinLanes - 1) * kFinWarps < a.num_splits; sp0 += kStep) {
+#pragma unroll
+      for (uint32_t u = 0; u < kFinLanes; ++u) {
+        const uint64_t at = uint64_t(sp0 + u * kFinWarps) * a.part_stride + f;
+        acc[u] += a.part_sum[at];
+        c += a.part_cnt[at];
+      }
     }
+#pragma unroll
+    for (uint32_t u = 0; u < kFinLanes; ++u) {   // the last, partial round
+      const uint32_t sp = sp0 + u * kFinWarps;
+      if (sp < a.num_splits) {
+        const uint64_t at = uint64_t(sp) * a.part_stride + f;
+        acc[u] += a.part_sum[at];
+        c += a.part_cnt[at];
+      }
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kFinLanes; ++u) s += acc[u];
   }
   s_sum[g][lane] = s;
   s_cnt[g][lane] = c;

@@ -364,12 +364,14 @@ struct T8Args {
   int32_t z0;              // first plane of this pass (TMA z coordinate)
 };
 
-// Per byte of y (genotype codes 0..3): the allele-2 dosage (00 -> 0, 01 -> 0,
-// 10 -> 1, 11 -> 2), or the missing indicator (01 -> 1).
+// Sixteen 2-bit genotype codes -> sixteen 2-bit operand values in place: the
+// allele-2 dosage (00 -> 0, 01 -> 0, 10 -> 1, 11 -> 2: low bit hi & ~lo, high
+// bit hi & lo), or the missing indicator (01 -> 1).  Person q's values of
+// four rows are then (w >> 2q) & 0x03030303, one per byte.
 template <bool MISSING>
-__device__ __forceinline__ uint32_t code_bytes(uint32_t y) {
-  const uint32_t hi = (y >> 1) & 0x01010101u, lo = y & 0x01010101u;
-  return MISSING ? (lo & ~hi) : hi + (hi & lo);
+__device__ __forceinline__ uint32_t code_fields(uint32_t x) {
+  const uint32_t hi = (x >> 1) & 0x55555555u, lo = x & 0x55555555u;
+  return MISSING ? (lo & ~hi) : ((hi & ~lo) | ((hi & lo) << 1));
 }
 
 template <int NP, int ST, bool MISSING, bool COUNT_LAST>
@@ -501,12 +503,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           for (uint32_t i = 0; i < 16; ++i)
             x[i >> 2] |= lds_u8(pk + (16 * c + i) * (kTcN / 4) + bc) << (8 * (i & 3));
 #pragma unroll
+          for (uint32_t i = 0; i < 4; ++i) x[i] = code_fields<MISSING>(x[i]);
+#pragma unroll
           for (uint32_t q = 0; q < 4; ++q) {
             uint4 v;
-            v.x = code_bytes<MISSING>((x[0] >> (2 * q)) & 0x03030303u);
-            v.y = code_bytes<MISSING>((x[1] >> (2 * q)) & 0x03030303u);
-            v.z = code_bytes<MISSING>((x[2] >> (2 * q)) & 0x03030303u);
-            v.w = code_bytes<MISSING>((x[3] >> (2 * q)) & 0x03030303u);
+            v.x = (x[0] >> (2 * q)) & 0x03030303u;
+            v.y = (x[1] >> (2 * q)) & 0x03030303u;
+            v.z = (x[2] >> (2 * q)) & 0x03030303u;
+            v.w = (x[3] >> (2 * q)) & 0x03030303u;
             // operand row of person 128h + 4col + q (conflict-free 16-byte stores)
             const uint32_t n = 128 * h + 32 * q + col;
             sts_u128(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4), v);
