@@ -372,7 +372,23 @@ def gpu_arm(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     plan.sync(stream)
-    l0 = plan.launches
+    launches_last_step = plan.launches   # the library's own count (reset each step)
+    graphs = None
+    if args.graph and grad_s is None:
+        # the scoring step (reset + accumulate + finalize) and the accumulate
+        # alone, each recorded once into a CUDA graph through the library's
+        # capture: replays launch the same kernels with no per-launch host work
+        step_graph, _, _ = plan.capture(rows, pitch, sums, counts)
+        acc_graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.graph(acc_graph, stream=side):
+            plan.accumulate(rows, pitch, 0, V, torch.cuda.current_stream())
+        graphs = (step_graph, acc_graph)
+        for _ in range(args.warmup):
+            with torch.cuda.stream(stream):
+                step_graph.replay()
+        plan.sync(stream)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -383,12 +399,27 @@ def gpu_arm(args, rank, world, local_rank):
                 with torch.cuda.stream(stream):
                     flush.fill_(i & 0xFF)
             s_ev[i][0].record(stream)
-            step(i)
+            if graphs is None:
+                step(i)
+            else:
+                with torch.cuda.stream(stream):
+                    graphs[0].replay()
             s_ev[i][1].record(stream)
         stop.record(stream)
         stop.synchronize()
     plan.sync(stream)
-    launches_last_step = plan.launches   # the library's own count (reset each step)
+    if graphs is not None:
+        # the accumulate's own time: its graph replayed between events
+        for i in range(args.steps):
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.fill_(i & 0xFF)
+            k_ev[i][0].record(stream)
+            with torch.cuda.stream(stream):
+                graphs[1].replay()
+            k_ev[i][1].record(stream)
+        stream.synchronize()
+        plan.sync(stream)
     if flush is None:
         ms = start.elapsed_time(stop) / args.steps
     else:
@@ -560,6 +591,9 @@ def gpu_arm(args, rank, world, local_rank):
                                   "split-BF16 tcgen05 (4+3 limbs), FP64 block reduce"),
                        "parallelism": f"person-shard x{world}" if world > 1 else "single GPU",
                        "launch_shape": tuned if tuned is not None else "default (not autotuned)",
+                       "timing": ("each step one replay of a CUDA graph of reset + accumulate + "
+                                  "finalize (DevicePlan.capture)" if graphs is not None else
+                                  "each step reset + accumulate + finalize launched from Python"),
                        "l2": (f"inputs ({V * bpv / 1e9:.1f} GB) larger than L2 "
                               f"({l2_bytes >> 20} MB); no flush" if flush is None else
                               f"inputs ({V * bpv / 1e6:.1f} MB) fit in L2 ({l2_bytes >> 20} MB): "
@@ -879,6 +913,8 @@ def main():
     ap.add_argument("--backward", action="store_true", help="add dW = G^T dS to each step")
     ap.add_argument("--stream-block", type=int, default=0,
                     help="stream rows from pinned host memory in blocks of this many variants")
+    ap.add_argument("--graph", action="store_true",
+                    help="time steps as replays of one CUDA graph of the step (plan capture)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the plan's default launch shape instead of autotuning it")
     ap.add_argument("--shape", default="",
