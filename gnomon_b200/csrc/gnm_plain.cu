@@ -98,11 +98,6 @@ __device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t addr, uint32_t v) 
   return old;
 }
 
-// Barrier `id` over the first `nthreads` threads of the CTA (a multiple of 32).
-__device__ __forceinline__ void named_barrier_sync(uint32_t id, uint32_t nthreads) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
-
 __device__ __forceinline__ void sts_u32(uint32_t addr, uint32_t v) {
   asm volatile("st.shared.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
@@ -248,15 +243,8 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
   // only its populated boxes are copied, so a partly filled tile costs in
   // proportion to its bytes.
   const uint64_t used = min(uint64_t(TILE), a.bytes_per_row - uint64_t(tile) * TILE);
-  const uint32_t cols = uint32_t((used + 127) / 128);   // warp columns holding row bytes
+  const uint32_t active_warps = uint32_t((used + 127) / 128);
   const uint32_t boxes = uint32_t((used + kPlainBoxBytes - 1) / kPlainBoxBytes);
-  // A tile that holds a quarter (a half) of its columns or fewer gives every
-  // column four (two) warps, which split each stage's group pairs and combine
-  // their sums at the end: a small cohort keeps the SM's warps busy without
-  // more CTAs (each CTA pays its own pipeline fill).
-  const uint32_t rep = 4 * cols <= L::kWarps ? 4u : (2 * cols <= L::kWarps ? 2u : 1u);
-  const uint32_t workers = cols * rep;                  // warps that score and release
-  const uint32_t warp = tid >> 5;
   const uint32_t bar0 = sbase + L::kBarOff;
   const uint32_t rel0 = sbase + L::kRelOff;
   const uint32_t empty0 = sbase + L::kEmptyOff;
@@ -266,7 +254,7 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     prefetch_tmap(&map);
     for (uint32_t b = 0; b < L::kStages; ++b) {
       mbar_init(bar0 + 8 * b, 1);
-      if (WS) mbar_init(empty0 + 8 * b, workers);
+      if (WS) mbar_init(empty0 + 8 * b, active_warps);
       sts_u32(rel0 + 4 * b, 0u);
       last_issued[b] = 0xFFFFFFFFu;
     }
@@ -324,16 +312,12 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
 #pragma unroll
   for (int i = 0; i < 16; ++i) iacc[i] = 0;
 
-  // warps past the scoring ones only hold padding; a scoring warp covers
-  // column `col` (128 bytes) and, with rep > 1, the group pairs p of a stage
-  // with p % rep == sub
-  const bool warp_active = warp < workers;
-  const uint32_t col = warp_active ? warp % cols : 0u, sub = warp_active ? warp / cols : 0u;
-  const uint32_t ctid = col * 32 + lane;   // word column of the tile this thread reads
-  // Each thread reads word column `ctid` of the TILE-byte stage row; the stage
+  // Each thread reads word column `tid` of the TILE-byte stage row; the stage
   // is stored as TILE / 256 TMA boxes of [kPlainRows rows][256 bytes].
-  const uint32_t word_off = (ctid / (kPlainBoxBytes / 4)) * L::kBoxBytes +
-                            (ctid % (kPlainBoxBytes / 4)) * 4;
+  const uint32_t word_off = (tid / (kPlainBoxBytes / 4)) * L::kBoxBytes +
+                            (tid % (kPlainBoxBytes / 4)) * 4;
+  // warps whose 128 bytes all lie past the row's last byte only hold padding
+  const bool warp_active = (tid >> 5) < active_warps;
 
   bool failed = false;
   for (uint32_t st = 0; st < (warp_active ? nstages : 0u); ++st) {
@@ -398,56 +382,30 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       }
       ev = (c0 & 0x33333333u) + (c1 & 0x33333333u) + ev;
       od = ((c0 >> 2) & 0x33333333u) + ((c1 >> 2) & 0x33333333u) + od;
+      if ((g / 2) % 2 == 1 || g + 2 == kPlainGroups) {
+        by[0] += ev & 0x0F0F0F0Fu;
+        by[2] += (ev >> 4) & 0x0F0F0F0Fu;
+        by[1] += od & 0x0F0F0F0Fu;
+        by[3] += (od >> 4) & 0x0F0F0F0Fu;
+        ev = 0u;
+        od = 0u;
+      }
     };
-    auto flush_nibbles = [&]() {
-      by[0] += ev & 0x0F0F0F0Fu;
-      by[2] += (ev >> 4) & 0x0F0F0F0Fu;
-      by[1] += od & 0x0F0F0F0Fu;
-      by[3] += (od >> 4) & 0x0F0F0F0Fu;
-      ev = 0u;
-      od = 0u;
-    };
-    auto pair_masked = [&](uint32_t g) {
-      uint32_t m[6];
-#pragma unroll
-      for (uint32_t r = 0; r < 6; ++r)
-        m[r] = (0u - uint32_t((members >> (3 * g + r)) & 1u)) & 0x55555555u;
-      pair(g, m[0], m[1], m[2], m[3], m[4], m[5]);
-    };
-    const bool all_members = members == (uint64_t(1) << kPlainRows) - 1;
     if (!warp_active) {
       // padding-only warp: nothing to score
-    } else if (rep == 1) {
-      if (all_members) {
-        // every row of the stage is a member of this score (the common case)
+    } else if (members == (uint64_t(1) << kPlainRows) - 1) {
+      // every row of the stage is a member of this score (the common case)
 #pragma unroll
-        for (uint32_t g = 0; g < kPlainGroups; g += 2) {
-          pair(g, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
-          if ((g / 2) % 2 == 1 || g + 2 == kPlainGroups) flush_nibbles();
-        }
-      } else {
-#pragma unroll
-        for (uint32_t g = 0; g < kPlainGroups; g += 2) {
-          pair_masked(g);
-          if ((g / 2) % 2 == 1 || g + 2 == kPlainGroups) flush_nibbles();
-        }
-      }
+      for (uint32_t g = 0; g < kPlainGroups; g += 2)
+        pair(g, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
     } else {
-      // this warp's share of the stage: pairs p with p % rep == sub; nibble
-      // counters flushed every two pairs and after the warp's last one
-      uint32_t since = 0;
 #pragma unroll
       for (uint32_t g = 0; g < kPlainGroups; g += 2) {
-        const uint32_t p = g / 2;
-        if (p % rep != sub) continue;
-        if (all_members)
-          pair(g, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
-        else
-          pair_masked(g);
-        if (++since == 2 || p + rep >= kPlainGroups / 2) {
-          flush_nibbles();
-          since = 0;
-        }
+        uint32_t m[6];
+#pragma unroll
+        for (uint32_t r = 0; r < 6; ++r)
+          m[r] = (0u - uint32_t((members >> (3 * g + r)) & 1u)) & 0x55555555u;
+        pair(g, m[0], m[1], m[2], m[3], m[4], m[5]);
       }
     }
 
@@ -460,7 +418,7 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
       if (lane == 0) mbar_arrive(empty0 + 8 * buf);
     } else if (lane == 0) {
       const uint32_t old = atom_add_acq_rel(rel0 + 4 * buf, 1u);
-      if (old == workers - 1) {
+      if (old == active_warps - 1) {
         sts_u32(rel0 + 4 * buf, 0u);
         const uint32_t nxt = st + L::kStages;
         if (nxt < nstages) {
@@ -506,40 +464,12 @@ __global__ void __launch_bounds__(PlainShape<TILE, WS>::kThreads, PlainShape<TIL
     return;
   }
 
-  // Warps that shared a column's stages hand their sums to the column's first
-  // warp through the (now idle) row buffers, in a fixed order.  Every scoring
-  // thread meets at a named barrier (the producer warp has left).
-  if (rep > 1) {
-    const uint32_t nslots = (rep - 1) * cols * 32;
-    double* xsum = reinterpret_cast<double*>(smem + L::kTileOff);
-    uint32_t* xcnt = reinterpret_cast<uint32_t*>(smem + L::kTileOff + nslots * 16 * 8);
-    if (warp_active && sub > 0) {
-      const uint32_t slot = ((sub - 1) * cols + col) * 32 + lane;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        xsum[i * nslots + slot] = acc64[i];
-        xcnt[i * nslots + slot] = cnt[i];
-      }
-    }
-    named_barrier_sync(1, L::kThreads);
-    if (warp_active && sub == 0) {
-      for (uint32_t s2 = 1; s2 < rep; ++s2) {
-        const uint32_t slot = ((s2 - 1) * cols + col) * 32 + lane;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          acc64[i] += xsum[i * nslots + slot];
-          cnt[i] += xcnt[i * nslots + slot];
-        }
-      }
-    }
-  }
-
   // FP64 partials for this (split, person) accumulate across calls; the first
   // launch after a reset writes them (every split of every tile has a CTA, so
   // every slot it covers is written).  Warps that only held padding added
   // nothing: their slots (people past the row) stay as they are.
-  if (!warp_active || sub > 0) return;
-  const uint64_t person0 = uint64_t(tile) * (TILE * 4) + uint64_t(ctid) * 16;
+  if (!warp_active) return;
+  const uint64_t person0 = uint64_t(tile) * (TILE * 4) + uint64_t(tid) * 16;
   double* ps = a.part_sum + uint64_t(split) * a.part_stride + person0;
   uint32_t* pc = a.part_cnt + uint64_t(split) * a.part_stride + person0;
   if (a.store) {
