@@ -335,6 +335,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 constexpr uint32_t kT8K = 128;       // variants per stage
 constexpr uint32_t kT8Flush = 128;   // stages per exact block (16384 variants)
 constexpr int kT8Planes = 9;
+constexpr uint32_t kT8Expand = 256;                 // expansion / epilogue threads (8 warps)
+constexpr uint32_t kT8Threads = 64 + kT8Expand;     // + TMA warp + MMA warp
 
 template <int NP, int ST>
 struct T8Smem {
@@ -375,7 +377,7 @@ __device__ __forceinline__ uint32_t code_fields(uint32_t x) {
 }
 
 template <int NP, int ST, bool MISSING, bool COUNT_LAST>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kT8Threads, 1)
     gnm_t8_accumulate(const __grid_constant__ CUtensorMap amap,
                       const __grid_constant__ CUtensorMap pmap, T8Args a) {
   using L = T8Smem<NP, ST>;
@@ -398,11 +400,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < ST; ++s) {
       mbar_init(full(s), 1);
-      mbar_init(bready(s), 128);
+      mbar_init(bready(s), kT8Expand);
       mbar_init(empty(s), 1);
     }
     mbar_init(accfull, 1);
-    mbar_init(accempty, 128);
+    mbar_init(accempty, kT8Expand);
     *abort_flag = 0u;
     fence_mbar_init();
     prefetch_tmap(&amap);
@@ -476,10 +478,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     }
   } else {
-    // ---------------- genotype expansion + epilogue (warps 2-5) ----------------
-    const uint32_t pt = threadIdx.x - 64;      // 0..127
-    const uint32_t col = pt & 31;              // byte column: people 4col..4col+3
-    const uint32_t vg = pt >> 5;               // 16-variant chunks 2vg, 2vg+1
+    // ---------------- genotype expansion + epilogue (warps 2-9) ----------------
+    // warp 2 + 4h + vg: people half h (128 people), 16-variant chunks 2vg and
+    // 2vg + 1; at block ends it drains TMEM lane quadrant warp % 4, column
+    // blocks of its half
+    const uint32_t ew = warp - 2;              // 0..7
+    const uint32_t col = lane;                 // byte column: people 4col..4col+3
+    const uint32_t vg = ew & 3;
+    const uint32_t h = ew >> 2;
     const uint32_t quad = warp & 3;            // TMEM lane quadrant of this warp
     uint32_t blk = 0;
     for (uint32_t it = 0; it < nit; ++it) {
@@ -492,8 +498,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (lds_volatile_u32(abort_addr)) break;
       const uint32_t pk = sb + L::kPkOff + s * L::kPk;
       const uint32_t bt = sb + L::kBOff + s * L::kB;
-#pragma unroll
-      for (uint32_t h = 0; h < kTcN / 128; ++h) {
+      {
         const uint32_t bc = 32 * h + col;   // byte column: people 4bc..4bc+3
 #pragma unroll
         for (uint32_t cc = 0; cc < 2; ++cc) {
@@ -536,7 +541,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
         for (uint32_t j = 0; j < uint32_t(NP); ++j) qv[j] = a.quanta[(a.z0 + j) * a.K_pad + k];
 #pragma unroll 1
-        for (uint32_t cb = 0; cb < kTcN / 32; ++cb) {
+        for (uint32_t cb = h * (kTcN / 64); cb < (h + 1) * (kTcN / 64); ++cb) {
           if constexpr (kSum > 0) {
             double acc[32];
 #pragma unroll
@@ -1354,7 +1359,7 @@ static cudaError_t launch_t8(const CUtensorMap& amap, const CUtensorMap& pmap, c
       int(L::kTotal));
   if (e != cudaSuccess) return e;
   const dim3 grid = a.raster ? dim3(stiles, ptiles) : dim3(ptiles, stiles);
-  gnm_t8_accumulate<NP, ST, MISSING, COUNT_LAST><<<grid, kTcThreads, L::kTotal, s>>>(amap, pmap,
+  gnm_t8_accumulate<NP, ST, MISSING, COUNT_LAST><<<grid, kT8Threads, L::kTotal, s>>>(amap, pmap,
                                                                                      a);
   return cudaGetLastError();
 }
