@@ -337,20 +337,28 @@ constexpr uint32_t kT8Flush = 128;   // stages per exact block (16384 variants)
 constexpr int kT8Planes = 9;
 constexpr uint32_t kT8Expand = 256;                 // expansion / epilogue threads (8 warps)
 constexpr uint32_t kT8Threads = 64 + kT8Expand;     // + TMA warp + MMA warp
+constexpr int kT8StagesPair = 4;   // TMA ring depth of two-plane passes (4 x 40 KB + 2 x 32 KB)
+constexpr int kT8StagesOne = 6;    // of the one-plane pass (6 x 24 KB + 2 x 32 KB)
 
+// ST: depth of the TMA ring (weight limbs + packed rows of a stage); the
+// expanded genotype operand has its own two-deep ring, freed as soon as the
+// stage's MMAs complete, so the TMA loads run ST stages ahead while the
+// operand takes only two slots.
 template <int NP, int ST>
 struct T8Smem {
+  static constexpr uint32_t kBStages = 2;
   static constexpr uint32_t kPlane = kTcM * kT8K;       // 16 KB
   static constexpr uint32_t kAStage = NP * kPlane;
   static constexpr uint32_t kB = kTcN * kT8K;           // 32 KB
   static constexpr uint32_t kPk = kT8K * (kTcN / 4);    // 8 KB
   static constexpr uint32_t kAOff = 0;
-  static constexpr uint32_t kBOff = kAOff + ST * kAStage;
-  static constexpr uint32_t kPkOff = kBOff + ST * kB;
-  static constexpr uint32_t kBarOff = kPkOff + ST * kPk;
-  static constexpr uint32_t kHolder = kBarOff + 8 * (3 * ST + 2);
+  static constexpr uint32_t kPkOff = kAOff + ST * kAStage;
+  static constexpr uint32_t kBOff = kPkOff + ST * kPk;
+  static constexpr uint32_t kBarOff = kBOff + kBStages * kB;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (2 * ST + 2 * kBStages + 2);
   static constexpr uint32_t kTotal = kHolder + 16 + 1024;  // + alignment slack
   static_assert(kTotal <= 227 * 1024, "shared memory");
+  static_assert(kBOff % 1024 == 0 && kPkOff % 1024 == 0, "swizzled operands need 1 KB alignment");
 };
 
 struct T8Args {
@@ -389,19 +397,24 @@ __global__ void __launch_bounds__(kT8Threads, 1)
   const uint32_t ptile = a.raster ? blockIdx.y : blockIdx.x;
   const uint32_t stile = a.raster ? blockIdx.x : blockIdx.y;
   const uint32_t nit = uint32_t((a.num_rows + kT8K - 1) / kT8K);
-  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
-  auto bready = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
-  auto empty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (2 * ST + s); };
-  const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
-  const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
+  constexpr uint32_t BS = L::kBStages;
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };          // TMA landed
+  auto aempty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); }; // TMA slot free
+  auto bready = [&](uint32_t b) { return sb + L::kBarOff + 8 * (2 * ST + b); };
+  auto bempty = [&](uint32_t b) { return sb + L::kBarOff + 8 * (2 * ST + BS + b); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (2 * ST + 2 * BS);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (2 * ST + 2 * BS + 1);
   volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
   const uint32_t abort_addr = sb + L::kHolder + 8;
 
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < ST; ++s) {
       mbar_init(full(s), 1);
-      mbar_init(bready(s), kT8Expand);
-      mbar_init(empty(s), 1);
+      mbar_init(aempty(s), 1);
+    }
+    for (uint32_t b = 0; b < BS; ++b) {
+      mbar_init(bready(b), kT8Expand);
+      mbar_init(bempty(b), 1);
     }
     mbar_init(accfull, 1);
     mbar_init(accempty, kT8Expand);
@@ -424,7 +437,7 @@ __global__ void __launch_bounds__(kT8Threads, 1)
     if (lane == 0) {
       for (uint32_t it = 0; it < nit; ++it) {
         const uint32_t s = it % ST, ph = (it / ST) & 1u;
-        if (!mbar_wait_bounded(empty(s), ph ^ 1u)) {
+        if (!mbar_wait_bounded(aempty(s), ph ^ 1u)) {
           *abort_flag = 1u;
           atomicOr(a.err, kErrMmaTimeout);
           break;
@@ -443,7 +456,8 @@ __global__ void __launch_bounds__(kT8Threads, 1)
       constexpr uint32_t idesc = idesc_s8u8_s32(kTcM, kTcN);
       uint32_t blk = 0;
       for (uint32_t it = 0; it < nit; ++it) {
-        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        const uint32_t s = it % ST;
+        const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
         const bool first = (it % kT8Flush) == 0;
         if (first && it > 0) {
           if (!mbar_wait_bounded(accempty, (blk - 1) & 1u)) {
@@ -452,7 +466,7 @@ __global__ void __launch_bounds__(kT8Threads, 1)
             break;
           }
         }
-        if (!mbar_wait_bounded(bready(s), ph)) {
+        if (!mbar_wait_bounded(bready(bsl), bph)) {
           *abort_flag = 1u;
           atomicOr(a.err, kErrMmaTimeout);
           break;
@@ -460,7 +474,7 @@ __global__ void __launch_bounds__(kT8Threads, 1)
         if (lds_volatile_u32(abort_addr)) break;
         tc_fence_after();
         const uint32_t a0 = sb + L::kAOff + s * L::kAStage;
-        const uint32_t b0 = sb + L::kBOff + s * L::kB;
+        const uint32_t b0 = sb + L::kBOff + bsl * L::kB;
 #pragma unroll
         for (uint32_t kk = 0; kk < kT8K / 32; ++kk) {   // K = 32 bytes per MMA
           const uint64_t bdesc = desc_kmajor_sw128(b0 + kk * 32);
@@ -470,7 +484,8 @@ __global__ void __launch_bounds__(kT8Threads, 1)
             tc_mma_i8(tmem + j * kTcN, adesc, bdesc, idesc, (first && kk == 0) ? 0u : 1u);
           }
         }
-        tc_commit(empty(s));
+        tc_commit(aempty(s));
+        tc_commit(bempty(bsl));
         if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
           tc_commit(accfull);
           ++blk;
@@ -490,14 +505,21 @@ __global__ void __launch_bounds__(kT8Threads, 1)
     uint32_t blk = 0;
     for (uint32_t it = 0; it < nit; ++it) {
       const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
       if (!mbar_wait_bounded(full(s), ph)) {
         *abort_flag = 1u;
         atomicOr(a.err, kErrTmaTimeout);
         break;
       }
+      // the operand slot is free once the MMAs of stage it - BS completed
+      if (!mbar_wait_bounded(bempty(bsl), bph ^ 1u)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrMmaTimeout);
+        break;
+      }
       if (lds_volatile_u32(abort_addr)) break;
       const uint32_t pk = sb + L::kPkOff + s * L::kPk;
-      const uint32_t bt = sb + L::kBOff + s * L::kB;
+      const uint32_t bt = sb + L::kBOff + bsl * L::kB;
       {
         const uint32_t bc = 32 * h + col;   // byte column: people 4bc..4bc+3
 #pragma unroll
@@ -523,7 +545,7 @@ __global__ void __launch_bounds__(kT8Threads, 1)
         }
       }
       fence_proxy_async_smem();
-      mbar_arrive(bready(s));
+      mbar_arrive(bready(bsl));
 
       if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
         if (!mbar_wait_bounded(accfull, blk & 1u)) {
@@ -1628,18 +1650,18 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
     if (b.raster && t->ptiles > 65535u) b.raster = 0;  // grid.y limit
     for (int32_t z : {0, 2}) {
       b.z0 = z;
-      check_cuda((launch_t8<2, kTcStages, false, false>(t->map8_2, pmap8, b, t->ptiles,
+      check_cuda((launch_t8<2, kT8StagesPair, false, false>(t->map8_2, pmap8, b, t->ptiles,
                                                         t->stiles, s)),
                  "8-bit tensor dosage launch");
     }
     for (int32_t z : {4, 6}) {
       b.z0 = z;
-      check_cuda((launch_t8<2, kTcStages, true, false>(t->map8_2, pmap8, b, t->ptiles,
+      check_cuda((launch_t8<2, kT8StagesPair, true, false>(t->map8_2, pmap8, b, t->ptiles,
                                                        t->stiles, s)),
                  "8-bit tensor missing launch");
     }
     b.z0 = 8;
-    check_cuda((launch_t8<1, kTcStages, true, true>(t->map8_1, pmap8, b, t->ptiles, t->stiles,
+    check_cuda((launch_t8<1, kT8StagesOne, true, true>(t->map8_1, pmap8, b, t->ptiles, t->stiles,
                                                     s)),
                "8-bit tensor count launch");
     p->launches += 5;
