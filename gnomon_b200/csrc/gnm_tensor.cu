@@ -326,14 +326,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // l0 q0 + l1 q1 + l2 q2 + l3 q3 with q0 = max |x| of the score / 127,
 // q(i+1) = q(i) / 128 and integers |l0| <= 127, |l1..l3| <= 64, so the residual
 // is below q0 / 2^22 (2^-29 of the score's largest weight).  Products and
-// their sums are exact integers (below 2^23 per 16384-variant block); each
-// plane's block sum reaches FP64 as int x its quantum at the flush.  Nine
+// their sums are exact integers in S32 for blocks of up to 2^23 variants; each
+// plane's block sum reaches FP64 as int x its quantum at the flush, once per
+// block (the flush's partial read-modify-write is one score row per lane, so
+// flushing rarely keeps the memory queues free for the expansion).  Nine
 // planes: dosage limbs 0-3, -correction limbs 0-3 and the member plane, in
 // five passes (two planes per pass, the member plane alone), each re-expanding
 // the genotypes.  K = 128 variants per stage (a 128-byte K-major row), so a
 // stage holds twice the variants of the BF16 kernel in the same bytes.
 constexpr uint32_t kT8K = 128;       // variants per stage
-constexpr uint32_t kT8Flush = 128;   // stages per exact block (16384 variants)
+// stages per flushed block: 2^23 variants, where |limb x dosage| <= 254 per
+// variant keeps every S32 sum exact (254 x 2^23 < 2^31); an accumulate call
+// shorter than that flushes once, at its end
+constexpr uint32_t kT8Flush = (1u << 23) / kT8K;
 constexpr int kT8Planes = 9;
 constexpr uint32_t kT8Expand = 256;                 // expansion / epilogue threads (8 warps)
 constexpr uint32_t kT8Threads = 64 + kT8Expand;     // + TMA warp + MMA warp
