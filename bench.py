@@ -318,7 +318,7 @@ def gpu_arm(args, rank, world, local_rank):
     tuned = None
     def tensor_shape(shape):
         return {"shape": shape, "raster": shape & 1, "narrow": bool(shape & 2),
-                "int8_limbs": bool(shape & 4)}
+                "int8_limbs": bool(shape & 4), "sm_pairs": bool(shape & 8)}
     if args.shape:
         # a pinned launch shape, as profiling runs use: kernel:splits (plain,
         # e.g. 512:94) or the tensor engine's shape bits (e.g. 4)
@@ -441,10 +441,13 @@ def gpu_arm(args, rank, world, local_rank):
     value = world * pairs / (ms / 1e3)
     peak_hbm, peak_kind = peaks()
     if tensor and tshape & 2:
-        # narrow engine: M = 128 people, N = 4 limb planes x 16 scores, two MMAs
-        # (dosage, missing) per 16-variant slice; one launch per block
-        ptiles, k16, vpad = -(-P // 128), -(-K // 16) * 16, -(-V // 64) * 64
-        executed = 2.0 * ptiles * 128 * vpad * (4 * k16) * 2
+        # narrow engine: M = 128 people, N = limb planes x 16 scores, two MMAs
+        # (dosage, missing) per slice; one launch per block.  BF16: 4 + 4
+        # planes (the missing operand's padded to four); 8-bit: 4 + 5 planes
+        i8 = bool(tshape & 4)
+        ptiles, k16 = -(-P // 128), -(-K // 16) * 16
+        vpad = -(-V // 128) * 128 if i8 else -(-V // 64) * 64
+        executed = 2.0 * ptiles * 128 * vpad * k16 * (9 if i8 else 8)
         # algorithmic: three BF16 weight limbs (hi/mid/lo) x the useful cells
         flops = 2.0 * P * nnz * 3
         achieved = flops / (kernel_ms / 1e3) / 1e12
@@ -452,19 +455,23 @@ def gpu_arm(args, rank, world, local_rank):
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                 "frac": achieved / pk, "traffic": None,
                 "peak_kind": peak_kind + " (bf16 sustained)",
-                "kernel": "gnm_tc_narrow (dosage + missing MMAs, one pass)",
+                "kernel": ("gnm_t8_narrow (8-bit limbs; " if i8 else "gnm_tc_narrow (")
+                + "dosage + missing MMAs, one pass)",
                 "kernel_ms": kernel_ms, "algorithmic_flops_per_launch": flops,
                 "algorithmic": "2 x people x cells x 3 weight limbs",
-                "executed_flops_per_launch": executed,
-                "executed_tflops": executed / (kernel_ms / 1e3) / 1e12,
+                ("executed_int_ops_per_launch" if i8 else "executed_flops_per_launch"): executed,
+                ("executed_tops" if i8 else "executed_tflops"):
+                    executed / (kernel_ms / 1e3) / 1e12,
                 "row_bytes_gbs": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9,
                 "row_bytes_frac_of_hbm": V * bpv * (k16 // 16) / (kernel_ms / 1e3) / 1e9
                 / peak_hbm}
     elif tensor and tshape & 4:
         # 8-bit limbs: 9 integer MMA planes (4 dosage, 4 correction, 1 count)
-        # over 256-person x 128-score tiles and 128-variant stages; the integer
-        # peak is taken as twice the BF16 one (the nominal dense ratio, 4.5 / 2.25)
-        ptiles, kpad, vpad = -(-P // 256), -(-K // 128) * 128, -(-V // 128) * 128
+        # over 256-person x 128-score tiles (256-score tiles on SM pairs) and
+        # 128-variant stages; the integer peak is taken as twice the BF16 one
+        # (the nominal dense ratio, 4.5 / 2.25)
+        mt = 256 if tshape & 8 else 128
+        ptiles, kpad, vpad = -(-P // 256), -(-K // mt) * mt, -(-V // 128) * 128
         executed = 2.0 * ptiles * 256 * vpad * kpad * 9
         flops = 2.0 * P * nnz * 3
         achieved = flops / (kernel_ms / 1e3) / 1e12
@@ -472,7 +479,9 @@ def gpu_arm(args, rank, world, local_rank):
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
                 "frac": achieved / pk, "traffic": None,
                 "peak_kind": peak_kind + " (bf16 sustained)",
-                "kernel": "gnm_t8_accumulate (8-bit limbs, dosage + missing + count passes)",
+                "kernel": ("gnm_t8_pair (8-bit limbs on SM pairs, cta_group::2; "
+                           if tshape & 8 else "gnm_t8_accumulate (8-bit limbs, ")
+                + "dosage + missing + count passes)",
                 "kernel_ms": kernel_ms, "algorithmic_flops_per_launch": flops,
                 "algorithmic": "2 x people x cells x 3 weight limbs",
                 "executed_int_ops_per_launch": executed,
@@ -586,8 +595,10 @@ def gpu_arm(args, rank, world, local_rank):
                        "packed_bytes": V * bpv,
                        "engine": ("plain (int32 stage-table LUT on CUDA cores, FP64 reduce)"
                                   if not tensor else
-                                  "tcgen05 kind::i8, 8-bit limbs (4 dosage + 4 correction + "
-                                  "count), FP64 block reduce" if tshape & 4 else
+                                  "tcgen05 kind::i8" + (" on SM pairs (cta_group::2)"
+                                                        if tshape & 8 else "")
+                                  + ", 8-bit limbs (4 dosage + 4 correction + count), "
+                                  "FP64 block reduce" if tshape & 4 else
                                   "split-BF16 tcgen05 (4+3 limbs), FP64 block reduce"),
                        "parallelism": f"person-shard x{world}" if world > 1 else "single GPU",
                        "launch_shape": tuned if tuned is not None else "default (not autotuned)",

@@ -703,21 +703,25 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
     plain_shape(p, best_kernel, best_mult);
   } else {
     // shape bit 0: raster order of the wide kernel; bit 1: the narrow kernel;
-    // bit 2: the wide kernel on 8-bit limbs
-    std::vector<uint32_t> cand = {0u, 1u, 4u, 5u};
-    if (tensor_can_narrow(p)) cand.insert(cand.begin(), 2u);
-    uint32_t best = (tensor_is_narrow(p) ? 2u : 0u) | (tensor_is_i8(p) ? 4u : 0u) | p->raster;
+    // bit 2: 8-bit limbs; bit 3: the 8-bit wide kernel over SM pairs
+    std::vector<uint32_t> cand = {0u, 1u, 4u, 5u, 12u, 13u};
+    if (tensor_can_narrow(p)) cand.insert(cand.begin(), {2u, 6u});
+    uint32_t best = (tensor_is_narrow(p) ? 2u : 0u) | (tensor_is_i8(p) ? 4u : 0u) |
+                    (tensor_is_pair(p) ? 8u : 0u) | p->raster;
     const char* tr = std::getenv("GNM_TRACE");
     const bool trace = tr && std::strcmp(tr, "0") != 0;
     for (uint32_t c : cand) {
       tensor_set_narrow(p, (c & 2u) != 0);
       tensor_set_i8(p, (c & 4u) != 0);
+      tensor_set_pair(p, (c & 8u) != 0);
       p->raster = c & 1u;
       const float ms = time_best();
       if (trace)
         std::fprintf(stderr, "[gnm autotune] tensor %s kernel%s: %.4f ms\n",
-                     (c & 2u) ? "narrow (people as M)"
-                              : ((c & 4u) ? "wide 8-bit (scores as M)" : "wide (scores as M)"),
+                     (c & 2u) ? ((c & 4u) ? "narrow 8-bit (people as M)" : "narrow (people as M)")
+                              : ((c & 8u) ? "wide 8-bit on SM pairs (scores as M)"
+                                          : ((c & 4u) ? "wide 8-bit (scores as M)"
+                                                      : "wide (scores as M)")),
                      (c & 2u) ? "" : ((c & 1u) ? ", score tiles fastest" : ", people tiles fastest"),
                      ms);
       if (ms < best_ms) {
@@ -727,6 +731,7 @@ static void autotune_impl(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, ui
     }
     tensor_set_narrow(p, (best & 2u) != 0);
     tensor_set_i8(p, (best & 4u) != 0);
+    tensor_set_pair(p, (best & 8u) != 0);
     p->raster = best & 1u;
   }
   plan_reset_impl(p, s);
@@ -1587,11 +1592,13 @@ gnm_status gnm_plan_set_shape(gnm_plan* p, uint32_t shape, gnm_error* err) {
   if (!p) return GNM_ERR_INVALID;
   return guarded(err, [&] {
     if (p->engine != GNM_ENGINE_PLAIN) {
-      if (shape > 7 || (shape & 6u) == 6u)
+      if (shape > 15 || ((shape & 8u) && (shape & 6u) != 4u))
         fail(GNM_ERR_INVALID,
-             "tensor engine shape is raster | (narrow << 1) | (8-bit wide << 2)");
+             "tensor engine shape is raster | (narrow << 1) | (8-bit limbs << 2) | "
+             "(8-bit wide kernel on SM pairs << 3)");
       tensor_set_narrow(p, (shape & 2u) != 0);
       tensor_set_i8(p, (shape & 4u) != 0);
+      tensor_set_pair(p, (shape & 8u) != 0);
       p->raster = shape & 1u;
       return;
     }
@@ -1619,7 +1626,8 @@ uint32_t gnm_plan_tuned_shape(const gnm_plan* p) {
   if (!p) return 0;
   return p->engine == GNM_ENGINE_PLAIN ? (p->kernel << 16) | std::min<uint32_t>(p->splits, 0xFFFFu)
                                        : (p->raster | (tensor_is_narrow(p) ? 2u : 0u) |
-                                          (tensor_is_i8(p) ? 4u : 0u));
+                                          (tensor_is_i8(p) ? 4u : 0u) |
+                                          (tensor_is_pair(p) ? 8u : 0u));
 }
 
 gnm_status gnm_decode_device(const uint8_t* d_rows, uint64_t pitch, uint64_t nv, uint64_t np,

@@ -1,5 +1,6 @@
 // gnm_tcgen05.cuh — sm_100a fifth-generation tensor-core primitives (inline PTX):
-// TMEM allocation, tcgen05.mma (kind::f16, cta_group::1), commit to mbarrier,
+// TMEM allocation, tcgen05.mma (kind::f16 / kind::i8; cta_group::1, and
+// cta_group::2 over an SM pair), commit to mbarrier,
 // TMEM -> register loads, and the shared-memory matrix descriptor for K-major
 // operands in the 128-byte swizzled layout produced by TMA SWIZZLE_128B.
 #pragma once
@@ -46,6 +47,47 @@ __device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint6
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// ---- SM pairs (cta_group::2): one MMA spans the two CTAs of a cluster ----
+// Allocation and release are collective over warp `w` of both CTAs (the same
+// warp index in each); each CTA's holder receives the same column address.
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t holder_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   holder_smem),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish_pair() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+
+// D (S32) (+)= A x B over an SM pair, issued by one thread of the even CTA:
+// A's M rows are split in halves between the two CTAs (each CTA's half at
+// the same shared address), B's N columns likewise, and each CTA's tensor
+// memory receives its M/2 rows of D over all N columns.
+__device__ __forceinline__ void tc_mma_i8_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                               uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrive once on the mbarrier at shared offset `bar` of every CTA in `mask`
+// (bit r = cluster rank r) when the pair MMAs this thread issued are done.
+__device__ __forceinline__ void tc_commit_pair(uint32_t bar, uint16_t mask) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(bar),
+      "h"(mask)
       : "memory");
 }
 
@@ -117,6 +159,12 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(uint32_t M, uint32_t N) {
 // 7-9 A format, 10-12 B format, 17-22 N / 8, 24-28 M / 16).
 __host__ __device__ constexpr uint32_t idesc_s8u8_s32(uint32_t M, uint32_t N) {
   return (2u << 4) | (1u << 7) | (0u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// kind::i8 with both operands signed 8-bit (genotype values 0-2 are the same
+// bytes either way).
+__host__ __device__ constexpr uint32_t idesc_s8s8_s32(uint32_t M, uint32_t N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }
 
 // 3D tiled TMA load (x innermost; x * element size must be a multiple of 16).

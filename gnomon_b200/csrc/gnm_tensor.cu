@@ -74,9 +74,11 @@ struct TensorPlan {
   uint64_t V_pad8 = 0;
   CUtensorMap map8_2, map8_1;             // boxes of two planes / one plane
   bool i8 = false;                        // wide GEMM on 8-bit limbs (gnm_t8_accumulate)
+  bool pair = false;                      // ... over SM pairs (gnm_t8_pair)
   bool narrow = false;                    // few scores: gnm_tc_narrow (people as M)
   bool can_narrow = false;                // K <= 64: either kernel can run the plan
   CUtensorMap nmap_dos, nmap_mis;         // narrow boxes: 16 scores x 4 planes
+  CUtensorMap nmap8_dos, nmap8_mis;       // narrow 8-bit boxes: 128 variants x 16 scores x 4 / 5 planes
 };
 
 struct TcArgs {
@@ -322,18 +324,25 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // The wide GEMM of gnm_tc_accumulate with tcgen05.mma kind::i8: twice the MMA
 // rate of BF16 per instruction, signed 8-bit weight limbs against unsigned
 // 8-bit genotype operands (dosage 0/1/2 or the missing indicator), S32
-// accumulators in tensor memory.  Every value x of score k is split as
-// l0 q0 + l1 q1 + l2 q2 + l3 q3 with q0 = max |x| of the score / 127,
-// q(i+1) = q(i) / 128 and integers |l0| <= 127, |l1..l3| <= 64, so the residual
-// is below q0 / 2^22 (2^-29 of the score's largest weight).  Products and
+// accumulators in tensor memory.  Every dosage weight of score k is split as
+// l0 q0 + l1 q1 + l2 q2 + l3 q3 with q0 = max |x| of the score's values / 127,
+// q(i+1) = q(i) / 254 and integers |l| <= 127 (each rounding leaves a
+// remainder of at most half a quantum, which the next limb covers at 1/254 of
+// that quantum), so the residual is below q3 / 2, 2^-31.9 of the score's
+// largest value; missing corrections likewise.  (Three correction limbs,
+// 2^-23.9, gave 5.4e-7 of the reference's 1e-6 tolerance on the biobank
+// workload at full length.)  Products and
 // their sums are exact integers in S32 for blocks of up to 2^23 variants; each
 // plane's block sum reaches FP64 as int x its quantum at the flush, once per
 // block (the flush's partial read-modify-write is one score row per lane, so
 // flushing rarely keeps the memory queues free for the expansion).  Nine
 // planes: dosage limbs 0-3, -correction limbs 0-3 and the member plane, in
-// five passes (two planes per pass, the member plane alone), each re-expanding
-// the genotypes.  K = 128 variants per stage (a 128-byte K-major row), so a
-// stage holds twice the variants of the BF16 kernel in the same bytes.
+// five passes (two planes fill tensor memory's 2 x 256 S32 columns; the
+// member plane runs alone), each re-expanding the genotypes: dosage limbs
+// 0-1 and 2-3 against the dosage operand, correction limbs 0-1 and 2-3 and
+// the member plane against the missing indicator.  K = 128 variants per
+// stage (a 128-byte K-major row), so a stage holds twice the variants of the
+// BF16 kernel in the same bytes.
 constexpr uint32_t kT8K = 128;       // variants per stage
 // stages per flushed block: 2^23 variants, where |limb x dosage| <= 254 per
 // variant keeps every S32 sum exact (254 x 2^23 < 2^31); an accumulate call
@@ -606,6 +615,282 @@ __global__ void __launch_bounds__(kT8Threads, 1)
   }
 }
 
+// ---- 8-bit wide engine on SM pairs ---------------------------------------------
+// gnm_t8_accumulate with one tcgen05.mma.cta_group::2 spanning the two CTAs of
+// a cluster: M = 256 scores (128 per CTA), N = 256 people (128 per CTA), K =
+// 32 variants per instruction.  On one SM the N = 256 operand is read from
+// shared memory once per plane and expanded by that SM alone, and the
+// stage's shared-memory traffic (weight and genotype TMA writes, operand
+// stores, MMA operand reads) takes longer than its MMAs; over a pair each SM
+// stores, expands and serves only its 128 people, and each CTA's tensor
+// memory still holds its 128 scores x all 256 people per plane.
+//
+// Roles per CTA: warp 0 issues the CTA's own TMA loads (its 128 scores' limb
+// planes, its 128 people's packed rows) onto its own mbarriers; warps 2-9
+// expand the CTA's genotypes into its half of the B operand and arrive (one
+// lane per warp) on the even (leader) CTA's operand barrier with
+// cluster-scope release (after the
+// CTA's own TMA for the stage landed, so the arrival also vouches for its A
+// half); warp 1 of the leader alone issues the MMAs, and its commits arrive
+// on the freeing barriers of both CTAs (tcgen05.commit multicast).  Each
+// CTA's epilogue drains its own 128 score rows; the leader waits for both
+// epilogues before it overwrites the accumulators of the next block.  Every
+// wait is bounded; a cluster barrier keeps both CTAs resident until neither
+// can touch the other's shared memory, and tensor memory is allocated and
+// released by warp 1 of both CTAs together.
+// The operand ring is four deep: every hand-off between the CTAs of a pair
+// (operand ready, slot free) crosses SMs, so the expansion runs further ahead
+// of the MMAs than on one SM.
+constexpr int kT8PairStagesPair = 4;  // TMA ring depth, two planes (4 x 36 KB + 4 x 16 KB)
+constexpr int kT8PairStagesOne = 7;   // one plane (7 x 20 KB + 4 x 16 KB)
+
+template <int NP, int ST>
+struct T8PairSmem {
+  static constexpr uint32_t kBStages = 4;
+  static constexpr uint32_t kPlane = kTcM * kT8K;         // 16 KB: 128 scores x 128 variants
+  static constexpr uint32_t kAStage = NP * kPlane;
+  static constexpr uint32_t kB = (kTcN / 2) * kT8K;       // 16 KB: this CTA's 128 people
+  static constexpr uint32_t kPkRow = kTcN / 8;            // 32 packed bytes per variant row
+  static constexpr uint32_t kPk = kT8K * kPkRow;          // 4 KB
+  static constexpr uint32_t kAOff = 0;
+  static constexpr uint32_t kPkOff = kAOff + ST * kAStage;
+  static constexpr uint32_t kBOff = kPkOff + ST * kPk;
+  static constexpr uint32_t kBarOff = kBOff + kBStages * kB;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (2 * ST + 2 * kBStages + 3);
+  static constexpr uint32_t kTotal = kHolder + 16 + 1024;  // + alignment slack
+  static_assert(kTotal <= 227 * 1024, "shared memory");
+  static_assert(kBOff % 1024 == 0 && kPkOff % 1024 == 0, "swizzled operands need 1 KB alignment");
+};
+
+template <int NP, int ST, bool MISSING, bool COUNT_LAST>
+__global__ void __launch_bounds__(kT8Threads, 1)
+    gnm_t8_pair(const __grid_constant__ CUtensorMap amap,
+                const __grid_constant__ CUtensorMap pmap, T8Args a) {
+  using L = T8PairSmem<NP, ST>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sb = smem_u32(smem);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();   // 0: leader (issues the MMAs), 1: peer
+  const uint32_t pair_x = blockIdx.x >> 1;
+  const uint32_t ptile = a.raster ? blockIdx.y : pair_x;
+  const uint32_t spair = a.raster ? pair_x : blockIdx.y;
+  const uint32_t srow0 = (2 * spair + rank) * kTcM;      // this CTA's first score row
+  const bool has_scores = srow0 < a.K_pad;               // uniform per CTA
+  const uint32_t nit = uint32_t((a.num_rows + kT8K - 1) / kT8K);
+  constexpr uint32_t BS = L::kBStages;
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };          // TMA landed
+  auto aempty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); }; // TMA slot free
+  auto bready = [&](uint32_t b) { return sb + L::kBarOff + 8 * (2 * ST + b); };
+  auto bempty = [&](uint32_t b) { return sb + L::kBarOff + 8 * (2 * ST + BS + b); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (2 * ST + 2 * BS);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (2 * ST + 2 * BS + 1);
+  const uint32_t drain = sb + L::kBarOff + 8 * (2 * ST + 2 * BS + 2);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  const uint32_t abort_addr = sb + L::kHolder + 8;
+
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < ST; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(aempty(s), 1);
+    }
+    for (uint32_t b = 0; b < BS; ++b) {
+      mbar_init(bready(b), 2 * kT8Expand / 32);   // one arrival per expansion warp of both CTAs
+      mbar_init(bempty(b), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, 2 * kT8Expand);
+    mbar_init(drain, 1);
+    *abort_flag = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&amap);
+    prefetch_tmap(&pmap);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(sb + L::kHolder, 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  cluster_sync_all();   // barriers of both CTAs initialised, tensor memory allocated
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + L::kHolder);
+
+  if (warp == 0) {
+    // ---------------- TMA producer (each CTA its own halves) ----------------
+    if (lane == 0) {
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        if (!mbar_wait_bounded(aempty(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
+        tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kT8K),
+                    int32_t(srow0), a.z0, full(s));
+        tma_load_2d(sb + L::kPkOff + s * L::kPk, &pmap,
+                    int32_t(ptile * (kTcN / 4) + rank * L::kPkRow), int32_t(it * kT8K), full(s));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (leader CTA only) ----------------
+    if (lane == 0 && rank == 0) {
+      constexpr uint32_t idesc = idesc_s8u8_s32(2 * kTcM, kTcN);
+      uint32_t blk = 0;
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST;
+        const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
+        const bool first = (it % kT8Flush) == 0;
+        if (first && it > 0) {
+          if (!mbar_wait_bounded_cluster(accempty, (blk - 1) & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            break;
+          }
+        }
+        if (!mbar_wait_bounded_cluster(bready(bsl), bph)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        tc_fence_after();
+        const uint32_t a0 = sb + L::kAOff + s * L::kAStage;
+        const uint32_t b0 = sb + L::kBOff + bsl * L::kB;
+#pragma unroll
+        for (uint32_t kk = 0; kk < kT8K / 32; ++kk) {   // K = 32 bytes per MMA
+          const uint64_t bdesc = desc_kmajor_sw128(b0 + kk * 32);
+#pragma unroll
+          for (uint32_t j = 0; j < uint32_t(NP); ++j) {
+            const uint64_t adesc = desc_kmajor_sw128(a0 + j * L::kPlane + kk * 32);
+            tc_mma_i8_pair(tmem + j * kTcN, adesc, bdesc, idesc, (first && kk == 0) ? 0u : 1u);
+          }
+        }
+        tc_commit_pair(aempty(s), 0x3);
+        tc_commit_pair(bempty(bsl), 0x3);
+        if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+          tc_commit_pair(accfull, 0x3);
+          ++blk;
+        }
+      }
+      // every MMA this thread issued has completed before either CTA moves on
+      tc_commit_pair(drain, 0x1);
+      if (!mbar_wait_bounded(drain, 0)) atomicOr(a.err, kErrMmaTimeout);
+    }
+  } else {
+    // ---------------- genotype expansion + epilogue (warps 2-9) ----------------
+    // warp 2 + e: 16-variant chunk e of the stage for the CTA's 128 people
+    // (byte column `lane`: people 4 lane .. 4 lane + 3); at block ends it
+    // drains TMEM lane quadrant warp % 4, column blocks of half e / 4
+    const uint32_t ew = warp - 2;              // 0..7
+    const uint32_t col = lane;
+    const uint32_t c = ew;                     // 16-byte chunk (16 variants) of the operand row
+    const uint32_t h = ew >> 2;
+    const uint32_t quad = warp & 3;
+    const uint32_t lead_accempty = mapa_shared(accempty, 0);
+    uint32_t blk = 0;
+    for (uint32_t it = 0; it < nit; ++it) {
+      const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
+      if (!mbar_wait_bounded(full(s), ph)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrTmaTimeout);
+        break;
+      }
+      // the operand slot is free once the MMAs of stage it - BS completed
+      if (!mbar_wait_bounded(bempty(bsl), bph ^ 1u)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrMmaTimeout);
+        break;
+      }
+      if (lds_volatile_u32(abort_addr)) break;
+      const uint32_t pk = sb + L::kPkOff + s * L::kPk;
+      const uint32_t bt = sb + L::kBOff + bsl * L::kB;
+      {
+        uint32_t x[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (uint32_t i = 0; i < 16; ++i)
+          x[i >> 2] |= lds_u8(pk + (16 * c + i) * L::kPkRow + col) << (8 * (i & 3));
+#pragma unroll
+        for (uint32_t i = 0; i < 4; ++i) x[i] = code_fields<MISSING>(x[i]);
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+          uint4 v;
+          v.x = (x[0] >> (2 * q)) & 0x03030303u;
+          v.y = (x[1] >> (2 * q)) & 0x03030303u;
+          v.z = (x[2] >> (2 * q)) & 0x03030303u;
+          v.w = (x[3] >> (2 * q)) & 0x03030303u;
+          // operand row of person 4col + q of this CTA's half; the pair's
+          // TMEM column is 128 rank + row, the wide kernels' slot order
+          const uint32_t n = 32 * q + col;
+          sts_u128(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4), v);
+        }
+      }
+      // the warp's operand stores, made visible to the tensor core's proxy,
+      // are ordered before one cluster-scope arrival on the leader's barrier
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(mapa_shared(bready(bsl), 0));
+
+      if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        tc_fence_after();
+        if (has_scores) {
+          const uint64_t k = uint64_t(srow0) + 32 * quad + lane;
+          double* ps = a.part_sum + k * a.P_pad + uint64_t(ptile) * kTcN;
+          uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(ptile) * kTcN;
+          const uint32_t lane_base = tmem + ((32 * quad) << 16);
+          constexpr uint32_t kSum = COUNT_LAST ? uint32_t(NP) - 1u : uint32_t(NP);
+          double qv[NP];
+#pragma unroll
+          for (uint32_t j = 0; j < uint32_t(NP); ++j) qv[j] = a.quanta[(a.z0 + j) * a.K_pad + k];
+#pragma unroll 1
+          for (uint32_t cb = h * (kTcN / 64); cb < (h + 1) * (kTcN / 64); ++cb) {
+            if constexpr (kSum > 0) {
+              double acc[32];
+#pragma unroll
+              for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+#pragma unroll
+              for (uint32_t j = 0; j < kSum; ++j) {
+                uint32_t r[32];
+                tmem_ld32(lane_base + j * kTcN + 32 * cb, r);
+                tmem_ld_wait();
+#pragma unroll
+                for (int i = 0; i < 32; ++i) acc[i] = fma(double(int32_t(r[i])), qv[j], acc[i]);
+              }
+#pragma unroll
+              for (int i = 0; i < 32; ++i) ps[32 * cb + i] += acc[i];
+            }
+            if (COUNT_LAST) {
+              uint32_t r[32];
+              tmem_ld32(lane_base + (NP - 1) * kTcN + 32 * cb, r);
+              tmem_ld_wait();
+#pragma unroll
+              for (int i = 0; i < 32; ++i) pc[32 * cb + i] += r[i];
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive_cluster(lead_accempty);
+        ++blk;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncwarp();
+  cluster_sync_all();   // no CTA leaves while the other may read or signal its shared memory
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem, 512);
+  }
+}
+
 // 8-bit limb planes [kT8Planes][K_pad][V_pad] and their quanta [kT8Planes][K_pad]
 // from the CSR: one thread per variant; the quanta by one thread per score.
 __global__ void gnm_t8_quanta(const uint32_t* amax_bits, uint64_t K_pad, double* quanta) {
@@ -613,7 +898,7 @@ __global__ void gnm_t8_quanta(const uint32_t* amax_bits, uint64_t K_pad, double*
   if (k >= K_pad) return;
   const float am = __uint_as_float(amax_bits[k]);
   double q = am > 0.0f ? double(am) / 127.0 : 1.0;
-  for (int l = 0; l < 4; ++l, q /= 128.0) {
+  for (int l = 0; l < 4; ++l, q /= 254.0) {
     quanta[l * K_pad + k] = q;          // dosage limb l
     quanta[(4 + l) * K_pad + k] = q;    // correction limb l
   }
@@ -898,6 +1183,268 @@ __global__ void __launch_bounds__(kNrThreads, 1)
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, 2 * kNrN);
+  }
+}
+
+// ---- narrow engine on 8-bit limbs -------------------------------------------------
+// gnm_tc_narrow with tcgen05.mma kind::i8: M = 128 people, N = 16 scores x
+// the 8-bit planes of each operand (row n = 16 * plane + score, one 3D TMA box
+// of the wide engine's [9][K_pad][V] limb planes: dosage limbs 0-3, N = 64;
+// correction limbs 0-3 and the member plane, N = 80), K = 128 variants per
+// stage.  Per 32-variant slice two MMAs, the dosage operand against the
+// dosage limbs and the missing indicator against the rest, into 64 + 80 S32
+// accumulator columns.  Every operand byte is half the BF16 kernel's, which is what
+// bounds that kernel: its stage time is set by shared-memory traffic (TMA
+// writes, operand stores, MMA operand reads), not by the MMAs.  The TMA ring
+// (limb planes + packed rows) runs ST stages deep beside a two-deep ring of
+// expanded operands, as in gnm_t8_accumulate; sums stay exact in S32 for
+// blocks of up to 2^23 variants and reach the FP64 partials of the CTA's
+// variant split (natural person order) once per block.
+constexpr int kT8NrStages = 5;
+
+constexpr uint32_t kT8NrNDos = 4 * kNrScores;   // dosage limbs 0-3
+constexpr uint32_t kT8NrNMis = 5 * kNrScores;   // correction limbs 0-3, member plane
+
+struct T8NrSmem {
+  static constexpr uint32_t kBStages = 2;
+  static constexpr uint32_t kA = kNrM * kT8K;               // 16 KB per operand (people rows)
+  static constexpr uint32_t kPkRow = kNrM / 4;              // 32 packed bytes per variant row
+  static constexpr uint32_t kPk = kT8K * kPkRow;            // 4 KB
+  static constexpr uint32_t kBDos = 0;                      // offsets inside a TMA stage
+  static constexpr uint32_t kBMis = kT8NrNDos * kT8K;       // 8 KB
+  static constexpr uint32_t kPkIn = kBMis + kT8NrNMis * kT8K;   // + 10 KB
+  static constexpr uint32_t kTma = kPkIn + kPk;             // one TMA stage: 22 KB
+  static constexpr uint32_t kAOff = kT8NrStages * kTma;     // operand ring
+  static constexpr uint32_t kBarOff = kAOff + kBStages * 2 * kA;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (2 * kT8NrStages + 2 * kBStages + 2);
+  static constexpr uint32_t kTotal = kHolder + 16 + 1024;  // + alignment slack
+  static_assert(kTotal <= 227 * 1024, "shared memory");
+  static_assert(kTma % 1024 == 0 && kAOff % 1024 == 0 && kBMis % 1024 == 0 && kPkIn % 1024 == 0,
+                "operand alignment");
+};
+
+__global__ void __launch_bounds__(kNrThreads, 1)
+    gnm_t8_narrow(const __grid_constant__ CUtensorMap dmap,
+                  const __grid_constant__ CUtensorMap mmap,
+                  const __grid_constant__ CUtensorMap pmap, NrArgs a, const double* quanta,
+                  uint64_t K_pad) {
+  using L = T8NrSmem;
+  constexpr uint32_t ST = kT8NrStages;
+  constexpr uint32_t BS = L::kBStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sb = smem_u32(smem);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ptile = blockIdx.x, stile = blockIdx.y, split = blockIdx.z;
+  const uint32_t nall = uint32_t((a.num_rows + kT8K - 1) / kT8K);
+  const uint32_t it0 = split * a.stages_per_split;
+  const uint32_t nit = it0 < nall ? min(a.stages_per_split, nall - it0) : 0u;
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
+  auto tempty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
+  auto bready = [&](uint32_t b) { return sb + L::kBarOff + 8 * (2 * ST + b); };
+  auto bempty = [&](uint32_t b) { return sb + L::kBarOff + 8 * (2 * ST + BS + b); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (2 * ST + 2 * BS);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (2 * ST + 2 * BS + 1);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  const uint32_t abort_addr = sb + L::kHolder + 8;
+  if (nit == 0) return;   // a split past the block's last stage (uniform per CTA)
+
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < ST; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(tempty(s), 1);
+    }
+    for (uint32_t b = 0; b < BS; ++b) {
+      mbar_init(bready(b), kNrExpand);
+      mbar_init(bempty(b), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, kNrExpand);
+    *abort_flag = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&dmap);
+    prefetch_tmap(&mmap);
+    prefetch_tmap(&pmap);
+  }
+  if (warp == 1) {
+    tmem_alloc(sb + L::kHolder, 256);   // 64 + 80 columns
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + L::kHolder);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        if (!mbar_wait_bounded(tempty(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        const uint32_t st = sb + s * L::kTma;
+        mbar_arrive_expect_tx(full(s), L::kTma);
+        const int32_t x = a.a_x0 + int32_t((it0 + it) * kT8K);
+        tma_load_3d(st + L::kBDos, &dmap, x, int32_t(stile * kNrScores), 0, full(s));
+        tma_load_3d(st + L::kBMis, &mmap, x, int32_t(stile * kNrScores), 4, full(s));
+        tma_load_2d(st + L::kPkIn, &pmap, int32_t(ptile * L::kPkRow),
+                    int32_t((it0 + it) * kT8K), full(s));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc_d = idesc_s8s8_s32(kNrM, kT8NrNDos);
+      constexpr uint32_t idesc_m = idesc_s8s8_s32(kNrM, kT8NrNMis);
+      uint32_t blk = 0;
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST;
+        const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
+        const bool first = (it % kT8Flush) == 0;
+        if (first && it > 0) {
+          if (!mbar_wait_bounded(accempty, (blk - 1) & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            break;
+          }
+        }
+        if (!mbar_wait_bounded(bready(bsl), bph)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        tc_fence_after();
+        const uint32_t st = sb + s * L::kTma;
+        const uint32_t ad = sb + L::kAOff + bsl * 2 * L::kA;
+        const uint32_t am = ad + L::kA;
+#pragma unroll
+        for (uint32_t kk = 0; kk < kT8K / 32; ++kk) {   // K = 32 bytes per MMA
+          const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+          tc_mma_i8(tmem, desc_kmajor_sw128(ad + kk * 32),
+                    desc_kmajor_sw128(st + L::kBDos + kk * 32), idesc_d, acc);
+          tc_mma_i8(tmem + kT8NrNDos, desc_kmajor_sw128(am + kk * 32),
+                    desc_kmajor_sw128(st + L::kBMis + kk * 32), idesc_m, acc);
+        }
+        tc_commit(tempty(s));
+        tc_commit(bempty(bsl));
+        if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+          tc_commit(accfull);
+          ++blk;
+        }
+      }
+    }
+  } else {
+    // ---------------- genotype expansion + epilogue (warps 2-9) ----------------
+    // warp 2 + e: 16-variant chunk e of the stage; lane = byte column (people
+    // 4 lane .. 4 lane + 3); both operands from the same packed bytes
+    const uint32_t c = warp - 2;
+    const uint32_t col = lane;
+    const uint32_t quad = warp & 3;         // TMEM lane quadrant of this warp
+    const uint32_t half = (warp - 2) >> 2;  // epilogue: scores 8 half .. 8 half + 7
+    double* ps = a.part_sum + uint64_t(split) * a.slot_stride;
+    uint32_t* pc = a.part_cnt + uint64_t(split) * a.slot_stride;
+    uint32_t blk = 0;
+    for (uint32_t it = 0; it < nit; ++it) {
+      const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
+      if (!mbar_wait_bounded(full(s), ph)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrTmaTimeout);
+        break;
+      }
+      if (!mbar_wait_bounded(bempty(bsl), bph ^ 1u)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrMmaTimeout);
+        break;
+      }
+      if (lds_volatile_u32(abort_addr)) break;
+      const uint32_t pk = sb + s * L::kTma + L::kPkIn;
+      const uint32_t ad = sb + L::kAOff + bsl * 2 * L::kA;
+      const uint32_t am = ad + L::kA;
+      {
+        uint32_t x[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (uint32_t i = 0; i < 16; ++i)
+          x[i >> 2] |= lds_u8(pk + (16 * c + i) * L::kPkRow + col) << (8 * (i & 3));
+        uint32_t xd[4], xm[4];
+#pragma unroll
+        for (uint32_t i = 0; i < 4; ++i) {
+          xd[i] = code_fields<false>(x[i]);
+          xm[i] = code_fields<true>(x[i]);
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+          uint4 vd, vm;
+          vd.x = (xd[0] >> (2 * q)) & 0x03030303u;
+          vd.y = (xd[1] >> (2 * q)) & 0x03030303u;
+          vd.z = (xd[2] >> (2 * q)) & 0x03030303u;
+          vd.w = (xd[3] >> (2 * q)) & 0x03030303u;
+          vm.x = (xm[0] >> (2 * q)) & 0x03030303u;
+          vm.y = (xm[1] >> (2 * q)) & 0x03030303u;
+          vm.z = (xm[2] >> (2 * q)) & 0x03030303u;
+          vm.w = (xm[3] >> (2 * q)) & 0x03030303u;
+          // operand row of person 4col + q (conflict-free 16-byte stores)
+          const uint32_t n = 32 * q + col;
+          const uint32_t off = (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4);
+          sts_u128(ad + off, vd);
+          sts_u128(am + off, vm);
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(bready(bsl));
+
+      if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        tc_fence_after();
+        // TMEM lane 32 quad + lane = operand row n -> person 4 (n % 32) + n / 32.
+        // Column group g (16 columns): dosage limbs 0-3, -C limbs 0-3, member
+        // (plane g of the limb planes); this thread reads its 8 scores of
+        // every group.
+        const uint64_t person = uint64_t(ptile) * kNrM + 4 * lane + quad;
+        const uint32_t lane_base = tmem + ((32 * quad) << 16) + 8 * half;
+        const uint64_t k0 = uint64_t(stile) * kNrScores + 8 * half;
+        double acc[8];
+        uint32_t cnt[8];
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) acc[k] = 0.0;
+#pragma unroll
+        for (uint32_t g = 0; g < 9; ++g) {
+          uint32_t d[8];
+          tmem_ld8(lane_base + 16 * g, d);
+          tmem_ld_wait();
+#pragma unroll
+          for (uint32_t k = 0; k < 8; ++k) {
+            if (g < 8) acc[k] = fma(double(int32_t(d[k])), quanta[g * K_pad + k0 + k], acc[k]);
+            else cnt[k] = d[k];
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(accempty);
+        ++blk;
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) {
+          const uint64_t at = (k0 + k) * a.P_pad + person;
+          ps[at] += acc[k];
+          pc[at] += cnt[k];
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
   }
 }
 
@@ -1391,6 +1938,30 @@ static cudaError_t launch_t8(const CUtensorMap& amap, const CUtensorMap& pmap, c
   return cudaGetLastError();
 }
 
+// Clusters of two CTAs along x: CTA 2i + r is rank r of pair i.
+template <int NP, int ST, bool MISSING, bool COUNT_LAST>
+static cudaError_t launch_t8_pair(const CUtensorMap& amap, const CUtensorMap& pmap,
+                                  const T8Args& a, uint32_t ptiles, uint32_t spairs,
+                                  cudaStream_t s) {
+  using L = T8PairSmem<NP, ST>;
+  const void* fn = reinterpret_cast<const void*>(gnm_t8_pair<NP, ST, MISSING, COUNT_LAST>);
+  const cudaError_t e = raise_smem_limit(fn, int(L::kTotal));
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = a.raster ? dim3(2 * spairs, ptiles) : dim3(2 * ptiles, spairs);
+  cfg.blockDim = dim3(kT8Threads);
+  cfg.dynamicSmemBytes = L::kTotal;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, gnm_t8_pair<NP, ST, MISSING, COUNT_LAST>, amap, pmap, a);
+}
+
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -1421,13 +1992,14 @@ static CUtensorMap make_plane_map(const __nv_bfloat16* planes, uint64_t V_pad, u
   return map;
 }
 
-// 8-bit limb planes [kT8Planes][K_pad][V_pad]; a box holds `np` consecutive planes.
+// 8-bit limb planes [kT8Planes][K_pad][V_pad]; a box holds `rows` scores of `np`
+// consecutive planes.
 static CUtensorMap make_plane_map8(const int8_t* planes, uint64_t V_pad, uint64_t K_pad,
-                                   uint32_t np) {
+                                   uint32_t rows, uint32_t np) {
   CUtensorMap map;
   cuuint64_t dims[3] = {V_pad, K_pad, uint64_t(kT8Planes)};
   cuuint64_t strides[2] = {V_pad, K_pad * V_pad};
-  cuuint32_t box[3] = {kT8K, kTcM, np};
+  cuuint32_t box[3] = {kT8K, rows, np};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = tensor_map_encoder()(
       &map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(planes), dims, strides, box,
@@ -1574,13 +2146,15 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   }
   check_cuda(cudaStreamSynchronize(0), "plane build");
   mark("  tensor: plane build");
-  t->map8_2 = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, 2);
-  t->map8_1 = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, 1);
+  t->map8_2 = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, kTcM, 2);
+  t->map8_1 = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, kTcM, 1);
   t->map_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kTcM, kTcPlanes);
   t->map_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kTcM, kTcPlanes);
   if (t->can_narrow) {
     t->nmap_dos = make_plane_map(t->d_planes_dos, t->V_pad, t->K_pad, kNrScores, 4);
     t->nmap_mis = make_plane_map(t->d_planes_mis, t->V_pad, t->K_pad, kNrScores, 4);
+    t->nmap8_dos = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, kNrScores, 4);
+    t->nmap8_mis = make_plane_map8(t->d_planes8, t->V_pad8, t->K_pad, kNrScores, 5);
   }
 }
 
@@ -1601,6 +2175,8 @@ bool tensor_can_narrow(const gnm_plan* p) { return p->tensor && p->tensor->can_n
 bool tensor_is_narrow(const gnm_plan* p) { return p->tensor && p->tensor->narrow; }
 bool tensor_is_i8(const gnm_plan* p) { return p->tensor && p->tensor->i8; }
 void tensor_set_i8(gnm_plan* p, bool i8) { p->tensor->i8 = i8; }
+bool tensor_is_pair(const gnm_plan* p) { return p->tensor && p->tensor->pair; }
+void tensor_set_pair(gnm_plan* p, bool pair) { p->tensor->pair = pair; }
 void tensor_set_narrow(gnm_plan* p, bool narrow) {
   if (narrow && !tensor_can_narrow(p))
     fail(GNM_ERR_INVALID, "the narrow tensor kernel serves at most 64 scores");
@@ -1618,6 +2194,29 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
   TensorPlan* t = p->tensor;
   if (v0 % kTcK != 0)
     fail(GNM_ERR_INVALID, "tensor engine blocks must start at a multiple of 64 variants");
+  if (t->narrow && t->i8 && v0 % kT8K == 0) {
+    const CUtensorMap pmap8 = make_row_map(d_rows, p->bpv, nv, pitch, kNrM / 4, kT8K);
+    check_cuda(raise_smem_limit(reinterpret_cast<const void*>(gnm_t8_narrow),
+                                int(T8NrSmem::kTotal)),
+               "narrow 8-bit shared memory");
+    NrArgs a;
+    a.num_rows = nv;
+    a.a_x0 = int32_t(v0);
+    const uint32_t nall = uint32_t((nv + kT8K - 1) / kT8K);
+    a.stages_per_split = (nall + t->nsplits - 1) / t->nsplits;
+    a.part_sum = t->d_part_sum;
+    a.part_cnt = t->d_part_cnt;
+    a.P_pad = t->P_pad;
+    a.slot_stride = t->nslot;
+    a.err = p->d_err;
+    const dim3 grid(uint32_t((p->fam + kNrM - 1) / kNrM),
+                    uint32_t((p->K + kNrScores - 1) / kNrScores), t->nsplits);
+    gnm_t8_narrow<<<grid, kNrThreads, T8NrSmem::kTotal, s>>>(t->nmap8_dos, t->nmap8_mis, pmap8,
+                                                             a, t->d_quanta8, t->K_pad);
+    check_cuda(cudaGetLastError(), "narrow 8-bit tensor launch");
+    p->launches += 1;
+    return;
+  }
   if (t->narrow) {
     const CUtensorMap pmap = make_row_map(d_rows, p->bpv, nv, pitch, kNrM / 4, kTcK);
     check_cuda(raise_smem_limit(reinterpret_cast<const void*>(gnm_tc_narrow), int(NrSmem::kTotal)),
@@ -1653,6 +2252,29 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
     b.err = p->d_err;
     b.raster = p->raster;
     if (b.raster && t->ptiles > 65535u) b.raster = 0;  // grid.y limit
+    if (t->pair) {
+      // SM pairs: each CTA loads its 128 people's packed bytes (32 per row)
+      const CUtensorMap pmap_half = make_row_map(d_rows, p->bpv, nv, pitch, kTcN / 8, kT8K);
+      const uint32_t spairs = (t->stiles + 1) / 2;
+      for (int32_t z : {0, 2}) {
+        b.z0 = z;
+        check_cuda((launch_t8_pair<2, kT8PairStagesPair, false, false>(
+                       t->map8_2, pmap_half, b, t->ptiles, spairs, s)),
+                   "8-bit pair dosage launch");
+      }
+      for (int32_t z : {4, 6}) {
+        b.z0 = z;
+        check_cuda((launch_t8_pair<2, kT8PairStagesPair, true, false>(
+                       t->map8_2, pmap_half, b, t->ptiles, spairs, s)),
+                   "8-bit pair missing launch");
+      }
+      b.z0 = 8;
+      check_cuda((launch_t8_pair<1, kT8PairStagesOne, true, true>(t->map8_1, pmap_half, b,
+                                                                  t->ptiles, spairs, s)),
+                 "8-bit pair count launch");
+      p->launches += 5;
+      return;
+    }
     for (int32_t z : {0, 2}) {
       b.z0 = z;
       check_cuda((launch_t8<2, kT8StagesPair, false, false>(t->map8_2, pmap8, b, t->ptiles,

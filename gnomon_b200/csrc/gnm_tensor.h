@@ -30,6 +30,9 @@ void tensor_set_narrow(gnm_plan* p, bool narrow);
 // The wide GEMM on 8-bit limbs (gnm_t8_accumulate) instead of BF16 limbs.
 bool tensor_is_i8(const gnm_plan* p);
 void tensor_set_i8(gnm_plan* p, bool i8);
+// The 8-bit wide GEMM over SM pairs (gnm_t8_pair, cta_group::2).
+bool tensor_is_pair(const gnm_plan* p);
+void tensor_set_pair(gnm_plan* p, bool pair);
 void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,
                        uint64_t nv, cudaStream_t s);
 void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_baseline,

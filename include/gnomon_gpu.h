@@ -223,8 +223,10 @@ uint64_t gnm_plan_launch_count(const gnm_plan* plan);
  * with 16 warps and a producer warp) times the variant-split count (0.5x to
  * 8x the SMs' CTA slots, the same count for every people tile);
  * tensor engine: up to 64 scores the narrow kernel (people as the MMA's M)
- * against the wide kernel (scores as M) on BF16 limbs and on 8-bit integer
- * limbs, each wide form in both CTA raster orders — keeps the fastest, and
+ * on BF16 and on 8-bit limbs, against the wide kernel (scores as M) on BF16
+ * limbs, on 8-bit integer limbs, and on 8-bit limbs over SM pairs (one MMA
+ * across the two CTAs of a cluster), each wide form in both CTA raster
+ * orders — keeps the fastest, and
  * leaves the plan reset.  Blocks until done.  With the environment variable
  * GNM_TRACE set, every candidate's time is printed on stderr. */
 gnm_status gnm_plan_autotune(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
@@ -233,13 +235,15 @@ gnm_status gnm_plan_autotune(gnm_plan* plan, const uint8_t* d_rows, uint64_t pit
 /* The tuned shape.  Plain engine: (kernel << 16) | splits per full people
  * tile, kernel = tile bytes (512, 1024, 2048) + 1 with a producer warp;
  * tensor engine: raster order | (2 if the narrow kernel runs the plan) |
- * (4 if the wide kernel runs on 8-bit limbs; its blocks then start at
- * multiples of 128 variants, others fall back to the BF16 limbs). */
+ * (4 if it runs on 8-bit limbs; its blocks then start at multiples of 128
+ * variants, others fall back to the BF16 limbs) | (8 if the wide kernel's
+ * 8-bit MMAs span SM pairs; only with 4 and without 2). */
 uint32_t gnm_plan_tuned_shape(const gnm_plan* plan);
 
 /* Pin a shape (a value gnm_plan_tuned_shape returned, e.g. saved from an
  * earlier autotune of the same workload).  GNM_ERR_INVALID for an unknown
- * kernel or more splits than the plan's partial slots hold. */
+ * kernel, more splits than the plan's partial slots hold, or a tensor shape
+ * with unknown bits or SM pairs on anything but the 8-bit wide kernel. */
 gnm_status gnm_plan_set_shape(gnm_plan* plan, uint32_t shape, gnm_error* err);
 
 /* ---- Packed-row utilities ------------------------------------------------ */

@@ -6,9 +6,11 @@ The engines round inside blocks (the plain kernel's int32 stage grid, the
 split-BF16 and 8-bit limb residuals) and sum in FP64 across them, so the
 error of a sum depends on how many blocks it crosses: only full-length runs
 give the per-workload error figures.  ``tensor`` is the engine's default
-(the narrow kernel up to 64 scores, else the wide kernel on 8-bit limbs);
-``tensor_i8`` and ``tensor_bf16`` pin the wide kernel on 8-bit and on BF16
-limbs through a device plan.  People are the first ``people`` of each cohort
+(8-bit limbs; the narrow kernel up to 64 scores, else the wide kernel);
+``tensor_i8``, ``tensor_i8_pair`` and ``tensor_bf16`` pin the wide kernel on
+8-bit limbs (one SM per tile, SM pairs) and on BF16 limbs, and
+``tensor_narrow_bf16`` the narrow kernel on BF16 limbs, through a device
+plan.  People are the first ``people`` of each cohort
 (the generator keys every call by (variant, person), so these are exactly the
 full workload's genotypes for those people); weights and score subsets are
 the full workload's.
@@ -89,8 +91,8 @@ def sum_abs_terms(prep, rows, people):
 
 
 def score_shape(prep, rows, shape):
-    """The tensor engine pinned to a shape (4: wide on 8-bit limbs, 0: wide
-    on BF16 limbs), through a device plan."""
+    """The tensor engine pinned to a shape (gnm_plan_set_shape bits), through
+    a device plan."""
     import torch
     from gnomon_b200.device import DevicePlan, row_pitch
     bpv = prep.bytes_per_variant
@@ -106,12 +108,18 @@ def score_shape(prep, rows, shape):
     return out
 
 
-@pytest.mark.parametrize("engine", ["plain", "tensor", "tensor_i8", "tensor_bf16"])
+SHAPES = {"tensor_i8": 4, "tensor_i8_pair": 12, "tensor_bf16": 0, "tensor_narrow_bf16": 2}
+
+
+@pytest.mark.parametrize("engine", ["plain", "tensor", "tensor_i8", "tensor_i8_pair",
+                                    "tensor_bf16", "tensor_narrow_bf16"])
 @pytest.mark.parametrize("name", list(FULL_LENGTH))
 def test_full_length_parity(cuda, name, engine):
+    if engine == "tensor_narrow_bf16" and synth.WORKLOADS[name].scores > 64:
+        pytest.skip("the narrow kernel serves at most 64 scores")
     w, prep, rows, (es, ec) = full_length_case(name)
-    if engine in ("tensor_i8", "tensor_bf16"):
-        s, c = score_shape(prep, rows, 4 if engine == "tensor_i8" else 0)
+    if engine in SHAPES:
+        s, c = score_shape(prep, rows, SHAPES[engine])
     else:
         eng = _lib.ENGINE_PLAIN if engine == "plain" else _lib.ENGINE_TENSOR
         s, c = run(PipelineContext(prep), np.ascontiguousarray(rows).reshape(-1), engine=eng)
