@@ -618,17 +618,18 @@ def gpu_arm(args, rank, world, local_rank):
         }
         if bwd_ms is not None:
             # tcgen05 GEMM: M = variants (tiles of 128), N = 4 limbs x 16 scores per
-            # score tile, K = people (stages of 64); executed work and packed-row bytes
+            # score tile, K = people (stages of 128 on 8-bit limbs, the default);
+            # executed work and packed-row bytes
             v_pad = -(-V // 128) * 128
-            p_pad = -(-w.people // 64) * 64
+            p_pad = -(-w.people // 128) * 128
             k_pad = -(-K // 16) * 16
             bw_flops = 2.0 * v_pad * p_pad * 4 * k_pad
             bw_tflops = bw_flops / (bwd_ms / 1e3) / 1e12
             line["backward"] = {
                 "ms": bwd_ms, "pairs_per_s": P * V * K / (bwd_ms / 1e3),
-                "kernel": "gnm_tc_backward (+ dS limb build)",
-                "executed_tflops": bw_tflops,
-                "tensor_frac_of_sustained": bw_tflops / peaks_tc()[0],
+                "kernel": "gnm_t8_backward (8-bit dS limbs, + limb build)",
+                "executed_tops": bw_tflops,
+                "executed_frac_of_int8_peak": bw_tflops / (2 * peaks_tc()[0]),
                 "row_bytes_gbs": V * bpv * (k_pad // 16) / (bwd_ms / 1e3) / 1e9}
         print(json.dumps(line), flush=True)
     plan.close()

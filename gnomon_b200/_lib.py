@@ -88,6 +88,7 @@ SIGNATURES = {
                                     C.POINTER(gnm_error)]),
     "gnm_plan_tuned_shape": (C.c_uint32, [C.c_void_p]),
     "gnm_plan_set_shape": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(gnm_error)]),
+    "gnm_plan_set_backward_limbs": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(gnm_error)]),
     "gnm_decode_device": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                     C.c_uint64, C.c_void_p, C.POINTER(gnm_error)]),
     "gnm_release_cached_memory": (C.c_int, [C.c_int, C.POINTER(gnm_error)]),

@@ -953,9 +953,12 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   if (resume && (!resume->sums || !resume->counts))
     fail(GNM_ERR_INVALID, "resume state has NULL buffers");
   const uint64_t pitch = (bpv + 127) / 128 * 128;
-  // tensor-engine blocks start on 64-variant boundaries; rows between the
-  // boundary and the resume point are staged as zeros (they contribute nothing)
-  const uint64_t v_first = engine == GNM_ENGINE_TENSOR ? v_start - v_start % 64 : v_start;
+  // tensor-engine blocks start on 128-variant boundaries (the 8-bit kernels'
+  // stage; other blocks fall back to BF16 limbs); rows between the boundary
+  // and the resume point are staged as zeros (they contribute nothing)
+  constexpr uint64_t kTensorAlign = 128;
+  const uint64_t v_first =
+      engine == GNM_ENGINE_TENSOR ? v_start - v_start % kTensorAlign : v_start;
   HostRun r{bpv, prep, bed, pitch, v_start};
 
   RunResources res(device);
@@ -976,7 +979,7 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   if (!o.block_variants && engine == GNM_ENGINE_TENSOR && remaining >= 4 * kTensorMinBlock)
     block = std::min(block, (remaining + 3) / 4);
   block = std::max<uint64_t>(1, std::min<uint64_t>(block, std::max<uint64_t>(1, remaining)));
-  if (engine == GNM_ENGINE_TENSOR) block = (block + 63) / 64 * 64;
+  if (engine == GNM_ENGINE_TENSOR) block = (block + kTensorAlign - 1) / kTensorAlign * kTensorAlign;
   const int nbuf = remaining > block ? 2 : 1;
 
   std::vector<uint8_t*> dbuf(nbuf, nullptr);
@@ -1695,6 +1698,14 @@ gnm_status gnm_backward_dw_device(gnm_plan* p, const uint8_t* d_rows, uint64_t p
     DeviceGuard g(p->device);
     backward_dw(p, d_rows, pitch, d_grad_s, d_grad_w, d_grad_corr,
                 static_cast<cudaStream_t>(stream));
+  });
+}
+
+gnm_status gnm_plan_set_backward_limbs(gnm_plan* p, uint32_t bits, gnm_error* err) {
+  if (!p) return GNM_ERR_INVALID;
+  return guarded(err, [&] {
+    if (bits != 8 && bits != 16) fail(GNM_ERR_INVALID, "backward limbs are 8 or 16 bits wide");
+    p->bw_limb_bits = bits;
   });
 }
 

@@ -93,10 +93,18 @@ __device__ __forceinline__ uint32_t mapa_shared(uint32_t addr, uint32_t rank) {
 }
 
 // Arrive on an mbarrier of any CTA of the cluster (a mapa address), ordering
-// this thread's earlier writes before the arrival at cluster scope.
+// this thread's earlier writes before the arrival at cluster scope (a
+// cluster-scope fence: costly on a per-stage path).
 __device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
                : "memory");
+}
+
+// Arrive on an mbarrier of any CTA of the cluster with the default (CTA-scope)
+// release: for hand-offs whose consumer is the tensor core reading operands
+// that the arriving threads fenced into the async proxy beforehand.
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait_cluster(uint32_t bar, uint32_t parity) {

@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kPgThreads) gnm_pgen_direct(PgArgs a) {
 }
 
 // One warp per LD-compressed record of the range or list (others return at
-// once; five CTAs, 40 warps, per SM): copy the anchor row (16-byte vectors; type 3 swaps REF and ALT homozygotes
+// once; eight CTAs, 64 warps, per SM): copy the anchor row (16-byte vectors; type 3 swaps REF and ALT homozygotes
 // on the way), then patch it with the record's difflist.  The anchor row is an
 // output row, or a scratch row when it is outside the output.
 __global__ void __launch_bounds__(kPgThreads, 8) gnm_pgen_ld(PgArgs a) {
@@ -1255,31 +1255,10 @@ static void check_rows(const gnm_pgen* pg, const uint8_t* d_rows, uint64_t pitch
                           "a multiple of 16");
 }
 
-// LD records copy their anchor row and then patch it; with every SM full of
-// such warps (64) about 118 MB of rows are in flight and L2 evicts copied
-// lines before their patches land, so they are read back from DRAM.  The LD
-// kernel reserves (and never touches) enough dynamic shared memory that at
-// most kPgLdCtasPerSm CTAs (40 warps) share an SM.
-constexpr int kPgLdCtasPerSm = 5;
-
-static uint32_t ld_occupancy_smem() {
-  int dev = 0, per_sm = 0;
-  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-  check_cuda(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev),
-             "cudaDeviceGetAttribute");
-  // (n + 1) CTAs of per_sm / (n + 1) bytes plus the 1 KB each CTA reserves do
-  // not fit; n do
-  return uint32_t(per_sm / (kPgLdCtasPerSm + 1));
-}
-
 static void launch_decode(const PgArgs& a, cudaStream_t s) {
   gnm_pgen_direct<<<a.count + a.extra_rows, kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen decode launch");
-  const uint32_t cap = ld_occupancy_smem();
-  if (cap > 48 * 1024)
-    check_cuda(raise_smem_limit(reinterpret_cast<const void*>(gnm_pgen_ld), int(cap)),
-               "pgen LD shared memory");
-  gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, cap, s>>>(a);
+  gnm_pgen_ld<<<uint32_t((uint64_t(a.count) + kPgWarps - 1) / kPgWarps), kPgThreads, 0, s>>>(a);
   check_cuda(cudaGetLastError(), "pgen LD decode launch");
   if (a.any_dosage || a.any_multi) {   // patches and dosages, on the finished rows
     if (a.ma_smem > 48 * 1024)

@@ -160,6 +160,7 @@ struct gnm_plan {
   float* d_grad_fam = nullptr;     // backward: dS in .bed person order (keep subsets)
   uint8_t* d_bw = nullptr;         // backward: dS limb rows, FP32 dS, per-score maxima
   uint64_t bw_bytes = 0;
+  uint32_t bw_limb_bits = 8;       // backward dS limbs: 8 (gnm_t8_backward) or 16 (BF16)
   std::vector<double> h_baseline;
   uint64_t device_bytes = 0;
   uint64_t launches = 0;

@@ -628,21 +628,20 @@ __global__ void __launch_bounds__(kT8Threads, 1)
 // Roles per CTA: warp 0 issues the CTA's own TMA loads (its 128 scores' limb
 // planes, its 128 people's packed rows) onto its own mbarriers; warps 2-9
 // expand the CTA's genotypes into its half of the B operand and arrive (one
-// lane per warp) on the even (leader) CTA's operand barrier with
-// cluster-scope release (after the
-// CTA's own TMA for the stage landed, so the arrival also vouches for its A
-// half); warp 1 of the leader alone issues the MMAs, and its commits arrive
-// on the freeing barriers of both CTAs (tcgen05.commit multicast).  Each
-// CTA's epilogue drains its own 128 score rows; the leader waits for both
-// epilogues before it overwrites the accumulators of the next block.  Every
-// wait is bounded; a cluster barrier keeps both CTAs resident until neither
-// can touch the other's shared memory, and tensor memory is allocated and
-// released by warp 1 of both CTAs together.
-// The operand ring is four deep: every hand-off between the CTAs of a pair
-// (operand ready, slot free) crosses SMs, so the expansion runs further ahead
-// of the MMAs than on one SM.
+// lane per warp, after an async-proxy fence) on the even (leader) CTA's
+// operand barrier, after the CTA's own TMA for the stage landed, so the
+// arrival also vouches for its A half; warp 1 of the leader alone issues the
+// MMAs, and its commits arrive on the freeing barriers of both CTAs
+// (tcgen05.commit multicast).  Each CTA's epilogue drains its own 128 score
+// rows; the leader waits for both epilogues before it overwrites the
+// accumulators of the next block.  Every wait is bounded; a cluster barrier
+// keeps both CTAs resident until neither can touch the other's shared
+// memory, and tensor memory is allocated and released by warp 1 of both CTAs
+// together.  The operand ring is four deep: every hand-off between the CTAs
+// of a pair (operand ready, slot free) crosses SMs, so the expansion runs
+// further ahead of the MMAs than on one SM.  The member plane's pass spans
+// two score pairs per cluster (two planes' MMA work, like the other passes).
 constexpr int kT8PairStagesPair = 4;  // TMA ring depth, two planes (4 x 36 KB + 4 x 16 KB)
-constexpr int kT8PairStagesOne = 7;   // one plane (7 x 20 KB + 4 x 16 KB)
 
 template <int NP, int ST>
 struct T8PairSmem {
@@ -662,7 +661,10 @@ struct T8PairSmem {
   static_assert(kBOff % 1024 == 0 && kPkOff % 1024 == 0, "swizzled operands need 1 KB alignment");
 };
 
-template <int NP, int ST, bool MISSING, bool COUNT_LAST>
+// SPAN: the planes of a pass are the member plane of NP different score
+// pairs (rows 256 (NP * pair index + j) + 128 rank), every one a count;
+// otherwise NP consecutive planes of one score pair.
+template <int NP, int ST, bool MISSING, bool COUNT_LAST, bool SPAN>
 __global__ void __launch_bounds__(kT8Threads, 1)
     gnm_t8_pair(const __grid_constant__ CUtensorMap amap,
                 const __grid_constant__ CUtensorMap pmap, T8Args a) {
@@ -676,8 +678,11 @@ __global__ void __launch_bounds__(kT8Threads, 1)
   const uint32_t pair_x = blockIdx.x >> 1;
   const uint32_t ptile = a.raster ? blockIdx.y : pair_x;
   const uint32_t spair = a.raster ? pair_x : blockIdx.y;
-  const uint32_t srow0 = (2 * spair + rank) * kTcM;      // this CTA's first score row
-  const bool has_scores = srow0 < a.K_pad;               // uniform per CTA
+  static_assert(!SPAN || (MISSING && COUNT_LAST), "spanning passes count missing calls");
+  // this CTA's first score row of plane j (uniform per CTA)
+  auto srow = [&](uint32_t j) -> uint32_t {
+    return SPAN ? (2 * (uint32_t(NP) * spair + j) + rank) * kTcM : (2 * spair + rank) * kTcM;
+  };
   const uint32_t nit = uint32_t((a.num_rows + kT8K - 1) / kT8K);
   constexpr uint32_t BS = L::kBStages;
   auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };          // TMA landed
@@ -728,8 +733,15 @@ __global__ void __launch_bounds__(kT8Threads, 1)
         }
         if (lds_volatile_u32(abort_addr)) break;
         mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
-        tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kT8K),
-                    int32_t(srow0), a.z0, full(s));
+        if (SPAN) {   // one plane box per score pair
+#pragma unroll
+          for (uint32_t j = 0; j < uint32_t(NP); ++j)
+            tma_load_3d(sb + L::kAOff + s * L::kAStage + j * L::kPlane, &amap,
+                        a.a_x0 + int32_t(it * kT8K), int32_t(srow(j)), a.z0, full(s));
+        } else {
+          tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kT8K),
+                      int32_t(srow(0)), a.z0, full(s));
+        }
         tma_load_2d(sb + L::kPkOff + s * L::kPk, &pmap,
                     int32_t(ptile * (kTcN / 4) + rank * L::kPkRow), int32_t(it * kT8K), full(s));
       }
@@ -750,7 +762,7 @@ __global__ void __launch_bounds__(kT8Threads, 1)
             break;
           }
         }
-        if (!mbar_wait_bounded_cluster(bready(bsl), bph)) {
+        if (!mbar_wait_bounded(bready(bsl), bph)) {
           *abort_flag = 1u;
           atomicOr(a.err, kErrMmaTimeout);
           break;
@@ -828,11 +840,13 @@ __global__ void __launch_bounds__(kT8Threads, 1)
           sts_u128(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4), v);
         }
       }
-      // the warp's operand stores, made visible to the tensor core's proxy,
-      // are ordered before one cluster-scope arrival on the leader's barrier
+      // the warp's operand stores, fenced into the tensor core's (async)
+      // proxy, are ordered before one arrival on the leader's barrier; its
+      // consumer is the MMA, so no cluster-scope release is needed (one cost
+      // a memory-barrier stall per stage that halved the tensor pipe's use)
       fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive_cluster(mapa_shared(bready(bsl), 0));
+      if (lane == 0) mbar_arrive_remote(mapa_shared(bready(bsl), 0));
 
       if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
         if (!mbar_wait_bounded(accfull, blk & 1u)) {
@@ -841,8 +855,24 @@ __global__ void __launch_bounds__(kT8Threads, 1)
           break;
         }
         tc_fence_after();
-        if (has_scores) {
-          const uint64_t k = uint64_t(srow0) + 32 * quad + lane;
+        if (SPAN) {
+          const uint32_t lane_base = tmem + ((32 * quad) << 16);
+#pragma unroll
+          for (uint32_t j = 0; j < uint32_t(NP); ++j) {
+            if (srow(j) >= a.K_pad) continue;
+            const uint64_t k = uint64_t(srow(j)) + 32 * quad + lane;
+            uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(ptile) * kTcN;
+#pragma unroll 1
+            for (uint32_t cb = h * (kTcN / 64); cb < (h + 1) * (kTcN / 64); ++cb) {
+              uint32_t r[32];
+              tmem_ld32(lane_base + j * kTcN + 32 * cb, r);
+              tmem_ld_wait();
+#pragma unroll
+              for (int i = 0; i < 32; ++i) pc[32 * cb + i] += r[i];
+            }
+          }
+        } else if (srow(0) < a.K_pad) {
+          const uint64_t k = uint64_t(srow(0)) + 32 * quad + lane;
           double* ps = a.part_sum + k * a.P_pad + uint64_t(ptile) * kTcN;
           uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(ptile) * kTcN;
           const uint32_t lane_base = tmem + ((32 * quad) << 16);
@@ -1853,6 +1883,302 @@ __global__ void __launch_bounds__(kBwThreads, 1)
   }
 }
 
+// ---- backward on 8-bit limbs -------------------------------------------------------
+// gnm_tc_backward with tcgen05.mma kind::i8: A = the allele-2 dosage of 128
+// variants (one byte per person, K-major rows expanded in place from the
+// packed rows), B = dS split into four signed 8-bit limbs per score (row
+// n = 16 * limb + score; q0 = max_p |dS[p,k]| / 127, q(j+1) = q(j) / 254, every
+// |limb| <= 127, residual below 2^-31.9 of the score's largest |dS|), S32
+// accumulators exact for up to 2^23 people, converted to FP64 with the
+// quanta once per call.  K = 128 people per stage (a 128-byte operand row),
+// so every operand byte is half the BF16 kernel's.  The sparse missing-call
+// term is the BF16 kernel's: the thread that expands a row adds the FP32 dS
+// row of each code-01 call, flushed to FP64 every 4096 people.
+constexpr uint32_t kBw8K = 128;                      // people per stage
+constexpr uint32_t kBw8Stages = 6;
+constexpr uint32_t kBw8Flush = (1u << 23) / kBw8K;   // stages per exact S32 block
+constexpr uint32_t kBw8MissFlush = 4096 / kBw8K;     // stages per FP32 missing-term sum
+
+struct Bw8Smem {
+  static constexpr uint32_t kA = kBwM * kBw8K;               // 16 KB dosage operand
+  static constexpr uint32_t kB = kBwN * kBw8K;               // 8 KB dS limbs
+  static constexpr uint32_t kPkRow = kBw8K / 4;              // 32 packed bytes per variant
+  static constexpr uint32_t kPk = kBwM * kPkRow;             // 4 KB packed rows
+  static constexpr uint32_t kDs = kBw8K * kBwScores * 4;     // 8 KB FP32 dS
+  static constexpr uint32_t kAOff = 0;
+  static constexpr uint32_t kBOff = kAOff + kA;
+  static constexpr uint32_t kPkOff = kBOff + kB;
+  static constexpr uint32_t kDsOff = kPkOff + kPk;
+  static constexpr uint32_t kStage = kDsOff + kDs;            // 36 KB
+  static constexpr uint32_t kBarOff = kBw8Stages * kStage;
+  static constexpr uint32_t kHolder = kBarOff + 8 * (3 * kBw8Stages + 2);
+  static constexpr uint32_t kTotal = kHolder + 16 + 1024;     // + alignment slack
+  static constexpr uint32_t kSwap = 2 * kBwM * kBwScores * 8;
+  static_assert(kTotal <= 227 * 1024, "shared memory");
+};
+static_assert(Bw8Smem::kStage % 1024 == 0 && Bw8Smem::kBOff % 1024 == 0, "operand alignment");
+static_assert(Bw8Smem::kSwap <= Bw8Smem::kBarOff, "swap area");
+
+__global__ void __launch_bounds__(kBwThreads, 1)
+    gnm_t8_backward(const __grid_constant__ CUtensorMap rmap,
+                    const __grid_constant__ CUtensorMap bmap,
+                    const __grid_constant__ CUtensorMap dmap, BwArgs a, const double* quanta,
+                    uint64_t K16) {
+  using L = Bw8Smem;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const uint32_t sb = smem_u32(smem);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t vtile = blockIdx.x, stile = blockIdx.y;
+  const uint32_t nit = a.nstages;
+  constexpr uint32_t ST = kBw8Stages;
+  auto full = [&](uint32_t s) { return sb + L::kBarOff + 8 * s; };
+  auto aready = [&](uint32_t s) { return sb + L::kBarOff + 8 * (ST + s); };
+  auto empty = [&](uint32_t s) { return sb + L::kBarOff + 8 * (2 * ST + s); };
+  const uint32_t accfull = sb + L::kBarOff + 8 * (3 * ST);
+  const uint32_t accempty = sb + L::kBarOff + 8 * (3 * ST + 1);
+  volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + L::kHolder + 8);
+  const uint32_t abort_addr = sb + L::kHolder + 8;
+
+  if (threadIdx.x == 0) {
+    for (uint32_t s = 0; s < ST; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(aready(s), kBwExpand);
+      mbar_init(empty(s), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, kBwExpand);
+    *abort_flag = 0u;
+    fence_mbar_init();
+    prefetch_tmap(&rmap);
+    prefetch_tmap(&bmap);
+    prefetch_tmap(&dmap);
+  }
+  if (warp == 1) {
+    tmem_alloc(sb + L::kHolder, kBwN);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + L::kHolder);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        if (!mbar_wait_bounded(empty(s), ph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        const uint32_t st = sb + s * L::kStage;
+        mbar_arrive_expect_tx(full(s), L::kB + L::kPk + L::kDs);
+        tma_load_2d(st + L::kPkOff, &rmap, int32_t(it * L::kPkRow), int32_t(vtile * kBwM),
+                    full(s));
+        tma_load_2d(st + L::kBOff, &bmap, int32_t(it * kBw8K), int32_t(stile * kBwN), full(s));
+        tma_load_2d(st + L::kDsOff, &dmap, int32_t(stile * kBwScores), int32_t(it * kBw8K),
+                    full(s));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_s8s8_s32(kBwM, kBwN);
+      uint32_t blk = 0;
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t s = it % ST, ph = (it / ST) & 1u;
+        const bool first = (it % kBw8Flush) == 0;
+        if (first && it > 0) {
+          if (!mbar_wait_bounded(accempty, (blk - 1) & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            break;
+          }
+        }
+        if (!mbar_wait_bounded(aready(s), ph)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) break;
+        tc_fence_after();
+        const uint32_t a0 = sb + s * L::kStage + L::kAOff;
+        const uint32_t b0 = sb + s * L::kStage + L::kBOff;
+#pragma unroll
+        for (uint32_t kk = 0; kk < kBw8K / 32; ++kk)
+          tc_mma_i8(tmem, desc_kmajor_sw128(a0 + kk * 32), desc_kmajor_sw128(b0 + kk * 32), idesc,
+                    (first && kk == 0) ? 0u : 1u);
+        tc_commit(empty(s));
+        if ((it % kBw8Flush) == kBw8Flush - 1 || it == nit - 1) {
+          tc_commit(accfull);
+          ++blk;
+        }
+      }
+    }
+  } else {
+    // ---------------- genotype expansion + epilogue (warps 2-9) ----------------
+    const uint32_t quad = warp & 3;
+    const uint32_t half = (warp - 2) >> 2;  // people 64 half .. of each stage; scores 8 half ..
+    const uint32_t r = 32 * quad + lane;    // variant row of this thread and its TMEM lane
+    double gwd[8], gcd[kBwScores];
+    float gcf[kBwScores];   // missing term of the last <= kBw8MissFlush stages
+#pragma unroll
+    for (uint32_t k = 0; k < kBwScores; ++k) {
+      gcd[k] = 0.0;
+      gcf[k] = 0.0f;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) gwd[k] = 0.0;
+    bool ok = true;
+    uint32_t blk = 0;
+    for (uint32_t it = 0; it < nit; ++it) {
+      const uint32_t s = it % ST, ph = (it / ST) & 1u;
+      if (!mbar_wait_bounded(full(s), ph)) {
+        *abort_flag = 1u;
+        atomicOr(a.err, kErrTmaTimeout);
+        ok = false;
+        break;
+      }
+      if (lds_volatile_u32(abort_addr)) {
+        ok = false;
+        break;
+      }
+      const uint32_t st = sb + s * L::kStage;
+      // words 4 half .. 4 half + 3 of the row: people 64 half + 16 w ..
+      const uint4 x4 = lds_u128(st + L::kPkOff + r * L::kPkRow + 16 * half);
+      const uint32_t xw[4] = {x4.x, x4.y, x4.z, x4.w};
+      const uint32_t arow = st + L::kAOff + (r >> 3) * 1024 + (r & 7) * 128;
+#pragma unroll
+      for (uint32_t w = 0; w < 4; ++w) {
+        // byte t of s_q = dosage of person 4t + q of the word; a 4 x 4 byte
+        // transpose puts person 4t + i at byte i of word t
+        const uint32_t d = code_fields<false>(xw[w]);
+        const uint32_t s0 = d & 0x03030303u, s1 = (d >> 2) & 0x03030303u;
+        const uint32_t s2 = (d >> 4) & 0x03030303u, s3 = (d >> 6) & 0x03030303u;
+        const uint32_t lo01 = __byte_perm(s0, s1, 0x5140u), hi01 = __byte_perm(s0, s1, 0x7362u);
+        const uint32_t lo23 = __byte_perm(s2, s3, 0x5140u), hi23 = __byte_perm(s2, s3, 0x7362u);
+        uint4 v;
+        v.x = __byte_perm(lo01, lo23, 0x5410u);
+        v.y = __byte_perm(lo01, lo23, 0x7632u);
+        v.z = __byte_perm(hi01, hi23, 0x5410u);
+        v.w = __byte_perm(hi01, hi23, 0x7632u);
+        const uint32_t c = 4 * half + w;   // 16-byte chunk: people 16c .. 16c + 15
+        sts_u128(arow + ((c ^ (r & 7)) << 4), v);
+      }
+      // missing calls (code 01): add the person's FP32 dS row; bit 2i of m is
+      // person i of the word
+#pragma unroll
+      for (uint32_t w = 0; w < 4; ++w) {
+        uint32_t m = xw[w] & ~(xw[w] >> 1) & 0x55555555u;
+        while (m) {
+          const uint32_t b = 31u - __clz(m);
+          m ^= 1u << b;
+          const uint32_t drow = st + L::kDsOff + (64 * half + 16 * w + b / 2) * (kBwScores * 4);
+#pragma unroll
+          for (uint32_t q = 0; q < kBwScores / 4; ++q) {
+            const uint4 f = lds_u128(drow + 16 * q);
+            gcf[4 * q + 0] += __uint_as_float(f.x);
+            gcf[4 * q + 1] += __uint_as_float(f.y);
+            gcf[4 * q + 2] += __uint_as_float(f.z);
+            gcf[4 * q + 3] += __uint_as_float(f.w);
+          }
+        }
+      }
+      if ((it % kBw8MissFlush) == kBw8MissFlush - 1 || it == nit - 1) {
+#pragma unroll
+        for (uint32_t k = 0; k < kBwScores; ++k) {
+          gcd[k] += double(gcf[k]);
+          gcf[k] = 0.0f;
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(aready(s));
+
+      if ((it % kBw8Flush) == kBw8Flush - 1 || it == nit - 1) {
+        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        // columns 16 j + 8 half + k: limb j of score 8 half + k
+        const uint32_t lane_base = tmem + ((32 * quad) << 16) + 8 * half;
+        const uint64_t k0 = uint64_t(stile) * kBwScores + 8 * half;
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+          uint32_t d[8];
+          tmem_ld8(lane_base + 16 * j, d);
+          tmem_ld_wait();
+#pragma unroll
+          for (uint32_t k = 0; k < 8; ++k)
+            gwd[k] = fma(double(int32_t(d[k])), quanta[j * K16 + k0 + k], gwd[k]);
+        }
+        tc_fence_before();
+        mbar_arrive(accempty);
+        ++blk;
+      }
+    }
+    // The two halves of a row hold the missing term of different people: add
+    // them in a fixed order through shared memory (stage buffers are idle: the
+    // last accumulator commit followed every MMA, and every TMA was consumed).
+    named_barrier(1, kBwExpand);
+    double* swap = reinterpret_cast<double*>(smem);
+#pragma unroll
+    for (uint32_t k = 0; k < kBwScores; ++k) swap[(half * kBwM + r) * kBwScores + k] = gcd[k];
+    named_barrier(1, kBwExpand);
+    const uint64_t v = uint64_t(vtile) * kBwM + r;
+    if (ok && !lds_volatile_u32(abort_addr) && v < a.V) {
+#pragma unroll
+      for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t kl = 8 * half + k;
+        const uint64_t kk = uint64_t(stile) * kBwScores + kl;
+        if (kk < a.K) {
+          a.gw[v * a.K + kk] = float(gwd[k]);
+          if (a.gc)
+            a.gc[v * a.K + kk] =
+                float(-(swap[r * kBwScores + kl] + swap[(kBwM + r) * kBwScores + kl]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kBwN);
+  }
+}
+
+// dS [rows][K] -> 8-bit limb rows (tile t = k / 16: rows 64t + 16j + k % 16,
+// limb j) of P_pad people each, their quanta [4][K16], and the FP32 copy
+// [P_pad][K16] for the missing term; zeros past the last person and score.
+__global__ void gnm_bw_build8(const float* g, uint64_t rows, uint64_t K, uint64_t K16,
+                              uint64_t P_pad, const uint32_t* amax_bits, int8_t* planes,
+                              double* quanta, float* ds) {
+  const uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (x >= K16 * P_pad) return;
+  const uint64_t p = x % P_pad, k = x / P_pad;
+  const bool in = p < rows && k < K;
+  const float val = in ? g[p * K + k] : 0.0f;
+  ds[p * K16 + k] = val;
+  const float am = k < K ? __uint_as_float(amax_bits[k]) : 0.0f;
+  double q = am > 0.0f ? double(am) / 127.0 : 1.0;
+  const uint64_t row0 = (k / kBwScores) * kBwN + (k % kBwScores);
+  double rem = double(val);
+#pragma unroll
+  for (uint32_t j = 0; j < 4; ++j, q /= 254.0) {
+    const double li = fmin(fmax(rint(rem / q), -127.0), 127.0);
+    rem -= li * q;
+    planes[(row0 + kBwScores * j) * P_pad + p] = int8_t(li);
+    if (p == 0) quanta[j * K16 + k] = q;
+  }
+}
+
 // dS in output order -> fam order (zero for people outside the keep set).
 __global__ void gnm_scatter_grad(const float* gs, const uint32_t* out_to_fam, uint64_t P,
                                  uint64_t K, float* gsf) {
@@ -1939,12 +2265,13 @@ static cudaError_t launch_t8(const CUtensorMap& amap, const CUtensorMap& pmap, c
 }
 
 // Clusters of two CTAs along x: CTA 2i + r is rank r of pair i.
-template <int NP, int ST, bool MISSING, bool COUNT_LAST>
+template <int NP, int ST, bool MISSING, bool COUNT_LAST, bool SPAN = false>
 static cudaError_t launch_t8_pair(const CUtensorMap& amap, const CUtensorMap& pmap,
                                   const T8Args& a, uint32_t ptiles, uint32_t spairs,
                                   cudaStream_t s) {
   using L = T8PairSmem<NP, ST>;
-  const void* fn = reinterpret_cast<const void*>(gnm_t8_pair<NP, ST, MISSING, COUNT_LAST>);
+  const void* fn =
+      reinterpret_cast<const void*>(gnm_t8_pair<NP, ST, MISSING, COUNT_LAST, SPAN>);
   const cudaError_t e = raise_smem_limit(fn, int(L::kTotal));
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
@@ -1959,7 +2286,8 @@ static cudaError_t launch_t8_pair(const CUtensorMap& amap, const CUtensorMap& pm
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, gnm_t8_pair<NP, ST, MISSING, COUNT_LAST>, amap, pmap, a);
+  return cudaLaunchKernelEx(&cfg, gnm_t8_pair<NP, ST, MISSING, COUNT_LAST, SPAN>, amap, pmap,
+                            a);
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -2268,9 +2596,11 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
                        t->map8_2, pmap_half, b, t->ptiles, spairs, s)),
                    "8-bit pair missing launch");
       }
+      // the member plane of two score pairs per cluster (one pass's MMA work
+      // on half the clusters)
       b.z0 = 8;
-      check_cuda((launch_t8_pair<1, kT8PairStagesOne, true, true>(t->map8_1, pmap_half, b,
-                                                                  t->ptiles, spairs, s)),
+      check_cuda((launch_t8_pair<2, kT8PairStagesPair, true, true, true>(
+                     t->map8_1, pmap_half, b, t->ptiles, (spairs + 1) / 2, s)),
                  "8-bit pair count launch");
       p->launches += 5;
       return;
@@ -2336,6 +2666,66 @@ void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_b
   p->launches += 1;
 }
 
+// dS limbs in 8 bits (gnm_t8_backward): buffers [limb rows][P_pad] int8,
+// [P_pad][K16] FP32 dS, [4][K16] FP64 quanta, [K16] maxima, re-derived on
+// every call.
+static void backward_dw8(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float* gsf,
+                         float* d_grad_w, float* d_grad_corr, cudaStream_t s) {
+  const uint64_t K16 = (p->K + kBwScores - 1) / kBwScores * kBwScores;
+  const uint64_t P_pad = std::max<uint64_t>(kBw8K, (p->fam + kBw8K - 1) / kBw8K * kBw8K);
+  const uint64_t limb_rows = K16 / kBwScores * kBwN;
+  const uint64_t planes_bytes = (limb_rows * P_pad + 255) / 256 * 256;
+  const uint64_t ds_bytes = (P_pad * K16 * 4 + 255) / 256 * 256;
+  const uint64_t q_bytes = 4 * K16 * 8;
+  const uint64_t need = planes_bytes + ds_bytes + q_bytes + K16 * 4;
+  if (p->bw_bytes < need) {
+    check_cuda(cudaStreamSynchronize(s), "backward buffer resize");
+    pool_free(p->d_bw);
+    p->d_bw = nullptr;
+    p->device_bytes -= p->bw_bytes;
+    p->bw_bytes = 0;
+    p->d_bw = static_cast<uint8_t*>(pool_alloc(p->device, need, "backward dS limbs"));
+    p->bw_bytes = need;
+    p->device_bytes += need;
+  }
+  auto* planes = reinterpret_cast<int8_t*>(p->d_bw);
+  auto* ds = reinterpret_cast<float*>(p->d_bw + planes_bytes);
+  auto* quanta = reinterpret_cast<double*>(p->d_bw + planes_bytes + ds_bytes);
+  auto* amax = reinterpret_cast<uint32_t*>(p->d_bw + planes_bytes + ds_bytes + q_bytes);
+  check_cuda(cudaMemsetAsync(amax, 0, K16 * 4, s), "memset");
+  const uint64_t na = (p->fam + 63) / 64 * p->K;
+  if (na) {
+    gnm_bw_amax<<<uint32_t((na + 255) / 256), 256, 0, s>>>(gsf, p->fam, p->K, amax);
+    check_cuda(cudaGetLastError(), "gradient maximum launch");
+    p->launches += 1;
+  }
+  const uint64_t nb = K16 * P_pad;
+  gnm_bw_build8<<<uint32_t((nb + 255) / 256), 256, 0, s>>>(gsf, p->fam, p->K, K16, P_pad, amax,
+                                                           planes, quanta, ds);
+  check_cuda(cudaGetLastError(), "gradient limb launch");
+  p->launches += 1;
+
+  const CUtensorMap rmap = make_row_map(d_rows, p->bpv, p->V, pitch, Bw8Smem::kPkRow, kBwM);
+  const CUtensorMap bmap =
+      make_2d_map(CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, planes, P_pad, limb_rows, kBw8K, kBwN,
+                  CU_TENSOR_MAP_SWIZZLE_128B, "gradient limbs");
+  const CUtensorMap dmap = make_2d_map(CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ds, K16, P_pad,
+                                       kBwScores, kBw8K, CU_TENSOR_MAP_SWIZZLE_NONE, "gradient");
+  check_cuda(raise_smem_limit(reinterpret_cast<const void*>(gnm_t8_backward), int(Bw8Smem::kTotal)),
+             "backward shared memory");
+  BwArgs a;
+  a.V = p->V;
+  a.K = p->K;
+  a.nstages = uint32_t(P_pad / kBw8K);
+  a.gw = d_grad_w;
+  a.gc = d_grad_corr;
+  a.err = p->d_err;
+  const dim3 grid(uint32_t((p->V + kBwM - 1) / kBwM), uint32_t(K16 / kBwScores));
+  gnm_t8_backward<<<grid, kBwThreads, Bw8Smem::kTotal, s>>>(rmap, bmap, dmap, a, quanta, K16);
+  check_cuda(cudaGetLastError(), "backward launch");
+  p->launches += 1;
+}
+
 void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float* d_grad_s,
                  float* d_grad_w, float* d_grad_corr, cudaStream_t s) {
   if (!d_rows || !d_grad_s || !d_grad_w) fail(GNM_ERR_INVALID, "NULL buffer");
@@ -2360,6 +2750,10 @@ void backward_dw(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, const float
       p->launches += 1;
     }
     gsf = p->d_grad_fam;
+  }
+  if (p->bw_limb_bits == 8) {
+    backward_dw8(p, d_rows, pitch, gsf, d_grad_w, d_grad_corr, s);
+    return;
   }
   // dS limb rows and the FP32 copy, re-derived on every call
   const uint64_t K16 = (p->K + kBwScores - 1) / kBwScores * kBwScores;

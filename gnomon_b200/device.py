@@ -124,6 +124,11 @@ class DevicePlan:
     def shape(self) -> int:
         return int(self.lib.gnm_plan_tuned_shape(self.handle))
 
+    def set_backward_limbs(self, bits: int) -> None:
+        """dS limb width of ``backward``: 8 (default) or 16 (BF16)."""
+        e = self._err()
+        _lib.check(self.lib.gnm_plan_set_backward_limbs(self.handle, int(bits), C.byref(e)), e)
+
     def capture(self, rows: torch.Tensor, pitch: int, sums=None, counts=None):
         """Record one full scoring pass (reset + accumulate + finalize) into a CUDA
         graph; ``graph.replay()`` reruns it with no per-launch host work.  Returns

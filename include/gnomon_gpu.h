@@ -124,7 +124,9 @@ typedef struct gnm_run_options {
   uint64_t block_variants;        /* streaming block; 0 = default: the whole matrix
                                      if it fits (tensor engine: four blocks of at
                                      least 16,384 variants, each block's compute
-                                     overlapping the next block's copy)           */
+                                     overlapping the next block's copy); the
+                                     tensor engine rounds it up to a multiple of
+                                     128 variants                                 */
   gnm_block_callback on_block;    /* may be NULL                                  */
   void* on_block_ctx;
 } gnm_run_options;
@@ -277,6 +279,12 @@ gnm_status gnm_synth_fill_device(uint8_t* d_rows, uint64_t pitch, uint64_t varia
 gnm_status gnm_backward_dw_device(gnm_plan* plan, const uint8_t* d_rows, uint64_t pitch,
                                   const float* d_grad_s, float* d_grad_w,
                                   float* d_grad_corr, void* stream, gnm_error* err);
+
+/* Limb width of the backward's dS split: 8 (the default: signed 8-bit limbs,
+ * tcgen05 kind::i8, 128 people per stage) or 16 (BF16 limbs, kind::f16, 64
+ * people per stage).  Both leave each dS within 2^-31.9 (8) / 2^-33 (16) of
+ * its score's largest |dS|.  GNM_ERR_INVALID for any other width. */
+gnm_status gnm_plan_set_backward_limbs(gnm_plan* plan, uint32_t bits, gnm_error* err);
 
 /* ---- PLINK 2 .pgen input ---------------------------------------------------
  * gnomon scores a .pgen through a virtual .bed (shared/adapt_plink2.rs:1093-

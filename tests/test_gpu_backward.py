@@ -1,4 +1,6 @@
-"""Backward kernel dW = G^T dS (re-unpacking genotypes) and the autograd Function."""
+"""Backward kernel dW = G^T dS (re-unpacking genotypes) and the autograd Function.
+The kernel tests run both dS limb widths: 8-bit limbs (gnm_t8_backward, the
+default) and BF16 limbs (gnm_tc_backward)."""
 import numpy as np
 import pytest
 
@@ -17,8 +19,9 @@ def _device_rows(rows, pitch):
     return torch.from_numpy(dev).cuda()
 
 
+@pytest.mark.parametrize("bits", [8, 16])
 @pytest.mark.parametrize("keep", [False, True])
-def test_backward_kernel_vs_extended(cuda, keep):
+def test_backward_kernel_vs_extended(cuda, keep, bits):
     import torch
     from gnomon_b200.device import DevicePlan, row_pitch
     _, prep, rows, _ = synth_case(3001, 517, scores=19, config="diff_20k_x_200k_k16")
@@ -31,6 +34,7 @@ def test_backward_kernel_vs_extended(cuda, keep):
     gs = np.random.default_rng(2).standard_normal((P, K)).astype(np.float32)
     pitch = row_pitch(prep.bytes_per_variant)
     plan = DevicePlan(prep, engine=_lib.ENGINE_PLAIN)
+    plan.set_backward_limbs(bits)
     gw, gc = plan.backward(_device_rows(rows, pitch), pitch, torch.from_numpy(gs).cuda(),
                            grad_corr=True)
     plan.sync()
@@ -92,10 +96,11 @@ def test_autograd_finite_differences_and_fp64_gradient(cuda):
         assert abs(fd - g[v, k]) <= 1e-4 * max(1.0, abs(g[v, k])) + 1e-7, (v, k, fd, g[v, k])
 
 
-def test_backward_many_people_and_score_scales(cuda):
-    """More than 32768 people (two exact FP32 blocks of the tensor-core
-    backward), a ragged last variant tile, and scores whose dS magnitudes
-    differ by 60 orders (the per-score limb quantum), one all-zero."""
+@pytest.mark.parametrize("bits", [8, 16])
+def test_backward_many_people_and_score_scales(cuda, bits):
+    """More than 32768 people (two exact FP32 blocks of the BF16 backward), a
+    ragged last variant tile, and scores whose dS magnitudes differ by 60
+    orders (the per-score limb quantum), one all-zero."""
     import torch
     from gnomon_b200.device import DevicePlan, row_pitch
     _, prep, rows, _ = synth_case(40001, 260, scores=5, config="diff_20k_x_200k_k16")
@@ -109,6 +114,7 @@ def test_backward_many_people_and_score_scales(cuda):
     gs[::7, 4] = np.float32(0.0)
     pitch = row_pitch(prep.bytes_per_variant)
     plan = DevicePlan(prep, engine=_lib.ENGINE_PLAIN)
+    plan.set_backward_limbs(bits)
     gw, gc = plan.backward(_device_rows(rows, pitch), pitch, torch.from_numpy(gs).cuda(),
                            grad_corr=True)
     plan.sync()
@@ -121,3 +127,14 @@ def test_backward_many_people_and_score_scales(cuda):
             continue
         assert np.abs(gw[:, k] - ew[:, k]).max() / scale < 1e-6, k
         assert np.abs(gc[:, k] - ec[:, k]).max() / scale < 1e-6, k
+
+
+def test_backward_limbs_rejects_other_widths(cuda):
+    _, prep, _, _ = synth_case(100, 64, scores=2, config="diff_20k_x_200k_k16")
+    from gnomon_b200.device import DevicePlan
+    plan = DevicePlan(prep, engine=_lib.ENGINE_PLAIN)
+    for bad in (0, 4, 32):
+        with pytest.raises(_lib.GnomonGpuError) as ei:
+            plan.set_backward_limbs(bad)
+        assert ei.value.status == _lib.GNM_ERR_INVALID
+    plan.close()
