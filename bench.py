@@ -35,6 +35,10 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "bandwidth_50k_x_1m"
 METRIC = "genotype*score pairs/s"
+# B200 dense 8-bit integer tensor throughput, NVIDIA's nominal figure (the
+# 2:4-sparse figure halved); the pool measures no int8 peak, and twice its
+# measured BF16 GEMM understates what the 8-bit kernels reach
+INT8_NOMINAL_TOPS = 4500.0
 PROFILE = ROOT / "profiles" / "plain_accumulate_bandwidth_50k_x_1m.md"
 
 
@@ -486,8 +490,10 @@ def gpu_arm(args, rank, world, local_rank):
                 "algorithmic": "2 x people x cells x 3 weight limbs",
                 "executed_int_ops_per_launch": executed,
                 "executed_tops": executed / (kernel_ms / 1e3) / 1e12,
-                "executed_frac_of_int8_peak": executed / (kernel_ms / 1e3) / 1e12 / (2 * pk),
-                "int8_peak": "2 x the bf16 figure (nominal dense ratio)"}
+                "executed_frac_of_int8_nominal": executed / (kernel_ms / 1e3) / 1e12
+                / INT8_NOMINAL_TOPS,
+                "int8_peak": f"{INT8_NOMINAL_TOPS:.0f} TOPS, B200 nominal dense (no measured "
+                             "int8 figure on this pool)"}
     elif tensor:
         # executed tensor-core work: 8 limb MMAs (4 dosage, 3 correction, 1 count)
         # over 256-person x 128-score tiles and 64-variant stages
@@ -629,7 +635,7 @@ def gpu_arm(args, rank, world, local_rank):
                 "ms": bwd_ms, "pairs_per_s": P * V * K / (bwd_ms / 1e3),
                 "kernel": "gnm_t8_backward (8-bit dS limbs, + limb build)",
                 "executed_tops": bw_tflops,
-                "executed_frac_of_int8_peak": bw_tflops / (2 * peaks_tc()[0]),
+                "executed_frac_of_int8_nominal": bw_tflops / INT8_NOMINAL_TOPS,
                 "row_bytes_gbs": V * bpv * (k_pad // 16) / (bwd_ms / 1e3) / 1e9}
         print(json.dumps(line), flush=True)
     plan.close()

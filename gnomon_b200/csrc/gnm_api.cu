@@ -953,12 +953,13 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   if (resume && (!resume->sums || !resume->counts))
     fail(GNM_ERR_INVALID, "resume state has NULL buffers");
   const uint64_t pitch = (bpv + 127) / 128 * 128;
-  // tensor-engine blocks start on 128-variant boundaries (the 8-bit kernels'
-  // stage; other blocks fall back to BF16 limbs); rows between the boundary
-  // and the resume point are staged as zeros (they contribute nothing)
+  // tensor-engine blocks start on 64-variant boundaries, by default on
+  // 128-variant ones (the 8-bit kernels' stage; other blocks fall back to
+  // BF16 limbs); rows between the boundary and the resume point are staged
+  // as zeros (they contribute nothing)
   constexpr uint64_t kTensorAlign = 128;
-  const uint64_t v_first =
-      engine == GNM_ENGINE_TENSOR ? v_start - v_start % kTensorAlign : v_start;
+  const uint64_t t_align = o.block_variants ? 64 : kTensorAlign;
+  const uint64_t v_first = engine == GNM_ENGINE_TENSOR ? v_start - v_start % t_align : v_start;
   HostRun r{bpv, prep, bed, pitch, v_start};
 
   RunResources res(device);
@@ -979,7 +980,9 @@ static void host_run_impl(const gnm_prep_view* prep, const gnm_bed_view* bed,
   if (!o.block_variants && engine == GNM_ENGINE_TENSOR && remaining >= 4 * kTensorMinBlock)
     block = std::min(block, (remaining + 3) / 4);
   block = std::max<uint64_t>(1, std::min<uint64_t>(block, std::max<uint64_t>(1, remaining)));
-  if (engine == GNM_ENGINE_TENSOR) block = (block + kTensorAlign - 1) / kTensorAlign * kTensorAlign;
+  // a caller's block size is kept to the engine's 64-variant granularity (its
+  // blocks then may run on BF16 limbs); the default one is a multiple of 128
+  if (engine == GNM_ENGINE_TENSOR) block = (block + t_align - 1) / t_align * t_align;
   const int nbuf = remaining > block ? 2 : 1;
 
   std::vector<uint8_t*> dbuf(nbuf, nullptr);

@@ -126,7 +126,10 @@ typedef struct gnm_run_options {
                                      least 16,384 variants, each block's compute
                                      overlapping the next block's copy); the
                                      tensor engine rounds it up to a multiple of
-                                     128 variants                                 */
+                                     64 variants (its 8-bit kernels take blocks
+                                     starting at multiples of 128; others run on
+                                     BF16 limbs); its default blocks are
+                                     multiples of 128                             */
   gnm_block_callback on_block;    /* may be NULL                                  */
   void* on_block_ctx;
 } gnm_run_options;
