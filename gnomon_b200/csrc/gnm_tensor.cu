@@ -2392,6 +2392,9 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   // the BF16 limbs' speed on the batched workload, errors below 2.3e-7 at full
   // length on every workload
   t->i8 = true;
+  // SM pairs when the plan fills pairs of 128-score tiles (with one tile the
+  // pair's second CTA would hold no scores)
+  t->pair = t->stiles >= 2;
   if (t->V_pad > (uint64_t(1) << 31)) fail(GNM_ERR_INVALID, "too many variants for the tensor engine");
 
   const uint64_t plane = t->K_pad * t->V_pad;
