@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "gnm_device.cuh"
@@ -74,7 +75,9 @@ struct TensorPlan {
   uint64_t V_pad8 = 0;
   CUtensorMap map8_2, map8_1;             // boxes of two planes / one plane
   bool i8 = false;                        // wide GEMM on 8-bit limbs (gnm_t8_accumulate)
-  bool pair = false;                      // ... over SM pairs (gnm_t8_pair)
+  bool pair = false;                      // ... over SM pairs (gnm_t8_pairs)
+  double* d_part_pass = nullptr;          // SM pairs, passes 1-3: [3][K_pad][P_pad]
+  bool pass_valid = false;                // d_part_pass written since the last reset
   bool narrow = false;                    // few scores: gnm_tc_narrow (people as M)
   bool can_narrow = false;                // K <= 64: either kernel can run the plan
   CUtensorMap nmap_dos, nmap_mis;         // narrow boxes: 16 scores x 4 planes
@@ -661,27 +664,68 @@ struct T8PairSmem {
   static_assert(kBOff % 1024 == 0 && kPkOff % 1024 == 0, "swizzled operands need 1 KB alignment");
 };
 
-// SPAN: the planes of a pass are the member plane of NP different score
-// pairs (rows 256 (NP * pair index + j) + 128 rank), every one a count;
-// otherwise NP consecutive planes of one score pair.
-template <int NP, int ST, bool MISSING, bool COUNT_LAST, bool SPAN>
+// One persistent launch per accumulate call: each cluster walks the work items
+// w = cluster, cluster + clusters, ... of a static list, pass-major: passes
+// 0-3 (dosage limbs 0-1 and 2-3, correction limbs 0-1 and 2-3) over every
+// (people tile, score pair), then pass 4 (the member plane) over every
+// (people tile, two score pairs).  Passes 1-3 add into FP64 partial arrays of
+// their own, since a tile's passes may run on different clusters at the same
+// time; pass 0 adds into the plan's partials with the other kernels, and the
+// first call after a reset writes the pass arrays instead of adding to them.
+struct T8PairArgs {
+  uint64_t num_rows;       // rows of this block
+  int32_t a_x0;            // absolute variant index of block row 0 (multiple of 128)
+  double* part_sum;        // pass 0 (and every other kernel): [K_pad][P_pad]
+  double* part_pass;       // passes 1-3: [3][K_pad][P_pad]
+  uint32_t* part_cnt;
+  uint64_t P_pad;
+  uint64_t K_pad;
+  const double* quanta;    // [kT8Planes][K_pad]
+  uint32_t* err;
+  uint32_t raster;         // 1: score pairs fastest within a pass
+  uint32_t ptiles, spairs, spairs_m;   // people tiles, score pairs, pairs of score pairs
+  uint32_t items;          // 4 * ptiles * spairs + ptiles * spairs_m
+  uint32_t store;          // the pass arrays are written, not added to
+};
+
+struct PairItem {
+  uint32_t pass, ptile, spair;   // pass 4: spair = index of the pair of score pairs
+};
+
+__device__ __forceinline__ PairItem pair_item(const T8PairArgs& a, uint32_t w) {
+  const uint32_t per = a.ptiles * a.spairs;
+  PairItem r;
+  uint32_t t, sp;
+  if (w < 4 * per) {
+    r.pass = w / per;
+    t = w % per;
+    sp = a.spairs;
+  } else {
+    r.pass = 4;
+    t = w - 4 * per;
+    sp = a.spairs_m;
+  }
+  r.ptile = a.raster ? t / sp : t % a.ptiles;
+  r.spair = a.raster ? t % sp : t / a.ptiles;
+  return r;
+}
+
+template <int ST>
 __global__ void __launch_bounds__(kT8Threads, 1)
-    gnm_t8_pair(const __grid_constant__ CUtensorMap amap,
-                const __grid_constant__ CUtensorMap pmap, T8Args a) {
-  using L = T8PairSmem<NP, ST>;
+    gnm_t8_pairs(const __grid_constant__ CUtensorMap amap2,
+                 const __grid_constant__ CUtensorMap amap1,
+                 const __grid_constant__ CUtensorMap pmap, T8PairArgs a) {
+  using L = T8PairSmem<2, ST>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t sb = smem_u32(smem);
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_ctarank();   // 0: leader (issues the MMAs), 1: peer
-  const uint32_t pair_x = blockIdx.x >> 1;
-  const uint32_t ptile = a.raster ? blockIdx.y : pair_x;
-  const uint32_t spair = a.raster ? pair_x : blockIdx.y;
-  static_assert(!SPAN || (MISSING && COUNT_LAST), "spanning passes count missing calls");
-  // this CTA's first score row of plane j (uniform per CTA)
-  auto srow = [&](uint32_t j) -> uint32_t {
-    return SPAN ? (2 * (uint32_t(NP) * spair + j) + rank) * kTcM : (2 * spair + rank) * kTcM;
+  const uint32_t cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
+  // this CTA's first score row of plane j of an item (uniform per CTA)
+  auto srow = [&](const PairItem& w, uint32_t j) -> uint32_t {
+    return w.pass == 4 ? (2 * (2 * w.spair + j) + rank) * kTcM : (2 * w.spair + rank) * kTcM;
   };
   const uint32_t nit = uint32_t((a.num_rows + kT8K - 1) / kT8K);
   constexpr uint32_t BS = L::kBStages;
@@ -709,7 +753,8 @@ __global__ void __launch_bounds__(kT8Threads, 1)
     mbar_init(drain, 1);
     *abort_flag = 0u;
     fence_mbar_init();
-    prefetch_tmap(&amap);
+    prefetch_tmap(&amap2);
+    prefetch_tmap(&amap1);
     prefetch_tmap(&pmap);
   }
   if (warp == 1) {
@@ -724,67 +769,86 @@ __global__ void __launch_bounds__(kT8Threads, 1)
   if (warp == 0) {
     // ---------------- TMA producer (each CTA its own halves) ----------------
     if (lane == 0) {
-      for (uint32_t it = 0; it < nit; ++it) {
-        const uint32_t s = it % ST, ph = (it / ST) & 1u;
-        if (!mbar_wait_bounded(aempty(s), ph ^ 1u)) {
-          *abort_flag = 1u;
-          atomicOr(a.err, kErrMmaTimeout);
-          break;
+      uint32_t g = 0;   // stages issued so far, over every item
+      bool stop = false;
+      for (uint32_t wi = cid; wi < a.items && !stop; wi += ncl) {
+        const PairItem w = pair_item(a, wi);
+        for (uint32_t it = 0; it < nit; ++it, ++g) {
+          const uint32_t s = g % ST, ph = (g / ST) & 1u;
+          if (!mbar_wait_bounded(aempty(s), ph ^ 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            stop = true;
+            break;
+          }
+          if (lds_volatile_u32(abort_addr)) {
+            stop = true;
+            break;
+          }
+          mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
+          const uint32_t a_st = sb + L::kAOff + s * L::kAStage;
+          const int32_t x = a.a_x0 + int32_t(it * kT8K);
+          if (w.pass == 4) {   // the member plane of two score pairs
+            tma_load_3d(a_st, &amap1, x, int32_t(srow(w, 0)), 8, full(s));
+            tma_load_3d(a_st + L::kPlane, &amap1, x, int32_t(srow(w, 1)), 8, full(s));
+          } else {
+            tma_load_3d(a_st, &amap2, x, int32_t(srow(w, 0)), int32_t(2 * w.pass), full(s));
+          }
+          tma_load_2d(sb + L::kPkOff + s * L::kPk, &pmap,
+                      int32_t(w.ptile * (kTcN / 4) + rank * L::kPkRow), int32_t(it * kT8K),
+                      full(s));
         }
-        if (lds_volatile_u32(abort_addr)) break;
-        mbar_arrive_expect_tx(full(s), L::kAStage + L::kPk);
-        if (SPAN) {   // one plane box per score pair
-#pragma unroll
-          for (uint32_t j = 0; j < uint32_t(NP); ++j)
-            tma_load_3d(sb + L::kAOff + s * L::kAStage + j * L::kPlane, &amap,
-                        a.a_x0 + int32_t(it * kT8K), int32_t(srow(j)), a.z0, full(s));
-        } else {
-          tma_load_3d(sb + L::kAOff + s * L::kAStage, &amap, a.a_x0 + int32_t(it * kT8K),
-                      int32_t(srow(0)), a.z0, full(s));
-        }
-        tma_load_2d(sb + L::kPkOff + s * L::kPk, &pmap,
-                    int32_t(ptile * (kTcN / 4) + rank * L::kPkRow), int32_t(it * kT8K), full(s));
       }
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer (leader CTA only) ----------------
     if (lane == 0 && rank == 0) {
       constexpr uint32_t idesc = idesc_s8u8_s32(2 * kTcM, kTcN);
-      uint32_t blk = 0;
-      for (uint32_t it = 0; it < nit; ++it) {
-        const uint32_t s = it % ST;
-        const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
-        const bool first = (it % kT8Flush) == 0;
-        if (first && it > 0) {
-          if (!mbar_wait_bounded_cluster(accempty, (blk - 1) & 1u)) {
+      uint32_t g = 0, blk = 0;
+      bool stop = false;
+      for (uint32_t wi = cid; wi < a.items && !stop; wi += ncl) {
+        for (uint32_t it = 0; it < nit; ++it, ++g) {
+          const uint32_t s = g % ST;
+          const uint32_t bsl = g % BS, bph = (g / BS) & 1u;
+          const bool first = (it % kT8Flush) == 0;
+          if (first && blk > 0) {
+            // the epilogues of both CTAs drained the previous block
+            if (!mbar_wait_bounded_cluster(accempty, (blk - 1) & 1u)) {
+              *abort_flag = 1u;
+              atomicOr(a.err, kErrMmaTimeout);
+              stop = true;
+              break;
+            }
+          }
+          if (!mbar_wait_bounded(bready(bsl), bph)) {
             *abort_flag = 1u;
             atomicOr(a.err, kErrMmaTimeout);
+            stop = true;
             break;
           }
-        }
-        if (!mbar_wait_bounded(bready(bsl), bph)) {
-          *abort_flag = 1u;
-          atomicOr(a.err, kErrMmaTimeout);
-          break;
-        }
-        if (lds_volatile_u32(abort_addr)) break;
-        tc_fence_after();
-        const uint32_t a0 = sb + L::kAOff + s * L::kAStage;
-        const uint32_t b0 = sb + L::kBOff + bsl * L::kB;
-#pragma unroll
-        for (uint32_t kk = 0; kk < kT8K / 32; ++kk) {   // K = 32 bytes per MMA
-          const uint64_t bdesc = desc_kmajor_sw128(b0 + kk * 32);
-#pragma unroll
-          for (uint32_t j = 0; j < uint32_t(NP); ++j) {
-            const uint64_t adesc = desc_kmajor_sw128(a0 + j * L::kPlane + kk * 32);
-            tc_mma_i8_pair(tmem + j * kTcN, adesc, bdesc, idesc, (first && kk == 0) ? 0u : 1u);
+          if (lds_volatile_u32(abort_addr)) {
+            stop = true;
+            break;
           }
-        }
-        tc_commit_pair(aempty(s), 0x3);
-        tc_commit_pair(bempty(bsl), 0x3);
-        if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
-          tc_commit_pair(accfull, 0x3);
-          ++blk;
+          tc_fence_after();
+          const uint32_t a0 = sb + L::kAOff + s * L::kAStage;
+          const uint32_t b0 = sb + L::kBOff + bsl * L::kB;
+#pragma unroll
+          for (uint32_t kk = 0; kk < kT8K / 32; ++kk) {   // K = 32 bytes per MMA
+            const uint64_t bdesc = desc_kmajor_sw128(b0 + kk * 32);
+#pragma unroll
+            for (uint32_t j = 0; j < 2; ++j) {
+              const uint64_t adesc = desc_kmajor_sw128(a0 + j * L::kPlane + kk * 32);
+              tc_mma_i8_pair(tmem + j * kTcN, adesc, bdesc, idesc,
+                             (first && kk == 0) ? 0u : 1u);
+            }
+          }
+          tc_commit_pair(aempty(s), 0x3);
+          tc_commit_pair(bempty(bsl), 0x3);
+          if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+            tc_commit_pair(accfull, 0x3);
+            ++blk;
+          }
         }
       }
       // every MMA this thread issued has completed before either CTA moves on
@@ -802,113 +866,115 @@ __global__ void __launch_bounds__(kT8Threads, 1)
     const uint32_t h = ew >> 2;
     const uint32_t quad = warp & 3;
     const uint32_t lead_accempty = mapa_shared(accempty, 0);
-    uint32_t blk = 0;
-    for (uint32_t it = 0; it < nit; ++it) {
-      const uint32_t s = it % ST, ph = (it / ST) & 1u;
-      const uint32_t bsl = it % BS, bph = (it / BS) & 1u;
-      if (!mbar_wait_bounded(full(s), ph)) {
-        *abort_flag = 1u;
-        atomicOr(a.err, kErrTmaTimeout);
-        break;
-      }
-      // the operand slot is free once the MMAs of stage it - BS completed
-      if (!mbar_wait_bounded(bempty(bsl), bph ^ 1u)) {
-        *abort_flag = 1u;
-        atomicOr(a.err, kErrMmaTimeout);
-        break;
-      }
-      if (lds_volatile_u32(abort_addr)) break;
-      const uint32_t pk = sb + L::kPkOff + s * L::kPk;
-      const uint32_t bt = sb + L::kBOff + bsl * L::kB;
-      {
-        uint32_t x[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-        for (uint32_t i = 0; i < 16; ++i)
-          x[i >> 2] |= lds_u8(pk + (16 * c + i) * L::kPkRow + col) << (8 * (i & 3));
-#pragma unroll
-        for (uint32_t i = 0; i < 4; ++i) x[i] = code_fields<MISSING>(x[i]);
-#pragma unroll
-        for (uint32_t q = 0; q < 4; ++q) {
-          uint4 v;
-          v.x = (x[0] >> (2 * q)) & 0x03030303u;
-          v.y = (x[1] >> (2 * q)) & 0x03030303u;
-          v.z = (x[2] >> (2 * q)) & 0x03030303u;
-          v.w = (x[3] >> (2 * q)) & 0x03030303u;
-          // operand row of person 4col + q of this CTA's half; the pair's
-          // TMEM column is 128 rank + row, the wide kernels' slot order
-          const uint32_t n = 32 * q + col;
-          sts_u128(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4), v);
-        }
-      }
-      // the warp's operand stores, fenced into the tensor core's (async)
-      // proxy, are ordered before one arrival on the leader's barrier; its
-      // consumer is the MMA, so no cluster-scope release is needed (one cost
-      // a memory-barrier stall per stage that halved the tensor pipe's use)
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) mbar_arrive_remote(mapa_shared(bready(bsl), 0));
-
-      if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
-        if (!mbar_wait_bounded(accfull, blk & 1u)) {
+    const uint64_t pass_stride = a.K_pad * a.P_pad;
+    uint32_t g = 0, blk = 0;
+    bool stop = false;
+    for (uint32_t wi = cid; wi < a.items && !stop; wi += ncl) {
+      const PairItem w = pair_item(a, wi);
+      const bool missing = w.pass >= 2;
+      for (uint32_t it = 0; it < nit; ++it, ++g) {
+        const uint32_t s = g % ST, ph = (g / ST) & 1u;
+        const uint32_t bsl = g % BS, bph = (g / BS) & 1u;
+        if (!mbar_wait_bounded(full(s), ph)) {
           *abort_flag = 1u;
-          atomicOr(a.err, kErrMmaTimeout);
+          atomicOr(a.err, kErrTmaTimeout);
+          stop = true;
           break;
         }
-        tc_fence_after();
-        if (SPAN) {
-          const uint32_t lane_base = tmem + ((32 * quad) << 16);
+        // the operand slot is free once the MMAs of stage g - BS completed
+        if (!mbar_wait_bounded(bempty(bsl), bph ^ 1u)) {
+          *abort_flag = 1u;
+          atomicOr(a.err, kErrMmaTimeout);
+          stop = true;
+          break;
+        }
+        if (lds_volatile_u32(abort_addr)) {
+          stop = true;
+          break;
+        }
+        const uint32_t pk = sb + L::kPkOff + s * L::kPk;
+        const uint32_t bt = sb + L::kBOff + bsl * L::kB;
+        {
+          uint32_t x[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-          for (uint32_t j = 0; j < uint32_t(NP); ++j) {
-            if (srow(j) >= a.K_pad) continue;
-            const uint64_t k = uint64_t(srow(j)) + 32 * quad + lane;
-            uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(ptile) * kTcN;
-#pragma unroll 1
-            for (uint32_t cb = h * (kTcN / 64); cb < (h + 1) * (kTcN / 64); ++cb) {
-              uint32_t r[32];
-              tmem_ld32(lane_base + j * kTcN + 32 * cb, r);
-              tmem_ld_wait();
+          for (uint32_t i = 0; i < 16; ++i)
+            x[i >> 2] |= lds_u8(pk + (16 * c + i) * L::kPkRow + col) << (8 * (i & 3));
 #pragma unroll
-              for (int i = 0; i < 32; ++i) pc[32 * cb + i] += r[i];
-            }
+          for (uint32_t i = 0; i < 4; ++i)
+            x[i] = missing ? code_fields<true>(x[i]) : code_fields<false>(x[i]);
+#pragma unroll
+          for (uint32_t q = 0; q < 4; ++q) {
+            uint4 v;
+            v.x = (x[0] >> (2 * q)) & 0x03030303u;
+            v.y = (x[1] >> (2 * q)) & 0x03030303u;
+            v.z = (x[2] >> (2 * q)) & 0x03030303u;
+            v.w = (x[3] >> (2 * q)) & 0x03030303u;
+            // operand row of person 4col + q of this CTA's half; the pair's
+            // TMEM column is 128 rank + row, the wide kernels' slot order
+            const uint32_t n = 32 * q + col;
+            sts_u128(bt + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4), v);
           }
-        } else if (srow(0) < a.K_pad) {
-          const uint64_t k = uint64_t(srow(0)) + 32 * quad + lane;
-          double* ps = a.part_sum + k * a.P_pad + uint64_t(ptile) * kTcN;
-          uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(ptile) * kTcN;
+        }
+        // the warp's operand stores, fenced into the tensor core's (async)
+        // proxy, are ordered before one arrival on the leader's barrier; its
+        // consumer is the MMA, so no cluster-scope release is needed
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_remote(mapa_shared(bready(bsl), 0));
+
+        if ((it % kT8Flush) == kT8Flush - 1 || it == nit - 1) {
+          if (!mbar_wait_bounded(accfull, blk & 1u)) {
+            *abort_flag = 1u;
+            atomicOr(a.err, kErrMmaTimeout);
+            stop = true;
+            break;
+          }
+          tc_fence_after();
           const uint32_t lane_base = tmem + ((32 * quad) << 16);
-          constexpr uint32_t kSum = COUNT_LAST ? uint32_t(NP) - 1u : uint32_t(NP);
-          double qv[NP];
+          if (w.pass == 4) {
 #pragma unroll
-          for (uint32_t j = 0; j < uint32_t(NP); ++j) qv[j] = a.quanta[(a.z0 + j) * a.K_pad + k];
+            for (uint32_t j = 0; j < 2; ++j) {
+              if (srow(w, j) >= a.K_pad) continue;
+              const uint64_t k = uint64_t(srow(w, j)) + 32 * quad + lane;
+              uint32_t* pc = a.part_cnt + k * a.P_pad + uint64_t(w.ptile) * kTcN;
 #pragma unroll 1
-          for (uint32_t cb = h * (kTcN / 64); cb < (h + 1) * (kTcN / 64); ++cb) {
-            if constexpr (kSum > 0) {
-              double acc[32];
-#pragma unroll
-              for (int i = 0; i < 32; ++i) acc[i] = 0.0;
-#pragma unroll
-              for (uint32_t j = 0; j < kSum; ++j) {
+              for (uint32_t cb = h * (kTcN / 64); cb < (h + 1) * (kTcN / 64); ++cb) {
                 uint32_t r[32];
                 tmem_ld32(lane_base + j * kTcN + 32 * cb, r);
                 tmem_ld_wait();
 #pragma unroll
-                for (int i = 0; i < 32; ++i) acc[i] = fma(double(int32_t(r[i])), qv[j], acc[i]);
+                for (int i = 0; i < 32; ++i) pc[32 * cb + i] += r[i];
               }
-#pragma unroll
-              for (int i = 0; i < 32; ++i) ps[32 * cb + i] += acc[i];
             }
-            if (COUNT_LAST) {
-              uint32_t r[32];
-              tmem_ld32(lane_base + (NP - 1) * kTcN + 32 * cb, r);
+          } else if (srow(w, 0) < a.K_pad) {
+            const uint64_t k = uint64_t(srow(w, 0)) + 32 * quad + lane;
+            double* ps = (w.pass == 0 ? a.part_sum : a.part_pass + (w.pass - 1) * pass_stride) +
+                         k * a.P_pad + uint64_t(w.ptile) * kTcN;
+            // the pass arrays' first block after a reset is written, not added
+            const bool write = w.pass > 0 && a.store && it < kT8Flush;
+            const double q0 = a.quanta[(2 * w.pass) * a.K_pad + k];
+            const double q1 = a.quanta[(2 * w.pass + 1) * a.K_pad + k];
+#pragma unroll 1
+            for (uint32_t cb = h * (kTcN / 64); cb < (h + 1) * (kTcN / 64); ++cb) {
+              uint32_t r0[32], r1[32];
+              tmem_ld32(lane_base + 32 * cb, r0);
+              tmem_ld32(lane_base + kTcN + 32 * cb, r1);
               tmem_ld_wait();
+              if (write) {
 #pragma unroll
-              for (int i = 0; i < 32; ++i) pc[32 * cb + i] += r[i];
+                for (int i = 0; i < 32; ++i)
+                  ps[32 * cb + i] = fma(double(int32_t(r1[i])), q1, double(int32_t(r0[i])) * q0);
+              } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                  ps[32 * cb + i] += fma(double(int32_t(r1[i])), q1, double(int32_t(r0[i])) * q0);
+              }
             }
           }
+          tc_fence_before();
+          mbar_arrive_cluster(lead_accempty);
+          ++blk;
         }
-        tc_fence_before();
-        mbar_arrive_cluster(lead_accempty);
-        ++blk;
       }
     }
   }
@@ -1549,12 +1615,15 @@ __global__ void gnm_tc_build_planes(const float* w, const float* corr, const uin
 
 // out[o*K + k] = init[k] + part_sum[k][slot(fam(o))]; slot(f) is the operand
 // row of person f: tile (f / 256), row 128*h + 32*(r%4) + (r%128)/4 with
-// r = f % 256 and h = r / 128.  The narrow engine's epilogue writes in person
-// order, one slot per variant split: those slots are added in split order.
+// r = f % 256 and h = r / 128.  `pass` (may be null): the SM-pair kernel's
+// partials of passes 1-3, [3][pass_stride], added after part_sum in pass
+// order.  The narrow engine's epilogue writes in person order, one slot per
+// variant split: those slots are added in split order.
 __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt, uint64_t P_pad,
                                 const double* init, const uint32_t* out_to_fam, uint64_t P,
                                 uint64_t K, uint32_t nslots, uint64_t slot_stride,
-                                double* sums, uint32_t* counts) {
+                                const double* pass, uint64_t pass_stride, double* sums,
+                                uint32_t* counts) {
   const uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (x >= P * K) return;
   const uint64_t o = x / K, k = x % K;
@@ -1562,7 +1631,10 @@ __global__ void gnm_tc_finalize(const double* part_sum, const uint32_t* part_cnt
   if (nslots == 0) {   // wide engine: one slot, operand-row order
     const uint64_t r = f % kTcN, h = r / 128, rr = r % 128;
     const uint64_t slot = (f / kTcN) * kTcN + 128 * h + 32 * (rr % 4) + rr / 4;
-    sums[x] = init[k] + part_sum[k * P_pad + slot];
+    double s = part_sum[k * P_pad + slot];
+    if (pass)
+      for (uint32_t j = 0; j < 3; ++j) s += pass[j * pass_stride + k * P_pad + slot];
+    sums[x] = init[k] + s;
     counts[x] = part_cnt[k * P_pad + slot];
     return;
   }
@@ -2264,18 +2336,51 @@ static cudaError_t launch_t8(const CUtensorMap& amap, const CUtensorMap& pmap, c
   return cudaGetLastError();
 }
 
-// Clusters of two CTAs along x: CTA 2i + r is rank r of pair i.
-template <int NP, int ST, bool MISSING, bool COUNT_LAST, bool SPAN = false>
-static cudaError_t launch_t8_pair(const CUtensorMap& amap, const CUtensorMap& pmap,
-                                  const T8Args& a, uint32_t ptiles, uint32_t spairs,
-                                  cudaStream_t s) {
-  using L = T8PairSmem<NP, ST>;
-  const void* fn =
-      reinterpret_cast<const void*>(gnm_t8_pair<NP, ST, MISSING, COUNT_LAST, SPAN>);
-  const cudaError_t e = raise_smem_limit(fn, int(L::kTotal));
-  if (e != cudaSuccess) return e;
+// Persistent clusters of two CTAs along x (CTA 2i + r is rank r of cluster
+// i): as many as can be resident at once, at most one per work item.
+static uint32_t pair_clusters(int dev, uint32_t items) {
+  static std::mutex mu;
+  static int cached[64] = {};
+  int n = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64) n = cached[dev];
+  }
+  if (n == 0) {
+    using L = T8PairSmem<2, kT8PairStagesPair>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2);
+    cfg.blockDim = dim3(kT8Threads);
+    cfg.dynamicSmemBytes = L::kTotal;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaOccupancyMaxActiveClusters(&n, gnm_t8_pairs<kT8PairStagesPair>, &cfg) != cudaSuccess ||
+        n <= 0) {
+      (void)cudaGetLastError();
+      int sms = 0;
+      check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+                 "cudaDeviceGetAttribute");
+      n = std::max(1, sms / 2);
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64) cached[dev] = n;
+  }
+  return std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(n), items));
+}
+
+static void launch_t8_pairs(const CUtensorMap& amap2, const CUtensorMap& amap1,
+                            const CUtensorMap& pmap, const T8PairArgs& a, int dev,
+                            cudaStream_t s) {
+  using L = T8PairSmem<2, kT8PairStagesPair>;
+  const void* fn = reinterpret_cast<const void*>(gnm_t8_pairs<kT8PairStagesPair>);
+  check_cuda(raise_smem_limit(fn, int(L::kTotal)), "8-bit pair shared memory");
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = a.raster ? dim3(2 * spairs, ptiles) : dim3(2 * ptiles, spairs);
+  cfg.gridDim = dim3(2 * pair_clusters(dev, a.items));
   cfg.blockDim = dim3(kT8Threads);
   cfg.dynamicSmemBytes = L::kTotal;
   cfg.stream = s;
@@ -2286,8 +2391,8 @@ static cudaError_t launch_t8_pair(const CUtensorMap& amap, const CUtensorMap& pm
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, gnm_t8_pair<NP, ST, MISSING, COUNT_LAST, SPAN>, amap, pmap,
-                            a);
+  check_cuda(cudaLaunchKernelEx(&cfg, gnm_t8_pairs<kT8PairStagesPair>, amap2, amap1, pmap, a),
+             "8-bit pair launch");
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -2395,6 +2500,10 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   // SM pairs when the plan fills pairs of 128-score tiles (with one tile the
   // pair's second CTA would hold no scores)
   t->pair = t->stiles >= 2;
+  // score tiles fastest: the CTAs (clusters) running at once share a people
+  // tile's packed rows (batched workload: 126.8 against 144.6 ms per step on
+  // pairs, 159.4 against 165.7 on one SM)
+  p->raster = 1;
   if (t->V_pad > (uint64_t(1) << 31)) fail(GNM_ERR_INVALID, "too many variants for the tensor engine");
 
   const uint64_t plane = t->K_pad * t->V_pad;
@@ -2419,6 +2528,9 @@ void tensor_plan_create(gnm_plan* p, const gnm_prep_view* prep, PhaseTrace* trac
   }
   alloc(reinterpret_cast<void**>(&t->d_part_sum), t->part_elems * 8, "cudaMalloc(partials)");
   alloc(reinterpret_cast<void**>(&t->d_part_cnt), t->part_elems * 4, "cudaMalloc(partials)");
+  if (t->pair)   // the SM-pair kernel's passes 1-3 (written before being read)
+    alloc(reinterpret_cast<void**>(&t->d_part_pass), 3 * t->K_pad * t->P_pad * 8,
+          "cudaMalloc(pass partials)");
   check_cuda(cudaMemset(t->d_planes_dos, 0, 4 * plane * 2), "memset planes");
   check_cuda(cudaMemset(t->d_planes_mis, 0, 4 * plane * 2), "memset planes");
   t->V_pad8 = std::max<uint64_t>(kT8K, (p->V + kT8K - 1) / kT8K * kT8K);
@@ -2498,6 +2610,7 @@ void tensor_plan_destroy(gnm_plan* p) {
   pool_free(t->d_quanta8);
   pool_free(t->d_part_sum);
   pool_free(t->d_part_cnt);
+  pool_free(t->d_part_pass);
   delete t;
   p->tensor = nullptr;
 }
@@ -2507,7 +2620,16 @@ bool tensor_is_narrow(const gnm_plan* p) { return p->tensor && p->tensor->narrow
 bool tensor_is_i8(const gnm_plan* p) { return p->tensor && p->tensor->i8; }
 void tensor_set_i8(gnm_plan* p, bool i8) { p->tensor->i8 = i8; }
 bool tensor_is_pair(const gnm_plan* p) { return p->tensor && p->tensor->pair; }
-void tensor_set_pair(gnm_plan* p, bool pair) { p->tensor->pair = pair; }
+void tensor_set_pair(gnm_plan* p, bool pair) {
+  TensorPlan* t = p->tensor;
+  if (pair && !t->d_part_pass) {   // the pass arrays of the SM-pair kernel, on first use
+    const uint64_t bytes = 3 * t->K_pad * t->P_pad * 8;
+    t->d_part_pass = static_cast<double*>(pool_alloc(p->device, bytes, "pass partials"));
+    p->device_bytes += bytes;
+    t->pass_valid = false;
+  }
+  t->pair = pair;
+}
 void tensor_set_narrow(gnm_plan* p, bool narrow) {
   if (narrow && !tensor_can_narrow(p))
     fail(GNM_ERR_INVALID, "the narrow tensor kernel serves at most 64 scores");
@@ -2518,6 +2640,7 @@ void tensor_reset(gnm_plan* p, cudaStream_t s) {
   TensorPlan* t = p->tensor;
   check_cuda(cudaMemsetAsync(t->d_part_sum, 0, t->part_elems * 8, s), "reset partials");
   check_cuda(cudaMemsetAsync(t->d_part_cnt, 0, t->part_elems * 4, s), "reset partials");
+  t->pass_valid = false;   // the next SM-pair accumulate writes its pass arrays
 }
 
 void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint64_t v0,
@@ -2584,28 +2707,28 @@ void tensor_accumulate(gnm_plan* p, const uint8_t* d_rows, uint64_t pitch, uint6
     b.raster = p->raster;
     if (b.raster && t->ptiles > 65535u) b.raster = 0;  // grid.y limit
     if (t->pair) {
-      // SM pairs: each CTA loads its 128 people's packed bytes (32 per row)
+      // SM pairs, one persistent launch: each CTA loads its 128 people's
+      // packed bytes (32 per row)
       const CUtensorMap pmap_half = make_row_map(d_rows, p->bpv, nv, pitch, kTcN / 8, kT8K);
-      const uint32_t spairs = (t->stiles + 1) / 2;
-      for (int32_t z : {0, 2}) {
-        b.z0 = z;
-        check_cuda((launch_t8_pair<2, kT8PairStagesPair, false, false>(
-                       t->map8_2, pmap_half, b, t->ptiles, spairs, s)),
-                   "8-bit pair dosage launch");
-      }
-      for (int32_t z : {4, 6}) {
-        b.z0 = z;
-        check_cuda((launch_t8_pair<2, kT8PairStagesPair, true, false>(
-                       t->map8_2, pmap_half, b, t->ptiles, spairs, s)),
-                   "8-bit pair missing launch");
-      }
-      // the member plane of two score pairs per cluster (one pass's MMA work
-      // on half the clusters)
-      b.z0 = 8;
-      check_cuda((launch_t8_pair<2, kT8PairStagesPair, true, true, true>(
-                     t->map8_1, pmap_half, b, t->ptiles, (spairs + 1) / 2, s)),
-                 "8-bit pair count launch");
-      p->launches += 5;
+      T8PairArgs c;
+      c.num_rows = nv;
+      c.a_x0 = int32_t(v0);
+      c.part_sum = t->d_part_sum;
+      c.part_pass = t->d_part_pass;
+      c.part_cnt = t->d_part_cnt;
+      c.P_pad = t->P_pad;
+      c.K_pad = t->K_pad;
+      c.quanta = t->d_quanta8;
+      c.err = p->d_err;
+      c.raster = p->raster;
+      c.ptiles = t->ptiles;
+      c.spairs = (t->stiles + 1) / 2;
+      c.spairs_m = (c.spairs + 1) / 2;
+      c.items = 4 * c.ptiles * c.spairs + c.ptiles * c.spairs_m;
+      c.store = t->pass_valid ? 0u : 1u;
+      launch_t8_pairs(t->map8_2, t->map8_1, pmap_half, c, p->device, s);
+      t->pass_valid = true;
+      p->launches += 1;
       return;
     }
     for (int32_t z : {0, 2}) {
@@ -2664,7 +2787,8 @@ void tensor_finalize(gnm_plan* p, double* d_sums, uint32_t* d_counts, bool add_b
   if (n == 0) return;
   gnm_tc_finalize<<<uint32_t((n + 255) / 256), 256, 0, s>>>(
       t->d_part_sum, t->d_part_cnt, t->P_pad, add_baseline ? p->d_baseline : p->d_zero_base,
-      p->d_out_to_fam, p->P, p->K, t->narrow ? t->nsplits : 0u, t->nslot, d_sums, d_counts);
+      p->d_out_to_fam, p->P, p->K, t->narrow ? t->nsplits : 0u, t->nslot,
+      t->pass_valid ? t->d_part_pass : nullptr, t->K_pad * t->P_pad, d_sums, d_counts);
   check_cuda(cudaGetLastError(), "tensor finalize launch");
   p->launches += 1;
 }
