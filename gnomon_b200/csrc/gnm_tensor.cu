@@ -1,5 +1,12 @@
-// gnm_tensor.cu — split-BF16 tcgen05 engine (many score columns) and the
-// re-unpacking backward kernel dW = G^T dS.
+// gnm_tensor.cu — the tcgen05 tensor engine (many score columns) and the
+// re-unpacking backward kernel dW = G^T dS, each on BF16 limbs (kind::f16)
+// and on 8-bit integer limbs (kind::i8):
+//   gnm_tc_accumulate / gnm_t8_accumulate  wide: scores as M, one SM per tile
+//   gnm_t8_pairs                           wide, 8-bit, SM pairs (cta_group::2),
+//                                          one persistent launch per call
+//   gnm_tc_narrow / gnm_t8_narrow          narrow: people as M (<= 64 scores)
+//   gnm_tc_backward / gnm_t8_backward      dW = G^T dS, dC on CUDA cores
+// The BF16 forms come first below; each 8-bit form states what it changes.
 //
 // Scoring as a GEMM (the reference does this with three cuBLAS SGEMMs per
 // score tile, score/cuda_backend.rs:2196-2233):
